@@ -1,0 +1,488 @@
+// ref_shim.cpp -- flat C entry points over the reference solver's own C++ code.
+//
+// TEST INFRASTRUCTURE ONLY.  oracle/Makefile compiles the reference numerical
+// core from its sources (which stay where they are) together with this file
+// into oracle/_ref/libwaslref.so.  The tests call it to pin the C restatement
+// in wasl_oracle.c against the reference itself; nothing in the product links
+// it.  Every wr_* function mirrors the wo_* function of the same name.
+//
+// It also supplies stand-ins for the four HDF5 functions the case layer links
+// (cpp/src/io/checkpoint_file.cpp, cpp/src/io/prepared_mesh_file.cpp), in a
+// plain binary format, because HDF5 is not installed here.
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <filesystem>
+#include <fstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "wasl/boundaries/line_boundary_conditions.hpp"
+#include "wasl/boundaries/line_euler_exterior.hpp"
+#include "wasl/boundaries/periodic_triangle_trace.hpp"
+#include "wasl/dg/euler/line_residual.hpp"
+#include "wasl/dg/euler/triangle_residual.hpp"
+#include "wasl/dg/scalar_advection/line_residual.hpp"
+#include "wasl/dg/scalar_advection/triangle_residual.hpp"
+#include "wasl/flux/hllc.hpp"
+#include "wasl/io/checkpoint_file.hpp"
+#include "wasl/io/prepared_mesh_file.hpp"
+#include "wasl/limiting/euler_limiter_stencil.hpp"
+#include "wasl/limiting/euler_modal_limiter.hpp"
+#include "wasl/mesh/line/build_line_mesh.hpp"
+#include "wasl/mesh/msh/msh_document.hpp"
+#include "wasl/mesh/triangle/build_triangle_mesh.hpp"
+#include "wasl/time/cfl_timestep.hpp"
+#include "wasl/time/line_advection_step.hpp"
+#include "wasl/time/ssp_rk3.hpp"
+
+namespace {
+
+thread_local std::string last_error;
+
+template <typename F> int guarded(F &&body) {
+  try {
+    body();
+    return 0;
+  } catch (const std::exception &error) {
+    last_error = error.what();
+    return -1;
+  }
+}
+
+struct TriHandle {
+  wasl::TriangleMesh mesh;
+};
+struct LineHandle {
+  wasl::LineMesh mesh;
+};
+struct StencilHandle {
+  wasl::EulerLimiterStencil stencil;
+};
+
+// ---- binary stand-ins for the HDF5 files ----------------------------------
+
+template <typename T> void put(std::ofstream &out, const T &value) {
+  out.write(reinterpret_cast<const char *>(&value), sizeof(T));
+}
+template <typename T> void put_vector(std::ofstream &out, const std::vector<T> &values) {
+  put<std::uint64_t>(out, values.size());
+  out.write(reinterpret_cast<const char *>(values.data()),
+            static_cast<std::streamsize>(values.size() * sizeof(T)));
+}
+template <typename T> T get(std::ifstream &in) {
+  T value{};
+  in.read(reinterpret_cast<char *>(&value), sizeof(T));
+  return value;
+}
+template <typename T> std::vector<T> get_vector(std::ifstream &in) {
+  std::vector<T> values(get<std::uint64_t>(in));
+  in.read(reinterpret_cast<char *>(values.data()),
+          static_cast<std::streamsize>(values.size() * sizeof(T)));
+  return values;
+}
+
+} // namespace
+
+namespace wasl {
+
+void write_checkpoint(const std::filesystem::path &path, const Checkpoint &checkpoint) {
+  validate_checkpoint(checkpoint);
+  if (path.has_parent_path())
+    std::filesystem::create_directories(path.parent_path());
+  std::ofstream out(path, std::ios::binary | std::ios::trunc);
+  put(out, checkpoint.time);
+  put(out, checkpoint.step);
+  put(out, checkpoint.variable_count);
+  put(out, checkpoint.mode_count);
+  put(out, checkpoint.element_count);
+  put_vector(out, std::vector<char>(checkpoint.prepared_mesh.begin(), checkpoint.prepared_mesh.end()));
+  put_vector(out, checkpoint.coefficients);
+  put(out, checkpoint.partition_rank);
+  put(out, checkpoint.partition_rank_count);
+  put(out, checkpoint_global_element_count(checkpoint));
+  put_vector(out, checkpoint_element_indices(checkpoint));
+}
+
+Checkpoint read_checkpoint(const std::filesystem::path &path) {
+  if (!std::filesystem::is_regular_file(path))
+    throw std::runtime_error("checkpoint read: file does not exist: " + path.string());
+  std::ifstream in(path, std::ios::binary);
+  Checkpoint checkpoint;
+  checkpoint.time = get<double>(in);
+  checkpoint.step = get<std::uint64_t>(in);
+  checkpoint.variable_count = get<std::uint64_t>(in);
+  checkpoint.mode_count = get<std::uint64_t>(in);
+  checkpoint.element_count = get<std::uint64_t>(in);
+  const auto mesh = get_vector<char>(in);
+  checkpoint.prepared_mesh.assign(mesh.begin(), mesh.end());
+  checkpoint.coefficients = get_vector<double>(in);
+  checkpoint.partition_rank = get<int>(in);
+  checkpoint.partition_rank_count = get<int>(in);
+  checkpoint.global_element_count = get<std::uint64_t>(in);
+  checkpoint.element_indices = get_vector<std::int64_t>(in);
+  validate_checkpoint(checkpoint);
+  return checkpoint;
+}
+
+void write_prepared_mesh(const std::filesystem::path &path, const PreparedMesh &m) {
+  if (path.has_parent_path())
+    std::filesystem::create_directories(path.parent_path());
+  std::ofstream out(path, std::ios::binary | std::ios::trunc);
+  put(out, m.dimension);
+  put(out, m.nodes_per_element);
+  put_vector(out, m.node_tags);
+  put_vector(out, m.points);
+  put_vector(out, m.element_nodes);
+  put_vector(out, m.element_physical_tags);
+  put_vector(out, m.element_metrics);
+  put_vector(out, m.face_nodes);
+  put_vector(out, m.face_elements);
+  put_vector(out, m.face_local_edges);
+  put_vector(out, m.face_normals);
+  put_vector(out, m.face_measures);
+  put_vector(out, m.face_physical_tags);
+  put_vector(out, m.physical_name_dimensions);
+  put_vector(out, m.physical_name_tags);
+  put_vector(out, m.physical_name_offsets);
+  put_vector(out, m.physical_name_bytes);
+  put(out, m.partition_rank_count);
+  put_vector(out, m.element_owners);
+  put_vector(out, m.face_owners);
+}
+
+PreparedMesh read_prepared_mesh(const std::filesystem::path &path) {
+  if (!std::filesystem::is_regular_file(path))
+    throw std::runtime_error("prepared mesh read: file does not exist: " + path.string());
+  std::ifstream in(path, std::ios::binary);
+  PreparedMesh m;
+  m.dimension = get<int>(in);
+  m.nodes_per_element = get<int>(in);
+  m.node_tags = get_vector<std::int64_t>(in);
+  m.points = get_vector<double>(in);
+  m.element_nodes = get_vector<std::int64_t>(in);
+  m.element_physical_tags = get_vector<std::int32_t>(in);
+  m.element_metrics = get_vector<double>(in);
+  m.face_nodes = get_vector<std::int64_t>(in);
+  m.face_elements = get_vector<std::int32_t>(in);
+  m.face_local_edges = get_vector<std::int32_t>(in);
+  m.face_normals = get_vector<double>(in);
+  m.face_measures = get_vector<double>(in);
+  m.face_physical_tags = get_vector<std::int32_t>(in);
+  m.physical_name_dimensions = get_vector<std::int32_t>(in);
+  m.physical_name_tags = get_vector<std::int32_t>(in);
+  m.physical_name_offsets = get_vector<std::uint64_t>(in);
+  m.physical_name_bytes = get_vector<unsigned char>(in);
+  m.partition_rank_count = get<int>(in);
+  m.element_owners = get_vector<std::int32_t>(in);
+  m.face_owners = get_vector<std::int32_t>(in);
+  return m;
+}
+
+} // namespace wasl
+
+extern "C" {
+
+const char *wr_last_error() { return last_error.c_str(); }
+
+// ---- meshes ----------------------------------------------------------------
+
+// A document holding the nodes and triangles, with one surface entity so that
+// build_triangle_mesh has the same input as the reference's in-code meshes.
+void *wr_tri_mesh_new(std::int64_t node_count, const std::int64_t *tags, const double *xy,
+                      std::int64_t element_count, const std::int64_t *element_nodes) {
+  auto *handle = new TriHandle;
+  const int rc = guarded([&] {
+    wasl::MshDocument document;
+    document.surface_entities.push_back({1, 0.0, 0.0, 0.0, 1.0, 1.0, 0.0, {1}, {}});
+    for (std::int64_t i = 0; i < node_count; ++i)
+      document.nodes.push_back({tags[i], 2, 1, xy[2 * i], xy[2 * i + 1], 0.0});
+    for (std::int64_t e = 0; e < element_count; ++e)
+      document.elements.push_back({e + 1, 2, 1, wasl::msh_triangle_element,
+                                   {element_nodes[3 * e], element_nodes[3 * e + 1],
+                                    element_nodes[3 * e + 2]}});
+    handle->mesh = wasl::build_triangle_mesh(document);
+  });
+  if (rc != 0) {
+    delete handle;
+    return nullptr;
+  }
+  return handle;
+}
+
+void wr_tri_mesh_free(void *handle) { delete static_cast<TriHandle *>(handle); }
+
+std::int64_t wr_tri_mesh_face_count(void *handle) {
+  return static_cast<std::int64_t>(static_cast<TriHandle *>(handle)->mesh.faces.size());
+}
+
+void wr_tri_mesh_export(void *handle, double *vertices, std::int64_t *nodes, std::int32_t *left,
+                        std::int32_t *right, std::int32_t *left_edge, std::int32_t *right_edge,
+                        std::int64_t *left_v0, std::int64_t *right_v0, double *nx, double *ny) {
+  const auto &mesh = static_cast<TriHandle *>(handle)->mesh;
+  for (std::size_t e = 0; e < mesh.elements.size(); ++e) {
+    const auto &el = mesh.elements[e];
+    const double v[6] = {el.x0, el.y0, el.x1, el.y1, el.x2, el.y2};
+    std::memcpy(vertices + 6 * e, v, sizeof(v));
+    nodes[3 * e] = el.node0;
+    nodes[3 * e + 1] = el.node1;
+    nodes[3 * e + 2] = el.node2;
+  }
+  for (std::size_t f = 0; f < mesh.faces.size(); ++f) {
+    const auto &face = mesh.faces[f];
+    left[f] = face.left_element;
+    right[f] = face.right_element;
+    left_edge[f] = face.left_local_edge;
+    right_edge[f] = face.right_local_edge;
+    left_v0[f] = face.left_vertex0;
+    right_v0[f] = face.right_vertex0;
+    nx[f] = face.outward_normal_x;
+    ny[f] = face.outward_normal_y;
+  }
+}
+
+void *wr_line_mesh_new(std::int64_t node_count, const std::int64_t *tags, const double *x,
+                       std::int64_t element_count, const std::int64_t *element_nodes) {
+  auto *handle = new LineHandle;
+  const int rc = guarded([&] {
+    wasl::MshDocument document;
+    document.point_entities.push_back({1, 0.0, 0.0, 0.0, {}});
+    document.curve_entities.push_back({1, 0, 0, 0, 1, 0, 0, {1}, {}});
+    for (std::int64_t i = 0; i < node_count; ++i)
+      document.nodes.push_back({tags[i], 1, 1, x[i], 0.0, 0.0});
+    for (std::int64_t e = 0; e < element_count; ++e)
+      document.elements.push_back({e + 1, 1, 1, wasl::msh_line_element,
+                                   {element_nodes[2 * e], element_nodes[2 * e + 1]}});
+    handle->mesh = wasl::build_line_mesh(document);
+  });
+  if (rc != 0) {
+    delete handle;
+    return nullptr;
+  }
+  return handle;
+}
+
+void wr_line_mesh_free(void *handle) { delete static_cast<LineHandle *>(handle); }
+
+void wr_line_mesh_export(void *handle, double *x_left, double *x_right) {
+  const auto &mesh = static_cast<LineHandle *>(handle)->mesh;
+  for (std::size_t e = 0; e < mesh.elements.size(); ++e) {
+    x_left[e] = mesh.elements[e].x_left;
+    x_right[e] = mesh.elements[e].x_right;
+  }
+}
+
+// ---- residuals -------------------------------------------------------------
+
+void wr_euler_tri_residual(void *handle, double gamma, int p, const double *c, const double *ext,
+                           double *rhs) {
+  wasl::euler_triangle_residual(static_cast<TriHandle *>(handle)->mesh, wasl::Euler{gamma},
+                                wasl::hllc_flux, p, c, ext, rhs);
+}
+
+void wr_euler_line_residual(void *handle, double gamma, int p, const double *c, const double *ext,
+                            double *rhs) {
+  wasl::euler_line_residual(static_cast<LineHandle *>(handle)->mesh, wasl::Euler{gamma},
+                            wasl::hllc_flux, p, c, ext, rhs);
+}
+
+void wr_scalar_line_residual(void *handle, double a, int p, const double *c, const double *ext,
+                             double *rhs) {
+  wasl::scalar_advection_residual(static_cast<LineHandle *>(handle)->mesh,
+                                  wasl::ScalarAdvection{a}, p, c, ext, rhs);
+}
+
+void wr_scalar_tri_residual(void *handle, double vx, double vy, int p, const double *c,
+                            const double *ext, double *rhs) {
+  wasl::triangle_scalar_advection_residual(static_cast<TriHandle *>(handle)->mesh,
+                                           wasl::ScalarAdvection2D{vx, vy}, p, c, ext, rhs);
+}
+
+void wr_hllc_flux(double gamma, const double *l, const double *r, double nx, double ny,
+                  double *flux) {
+  const auto f = wasl::hllc_flux(wasl::Euler{gamma}, {l[0], l[1], l[2], l[3]},
+                                 {r[0], r[1], r[2], r[3]}, nx, ny);
+  flux[0] = f.density;
+  flux[1] = f.momentum_x;
+  flux[2] = f.momentum_y;
+  flux[3] = f.total_energy;
+}
+
+// ---- exterior traces ---------------------------------------------------------
+
+int wr_periodic_tri_trace(void *handle, int p, std::int32_t *donors, double *basis) {
+  return guarded([&] {
+    const auto trace = wasl::periodic_triangle_trace(static_cast<TriHandle *>(handle)->mesh, p);
+    std::memcpy(donors, trace.elements.data(), trace.elements.size() * sizeof(std::int32_t));
+    std::memcpy(basis, trace.basis.data(), trace.basis.size() * sizeof(double));
+  });
+}
+
+void wr_periodic_tri_euler_exterior(void *handle, int p, const std::int32_t *donors,
+                                    const double *basis, const double *c, double *ext) {
+  const auto &mesh = static_cast<TriHandle *>(handle)->mesh;
+  const std::size_t M = wasl::triangle_mode_count(p), Q = p + 1, F = mesh.faces.size();
+  wasl::PeriodicTriangleTrace trace;
+  trace.elements.assign(donors, donors + F * Q);
+  trace.basis.assign(basis, basis + F * Q * M);
+  trace.point_count = static_cast<int>(Q);
+  const std::size_t ne = mesh.num_elements();
+  const std::vector<double> state(c, c + 4 * M * ne);
+  const auto out = wasl::periodic_triangle_euler_exterior(trace, state, ne, M, F);
+  std::memcpy(ext, out.data(), out.size() * sizeof(double));
+}
+
+int wr_line_euler_exterior(void *handle, int p, int left_kind, int right_kind, const double *c,
+                           double *ext) {
+  return guarded([&] {
+    const auto &mesh = static_cast<LineHandle *>(handle)->mesh;
+    wasl::LineBoundaryConditions conditions;
+    conditions.left.kind = static_cast<wasl::BoundaryKind>(left_kind);
+    conditions.right.kind = static_cast<wasl::BoundaryKind>(right_kind);
+    const std::size_t n = 4 * wasl::line_mode_count(p) * mesh.num_elements();
+    const auto out = wasl::line_euler_exterior(mesh, p, conditions, std::vector<double>(c, c + n));
+    std::memcpy(ext, out.data(), out.size() * sizeof(double));
+  });
+}
+
+// ---- limiter -------------------------------------------------------------------
+
+void *wr_tri_stencil_new(void *handle, int p, const std::int32_t *donors) {
+  auto *s = new StencilHandle;
+  const auto &mesh = static_cast<TriHandle *>(handle)->mesh;
+  std::vector<std::int32_t> periodic;
+  if (donors)
+    periodic.assign(donors, donors + mesh.faces.size() * static_cast<std::size_t>(p + 1));
+  s->stencil = wasl::make_euler_limiter_stencil(mesh, p, periodic, p + 1);
+  return s;
+}
+
+void *wr_line_stencil_new(void *handle, int p, int periodic) {
+  auto *s = new StencilHandle;
+  s->stencil = wasl::make_euler_limiter_stencil(
+      static_cast<LineHandle *>(handle)->mesh, p,
+      periodic ? wasl::LineEnds::periodic : wasl::LineEnds::open);
+  return s;
+}
+
+void wr_stencil_free(void *s) { delete static_cast<StencilHandle *>(s); }
+
+void wr_stencil_export(void *s, std::int32_t *neighbors, double *transforms, double *nx,
+                       double *ny, double *check, int *check_count) {
+  const auto &st = static_cast<StencilHandle *>(s)->stencil;
+  std::memcpy(neighbors, st.neighbors.data(), st.neighbors.size() * sizeof(std::int32_t));
+  std::memcpy(transforms, st.transforms.data(), st.transforms.size() * sizeof(double));
+  std::memcpy(nx, st.normal_x.data(), st.normal_x.size() * sizeof(double));
+  std::memcpy(ny, st.normal_y.data(), st.normal_y.size() * sizeof(double));
+  std::memcpy(check, st.check_basis.data(), st.check_basis.size() * sizeof(double));
+  *check_count = static_cast<int>(st.check_point_count());
+}
+
+int wr_limit_euler(void *s, double gamma, double threshold, double rf, double pf, double *c) {
+  return guarded([&] {
+    const auto &st = static_cast<StencilHandle *>(s)->stencil;
+    const std::size_t n = 4 * st.mode_count * st.element_count;
+    std::vector<double> state(c, c + n);
+    wasl::limit_euler_modal(st, wasl::Euler{gamma}, threshold, rf, pf, state);
+    std::memcpy(c, state.data(), n * sizeof(double));
+  });
+}
+
+// ---- time step -------------------------------------------------------------------
+
+int wr_euler_tri_cfl(void *handle, double gamma, const double *c, int p, double cfl, double *dt) {
+  return guarded([&] {
+    const auto &mesh = static_cast<TriHandle *>(handle)->mesh;
+    const std::size_t M = wasl::triangle_mode_count(p);
+    *dt = wasl::euler_cfl_timestep(mesh, wasl::Euler{gamma},
+                                   std::vector<double>(c, c + 4 * M * mesh.num_elements()), M, p,
+                                   cfl);
+  });
+}
+
+int wr_euler_line_cfl(void *handle, double gamma, const double *c, int p, double cfl, double *dt) {
+  return guarded([&] {
+    const auto &mesh = static_cast<LineHandle *>(handle)->mesh;
+    const std::size_t M = wasl::line_mode_count(p);
+    *dt = wasl::euler_cfl_timestep(mesh, wasl::Euler{gamma},
+                                   std::vector<double>(c, c + 4 * M * mesh.num_elements()), M, p,
+                                   cfl);
+  });
+}
+
+// One SSP-RK3 step of 2D Euler with the periodic exterior, as the case driver
+// composes it (cpp/src/case/euler_triangle.cpp:26-49).  stencil may be null.
+int wr_euler_tri_step(void *handle, const std::int32_t *donors, const double *basis, void *stencil,
+                      double threshold, double rf, double pf, double gamma, int p, double dt,
+                      double *c) {
+  return guarded([&] {
+    const auto &mesh = static_cast<TriHandle *>(handle)->mesh;
+    const std::size_t M = wasl::triangle_mode_count(p), Q = p + 1, F = mesh.faces.size();
+    const std::size_t ne = mesh.num_elements();
+    wasl::PeriodicTriangleTrace trace;
+    trace.elements.assign(donors, donors + F * Q);
+    trace.basis.assign(basis, basis + F * Q * M);
+    trace.point_count = static_cast<int>(Q);
+    const wasl::Euler equation{gamma};
+    const wasl::ResidualFunction residual = [&](std::vector<double> &stage,
+                                                std::vector<double> &rhs) {
+      const auto exterior = wasl::periodic_triangle_euler_exterior(trace, stage, ne, M, F);
+      wasl::euler_triangle_residual(mesh, equation, wasl::hllc_flux, p, stage.data(),
+                                    exterior.data(), rhs.data());
+    };
+    const wasl::StateFunction limit = [&](std::vector<double> &state) {
+      if (stencil)
+        wasl::limit_euler_modal(static_cast<StencilHandle *>(stencil)->stencil, equation,
+                                threshold, rf, pf, state);
+    };
+    std::vector<double> state(c, c + 4 * M * ne);
+    wasl::SspRk3Workspace workspace;
+    wasl::ssp_rk3_step(dt, residual, limit, state, workspace);
+    std::memcpy(c, state.data(), state.size() * sizeof(double));
+  });
+}
+
+int wr_euler_line_step(void *handle, int left_kind, int right_kind, void *stencil,
+                       double threshold, double rf, double pf, double gamma, int p, double dt,
+                       double *c) {
+  return guarded([&] {
+    const auto &mesh = static_cast<LineHandle *>(handle)->mesh;
+    const std::size_t M = wasl::line_mode_count(p), ne = mesh.num_elements();
+    wasl::LineBoundaryConditions conditions;
+    conditions.left.kind = static_cast<wasl::BoundaryKind>(left_kind);
+    conditions.right.kind = static_cast<wasl::BoundaryKind>(right_kind);
+    const wasl::Euler equation{gamma};
+    const wasl::ResidualFunction residual = [&](std::vector<double> &stage,
+                                                std::vector<double> &rhs) {
+      const auto exterior = wasl::line_euler_exterior(mesh, p, conditions, stage);
+      wasl::euler_line_residual(mesh, equation, wasl::hllc_flux, p, stage.data(),
+                                exterior.data(), rhs.data());
+    };
+    const wasl::StateFunction limit = [&](std::vector<double> &state) {
+      if (stencil)
+        wasl::limit_euler_modal(static_cast<StencilHandle *>(stencil)->stencil, equation,
+                                threshold, rf, pf, state);
+    };
+    std::vector<double> state(c, c + 4 * M * ne);
+    wasl::SspRk3Workspace workspace;
+    wasl::ssp_rk3_step(dt, residual, limit, state, workspace);
+    std::memcpy(c, state.data(), state.size() * sizeof(double));
+  });
+}
+
+void wr_scalar_line_step(void *handle, int left_kind, double left_value, int right_kind,
+                         double right_value, double a, int p, double dt, double *c) {
+  const auto &mesh = static_cast<LineHandle *>(handle)->mesh;
+  const wasl::LineBoundaryConditions conditions{
+      {static_cast<wasl::BoundaryKind>(left_kind), left_value},
+      {static_cast<wasl::BoundaryKind>(right_kind), right_value}};
+  const auto exterior = wasl::make_line_boundary_exterior(mesh, p, conditions);
+  std::vector<double> state(c, c + wasl::line_mode_count(p) * mesh.num_elements());
+  wasl::SspRk3Workspace workspace;
+  wasl::ssp_rk3_step(mesh, wasl::ScalarAdvection{a}, p, dt, exterior, state, workspace);
+  std::memcpy(c, state.data(), state.size() * sizeof(double));
+}
+
+} // extern "C"
