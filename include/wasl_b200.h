@@ -1,0 +1,141 @@
+/*
+ * wasl_b200.h -- C-ABI of the B200 modal RKDG solver (libwasl_b200.so).
+ *
+ * A step-level handle that is a drop-in for the reference's serial CPU solver
+ * of scalar advection and compressible Euler on 1D line and 2D triangle
+ * meshes.  Plain C types only: pointers, sizes, int status codes.  Every call
+ * returns 0 on success or a negative status; wasl_gpu_last_error() gives the
+ * message, worded like the exception the reference throws for the same
+ * failure.  Host arrays are copied in and out; the handle owns all device
+ * memory and one CUDA stream.  A handle is not thread-safe.
+ *
+ * Reference interfaces each entry point replaces (paths inside indrow/wasl):
+ *   SerialCaseModel                cpp/include/wasl/case/serial_case_runner.hpp:22-34
+ *     initial_state / from_checkpoint     -> wasl_gpu_set_state
+ *     to_checkpoint / cell_averages       -> wasl_gpu_get_state
+ *     stable_time_step                    -> wasl_gpu_stable_dt
+ *     advance (ssp_rk3_step)              -> wasl_gpu_step
+ *     mass                                -> wasl_gpu_mass_energy
+ *   run_serial_case loop           cpp/src/case/serial_case_runner.cpp:117-149 -> wasl_gpu_run
+ *   write_checkpoint/read_checkpoint cpp/include/wasl/io/checkpoint_file.hpp:9-11
+ *                                                -> wasl_gpu_write_checkpoint / _read_checkpoint
+ *   case setup (mesh, stencil, periodic trace)   cpp/src/case/euler_triangle.cpp:16-25,
+ *                                                cpp/src/case/euler_line.cpp:14-22 -> wasl_gpu_create
+ *   coarse FFI run_euler_case / run_scalar_advection_case
+ *                                  crates/wasl-bridge/include/bridge.hpp:13-32 -> wasl_run_case
+ */
+#ifndef WASL_B200_H
+#define WASL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct wasl_gpu wasl_gpu;
+
+enum wasl_equation { WASL_SCALAR_ADVECTION = 0, WASL_EULER = 1 };
+/* Boundary kinds; values match the bridge's u8 kinds (crates/wasl-bridge/src/ops.rs). */
+enum wasl_boundary { WASL_PERIODIC = 0, WASL_INFLOW = 1, WASL_OUTFLOW = 2, WASL_TRANSMISSIVE = 3 };
+enum wasl_precision { WASL_PLAIN_FP64 = 0, WASL_MIXED = 1 };
+enum wasl_status {
+  WASL_OK = 0,
+  WASL_ERR_ARGUMENT = -1,     /* invalid argument (std::invalid_argument) */
+  WASL_ERR_RUNTIME = -2,      /* simulation failure (std::runtime_error) */
+  WASL_ERR_CUDA = -3,         /* CUDA error, or no usable device */
+  WASL_ERR_NONPHYSICAL = -4,  /* a cell average is not physical (cfl_timestep.cpp:39-40) */
+  WASL_ERR_FLOOR = -5         /* positivity: average below a floor (euler_positivity.hpp:74-75) */
+};
+
+typedef struct {
+  int dimensions;            /* 1 line mesh, 2 triangle mesh */
+  int equation;              /* enum wasl_equation */
+  int polynomial_order;      /* lines 0..6, triangles 0..3 */
+  double heat_capacity_ratio;
+  double velocity_x;         /* scalar advection: wavespeed (1D) / velocity (2D) */
+  double velocity_y;
+  int boundary_left;         /* 1D: left end kind; 2D: every boundary (periodic/transmissive) */
+  int boundary_right;        /* 1D: right end kind */
+  double inflow_left;        /* 1D scalar inflow values */
+  double inflow_right;
+  int limiting;              /* Euler: modal-decay + characteristic WENO + positivity */
+  double sensor_threshold;   /* default 1e-3 */
+  double density_floor;      /* default 1e-10 */
+  double pressure_floor;     /* default 1e-10 */
+  int precision;             /* enum wasl_precision */
+  int device;                /* CUDA device ordinal */
+} wasl_gpu_config;
+
+/* Fill the reference's defaults (crates/wasl-bridge/src/config.rs:87-104). */
+void wasl_gpu_config_default(wasl_gpu_config *config);
+
+/* Build the solver on a mesh given as node tags, coordinates ([node][dimensions])
+ * and element connectivity ([element][dimensions+1] node tags).  The mesh is
+ * normalized exactly as the reference normalizes it, so element order is the
+ * caller's and face order is the reference's. */
+int wasl_gpu_create(const wasl_gpu_config *config, int64_t node_count, const int64_t *node_tags,
+                    const double *node_coordinates, int64_t element_count,
+                    const int64_t *element_nodes, wasl_gpu **handle, char *error,
+                    size_t error_length);
+void wasl_gpu_destroy(wasl_gpu *handle);
+const char *wasl_gpu_last_error(const wasl_gpu *handle);
+
+/* Counts: elements, faces, modes per variable, variables. */
+int wasl_gpu_sizes(const wasl_gpu *handle, int64_t *elements, int64_t *faces, int *modes,
+                   int *variables);
+
+/* Element geometry after normalization: [element][6] vertices (2D) or
+ * [element][2] ends (1D). */
+int wasl_gpu_element_vertices(const wasl_gpu *handle, double *vertices, int64_t count);
+
+/* Modal state in the checkpoint layout U[variable][mode][element], FP64. */
+int wasl_gpu_set_state(wasl_gpu *handle, const double *coefficients, int64_t count);
+int wasl_gpu_get_state(wasl_gpu *handle, double *coefficients, int64_t count);
+
+/* CFL time step of the current state, bit-identical to the reference's
+ * (the device finds the fastest cell, the host evaluates its speed). */
+int wasl_gpu_stable_dt(wasl_gpu *handle, double cfl, double *dt);
+
+/* One SSP-RK3 step with the stage limiter (when enabled). */
+int wasl_gpu_step(wasl_gpu *handle, double dt);
+
+/* The stage limiter applied to the current state, as the reference applies it
+ * to the projected initial state (cpp/src/case/euler_triangle.cpp:33-37).
+ * No-op without limiting. */
+int wasl_gpu_limit(wasl_gpu *handle);
+
+/* Troubled-cell flags of the three stages of the last step, [stage][element]. */
+int wasl_gpu_get_flags(wasl_gpu *handle, uint8_t *flags, int64_t count);
+
+/* Totals of density and energy: sum over elements of sqrt(2) det(J) c0
+ * (cpp/src/case/euler_diagnostics.cpp:26-39); scalar: energy = mass. */
+int wasl_gpu_mass_energy(wasl_gpu *handle, double *mass, double *energy);
+
+/* The serial run loop: dt = stable_dt clipped to land on end_time, advance,
+ * until end_time or max_steps (serial_case_runner.cpp:107-149). */
+int wasl_gpu_run(wasl_gpu *handle, double cfl, double start_time, double end_time,
+                 uint64_t max_steps, uint64_t *steps, double *time);
+
+/* Device-resident fast path: `steps` steps with the CFL step computed on the
+ * device each step, no host synchronization (capturable in a CUDA graph). */
+int wasl_gpu_advance(wasl_gpu *handle, double cfl, int64_t steps);
+
+/* Device pointer of the state U[variable][mode][element] and the handle's
+ * CUDA stream (cudaStream_t), for callers that keep data on the device. */
+int wasl_gpu_state_device(wasl_gpu *handle, double **device_pointer);
+int wasl_gpu_stream(wasl_gpu *handle, void **stream);
+
+/* Restart files with the fields of the reference Checkpoint
+ * (cpp/include/wasl/io/checkpoint.hpp:17-29) in a portable binary container
+ * (HDF5 is not available here). */
+int wasl_gpu_write_checkpoint(wasl_gpu *handle, const char *path, double time, uint64_t step,
+                              const char *prepared_mesh);
+int wasl_gpu_read_checkpoint(wasl_gpu *handle, const char *path, double *time, uint64_t *step);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,247 @@
+"""B200-native modal RKDG time step for the Wasl solver (scalar advection and
+compressible Euler on 1D line and 2D triangle meshes).
+
+The numerical work runs in ``libwasl_b200.so`` (CUDA kernels for sm_100a behind
+the C-ABI declared in ``include/wasl_b200.h``).  This module is a thin ctypes
+mirror of the reference's case-model interface
+(cpp/include/wasl/case/serial_case_runner.hpp:22-34):
+
+    Solver.set_state / get_state     initial_state, from_checkpoint / to_checkpoint
+    Solver.stable_dt                 stable_time_step
+    Solver.step                      advance (one SSP-RK3 step with the stage limiter)
+    Solver.mass_energy               mass
+    Solver.run                       the run_serial_case loop
+    Solver.write_checkpoint / read_checkpoint
+
+There is no CPU fallback: constructing a Solver without the built library or
+without a CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libwasl_b200.so")
+
+PERIODIC, INFLOW, OUTFLOW, TRANSMISSIVE = 0, 1, 2, 3
+SCALAR_ADVECTION, EULER = 0, 1
+PLAIN_FP64, MIXED = 0, 1
+BOUNDARY_KINDS = {"periodic": PERIODIC, "inflow": INFLOW, "outflow": OUTFLOW,
+                  "transmissive": TRANSMISSIVE}
+PRECISIONS = {"plain": PLAIN_FP64, "fp64": PLAIN_FP64, "mixed": MIXED}
+
+
+class WaslError(RuntimeError):
+    """A failure reported by the library; ``status`` is the C-ABI status code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+class Config(C.Structure):
+    _fields_ = [
+        ("dimensions", C.c_int), ("equation", C.c_int), ("polynomial_order", C.c_int),
+        ("heat_capacity_ratio", C.c_double), ("velocity_x", C.c_double),
+        ("velocity_y", C.c_double), ("boundary_left", C.c_int), ("boundary_right", C.c_int),
+        ("inflow_left", C.c_double), ("inflow_right", C.c_double), ("limiting", C.c_int),
+        ("sensor_threshold", C.c_double), ("density_floor", C.c_double),
+        ("pressure_floor", C.c_double), ("precision", C.c_int), ("device", C.c_int),
+    ]
+
+
+_d = C.POINTER(C.c_double)
+_i64 = C.POINTER(C.c_int64)
+_u8 = C.POINTER(C.c_uint8)
+_lib = None
+
+# name -> (restype, argtypes), one per declaration in include/wasl_b200.h
+SIGNATURES = {
+    "wasl_gpu_config_default": (None, [C.POINTER(Config)]),
+    "wasl_gpu_create": (C.c_int, [C.POINTER(Config), C.c_int64, _i64, _d, C.c_int64, _i64,
+                                  C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
+    "wasl_gpu_destroy": (None, [C.c_void_p]),
+    "wasl_gpu_last_error": (C.c_char_p, [C.c_void_p]),
+    "wasl_gpu_sizes": (C.c_int, [C.c_void_p, _i64, _i64, C.POINTER(C.c_int),
+                                 C.POINTER(C.c_int)]),
+    "wasl_gpu_element_vertices": (C.c_int, [C.c_void_p, _d, C.c_int64]),
+    "wasl_gpu_set_state": (C.c_int, [C.c_void_p, _d, C.c_int64]),
+    "wasl_gpu_get_state": (C.c_int, [C.c_void_p, _d, C.c_int64]),
+    "wasl_gpu_stable_dt": (C.c_int, [C.c_void_p, C.c_double, _d]),
+    "wasl_gpu_step": (C.c_int, [C.c_void_p, C.c_double]),
+    "wasl_gpu_limit": (C.c_int, [C.c_void_p]),
+    "wasl_gpu_get_flags": (C.c_int, [C.c_void_p, _u8, C.c_int64]),
+    "wasl_gpu_mass_energy": (C.c_int, [C.c_void_p, _d, _d]),
+    "wasl_gpu_run": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_uint64,
+                               C.POINTER(C.c_uint64), _d]),
+    "wasl_gpu_advance": (C.c_int, [C.c_void_p, C.c_double, C.c_int64]),
+    "wasl_gpu_state_device": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "wasl_gpu_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "wasl_gpu_write_checkpoint": (C.c_int, [C.c_void_p, C.c_char_p, C.c_double, C.c_uint64,
+                                            C.c_char_p]),
+    "wasl_gpu_read_checkpoint": (C.c_int, [C.c_void_p, C.c_char_p, _d,
+                                           C.POINTER(C.c_uint64)]),
+}
+
+
+def library(path: str = LIB_PATH):
+    """Load libwasl_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `python -m wasl_b200.build`")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _ptr(a, t=_d):
+    return a.ctypes.data_as(t)
+
+
+def default_config() -> Config:
+    cfg = Config()
+    library().wasl_gpu_config_default(C.byref(cfg))
+    return cfg
+
+
+class Solver:
+    """One mesh, one equation, one polynomial order, state resident on the GPU."""
+
+    def __init__(self, node_tags, node_coordinates, element_nodes, *, dimensions=2,
+                 equation="euler", polynomial_order=2, gamma=1.4, velocity=(0.0, 0.0),
+                 boundary="periodic", boundary_right=None, inflow=(0.0, 0.0), limiting=False,
+                 sensor_threshold=1e-3, density_floor=1e-10, pressure_floor=1e-10,
+                 precision="plain", device=0):
+        lib = library()
+        cfg = default_config()
+        cfg.dimensions = dimensions
+        cfg.equation = EULER if equation == "euler" else SCALAR_ADVECTION
+        cfg.polynomial_order = polynomial_order
+        cfg.heat_capacity_ratio = gamma
+        cfg.velocity_x, cfg.velocity_y = velocity
+        cfg.boundary_left = BOUNDARY_KINDS[boundary]
+        cfg.boundary_right = BOUNDARY_KINDS[boundary_right or boundary]
+        cfg.inflow_left, cfg.inflow_right = inflow
+        cfg.limiting = 1 if limiting else 0
+        cfg.sensor_threshold = sensor_threshold
+        cfg.density_floor = density_floor
+        cfg.pressure_floor = pressure_floor
+        cfg.precision = PRECISIONS[precision]
+        cfg.device = device
+        self.config = cfg
+        tags = np.ascontiguousarray(node_tags, dtype=np.int64)
+        coords = np.ascontiguousarray(node_coordinates, dtype=np.float64)
+        elems = np.ascontiguousarray(element_nodes, dtype=np.int64)
+        err = C.create_string_buffer(1024)
+        h = C.c_void_p()
+        rc = lib.wasl_gpu_create(C.byref(cfg), len(tags), _ptr(tags, _i64), _ptr(coords),
+                                 len(elems), _ptr(elems, _i64), C.byref(h), err, len(err))
+        if rc != 0:
+            raise WaslError(rc, err.value.decode())
+        self._lib, self._h = lib, h
+        ne, nf = C.c_int64(), C.c_int64()
+        nm, nv = C.c_int(), C.c_int()
+        lib.wasl_gpu_sizes(h, C.byref(ne), C.byref(nf), C.byref(nm), C.byref(nv))
+        self.elements, self.faces = ne.value, nf.value
+        self.modes, self.variables = nm.value, nv.value
+        self.state_size = self.elements * self.modes * self.variables
+
+    def _check(self, rc):
+        if rc != 0:
+            raise WaslError(rc, self._lib.wasl_gpu_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.wasl_gpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- state ------------------------------------------------------------
+    def set_state(self, coefficients):
+        c = np.ascontiguousarray(coefficients, dtype=np.float64).ravel()
+        self._check(self._lib.wasl_gpu_set_state(self._h, _ptr(c), c.size))
+
+    def get_state(self) -> np.ndarray:
+        c = np.empty(self.state_size)
+        self._check(self._lib.wasl_gpu_get_state(self._h, _ptr(c), c.size))
+        return c
+
+    def vertices(self) -> np.ndarray:
+        per = 6 if self.config.dimensions == 2 else 2
+        v = np.empty(self.elements * per)
+        self._check(self._lib.wasl_gpu_element_vertices(self._h, _ptr(v), v.size))
+        return v.reshape(self.elements, per)
+
+    # ---- stepping -----------------------------------------------------------
+    def stable_dt(self, cfl: float) -> float:
+        dt = C.c_double()
+        self._check(self._lib.wasl_gpu_stable_dt(self._h, cfl, C.byref(dt)))
+        return dt.value
+
+    def step(self, dt: float):
+        self._check(self._lib.wasl_gpu_step(self._h, dt))
+
+    def limit(self):
+        """Apply the stage limiter to the current state (initial-state limiting)."""
+        self._check(self._lib.wasl_gpu_limit(self._h))
+
+    def run(self, cfl, start_time, end_time, max_steps=2**62):
+        steps, time = C.c_uint64(), C.c_double()
+        self._check(self._lib.wasl_gpu_run(self._h, cfl, start_time, end_time, max_steps,
+                                           C.byref(steps), C.byref(time)))
+        return steps.value, time.value
+
+    def advance(self, cfl: float, steps: int):
+        self._check(self._lib.wasl_gpu_advance(self._h, cfl, steps))
+
+    def flags(self) -> np.ndarray:
+        f = np.empty(3 * self.elements, dtype=np.uint8)
+        self._check(self._lib.wasl_gpu_get_flags(self._h, _ptr(f, _u8), f.size))
+        return f.reshape(3, self.elements)
+
+    def mass_energy(self):
+        m, e = C.c_double(), C.c_double()
+        self._check(self._lib.wasl_gpu_mass_energy(self._h, C.byref(m), C.byref(e)))
+        return m.value, e.value
+
+    # ---- device interop -------------------------------------------------------
+    def state_device_pointer(self) -> int:
+        p = C.c_void_p()
+        self._check(self._lib.wasl_gpu_state_device(self._h, C.byref(p)))
+        return p.value
+
+    def stream_handle(self) -> int:
+        s = C.c_void_p()
+        self._check(self._lib.wasl_gpu_stream(self._h, C.byref(s)))
+        return s.value or 0
+
+    # ---- restart files ----------------------------------------------------------
+    def write_checkpoint(self, path, time, step, prepared_mesh=""):
+        self._check(self._lib.wasl_gpu_write_checkpoint(self._h, os.fsencode(path), time, step,
+                                                        os.fsencode(prepared_mesh)))
+
+    def read_checkpoint(self, path):
+        t, s = C.c_double(), C.c_uint64()
+        self._check(self._lib.wasl_gpu_read_checkpoint(self._h, os.fsencode(path), C.byref(t),
+                                                       C.byref(s)))
+        return t.value, s.value

@@ -1,0 +1,77 @@
+"""Build libwasl_b200.so in the package directory (sm_100a, in-tree).
+
+    python -m wasl_b200.build            # incremental
+    python -m wasl_b200.build --clean
+
+Kernels whose results must match the reference bit for bit are compiled with
+--fmad=false (no fused multiply-add contraction); host code with
+-ffp-contract=off for the same reason.  The mixed-precision kernels keep FMA.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libwasl_b200.so")
+INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", f"-I{INCLUDE}", f"-I{CSRC}",
+          "-Xcompiler", "-fPIC,-ffp-contract=off", "--expt-relaxed-constexpr"]
+
+# file -> extra flags
+SOURCES = {
+    "euler_tri_f64.cu": ["--fmad=false"],
+    "euler_tri_solver.cu": [],
+    "mesh.cpp": [],
+    "tables.cpp": [],
+    "capi.cpp": [],
+}
+HEADERS = [f for f in os.listdir(CSRC) if f.endswith((".hpp", ".cuh", ".h"))]
+
+
+def _newest_header() -> float:
+    paths = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "wasl_b200.h")]
+    return max(os.path.getmtime(p) for p in paths)
+
+
+def _compile(src: str, flags: list[str]) -> str:
+    obj = os.path.join(BUILD, src + ".o")
+    path = os.path.join(CSRC, src)
+    if (os.path.exists(obj) and os.path.getmtime(obj) >= os.path.getmtime(path)
+            and os.path.getmtime(obj) >= _newest_header()):
+        return obj
+    lang = [] if src.endswith(".cu") else ["-x", "cu"]
+    cmd = [NVCC, *ARCH, *COMMON, *flags, *lang, "-c", path, "-o", obj]
+    subprocess.run(cmd, check=True)
+    return obj
+
+
+def build(clean: bool = False, verbose: bool = False) -> str:
+    if clean and os.path.isdir(BUILD):
+        shutil.rmtree(BUILD)
+    os.makedirs(BUILD, exist_ok=True)
+    with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as pool:
+        futures = [pool.submit(_compile, s, f) for s, f in SOURCES.items()]
+        objs = [f.result() for f in futures]
+    if (not os.path.exists(LIB) or
+            max(os.path.getmtime(o) for o in objs) > os.path.getmtime(LIB)):
+        subprocess.run([NVCC, *ARCH, "-shared", "-o", LIB, *objs], check=True)
+    if verbose:
+        print(LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--clean", action="store_true")
+    args = ap.parse_args()
+    build(clean=args.clean, verbose=True)
+    sys.exit(0)

@@ -1,0 +1,307 @@
+// extern "C" entry points of libwasl_b200.so (declared in include/wasl_b200.h).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <memory>
+#include <string>
+
+#include "mesh.hpp"
+#include "solver.hpp"
+
+namespace wasl_b200 {
+std::unique_ptr<Solver> make_euler_tri_solver(const wasl_gpu_config &cfg, TriTopology &&topo);
+
+std::unique_ptr<Solver> make_solver(const wasl_gpu_config &cfg, std::int64_t node_count,
+                                    const std::int64_t *node_tags, const double *coordinates,
+                                    std::int64_t element_count, const std::int64_t *element_nodes) {
+  if (cfg.dimensions == 2 && cfg.equation == WASL_EULER)
+    return make_euler_tri_solver(cfg, build_triangle_topology(node_count, node_tags, coordinates,
+                                                              element_count, element_nodes));
+  throw SolverError(WASL_ERR_ARGUMENT, "unsupported dimension/equation combination");
+}
+} // namespace wasl_b200
+
+struct wasl_gpu {
+  std::unique_ptr<wasl_b200::Solver> solver;
+  std::string error;
+};
+
+namespace {
+
+template <typename F> int guarded(wasl_gpu *h, F &&body) {
+  if (!h)
+    return WASL_ERR_ARGUMENT;
+  try {
+    body();
+    h->error.clear();
+    return WASL_OK;
+  } catch (const wasl_b200::SolverError &e) {
+    h->error = e.what();
+    return e.status;
+  } catch (const std::invalid_argument &e) {
+    h->error = e.what();
+    return WASL_ERR_ARGUMENT;
+  } catch (const std::exception &e) {
+    h->error = e.what();
+    return WASL_ERR_RUNTIME;
+  }
+}
+
+void need(bool ok, const char *message) {
+  if (!ok)
+    throw wasl_b200::SolverError(WASL_ERR_ARGUMENT, message);
+}
+
+// Checkpoint container: magic, format version 2, then the reference fields in
+// declaration order (cpp/include/wasl/io/checkpoint.hpp:17-29).
+constexpr char kMagic[8] = {'W', 'A', 'S', 'L', 'C', 'K', 'P', 'T'};
+
+template <typename T> void put(std::ofstream &o, const T &v) {
+  o.write(reinterpret_cast<const char *>(&v), sizeof(T));
+}
+template <typename T> T get(std::ifstream &i) {
+  T v{};
+  i.read(reinterpret_cast<char *>(&v), sizeof(T));
+  if (!i)
+    throw std::runtime_error("checkpoint read: truncated file");
+  return v;
+}
+
+} // namespace
+
+extern "C" {
+
+void wasl_gpu_config_default(wasl_gpu_config *c) {
+  std::memset(c, 0, sizeof(*c));
+  c->dimensions = 2;
+  c->equation = WASL_EULER;
+  c->polynomial_order = 2;
+  c->heat_capacity_ratio = 1.4;
+  c->boundary_left = c->boundary_right = WASL_PERIODIC;
+  c->sensor_threshold = 1e-3;
+  c->density_floor = 1e-10;
+  c->pressure_floor = 1e-10;
+  c->precision = WASL_PLAIN_FP64;
+}
+
+int wasl_gpu_create(const wasl_gpu_config *config, int64_t node_count, const int64_t *node_tags,
+                    const double *node_coordinates, int64_t element_count,
+                    const int64_t *element_nodes, wasl_gpu **handle, char *error,
+                    size_t error_length) {
+  if (!handle || !config)
+    return WASL_ERR_ARGUMENT;
+  *handle = nullptr;
+  auto h = std::make_unique<wasl_gpu>();
+  const int rc = guarded(h.get(), [&] {
+    need(node_count > 0 && element_count > 0, "mesh: empty node or element list");
+    need(node_tags && node_coordinates && element_nodes, "mesh: null array");
+    need(config->density_floor >= 0.0 && config->pressure_floor >= 0.0,
+         "Euler positivity limiter: invalid modes or floors");
+    h->solver = wasl_b200::make_solver(*config, node_count, node_tags, node_coordinates,
+                                       element_count, element_nodes);
+  });
+  if (rc != WASL_OK) {
+    if (error && error_length) {
+      std::strncpy(error, h->error.c_str(), error_length - 1);
+      error[error_length - 1] = '\0';
+    }
+    return rc;
+  }
+  *handle = h.release();
+  return WASL_OK;
+}
+
+void wasl_gpu_destroy(wasl_gpu *h) { delete h; }
+
+const char *wasl_gpu_last_error(const wasl_gpu *h) { return h ? h->error.c_str() : "null handle"; }
+
+int wasl_gpu_sizes(const wasl_gpu *h, int64_t *elements, int64_t *faces, int *modes,
+                   int *variables) {
+  if (!h)
+    return WASL_ERR_ARGUMENT;
+  if (elements)
+    *elements = h->solver->elements();
+  if (faces)
+    *faces = h->solver->faces();
+  if (modes)
+    *modes = h->solver->modes();
+  if (variables)
+    *variables = h->solver->variables();
+  return WASL_OK;
+}
+
+int wasl_gpu_element_vertices(const wasl_gpu *h, double *vertices, int64_t count) {
+  return guarded(const_cast<wasl_gpu *>(h), [&] {
+    need(vertices != nullptr, "null vertex array");
+    h->solver->vertices(vertices);
+    (void)count;
+  });
+}
+
+static int64_t state_count(const wasl_gpu *h) {
+  return h->solver->elements() * h->solver->modes() * h->solver->variables();
+}
+
+int wasl_gpu_set_state(wasl_gpu *h, const double *c, int64_t count) {
+  return guarded(h, [&] {
+    need(c && count == state_count(h), "state: coefficient count does not match the layout");
+    h->solver->set_state(c);
+  });
+}
+
+int wasl_gpu_get_state(wasl_gpu *h, double *c, int64_t count) {
+  return guarded(h, [&] {
+    need(c && count == state_count(h), "state: coefficient count does not match the layout");
+    h->solver->get_state(c);
+  });
+}
+
+int wasl_gpu_stable_dt(wasl_gpu *h, double cfl, double *dt) {
+  return guarded(h, [&] {
+    need(dt != nullptr, "null dt");
+    *dt = h->solver->stable_dt(cfl);
+  });
+}
+
+int wasl_gpu_step(wasl_gpu *h, double dt) {
+  return guarded(h, [&] {
+    need(std::isfinite(dt), "step: time step is not finite");
+    h->solver->step(dt);
+  });
+}
+
+int wasl_gpu_limit(wasl_gpu *h) {
+  return guarded(h, [&] { h->solver->limit(); });
+}
+
+int wasl_gpu_get_flags(wasl_gpu *h, uint8_t *flags, int64_t count) {
+  return guarded(h, [&] {
+    need(flags && count == 3 * h->solver->elements(), "flags: count must be 3 x elements");
+    h->solver->flags(flags);
+  });
+}
+
+int wasl_gpu_mass_energy(wasl_gpu *h, double *mass, double *energy) {
+  return guarded(h, [&] {
+    double m = 0.0, e = 0.0;
+    h->solver->mass_energy(m, e);
+    if (mass)
+      *mass = m;
+    if (energy)
+      *energy = e;
+  });
+}
+
+int wasl_gpu_run(wasl_gpu *h, double cfl, double start_time, double end_time, uint64_t max_steps,
+                 uint64_t *steps, double *time) {
+  return guarded(h, [&] {
+    double t = start_time;
+    uint64_t n = 0;
+    while (t < end_time && n < max_steps) {
+      const double stable = h->solver->stable_dt(cfl);
+      const double remaining = end_time - t;
+      const double dt = std::min(stable > 0.0 ? stable : remaining, remaining);
+      if (dt <= 0.0 || t + dt == t)
+        throw std::runtime_error("simulation: timestep cannot advance time");
+      h->solver->step(dt);
+      t += dt;
+      ++n;
+    }
+    if (steps)
+      *steps = n;
+    if (time)
+      *time = t;
+  });
+}
+
+int wasl_gpu_advance(wasl_gpu *h, double cfl, int64_t steps) {
+  return guarded(h, [&] {
+    need(steps >= 0, "advance: negative step count");
+    h->solver->advance(cfl, steps);
+  });
+}
+
+int wasl_gpu_state_device(wasl_gpu *h, double **p) {
+  return guarded(h, [&] {
+    need(p != nullptr, "null pointer");
+    *p = h->solver->state_device();
+  });
+}
+
+int wasl_gpu_stream(wasl_gpu *h, void **s) {
+  return guarded(h, [&] {
+    need(s != nullptr, "null pointer");
+    *s = reinterpret_cast<void *>(h->solver->stream());
+  });
+}
+
+int wasl_gpu_write_checkpoint(wasl_gpu *h, const char *path, double time, uint64_t step,
+                              const char *prepared_mesh) {
+  return guarded(h, [&] {
+    need(path != nullptr, "checkpoint: null path");
+    std::vector<double> c(state_count(h));
+    h->solver->get_state(c.data());
+    std::ofstream o(path, std::ios::binary | std::ios::trunc);
+    if (!o)
+      throw std::runtime_error(std::string("checkpoint write: cannot open ") + path);
+    const std::string mesh = prepared_mesh ? prepared_mesh : "";
+    o.write(kMagic, sizeof(kMagic));
+    put<int32_t>(o, 2);
+    put<double>(o, time);
+    put<uint64_t>(o, step);
+    put<uint64_t>(o, h->solver->variables());
+    put<uint64_t>(o, h->solver->modes());
+    put<uint64_t>(o, h->solver->elements());
+    put<uint64_t>(o, mesh.size());
+    o.write(mesh.data(), static_cast<std::streamsize>(mesh.size()));
+    put<uint64_t>(o, c.size());
+    o.write(reinterpret_cast<const char *>(c.data()),
+            static_cast<std::streamsize>(c.size() * sizeof(double)));
+    put<int32_t>(o, 0);                          // partition_rank
+    put<int32_t>(o, 1);                          // partition_rank_count
+    put<uint64_t>(o, h->solver->elements());     // global_element_count
+    put<uint64_t>(o, 0);                         // element_indices: identity
+    if (!o)
+      throw std::runtime_error(std::string("checkpoint write: failed ") + path);
+  });
+}
+
+int wasl_gpu_read_checkpoint(wasl_gpu *h, const char *path, double *time, uint64_t *step) {
+  return guarded(h, [&] {
+    need(path != nullptr, "checkpoint: null path");
+    std::ifstream i(path, std::ios::binary);
+    if (!i)
+      throw std::runtime_error(std::string("checkpoint read: file does not exist: ") + path);
+    char magic[8];
+    i.read(magic, 8);
+    if (!i || std::memcmp(magic, kMagic, 8) != 0)
+      throw std::runtime_error("checkpoint read: not a checkpoint file");
+    const int32_t version = get<int32_t>(i);
+    if (version != 2)
+      throw std::runtime_error("checkpoint read: unsupported format_version");
+    const double t = get<double>(i);
+    const uint64_t s = get<uint64_t>(i);
+    const uint64_t nv = get<uint64_t>(i), nm = get<uint64_t>(i), ne = get<uint64_t>(i);
+    const uint64_t mesh_len = get<uint64_t>(i);
+    std::string mesh(mesh_len, '\0');
+    i.read(mesh.data(), static_cast<std::streamsize>(mesh_len));
+    const uint64_t n = get<uint64_t>(i);
+    if (nv != static_cast<uint64_t>(h->solver->variables()) ||
+        nm != static_cast<uint64_t>(h->solver->modes()) ||
+        ne != static_cast<uint64_t>(h->solver->elements()) || n != nv * nm * ne)
+      throw std::runtime_error(
+          "simulation restart: checkpoint layout or mesh provenance mismatch");
+    std::vector<double> c(n);
+    i.read(reinterpret_cast<char *>(c.data()), static_cast<std::streamsize>(n * sizeof(double)));
+    if (!i)
+      throw std::runtime_error("checkpoint read: truncated file");
+    h->solver->set_state(c.data());
+    if (time)
+      *time = t;
+    if (step)
+      *step = s;
+  });
+}
+
+} // extern "C"

@@ -1,0 +1,588 @@
+// Plain FP64 kernels of the 2D Euler SSP-RK3 stage, bit-consistent with the
+// reference CPU solver.
+//
+// This translation unit is compiled with --fmad=false: every product and sum
+// rounds separately, in the order of the reference expressions, so given the
+// same inputs and tables each element's result is the double the reference
+// computes.  Summation orders reproduced:
+//   * modal sums over modes 0..M-1 from 0.0   (dg/modal_layout.hpp:26-36)
+//   * the volume term accumulated over the points of the order-(p+2) rule,
+//     rhs += w (Fx gx + Fy gy)                 (dg/euler/triangle_residual.hpp:38-57)
+//   * face terms added in ascending global face index, points in order,
+//     rhs -= value * basis (left) / += (right) (triangle_residual.hpp:59-102)
+//   * rhs *= 1/det(J), then the Shu-Osher combination (time/ssp_rk3.hpp:44-60).
+// One thread owns one element, so no atomics touch the residual.
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+
+#include "euler_device.cuh"
+#include "kernels.hpp"
+#include "tri_tables.hpp"
+
+namespace wasl_b200 {
+
+__constant__ VolumeTable<0, double> c_vol0;
+__constant__ VolumeTable<1, double> c_vol1;
+__constant__ VolumeTable<2, double> c_vol2;
+__constant__ VolumeTable<3, double> c_vol3;
+
+template <int P> __device__ __forceinline__ const VolumeTable<P, double> &volume_table();
+template <> __device__ __forceinline__ const VolumeTable<0, double> &volume_table<0>() { return c_vol0; }
+template <> __device__ __forceinline__ const VolumeTable<1, double> &volume_table<1>() { return c_vol1; }
+template <> __device__ __forceinline__ const VolumeTable<2, double> &volume_table<2>() { return c_vol2; }
+template <> __device__ __forceinline__ const VolumeTable<3, double> &volume_table<3>() { return c_vol3; }
+
+// Euler state of element `e` of a global SoA array at a point with basis `b`.
+template <int M>
+__device__ __forceinline__ void eval_global(const double *__restrict__ u, std::int64_t ne,
+                                            std::int64_t e, const double *b, double *s) {
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    double acc = 0.0;
+#pragma unroll
+    for (int m = 0; m < M; ++m)
+      acc += __ldg(u + (static_cast<std::int64_t>(v) * M + m) * ne + e) * b[m];
+    s[v] = acc;
+  }
+}
+
+template <int M>
+__device__ __forceinline__ void eval_local(const double (&c)[4][M], const double *b, double *s) {
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    double acc = 0.0;
+#pragma unroll
+    for (int m = 0; m < M; ++m)
+      acc += c[v][m] * b[m];
+    s[v] = acc;
+  }
+}
+
+template <int P>
+__global__ void __launch_bounds__(128) euler_tri_stage_f64(const StageArgs a) {
+  using S = TriShape<P>;
+  constexpr int M = S::M, QV = S::QV, QF = S::QF;
+  const std::int64_t ne = a.mesh.ne;
+  const std::int64_t e = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= ne)
+    return;
+  const double *__restrict__ in = a.in;
+  const VolumeTable<P, double> &T = volume_table<P>();
+  const FaceTable<P, double> *__restrict__ F = static_cast<const FaceTable<P, double> *>(a.face_table);
+  const double gamma = a.gamma;
+
+  double c[4][M], r[4][M];
+#pragma unroll
+  for (int v = 0; v < 4; ++v)
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      c[v][m] = in[(static_cast<std::int64_t>(v) * M + m) * ne + e];
+      r[v][m] = 0.0;
+    }
+  const double *__restrict__ geo = a.mesh.geo;
+  const double ax = geo[e], ay = geo[ne + e], bx = geo[2 * ne + e], by = geo[3 * ne + e];
+
+  // Volume term: sum_q w_q (F_x . d(phi)/dx + F_y . d(phi)/dy) det(J).
+#pragma unroll 1
+  for (int q = 0; q < QV; ++q) {
+    double s[4], fx[4], fy[4];
+    eval_local<M>(c, T.phi[q], s);
+    flux_xy(gamma, s, fx, fy);
+    const double w = T.w[q];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const double gxi = T.dxi[q][m], geta = T.deta[q][m];
+      const double gx = 0.5 * (by * gxi - ay * geta);
+      const double gy = 0.5 * (-bx * gxi + ax * geta);
+#pragma unroll
+      for (int v = 0; v < 4; ++v)
+        r[v][m] += w * (fx[v] * gx + fy[v] * gy);
+    }
+  }
+
+  // Face terms in ascending global face index.
+#pragma unroll 1
+  for (int k = 0; k < 3; ++k) {
+    const std::int32_t nb = a.mesh.slot_nbr[k * ne + e];
+    const unsigned code = a.mesh.slot_code[k * ne + e];
+    const double nx = a.mesh.slot_geo[(3 * k) * ne + e];
+    const double ny = a.mesh.slot_geo[(3 * k + 1) * ne + e];
+    const double scale = a.mesh.slot_geo[(3 * k + 2) * ne + e];
+    const bool self_left = code & 1u;
+    const int le = (code >> 1) & 3u, re = (code >> 3) & 3u, flip = (code >> 5) & 1u;
+    const double(*lb)[M] = F->lb[le];
+    const double(*rb)[M] = F->rb[(le * 3 + re) * 2 + flip];
+#pragma unroll 1
+    for (int q = 0; q < QF; ++q) {
+      double ls[4], rs[4], f[4];
+      if (self_left) {
+        eval_local<M>(c, lb[q], ls);
+        if (nb >= 0) {
+          eval_global<M>(in, ne, nb, rb[q], rs);
+        } else if (a.mesh.boundary == 3) {
+#pragma unroll
+          for (int v = 0; v < 4; ++v)
+            rs[v] = ls[v];
+        } else {
+          const std::int64_t point = static_cast<std::int64_t>(-nb - 1) * QF + q;
+          eval_global<M>(in, ne, a.mesh.donor[point], a.mesh.donor_basis + point * M, rs);
+        }
+      } else {
+        eval_global<M>(in, ne, nb, lb[q], ls);
+        eval_local<M>(c, rb[q], rs);
+      }
+      hllc(gamma, ls, rs, nx, ny, f);
+      const double weight = F->ew[le][q] * scale;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const double value = f[v] * weight;
+        if (self_left) {
+#pragma unroll
+          for (int m = 0; m < M; ++m)
+            r[v][m] -= value * lb[q][m];
+        } else {
+#pragma unroll
+          for (int m = 0; m < M; ++m)
+            r[v][m] += value * rb[q][m];
+        }
+      }
+    }
+  }
+
+  // Mass inverse and the Shu-Osher combination.
+  const double inv = geo[4 * ne + e];
+  const double dt = *a.dt;
+  double rho[M];
+#pragma unroll
+  for (int v = 0; v < 4; ++v)
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const std::int64_t idx = (static_cast<std::int64_t>(v) * M + m) * ne + e;
+      const double rr = r[v][m] * inv;
+      double o;
+      if (a.stage == 0)
+        o = c[v][m] + dt * rr;
+      else if (a.stage == 1)
+        o = 0.75 * a.u0[idx] + 0.25 * (c[v][m] + dt * rr);
+      else
+        o = (1.0 / 3.0) * a.u0[idx] + (2.0 / 3.0) * (c[v][m] + dt * rr);
+      a.out[idx] = o;
+      if (v == 0)
+        rho[m] = o;
+    }
+
+  // Modal-decay sensor on the density modes of the new stage
+  // (limiting/troubled_cell/modal_decay.hpp:23-33, euler_modal_limiter.cpp:18-24).
+  if (a.sense) {
+    double total = 0.0, high = 0.0;
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      total += rho[m] * rho[m];
+      if (m >= a.highest_degree_begin)
+        high += rho[m] * rho[m];
+    }
+    const bool troubled = !(total == 0.0 || high / total <= a.threshold);
+    a.flags[e] = troubled ? 1 : 0;
+    const unsigned active = __activemask();
+    const unsigned ballot = __ballot_sync(active, troubled);
+    if (ballot) {
+      const int lane = threadIdx.x & 31;
+      const int leader = __ffs(ballot) - 1;
+      int base = 0;
+      if (lane == leader)
+        base = atomicAdd(a.troubled_count, __popc(ballot));
+      base = __shfl_sync(active, base, leader);
+      if (troubled)
+        a.troubled[base + __popc(ballot & ((1u << lane) - 1u))] = static_cast<std::int32_t>(e);
+    }
+  }
+}
+
+// ---- limiter ------------------------------------------------------------------
+
+// euler_characteristic.hpp:19-42
+__device__ __forceinline__ void to_characteristic(double gamma, const double *avg,
+                                                  const double *d, double nx, double ny,
+                                                  double *out) {
+  const Prim<double> mean = primitive(gamma, avg);
+  const double un = mean.vx * nx + mean.vy * ny;
+  const double ut = -mean.vx * ny + mean.vy * nx;
+  const double nm = d[1] * nx + d[2] * ny;
+  const double tm = -d[1] * ny + d[2] * nx;
+  const double c2 = gamma * mean.p / mean.rho;
+  const double c = sqrt(c2);
+  const double ke = 0.5 * (un * un + ut * ut);
+  const double factor = (gamma - 1.0) / c2;
+  const double common = factor * (ke * d[0] - un * nm - ut * tm + d[3]);
+  const double diff = (un * d[0] - nm) / c;
+  out[0] = 0.5 * (common + diff);
+  out[1] = d[0] - common;
+  out[2] = tm - ut * d[0];
+  out[3] = 0.5 * (common - diff);
+}
+
+// euler_characteristic.hpp:44-67
+__device__ __forceinline__ void from_characteristic(double gamma, const double *avg,
+                                                    const double *w, double nx, double ny,
+                                                    double *out) {
+  const Prim<double> mean = primitive(gamma, avg);
+  const double un = mean.vx * nx + mean.vy * ny;
+  const double ut = -mean.vx * ny + mean.vy * nx;
+  const double c = sound_speed(gamma, mean);
+  const double h = (avg[3] + mean.p) / avg[0];
+  const double ke = 0.5 * (un * un + ut * ut);
+  const double rho = w[0] + w[1] + w[3];
+  const double nm = (un - c) * w[0] + un * w[1] + (un + c) * w[3];
+  const double tm = ut * rho + w[2];
+  const double energy = (h - un * c) * w[0] + ke * w[1] + ut * w[2] + (h + un * c) * w[3];
+  out[0] = rho;
+  out[1] = nx * nm - ny * tm;
+  out[2] = ny * nm + nx * tm;
+  out[3] = energy;
+}
+
+template <int M> __device__ __forceinline__ double smoothness(const double *c) {
+  double value = 0.0;
+#pragma unroll
+  for (int m = 1; m < M; ++m)
+    value += c[m] * c[m];
+  return value;
+}
+
+template <int M, int NB>
+__global__ void __launch_bounds__(64) limit_f64(const LimitArgs a) {
+  const int count = *a.troubled_count;
+  const std::int64_t ne = a.ne;
+  const double *__restrict__ u = a.state;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+    const std::int64_t e = a.troubled[k];
+    double target[4 * M], cand[NB * 4 * M];
+#pragma unroll
+    for (int i = 0; i < 4 * M; ++i)
+      target[i] = u[i * ne + e];
+    // Candidates: each neighbour mapped into this element's basis, with this
+    // element's own mean (euler_modal_limiter.cpp:43-66).
+    int n = 0;
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+      const std::int32_t nb = a.neighbors[e * NB + j];
+      if (nb < 0)
+        continue;
+      const double *__restrict__ T = a.transforms + (e * NB + j) * M * M;
+      for (int v = 0; v < 4; ++v) {
+        for (int t = 0; t < M; ++t) {
+          double acc = 0.0;
+          for (int s = 0; s < M; ++s)
+            acc += T[t * M + s] * u[(static_cast<std::int64_t>(v) * M + s) * ne + nb];
+          cand[(n * 4 + v) * M + t] = acc;
+        }
+        cand[(n * 4 + v) * M] = target[v * M];
+      }
+      ++n;
+    }
+    const double root2 = sqrt(2.0);
+    const double avg[4] = {target[0] / root2, target[M] / root2, target[2 * M] / root2,
+                           target[3 * M] / root2};
+    const double nx = a.normal_x[e], ny = a.normal_y[e];
+
+    // Characteristic projection of target and candidates (euler_characteristic_weno.hpp:31-44).
+    double tc[4 * M], cc[NB * 4 * M], lim[4 * M];
+    for (int m = 0; m < M; ++m) {
+      const double d[4] = {target[m], target[M + m], target[2 * M + m], target[3 * M + m]};
+      double w[4];
+      to_characteristic(a.gamma, avg, d, nx, ny, w);
+      for (int wv = 0; wv < 4; ++wv)
+        tc[wv * M + m] = w[wv];
+    }
+    for (int i = 0; i < n; ++i)
+      for (int m = 0; m < M; ++m) {
+        const double *src = cand + i * 4 * M;
+        const double d[4] = {src[m], src[M + m], src[2 * M + m], src[3 * M + m]};
+        double w[4];
+        to_characteristic(a.gamma, avg, d, nx, ny, w);
+        for (int wv = 0; wv < 4; ++wv)
+          cc[(i * 4 + wv) * M + m] = w[wv];
+      }
+    // Simple WENO per wave (simple_weno.hpp:21-48).
+    double lc[4 * M];
+    for (int wv = 0; wv < 4; ++wv) {
+      const double *tw = tc + wv * M;
+      double *lw = lc + wv * M;
+      if (n == 0) {
+        for (int m = 0; m < M; ++m)
+          lw[m] = tw[m];
+        continue;
+      }
+      double weights[NB + 1];
+      const double td = 1e-12 + smoothness<M>(tw);
+      weights[0] = 0.5 / (td * td);
+      double sum = weights[0];
+      const double ideal = 0.5 / static_cast<double>(n);
+      for (int i = 0; i < n; ++i) {
+        const double dd = 1e-12 + smoothness<M>(cc + (i * 4 + wv) * M);
+        weights[i + 1] = ideal / (dd * dd);
+        sum += weights[i + 1];
+      }
+      lw[0] = tw[0];
+      for (int m = 1; m < M; ++m) {
+        double value = weights[0] * tw[m];
+        for (int i = 0; i < n; ++i)
+          value += weights[i + 1] * cc[(i * 4 + wv) * M + m];
+        lw[m] = value / sum;
+      }
+    }
+    for (int m = 0; m < M; ++m) {
+      const double w[4] = {lc[m], lc[M + m], lc[2 * M + m], lc[3 * M + m]};
+      double s[4];
+      from_characteristic(a.gamma, avg, w, nx, ny, s);
+      for (int v = 0; v < 4; ++v)
+        lim[v * M + m] = s[v];
+    }
+    for (int v = 0; v < 4; ++v)
+      lim[v * M] = target[v * M];
+
+    // Positivity (limiting/positivity/euler_positivity.hpp:63-102).
+    const double inv_root2 = 1.0 / sqrt(2.0);
+    const double pavg[4] = {lim[0] * inv_root2, lim[M] * inv_root2, lim[2 * M] * inv_root2,
+                            lim[3 * M] * inv_root2};
+    const double rf = a.density_floor, pf = a.pressure_floor;
+    if (pavg[0] <= rf || primitive(a.gamma, pavg).p <= pf) {
+      raise_error(a.error, kBelowFloor, e);
+    } else {
+      double dscale = 1.0;
+      for (int pt = 0; pt < a.check_points; ++pt) {
+        const double *b = a.check_basis + pt * M;
+        double rho = 0.0;
+        for (int m = 0; m < M; ++m)
+          rho += lim[m] * b[m];
+        if (rho < rf)
+          dscale = smin(dscale, (pavg[0] - rf) / (pavg[0] - rho));
+      }
+      for (int v = 0; v < 4; ++v)
+        for (int m = 1; m < M; ++m)
+          lim[v * M + m] *= dscale;
+      double pscale = 1.0;
+      for (int pt = 0; pt < a.check_points; ++pt) {
+        const double *b = a.check_basis + pt * M;
+        double s[4];
+        for (int v = 0; v < 4; ++v) {
+          double acc = 0.0;
+          for (int m = 0; m < M; ++m)
+            acc += lim[v * M + m] * b[m];
+          s[v] = acc;
+        }
+        if (primitive(a.gamma, s).p >= pf)
+          continue;
+        double lower = 0.0, upper = 1.0;
+        for (int it = 0; it < 64; ++it) {
+          const double middle = 0.5 * (lower + upper);
+          double x[4];
+          for (int v = 0; v < 4; ++v)
+            x[v] = pavg[v] + middle * (s[v] - pavg[v]);
+          if (primitive(a.gamma, x).p >= pf)
+            lower = middle;
+          else
+            upper = middle;
+        }
+        pscale = smin(pscale, lower);
+      }
+      for (int v = 0; v < 4; ++v)
+        for (int m = 1; m < M; ++m)
+          lim[v * M + m] *= pscale;
+    }
+    double *dst = a.limited + static_cast<std::int64_t>(k) * 4 * M;
+    for (int i = 0; i < 4 * M; ++i)
+      dst[i] = lim[i];
+  }
+}
+
+template <int M>
+__global__ void scatter_limited(double *state, std::int64_t ne, const std::int32_t *troubled,
+                                const std::int32_t *count, const double *limited) {
+  const int n = *count;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const std::int64_t e = troubled[k];
+#pragma unroll
+    for (int i = 0; i < 4 * M; ++i)
+      state[i * ne + e] = limited[static_cast<std::int64_t>(k) * 4 * M + i];
+  }
+}
+
+// Modal-decay sensor over a whole state (the stage kernels fuse it instead).
+template <int M>
+__global__ void sense_f64(SenseArgs a) {
+  const std::int64_t e = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= a.ne)
+    return;
+  double total = 0.0, high = 0.0;
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    const double value = a.state[static_cast<std::int64_t>(m) * a.ne + e];
+    total += value * value;
+    if (m >= a.highest_degree_begin)
+      high += value * value;
+  }
+  const bool troubled = !(total == 0.0 || high / total <= a.threshold);
+  a.flags[e] = troubled ? 1 : 0;
+  if (troubled)
+    a.troubled[atomicAdd(a.troubled_count, 1)] = static_cast<std::int32_t>(e);
+}
+
+// ---- CFL ------------------------------------------------------------------------
+
+__device__ __forceinline__ double cell_speed(const CflArgs &a, std::int64_t e, bool &physical) {
+  const double scale = 1.0 / sqrt(2.0);
+  const std::int64_t plane = static_cast<std::int64_t>(a.M) * a.ne;
+  const double s[4] = {scale * a.state[e], scale * a.state[plane + e],
+                       scale * a.state[2 * plane + e], scale * a.state[3 * plane + e]};
+  physical = s[0] > 0.0 && primitive(a.gamma, s).p > 0.0;
+  const Prim<double> v = primitive(a.gamma, s);
+  const double velocity = a.dimensions == 1 ? fabs(v.vx) : hypot(v.vx, v.vy);
+  return velocity + sound_speed(a.gamma, v);
+}
+
+__global__ void cfl_max(const CflArgs a) {
+  __shared__ unsigned long long block_max[32];
+  unsigned long long best = 0;
+  for (std::int64_t e = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; e < a.ne;
+       e += static_cast<std::int64_t>(gridDim.x) * blockDim.x) {
+    bool physical = true;
+    const double speed = cell_speed(a, e, physical);
+    if (!physical) {
+      raise_error(a.error, kNonPhysicalAverage, e);
+      continue;
+    }
+    const unsigned long long bits = __double_as_longlong(speed);
+    best = bits > best ? bits : best;
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    const unsigned long long o = __shfl_down_sync(0xffffffffu, best, off);
+    best = o > best ? o : best;
+  }
+  if ((threadIdx.x & 31) == 0)
+    block_max[threadIdx.x >> 5] = best;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    best = threadIdx.x < (blockDim.x >> 5) ? block_max[threadIdx.x] : 0ULL;
+    for (int off = 16; off > 0; off >>= 1) {
+      const unsigned long long o = __shfl_down_sync(0xffffffffu, best, off);
+      best = o > best ? o : best;
+    }
+    if (threadIdx.x == 0)
+      atomicMax(a.result, best);
+  }
+}
+
+// The smallest element index reaching the maximum, as ~index under atomicMax.
+__global__ void cfl_argmax(const CflArgs a) {
+  const unsigned long long target = a.result[0];
+  for (std::int64_t e = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; e < a.ne;
+       e += static_cast<std::int64_t>(gridDim.x) * blockDim.x) {
+    bool physical = true;
+    const double speed = cell_speed(a, e, physical);
+    if (physical && static_cast<unsigned long long>(__double_as_longlong(speed)) == target)
+      atomicMax(a.result + 1, ~static_cast<unsigned long long>(e));
+  }
+}
+
+__global__ void cfl_finish(const CflArgs a) {
+  const double speed = __longlong_as_double(static_cast<long long>(a.result[0]));
+  const std::int64_t e = a.result[1] ? static_cast<std::int64_t>(~a.result[1]) : 0;
+  const std::int64_t plane = static_cast<std::int64_t>(a.M) * a.ne;
+  for (int v = 0; v < 4; ++v)
+    a.result[2 + v] = static_cast<unsigned long long>(__double_as_longlong(a.state[v * plane + e]));
+  const double dt = speed > 0.0 ? a.cfl * a.length / (speed * (2 * a.p + 1)) : 0.0;
+  a.result[6] = static_cast<unsigned long long>(__double_as_longlong(dt));
+  if (a.dt)
+    *a.dt = dt;
+}
+
+// ---- host launchers -------------------------------------------------------------
+
+namespace {
+
+void check(cudaError_t rc, const char *what) {
+  if (rc != cudaSuccess)
+    throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(rc));
+}
+
+template <int P> void upload_volume(const void *symbol) {
+  static VolumeTable<P, double> table;
+  fill_volume_table<P, double>(table);
+  check(cudaMemcpyToSymbol(symbol, &table, sizeof(table)), "upload volume table");
+}
+
+template <int P> void stage(const StageArgs &a, cudaStream_t s) {
+  const unsigned blocks = static_cast<unsigned>((a.mesh.ne + 127) / 128);
+  euler_tri_stage_f64<P><<<blocks, 128, 0, s>>>(a);
+}
+
+} // namespace
+
+bool euler_tri_order_supported(int p) { return p >= 0 && p <= 3; }
+
+void upload_euler_tri_tables_f64(int p) {
+  switch (p) {
+  case 0: upload_volume<0>(reinterpret_cast<const void *>(&c_vol0)); break;
+  case 1: upload_volume<1>(reinterpret_cast<const void *>(&c_vol1)); break;
+  case 2: upload_volume<2>(reinterpret_cast<const void *>(&c_vol2)); break;
+  case 3: upload_volume<3>(reinterpret_cast<const void *>(&c_vol3)); break;
+  default: throw std::invalid_argument("triangle polynomial order must be 0..3");
+  }
+}
+
+void launch_euler_tri_stage_f64(int p, const StageArgs &a, cudaStream_t s) {
+  switch (p) {
+  case 0: stage<0>(a, s); break;
+  case 1: stage<1>(a, s); break;
+  case 2: stage<2>(a, s); break;
+  case 3: stage<3>(a, s); break;
+  default: throw std::invalid_argument("triangle polynomial order must be 0..3");
+  }
+}
+
+void launch_limit_f64(int M, int NB, const LimitArgs &a, cudaStream_t s) {
+  const unsigned blocks = static_cast<unsigned>(std::min<std::int64_t>((a.ne + 63) / 64, 148 * 16));
+  const unsigned sblocks = static_cast<unsigned>(std::min<std::int64_t>((a.ne + 255) / 256, 148 * 8));
+#define WASL_LIMIT(MM, NN)                                                                     \
+  if (M == MM && NB == NN) {                                                                   \
+    limit_f64<MM, NN><<<blocks, 64, 0, s>>>(a);                                                \
+    scatter_limited<MM><<<sblocks, 256, 0, s>>>(a.state, a.ne, a.troubled, a.troubled_count,   \
+                                                 a.limited);                                   \
+    return;                                                                                    \
+  }
+  WASL_LIMIT(3, 3)
+  WASL_LIMIT(6, 3)
+  WASL_LIMIT(10, 3)
+  WASL_LIMIT(2, 2)
+  WASL_LIMIT(3, 2)
+  WASL_LIMIT(4, 2)
+#undef WASL_LIMIT
+  throw std::invalid_argument("limiter: unsupported mode count");
+}
+
+void launch_sense_f64(int M, const SenseArgs &a, cudaStream_t s) {
+  const unsigned blocks = static_cast<unsigned>((a.ne + 255) / 256);
+  switch (M) {
+  case 1: sense_f64<1><<<blocks, 256, 0, s>>>(a); break;
+  case 2: sense_f64<2><<<blocks, 256, 0, s>>>(a); break;
+  case 3: sense_f64<3><<<blocks, 256, 0, s>>>(a); break;
+  case 4: sense_f64<4><<<blocks, 256, 0, s>>>(a); break;
+  case 5: sense_f64<5><<<blocks, 256, 0, s>>>(a); break;
+  case 6: sense_f64<6><<<blocks, 256, 0, s>>>(a); break;
+  case 7: sense_f64<7><<<blocks, 256, 0, s>>>(a); break;
+  case 10: sense_f64<10><<<blocks, 256, 0, s>>>(a); break;
+  default: throw std::invalid_argument("sensor: unsupported mode count");
+  }
+}
+
+void launch_cfl(const CflArgs &a, cudaStream_t s) {
+  check(cudaMemsetAsync(a.result, 0, 8 * sizeof(unsigned long long), s), "cfl reset");
+  const unsigned blocks = static_cast<unsigned>(std::min<std::int64_t>((a.ne + 255) / 256, 148 * 4));
+  cfl_max<<<blocks, 256, 0, s>>>(a);
+  cfl_argmax<<<blocks, 256, 0, s>>>(a);
+  cfl_finish<<<1, 1, 0, s>>>(a);
+}
+
+} // namespace wasl_b200

@@ -1,0 +1,397 @@
+// 2D Euler on triangles: setup data on the device and the SSP-RK3 step.
+//
+// Mirrors the reference case driver (cpp/src/case/euler_triangle.cpp:16-49):
+// periodic trace and limiter stencil built once, then per step the CFL time
+// step (cfl_timestep.cpp:78-84) and ssp_rk3_step with the stage limiter
+// (ssp_rk3.hpp:37-61, euler_state_operations.cpp:26-34).
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+
+#include "basis.hpp"
+#include "kernels.hpp"
+#include "mesh.hpp"
+#include "solver.hpp"
+#include "tri_tables.hpp"
+
+namespace wasl_b200 {
+
+void cuda_check(cudaError_t rc, const char *what) {
+  if (rc != cudaSuccess)
+    throw SolverError(WASL_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(rc));
+}
+
+namespace {
+
+// Pinned host scratch for the few scalars a step exchanges with the device.
+struct PinnedScratch {
+  double *dt = nullptr;
+  unsigned long long *words = nullptr; // error word + CFL result (8)
+  PinnedScratch() {
+    cuda_check(cudaMallocHost(reinterpret_cast<void **>(&dt), sizeof(double)), "pinned");
+    cuda_check(cudaMallocHost(reinterpret_cast<void **>(&words), 16 * sizeof(unsigned long long)),
+               "pinned");
+  }
+  ~PinnedScratch() {
+    cudaFreeHost(dt);
+    cudaFreeHost(words);
+  }
+};
+
+double bits_to_double(unsigned long long b) {
+  double d;
+  std::memcpy(&d, &b, sizeof(d));
+  return d;
+}
+
+} // namespace
+
+// Host evaluation of one cell-average wave speed with the C library's hypot,
+// as cfl_timestep.cpp:33-47 computes it.
+double host_cell_speed(double gamma, const double *mode0, int dimensions) {
+  const double scale = 1.0 / std::sqrt(2.0);
+  const double s[4] = {scale * mode0[0], scale * mode0[1], scale * mode0[2], scale * mode0[3]};
+  const double inv = 1.0 / s[0];
+  const double vx = s[1] * inv, vy = s[2] * inv;
+  const double ke = 0.5 * (s[1] * vx + s[2] * vy);
+  const double p = (gamma - 1.0) * (s[3] - ke);
+  const double velocity = dimensions == 1 ? std::fabs(vx) : std::hypot(vx, vy);
+  return velocity + std::sqrt(gamma * p / s[0]);
+}
+
+class EulerTriSolver final : public Solver {
+public:
+  EulerTriSolver(const wasl_gpu_config &cfg, TriTopology &&topo)
+      : cfg_(cfg), mesh_(std::move(topo)), p_(cfg.polynomial_order),
+        M_(tri_modes(cfg.polynomial_order)) {
+    if (!euler_tri_order_supported(p_))
+      throw SolverError(WASL_ERR_ARGUMENT, "2D Euler: polynomial order must be 0..3");
+    if (cfg.precision != WASL_PLAIN_FP64 && cfg.precision != WASL_MIXED)
+      throw SolverError(WASL_ERR_ARGUMENT, "unknown precision form");
+    cuda_check(cudaSetDevice(cfg.device), "cudaSetDevice");
+    cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
+    ne_ = mesh_.element_count;
+    const std::int64_t nf = mesh_.face_count();
+    const int QF = p_ + 1;
+
+    bool has_boundary = false;
+    for (std::int64_t f = 0; f < nf; ++f)
+      has_boundary |= mesh_.face_right[f] < 0;
+    boundary_ = cfg.boundary_left;
+    if (boundary_ != WASL_PERIODIC && boundary_ != WASL_TRANSMISSIVE)
+      throw SolverError(WASL_ERR_RUNTIME, "simulation: 2D Euler boundaries must be periodic");
+    PeriodicTrace trace;
+    if (has_boundary && boundary_ == WASL_PERIODIC)
+      trace = periodic_trace(mesh_, p_);
+
+    // Element geometry [5][ne] and the three face slots of each element.
+    std::vector<double> geo(5 * ne_);
+    for (std::int64_t e = 0; e < ne_; ++e) {
+      const TriMap &m = mesh_.maps[e];
+      geo[e] = m.ax();
+      geo[ne_ + e] = m.ay();
+      geo[2 * ne_ + e] = m.bx();
+      geo[3 * ne_ + e] = m.by();
+      geo[4 * ne_ + e] = 1.0 / m.jacobian_determinant();
+    }
+    std::vector<std::int32_t> slot_nbr(3 * ne_);
+    std::vector<std::uint8_t> slot_code(3 * ne_);
+    std::vector<double> slot_geo(9 * ne_);
+    std::vector<int> fill(ne_, 0);
+    std::vector<std::int32_t> donors;
+    std::vector<double> donor_basis;
+    std::int32_t boundary_index = 0;
+    for (std::int64_t f = 0; f < nf; ++f) { // ascending face index = slot order
+      const std::int32_t L = mesh_.face_left[f], R = mesh_.face_right[f];
+      const unsigned le = mesh_.face_left_edge[f], re = mesh_.face_right_edge[f];
+      const unsigned flip = mesh_.face_flip[f];
+      const unsigned shared = (le << 1) | (re << 3) | (flip << 5);
+      std::int32_t right_slot_value = R;
+      if (R < 0) {
+        right_slot_value = -(boundary_index + 1);
+        if (boundary_ == WASL_PERIODIC)
+          for (int q = 0; q < QF; ++q) {
+            donors.push_back(trace.donors[f * QF + q]);
+            donor_basis.insert(donor_basis.end(), trace.basis.begin() + (f * QF + q) * M_,
+                               trace.basis.begin() + (f * QF + q + 1) * M_);
+          }
+        ++boundary_index;
+      }
+      auto put = [&](std::int32_t e, std::int32_t other, unsigned code) {
+        const int k = fill[e]++;
+        slot_nbr[k * ne_ + e] = other;
+        slot_code[k * ne_ + e] = static_cast<std::uint8_t>(code);
+        slot_geo[(3 * k) * ne_ + e] = mesh_.face_nx[f];
+        slot_geo[(3 * k + 1) * ne_ + e] = mesh_.face_ny[f];
+        slot_geo[(3 * k + 2) * ne_ + e] = mesh_.face_scale[f];
+      };
+      put(L, right_slot_value, shared | 1u);
+      if (R >= 0)
+        put(R, L, shared);
+    }
+    for (std::int64_t e = 0; e < ne_; ++e)
+      if (fill[e] != 3)
+        throw SolverError(WASL_ERR_RUNTIME, "triangle mesh: element without three faces");
+
+    d_geo_.upload(geo, stream_);
+    d_slot_nbr_.upload(slot_nbr, stream_);
+    d_slot_code_.upload(slot_code, stream_);
+    d_slot_geo_.upload(slot_geo, stream_);
+    if (!donors.empty()) {
+      d_donor_.upload(donors, stream_);
+      d_donor_basis_.upload(donor_basis, stream_);
+    }
+    upload_euler_tri_tables_f64(p_);
+    std::vector<unsigned char> table(euler_tri_face_table_bytes(p_, false));
+    fill_euler_tri_face_table(p_, false, table.data());
+    d_face_table_.upload(table, stream_);
+
+    limiting_ = cfg.limiting && p_ > 0;
+    if (limiting_) {
+      stencil_ = triangle_stencil(mesh_, p_, trace.donors);
+      d_neighbors_.upload(stencil_.neighbors, stream_);
+      d_transforms_.upload(stencil_.transforms, stream_);
+      d_normal_x_.upload(stencil_.normal_x, stream_);
+      d_normal_y_.upload(stencil_.normal_y, stream_);
+      d_check_.upload(stencil_.check_basis, stream_);
+      d_limited_.resize(static_cast<std::size_t>(ne_) * 4 * M_);
+      d_troubled_.resize(ne_);
+    }
+    d_flags_.resize(3 * ne_);
+    cuda_check(cudaMemsetAsync(d_flags_.get(), 0, 3 * ne_, stream_), "memset");
+    d_count_.resize(4);
+    for (auto *b : {&d_u_, &d_e_, &d_s_})
+      b->resize(static_cast<std::size_t>(4) * M_ * ne_);
+    cuda_check(cudaMemsetAsync(d_u_.get(), 0, d_u_.size() * sizeof(double), stream_), "memset");
+    d_error_.resize(1);
+    d_cfl_.resize(8);
+    d_dt_.resize(1);
+    cuda_check(cudaMemsetAsync(d_error_.get(), 0, sizeof(unsigned long long), stream_), "memset");
+    length_ = minimum_altitude(mesh_);
+    cuda_check(cudaStreamSynchronize(stream_), "setup");
+  }
+
+  ~EulerTriSolver() override {
+    if (stream_)
+      cudaStreamDestroy(stream_);
+  }
+
+  std::int64_t elements() const override { return ne_; }
+  std::int64_t faces() const override { return mesh_.face_count(); }
+  int modes() const override { return M_; }
+  int variables() const override { return 4; }
+  double *state_device() override { return d_u_.get(); }
+
+  void vertices(double *out) const override {
+    for (std::int64_t e = 0; e < ne_; ++e) {
+      const TriMap &m = mesh_.maps[e];
+      const double v[6] = {m.x0, m.y0, m.x1, m.y1, m.x2, m.y2};
+      std::memcpy(out + 6 * e, v, sizeof(v));
+    }
+  }
+
+  void set_state(const double *host) override {
+    cuda_check(cudaMemcpyAsync(d_u_.get(), host, d_u_.size() * sizeof(double),
+                               cudaMemcpyHostToDevice, stream_),
+               "set_state");
+    cuda_check(cudaStreamSynchronize(stream_), "set_state");
+  }
+
+  void get_state(double *host) override {
+    cuda_check(cudaMemcpyAsync(host, d_u_.get(), d_u_.size() * sizeof(double),
+                               cudaMemcpyDeviceToHost, stream_),
+               "get_state");
+    cuda_check(cudaStreamSynchronize(stream_), "get_state");
+  }
+
+  CflArgs cfl_args(double cfl) {
+    CflArgs a;
+    a.ne = ne_;
+    a.M = M_;
+    a.dimensions = 2;
+    a.state = d_u_.get();
+    a.gamma = cfg_.heat_capacity_ratio;
+    a.cfl = cfl;
+    a.length = length_;
+    a.p = p_;
+    a.result = d_cfl_.get();
+    a.dt = d_dt_.get();
+    a.error = d_error_.get();
+    return a;
+  }
+
+  double stable_dt(double cfl) override {
+    launch_cfl(cfl_args(cfl), stream_);
+    cuda_check(cudaMemcpyAsync(scratch_.words, d_cfl_.get(), 8 * sizeof(unsigned long long),
+                               cudaMemcpyDeviceToHost, stream_),
+               "cfl result");
+    cuda_check(cudaMemcpyAsync(scratch_.words + 8, d_error_.get(), sizeof(unsigned long long),
+                               cudaMemcpyDeviceToHost, stream_),
+               "cfl error");
+    cuda_check(cudaStreamSynchronize(stream_), "cfl");
+    raise_device_error(scratch_.words[8]);
+    double mode0[4];
+    for (int v = 0; v < 4; ++v)
+      mode0[v] = bits_to_double(scratch_.words[2 + v]);
+    const double speed = host_cell_speed(cfg_.heat_capacity_ratio, mode0, 2);
+    return speed > 0.0 ? cfl * length_ / (speed * (2 * p_ + 1)) : 0.0;
+  }
+
+  void step(double dt) override {
+    *scratch_.dt = dt;
+    cuda_check(cudaMemcpyAsync(d_dt_.get(), scratch_.dt, sizeof(double), cudaMemcpyHostToDevice,
+                               stream_),
+               "dt");
+    enqueue_step();
+    if (limiting_)
+      check_error();
+  }
+
+  void limit() override {
+    if (!limiting_)
+      return;
+    cuda_check(cudaMemsetAsync(d_count_.get(), 0, sizeof(std::int32_t), stream_), "count");
+    SenseArgs sa;
+    sa.ne = ne_;
+    sa.state = d_u_.get();
+    sa.threshold = cfg_.sensor_threshold;
+    sa.highest_degree_begin = stencil_.highest_degree_begin;
+    sa.flags = d_flags_.get();
+    sa.troubled = d_troubled_.get();
+    sa.troubled_count = d_count_.get();
+    launch_sense_f64(M_, sa, stream_);
+    launch_limit_f64(M_, 3, limit_args(d_u_.get()), stream_);
+    check_error();
+  }
+
+  void advance(double cfl, std::int64_t steps) override {
+    for (std::int64_t n = 0; n < steps; ++n) {
+      launch_cfl(cfl_args(cfl), stream_);
+      enqueue_step();
+    }
+    check_error();
+  }
+
+  void flags(std::uint8_t *out) override {
+    cuda_check(cudaMemcpyAsync(out, d_flags_.get(), 3 * ne_, cudaMemcpyDeviceToHost, stream_),
+               "flags");
+    cuda_check(cudaStreamSynchronize(stream_), "flags");
+  }
+
+  void mass_energy(double &mass, double &energy) override {
+    std::vector<double> rho(ne_), en(ne_);
+    cuda_check(cudaMemcpyAsync(rho.data(), d_u_.get(), ne_ * sizeof(double),
+                               cudaMemcpyDeviceToHost, stream_),
+               "mass");
+    cuda_check(cudaMemcpyAsync(en.data(), d_u_.get() + static_cast<std::size_t>(3) * M_ * ne_,
+                               ne_ * sizeof(double), cudaMemcpyDeviceToHost, stream_),
+               "energy");
+    cuda_check(cudaStreamSynchronize(stream_), "mass");
+    mass = energy = 0.0;
+    for (std::int64_t e = 0; e < ne_; ++e) {
+      const double w = std::sqrt(2.0) * mesh_.maps[e].jacobian_determinant();
+      mass += w * rho[e];
+      energy += w * en[e];
+    }
+  }
+
+private:
+  void enqueue_step() {
+    StageArgs a;
+    a.mesh.ne = ne_;
+    a.mesh.geo = d_geo_.get();
+    a.mesh.slot_nbr = d_slot_nbr_.get();
+    a.mesh.slot_code = d_slot_code_.get();
+    a.mesh.slot_geo = d_slot_geo_.get();
+    a.mesh.donor = d_donor_.get();
+    a.mesh.donor_basis = d_donor_basis_.get();
+    a.mesh.boundary = boundary_;
+    a.face_table = d_face_table_.get();
+    a.dt = d_dt_.get();
+    a.gamma = cfg_.heat_capacity_ratio;
+    a.sense = limiting_ ? 1 : 0;
+    a.threshold = cfg_.sensor_threshold;
+    a.highest_degree_begin = stencil_.highest_degree_begin;
+    a.troubled = d_troubled_.get();
+    a.troubled_count = d_count_.get();
+    double *ins[3] = {d_u_.get(), d_e_.get(), d_s_.get()};
+    double *outs[3] = {d_e_.get(), d_s_.get(), d_u_.get()};
+    for (int k = 0; k < 3; ++k) {
+      a.stage = k;
+      a.in = ins[k];
+      a.u0 = d_u_.get();
+      a.out = outs[k];
+      a.flags = d_flags_.get() + k * ne_;
+      if (limiting_)
+        cuda_check(cudaMemsetAsync(d_count_.get(), 0, sizeof(std::int32_t), stream_), "count");
+      launch_euler_tri_stage_f64(p_, a, stream_);
+      if (limiting_)
+        launch_limit_f64(M_, 3, limit_args(outs[k]), stream_);
+    }
+    cuda_check(cudaGetLastError(), "stage launch");
+  }
+
+  LimitArgs limit_args(double *state) {
+    LimitArgs l;
+    l.ne = ne_;
+    l.state = state;
+    l.troubled = d_troubled_.get();
+    l.troubled_count = d_count_.get();
+    l.neighbors = d_neighbors_.get();
+    l.transforms = d_transforms_.get();
+    l.normal_x = d_normal_x_.get();
+    l.normal_y = d_normal_y_.get();
+    l.check_basis = d_check_.get();
+    l.check_points = stencil_.check_point_count();
+    l.gamma = cfg_.heat_capacity_ratio;
+    l.density_floor = cfg_.density_floor;
+    l.pressure_floor = cfg_.pressure_floor;
+    l.limited = d_limited_.get();
+    l.error = d_error_.get();
+    return l;
+  }
+
+  void check_error() {
+    cuda_check(cudaMemcpyAsync(scratch_.words + 8, d_error_.get(), sizeof(unsigned long long),
+                               cudaMemcpyDeviceToHost, stream_),
+               "error word");
+    cuda_check(cudaStreamSynchronize(stream_), "step");
+    raise_device_error(scratch_.words[8]);
+  }
+
+  void raise_device_error(unsigned long long word) {
+    if (!word)
+      return;
+    cuda_check(cudaMemsetAsync(d_error_.get(), 0, sizeof(unsigned long long), stream_), "memset");
+    const int code = static_cast<int>(word >> 56);
+    const long long element = static_cast<long long>(word & 0xffffffffffffffULL);
+    if (code == 1)
+      throw SolverError(WASL_ERR_NONPHYSICAL, "simulation: Euler cell average is not physical"
+                                              " (element " + std::to_string(element) + ")");
+    throw SolverError(WASL_ERR_FLOOR, "Euler positivity limiter: cell average is below a floor"
+                                      " (element " + std::to_string(element) + ")");
+  }
+
+  wasl_gpu_config cfg_;
+  TriTopology mesh_;
+  int p_, M_;
+  std::int64_t ne_ = 0;
+  int boundary_ = 0;
+  bool limiting_ = false;
+  double length_ = 0.0;
+  LimiterStencil stencil_;
+  PinnedScratch scratch_;
+  DeviceArray<double> d_geo_, d_slot_geo_, d_donor_basis_, d_transforms_, d_normal_x_,
+      d_normal_y_, d_check_, d_limited_, d_u_, d_e_, d_s_, d_dt_;
+  DeviceArray<std::int32_t> d_slot_nbr_, d_donor_, d_neighbors_, d_troubled_, d_count_;
+  DeviceArray<std::uint8_t> d_slot_code_, d_flags_;
+  DeviceArray<unsigned char> d_face_table_;
+  DeviceArray<unsigned long long> d_error_, d_cfl_;
+};
+
+std::unique_ptr<Solver> make_euler_tri_solver(const wasl_gpu_config &cfg, TriTopology &&topo) {
+  return std::make_unique<EulerTriSolver>(cfg, std::move(topo));
+}
+
+} // namespace wasl_b200

@@ -1,0 +1,108 @@
+// Launch interface of the CUDA kernels (host side; no device code here).
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace wasl_b200 {
+
+// Device view of a triangle mesh, structure of arrays over elements.
+//   geo       [5][ne]    ax, ay, bx, by (columns of the affine map), 1/det(J)
+//   slot_*    [3][ne]    the element's three faces in ascending global face
+//                        index (the reference's flux summation order):
+//     slot_nbr   the other element, or -(b+1) for boundary face b
+//     slot_code  bit 0: this element is the face's left side; bits 1-2 left
+//                local edge; bits 3-4 right local edge; bit 5 orientation flip
+//     slot_geo   [3][3][ne] face normal x, normal y (left to right), edge scale
+//   donor       [nb][QF] periodic donor element of each boundary edge point
+//   donor_basis [nb][QF][M] donor basis at the periodic image
+struct TriMeshView {
+  std::int64_t ne = 0;
+  const double *geo = nullptr;
+  const std::int32_t *slot_nbr = nullptr;
+  const std::uint8_t *slot_code = nullptr;
+  const double *slot_geo = nullptr;
+  const std::int32_t *donor = nullptr;
+  const double *donor_basis = nullptr;
+  int boundary = 0; // 0 periodic, 3 transmissive (the owner's own trace)
+};
+
+// One SSP-RK3 stage: residual of `in`, then
+//   stage 0: out = in + dt r
+//   stage 1: out = 0.75 u0 + 0.25 (in + dt r)
+//   stage 2: out = (1/3) u0 + (2/3) (in + dt r)
+// (cpp/include/wasl/time/ssp_rk3.hpp:44-60).  With sense != 0 the kernel also
+// evaluates the modal-decay sensor on `out` and appends troubled elements.
+struct StageArgs {
+  TriMeshView mesh;
+  const void *face_table = nullptr; // FaceTable<P, real> in device memory
+  const double *in = nullptr;
+  const double *u0 = nullptr;
+  double *out = nullptr;
+  const double *dt = nullptr; // device scalar
+  double gamma = 1.4;
+  int stage = 0;
+  int sense = 0;
+  double threshold = 1e-3;
+  int highest_degree_begin = 0;
+  std::uint8_t *flags = nullptr;       // [ne]
+  std::int32_t *troubled = nullptr;    // [ne] compacted list
+  std::int32_t *troubled_count = nullptr;
+};
+
+// Limiter over the compacted troubled list (cpp/src/limiting/euler_modal_limiter.cpp:70-98).
+struct LimitArgs {
+  std::int64_t ne = 0;
+  double *state = nullptr;              // U[var][mode][elem], unlimited on entry
+  const std::int32_t *troubled = nullptr;
+  const std::int32_t *troubled_count = nullptr;
+  const std::int32_t *neighbors = nullptr;   // [ne][NB]
+  const double *transforms = nullptr;        // [ne][NB][M][M]
+  const double *normal_x = nullptr, *normal_y = nullptr;
+  const double *check_basis = nullptr;       // [points][M]
+  int check_points = 0;
+  double gamma = 1.4, density_floor = 1e-10, pressure_floor = 1e-10;
+  double *limited = nullptr;                 // [ne][4][M] scratch, by list position
+  unsigned long long *error = nullptr;
+};
+
+// Modal-decay sensor on the density modes of `state` (modal_decay.hpp:23-33).
+struct SenseArgs {
+  std::int64_t ne = 0;
+  const double *state = nullptr;
+  double threshold = 1e-3;
+  int highest_degree_begin = 0;
+  std::uint8_t *flags = nullptr;
+  std::int32_t *troubled = nullptr;
+  std::int32_t *troubled_count = nullptr;
+};
+
+// Largest cell-average wave speed |u| + c (cpp/src/time/cfl_timestep.cpp:33-47).
+// result[0] = speed bits (max), result[1] = smallest element index reaching it,
+// result[2..5] = that element's mode-0 coefficients, then dt in result[6]
+// computed on the device as cfl h / (speed (2p+1)).
+struct CflArgs {
+  std::int64_t ne = 0;
+  int M = 1;
+  int dimensions = 2;
+  const double *state = nullptr;
+  double gamma = 1.4;
+  double cfl = 0.1;
+  double length = 0.0; // minimum altitude (2D) or length (1D)
+  int p = 0;
+  unsigned long long *result = nullptr; // 8 words, zeroed by the first kernel
+  double *dt = nullptr;                 // device dt written by the final kernel
+  unsigned long long *error = nullptr;
+};
+
+bool euler_tri_order_supported(int p);
+void upload_euler_tri_tables_f64(int p);
+std::size_t euler_tri_face_table_bytes(int p, bool fp32);
+void fill_euler_tri_face_table(int p, bool fp32, void *host_buffer);
+void launch_euler_tri_stage_f64(int p, const StageArgs &a, cudaStream_t stream);
+void launch_limit_f64(int M, int NB, const LimitArgs &a, cudaStream_t stream);
+void launch_sense_f64(int M, const SenseArgs &a, cudaStream_t stream);
+void launch_cfl(const CflArgs &a, cudaStream_t stream);
+
+} // namespace wasl_b200

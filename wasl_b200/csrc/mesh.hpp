@@ -1,0 +1,104 @@
+// Host-side mesh setup: canonical topology and the per-mesh data the kernels read.
+//
+// The topology follows the reference's canonical rules so face indices, and with
+// them the flux summation order, are the same:
+//   * triangles reoriented counter-clockwise (build_triangle_mesh.cpp:38-65);
+//   * an edge's left element is the first element (by index, then local edge)
+//     that has it, the right element the second; faces sorted by
+//     (left element, left local edge) (build_triangle_mesh.cpp:67-148);
+//   * the stored normal is the left element's outward unit normal.
+// Lines are oriented left to right, stably sorted by left end, with faces
+// [left boundary, interior pairs..., right boundary] (build_line_mesh.cpp:14-84).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace wasl_b200 {
+
+struct TriMap {
+  double x0, y0, x1, y1, x2, y2;
+
+  double ax() const { return x1 - x0; }
+  double ay() const { return y1 - y0; }
+  double bx() const { return x2 - x0; }
+  double by() const { return y2 - y0; }
+  double det_a() const { return ax() * by() - bx() * ay(); }
+  double jacobian_determinant() const { return det_a() / 4.0; }
+  int orientation() const { return det_a() > 0.0 ? 1 : -1; }
+  void to_physical(double xi, double eta, double &x, double &y) const;
+  void to_reference(double x, double y, double &xi, double &eta) const;
+  void edge_vector(int edge, double &ex, double &ey) const;
+  double edge_length(int edge) const;
+  void edge_normal(int edge, double &nx, double &ny) const;
+  void shift(double ox, double oy);
+};
+
+struct TriTopology {
+  std::int64_t element_count = 0;
+  std::vector<TriMap> maps;               // [element], counter-clockwise
+  std::vector<std::int64_t> nodes;        // [element][3] node tags after reorientation
+  std::vector<std::int32_t> face_left;    // [face]
+  std::vector<std::int32_t> face_right;   // [face], -1 on a boundary
+  std::vector<std::int32_t> face_left_edge, face_right_edge;
+  std::vector<std::uint8_t> face_flip;    // the two sides traverse the edge oppositely
+  std::vector<double> face_nx, face_ny;   // left element's outward unit normal
+  std::vector<double> face_scale;         // physical / reference length of the left edge
+  std::int64_t face_count() const { return static_cast<std::int64_t>(face_left.size()); }
+};
+
+// Throws std::runtime_error with the reference's messages on a bad mesh.
+TriTopology build_triangle_topology(std::int64_t node_count, const std::int64_t *node_tags,
+                                    const double *node_xy, std::int64_t element_count,
+                                    const std::int64_t *element_nodes);
+
+struct LineTopology {
+  std::int64_t element_count = 0;
+  std::vector<double> x_left, x_right;
+  std::vector<std::int32_t> face_left, face_right; // right -1 on a boundary
+  std::vector<double> face_normal;
+  std::int64_t face_count() const { return static_cast<std::int64_t>(face_left.size()); }
+};
+
+LineTopology build_line_topology(std::int64_t node_count, const std::int64_t *node_tags,
+                                 const double *node_x, std::int64_t element_count,
+                                 const std::int64_t *element_nodes);
+
+// Periodic images of every boundary edge point, located once
+// (cpp/src/boundaries/periodic_triangle_trace.cpp:40-67).  The donor of each
+// point is the first element, by index, whose reference coordinates contain it
+// within 1e-10; a uniform bucket grid narrows the candidates, so the search is
+// near-linear instead of the reference's O(boundary x elements), with the same
+// answer.  donors [face][point] (-1 on interior faces), basis
+// [face][point][mode].
+struct PeriodicTrace {
+  std::vector<std::int32_t> donors;
+  std::vector<double> basis;
+};
+PeriodicTrace periodic_trace(const TriTopology &mesh, int p);
+
+// Immediate-neighbour limiter stencil (cpp/include/wasl/limiting/euler_limiter_stencil.hpp:19-50).
+struct LimiterStencil {
+  int mode_count = 0;
+  int maximum_neighbors = 0;
+  int highest_degree_begin = 0;
+  std::vector<std::int32_t> neighbors; // [element][candidate], -1 if absent
+  std::vector<double> transforms;      // [element][candidate][target][source]
+  std::vector<double> normal_x, normal_y;
+  std::vector<double> check_basis;     // [point][mode]
+  int check_point_count() const {
+    return mode_count ? static_cast<int>(check_basis.size()) / mode_count : 0;
+  }
+};
+
+// periodic_donors may be empty (open boundaries).
+LimiterStencil triangle_stencil(const TriTopology &mesh, int p,
+                                const std::vector<std::int32_t> &periodic_donors);
+LimiterStencil line_stencil(const LineTopology &mesh, int p, bool periodic);
+
+// cpp/src/time/cfl_timestep.cpp:14-30
+double minimum_altitude(const TriTopology &mesh);
+double minimum_length(const LineTopology &mesh);
+
+} // namespace wasl_b200

@@ -1,0 +1,86 @@
+// Solver handles behind the C-ABI: device-resident state, per-mesh setup data,
+// and the SSP-RK3 step orchestration.
+#pragma once
+
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/wasl_b200.h"
+
+namespace wasl_b200 {
+
+// Failure carrying a C-ABI status code.
+struct SolverError : std::runtime_error {
+  int status;
+  SolverError(int s, const std::string &m) : std::runtime_error(m), status(s) {}
+};
+
+void cuda_check(cudaError_t rc, const char *what);
+
+// Owning device allocation.
+template <typename T> class DeviceArray {
+public:
+  DeviceArray() = default;
+  explicit DeviceArray(std::size_t n) { resize(n); }
+  DeviceArray(const DeviceArray &) = delete;
+  DeviceArray &operator=(const DeviceArray &) = delete;
+  DeviceArray(DeviceArray &&o) noexcept : p_(o.p_), n_(o.n_) { o.p_ = nullptr, o.n_ = 0; }
+  ~DeviceArray() {
+    if (p_)
+      cudaFree(p_);
+  }
+  void resize(std::size_t n) {
+    if (p_)
+      cudaFree(p_);
+    p_ = nullptr;
+    n_ = n;
+    if (n)
+      cuda_check(cudaMalloc(reinterpret_cast<void **>(&p_), n * sizeof(T)), "cudaMalloc");
+  }
+  void upload(const std::vector<T> &h, cudaStream_t s = nullptr) {
+    resize(h.size());
+    if (!h.empty())
+      cuda_check(cudaMemcpyAsync(p_, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s),
+                 "upload");
+  }
+  T *get() const { return p_; }
+  std::size_t size() const { return n_; }
+
+private:
+  T *p_ = nullptr;
+  std::size_t n_ = 0;
+};
+
+class Solver {
+public:
+  virtual ~Solver() = default;
+  virtual std::int64_t elements() const = 0;
+  virtual std::int64_t faces() const = 0;
+  virtual int modes() const = 0;
+  virtual int variables() const = 0;
+  virtual void vertices(double *out) const = 0;
+  virtual void set_state(const double *host) = 0;
+  virtual void get_state(double *host) = 0;
+  virtual double stable_dt(double cfl) = 0;
+  virtual void step(double dt) = 0;
+  virtual void limit() = 0; // the stage limiter applied to the current state
+  virtual void advance(double cfl, std::int64_t steps) = 0;
+  virtual void flags(std::uint8_t *out) = 0;
+  virtual void mass_energy(double &mass, double &energy) = 0;
+  virtual double *state_device() = 0;
+  cudaStream_t stream() const { return stream_; }
+
+protected:
+  cudaStream_t stream_ = nullptr;
+};
+
+std::unique_ptr<Solver> make_solver(const wasl_gpu_config &config, std::int64_t node_count,
+                                    const std::int64_t *node_tags, const double *coordinates,
+                                    std::int64_t element_count, const std::int64_t *element_nodes);
+
+} // namespace wasl_b200
