@@ -1,0 +1,413 @@
+#!/usr/bin/env python
+"""DOF x RK-stage throughput of the Wasl SSP-RK3 step on one B200.
+
+Workload (the metric's quoted configuration): 2D Euler (gamma 1.4) isentropic
+vortex of strength 5 centred at (5,5), advected with (1,1) on the periodic
+square [0,10]^2; 256x256 quads split along seeded random diagonals with
+interior vertices jittered +-0.15h (131,072 triangles); P2 (6 modes x 4
+variables, 3,145,728 DOF); CFL 0.15; limiter off.  A step is one SSP-RK3 step
+(three stages plus the device CFL reduction).  L2 is flushed (256 MiB write)
+between timed steps, outside the timed events.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on rank 0.  Under torchrun each rank advances its own replica
+(the path shards by element but this benchmark runs replicas: weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("DOF·RK-stage/s on 1 B200: chosen form vs plain FP64 path at matched L1 error")
+UNIT = "DOF*stage/s"
+CFL = 0.15
+# Algorithmic bytes per stage launch (per DOF and per element): each stage
+# reads its input state (8 B/DOF), stages 2-3 also read u^n, and every stage
+# writes its output -> (16+24+24)/3 B/DOF on average; per element 40 B of
+# geometry, 16 B of face indices/codes and 1.5 faces x 24 B of normals and
+# edge scales = 92 B.
+BYTES_PER_DOF = 64.0 / 3.0
+BYTES_PER_ELEMENT = 92.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--form", choices=["chosen", "plain", "mixed"], default="chosen")
+    ap.add_argument("--n", type=int, default=256, help="quads per side")
+    ap.add_argument("--p", type=int, default=2)
+    ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.proc, self.lines = index, None, []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "50"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, f[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------------
+
+def build_solver(args, form, device):
+    import wasl_b200
+    from wasl_b200 import cases
+    arrays = cases.vortex_mesh(args.n)
+    vortex = cases.IsentropicVortex()
+    g = wasl_b200.Solver(*arrays, polynomial_order=args.p, precision=form, device=device)
+    cases.project_initial(g, vortex.conserved)
+    return g, vortex
+
+
+def time_device_steps(g, args, torch, flush, stream):
+    """W untimed steps, then K steps each bracketed by events; L2 flushed between."""
+    g.advance(CFL, args.warmup)
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    g.profile_begin()
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.zero_()
+            starts[k].record(stream)
+            g.advance(CFL, 1)
+            ends[k].record(stream)
+    torch.cuda.synchronize()
+    stage_ms, stage_kernels, launches = g.profile_end()
+    total_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    return total_ms, stage_ms, stage_kernels, launches
+
+
+def time_e2e(g, args, torch, stream):
+    """Through the C-ABI with host buffers: each step copies the state in from
+    pinned host memory, computes the CFL step, advances, and copies it out."""
+    n = g.state_size
+    host_in = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    host_out = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    g.get_state_into(host_in)
+    steps = max(5, min(args.steps, 50))
+    for _ in range(2):
+        g.set_state(host_in)
+        g.step(g.stable_dt(CFL))
+        g.get_state_into(host_out)
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(steps):
+        g.set_state(host_in)
+        g.step(g.stable_dt(CFL))
+        g.get_state_into(host_out)
+        host_in, host_out = host_out, host_in
+    end.record(stream)
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(end)
+    return 3.0 * n * steps / (ms * 1e-3), steps, 8 * n, 8 * n
+
+
+def accuracy(args, form, device):
+    """Run the vortex to t=1 with the plain and the chosen form; L1 density error."""
+    from wasl_b200 import cases
+    out = {}
+    for name in sorted({"plain", form}):
+        g, vortex = build_solver(args, name, device)
+        steps, t = g.run(CFL, 0.0, 1.0)
+        out[name] = (cases.l1_density_error(g, lambda x, y: vortex.conserved(x, y, t)), steps)
+        g.close()
+    res = {"t_end": 1.0, "l1_plain_fp64": out["plain"][0], "steps": out["plain"][1]}
+    if form != "plain":
+        res[f"l1_{form}"] = out[form][0]
+        res["ratio"] = out[form][0] / out["plain"][0]
+    return res
+
+
+def cpu_baseline(args):
+    """The reference CPU solver (oracle/_ref, else the oracle port) on one core:
+    two SSP-RK3 steps of the same workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from wasl_b200 import cases
+    arrays = cases.vortex_mesh(args.n)
+    vortex = cases.IsentropicVortex()
+    oracle = pyoracle.Oracle()
+    om = oracle.tri_mesh(*arrays)
+    rule = max(args.p, 5)
+    xs, ys = om.rule_points(rule)
+    c = om.project(args.p, rule, vortex.conserved(xs, ys))
+    steps = 2
+    if pyoracle.Reference.available():
+        ref = pyoracle.Reference()
+        mesh = ref.tri_mesh(*arrays)
+        donors, basis = mesh.periodic_trace(args.p)
+        dt = mesh.cfl(1.4, c, args.p, CFL)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            mesh.euler_step(1.4, args.p, dt, c, donors, basis)
+        elapsed = time.perf_counter() - t0
+        kind = "reference"
+    else:
+        donors, basis = om.periodic_trace(args.p)
+        dt = om.cfl(1.4, c, args.p, CFL)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            om.euler_step(1.4, args.p, dt, c, donors=donors, basis=basis)
+        elapsed = time.perf_counter() - t0
+        kind = "port"
+    dofs = c.size
+    return {"value": 3.0 * dofs * steps / elapsed, "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": f"{steps} SSP-RK3 steps of the full workload ({om.ne} triangles, P{args.p}),"
+                      f" single-threaded, {elapsed:.1f} s"}
+
+
+def ours(args, rank, world, local_rank):
+    import torch
+    import wasl_b200
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    form = args.form
+    if form == "chosen":
+        form = "mixed" if wasl_b200.form_available("mixed") else "plain"
+    g, _ = build_solver(args, form, local_rank)
+    stream = torch.cuda.ExternalStream(g.stream_handle())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    sampler = ClockSampler(local_rank)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    total_ms, stage_ms, stage_kernels, launches = time_device_steps(g, args, torch, flush, stream)
+    clocks = sampler.stop()
+    if dist:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    dofs = g.state_size
+    value = world * 3.0 * dofs * args.steps / (total_ms * 1e-3)
+    e2e_value, e2e_steps, h2d, d2h = time_e2e(g, args, torch, stream)
+    if dist:
+        t = torch.tensor([e2e_value], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MIN)
+        e2e_value = float(t.item()) * world
+    peaks, peak_kind = measured_peaks()
+    per_launch_bytes = BYTES_PER_DOF * dofs + BYTES_PER_ELEMENT * g.elements
+    kernel_s = stage_ms * 1e-3 / max(stage_kernels, 1)
+    achieved = per_launch_bytes / kernel_s / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "stage_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get(f"{form}_p{args.p}_n{args.n}")
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if form == "plain" else "f32+f64",
+        "data": "synthetic (seeded jittered mesh, projected isentropic vortex)",
+        "config": {"workload": f"isentropic vortex, {args.n}x{args.n} quads -> {g.elements}"
+                               f" jittered triangles, P{args.p} Euler, periodic, CFL {CFL},"
+                               " limiter off",
+                   "form": "plain-fp64" if form == "plain" else "mixed-precision",
+                   "elements": g.elements, "dof": dofs, "parallelism": f"replicas x{world}",
+                   "l2": "flushed between timed steps (256 MiB write)"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "steps": e2e_steps,
+                "path": "C-ABI set_state/stable_dt/step/get_state with pinned host buffers"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                     "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                     "peak_source": f"{peak_kind} hbm_gbs",
+                     "kernel": "euler_tri_stage", "kernel_ms": kernel_s * 1e3,
+                     "bytes_per_launch": per_launch_bytes},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_accuracy:
+        line["accuracy"] = accuracy(args, form, local_rank)
+    if rank == 0 and form != "plain":
+        gp, _ = build_solver(args, "plain", local_rank)
+        p_ms, _, _, _ = time_device_steps(gp, args, torch, flush, stream_of(gp, torch))
+        line["plain_fp64"] = {"value": 3.0 * gp.state_size * args.steps / (p_ms * 1e-3),
+                              "ms_per_step": p_ms / args.steps}
+        line["chosen_vs_plain"] = value / world / line["plain_fp64"]["value"]
+        gp.close()
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(args)
+    g.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def stream_of(g, torch):
+    return torch.cuda.ExternalStream(g.stream_handle())
+
+
+# ---------------------------------------------------------------------------------
+# reference arm: the reference CPU solver on the host cores
+# ---------------------------------------------------------------------------------
+
+REF_SAMPLE_N = 64  # quads per side of the per-process sample mesh
+
+
+def _ref_worker(n, p, steps, warmup, queue, barrier):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from wasl_b200 import cases
+    arrays = cases.vortex_mesh(n)
+    vortex = cases.IsentropicVortex()
+    oracle = pyoracle.Oracle()
+    om = oracle.tri_mesh(*arrays)
+    rule = max(p, 5)
+    xs, ys = om.rule_points(rule)
+    c = om.project(p, rule, vortex.conserved(xs, ys))
+    if pyoracle.Reference.available():
+        mesh = pyoracle.Reference().tri_mesh(*arrays)
+        donors, basis = mesh.periodic_trace(p)
+        advance = lambda dt: mesh.euler_step(1.4, p, dt, c, donors, basis)  # noqa: E731
+        cfl = lambda: mesh.cfl(1.4, c, p, CFL)  # noqa: E731
+        kind = "reference"
+    else:
+        donors, basis = om.periodic_trace(p)
+        advance = lambda dt: om.euler_step(1.4, p, dt, c, donors=donors, basis=basis)  # noqa
+        cfl = lambda: om.cfl(1.4, c, p, CFL)  # noqa: E731
+        kind = "port"
+    for _ in range(warmup):
+        advance(cfl())
+    barrier.wait()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        advance(cfl())
+    queue.put((time.perf_counter() - t0, c.size, kind))
+
+
+def reference(args, rank):
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    queue, barrier = ctx.Queue(), ctx.Barrier(cores)
+    procs = [ctx.Process(target=_ref_worker,
+                         args=(REF_SAMPLE_N, args.p, args.steps, args.warmup, queue, barrier))
+             for _ in range(cores)]
+    for pr in procs:
+        pr.start()
+    results = [queue.get() for _ in procs]
+    for pr in procs:
+        pr.join()
+    elapsed = max(r[0] for r in results)
+    dofs = results[0][1]
+    kind = results[0][2]
+    value = cores * 3.0 * dofs * args.steps / elapsed
+    sample = (f"{cores} independent processes (one per host core), each {args.steps} SSP-RK3"
+              f" steps of the same vortex workload on a {REF_SAMPLE_N}x{REF_SAMPLE_N}-quad"
+              f" sample mesh ({2 * REF_SAMPLE_N ** 2} triangles, P{args.p});"
+              " the reference solver is single-threaded")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": elapsed * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded jittered mesh, projected isentropic vortex)",
+        "config": {"workload": f"isentropic vortex, {args.n}x{args.n} quads ->"
+                               f" {2 * args.n * args.n} jittered triangles, P{args.p} Euler,"
+                               f" periodic, CFL {CFL}, limiter off",
+                   "form": "reference CPU (oracle/_ref)" if kind == "reference" else "oracle port",
+                   "parallelism": f"{cores} host processes"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference(args, rank)
+    else:
+        ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -71,6 +71,10 @@ typedef struct {
 /* Fill the reference's defaults (crates/wasl-bridge/src/config.rs:87-104). */
 void wasl_gpu_config_default(wasl_gpu_config *config);
 
+/* 1 when the library implements `precision` (enum wasl_precision) for this
+ * dimension, equation and polynomial order, else 0. */
+int wasl_gpu_form_supported(int precision, int dimensions, int equation, int polynomial_order);
+
 /* Build the solver on a mesh given as node tags, coordinates ([node][dimensions])
  * and element connectivity ([element][dimensions+1] node tags).  The mesh is
  * normalized exactly as the reference normalizes it, so element order is the
@@ -93,6 +97,23 @@ int wasl_gpu_element_vertices(const wasl_gpu *handle, double *vertices, int64_t 
 /* Modal state in the checkpoint layout U[variable][mode][element], FP64. */
 int wasl_gpu_set_state(wasl_gpu *handle, const double *coefficients, int64_t count);
 int wasl_gpu_get_state(wasl_gpu *handle, double *coefficients, int64_t count);
+
+/* Quadrature of rule order r (the collapsed (r+1)^2-point triangle rule, or
+ * the (r+1)-point Gauss rule on lines): physical points and physical weights
+ * (reference weight x |det J|), packed [element][point]; y may be NULL in 1D.
+ * wasl_gpu_rule_points gives the points per element. */
+int wasl_gpu_rule_points(const wasl_gpu *handle, int rule_order, int *points);
+int wasl_gpu_quadrature(const wasl_gpu *handle, int rule_order, double *x, double *y,
+                        double *weights);
+
+/* Initial state by L2 projection of point values [element][point][variable]
+ * at the rule's points (cpp/include/wasl/dg/l2_projection.hpp:36-76;
+ * cpp/src/case/initial_state.cpp:16-64 uses rule order max(p, 5) on triangles
+ * and 7 Gauss points on lines). */
+int wasl_gpu_project(wasl_gpu *handle, int rule_order, const double *values, int64_t count);
+
+/* The state evaluated at the rule's points, [element][point][variable]. */
+int wasl_gpu_evaluate(wasl_gpu *handle, int rule_order, double *values, int64_t count);
 
 /* CFL time step of the current state, bit-identical to the reference's
  * (the device finds the fastest cell, the host evaluates its speed). */
@@ -126,6 +147,14 @@ int wasl_gpu_advance(wasl_gpu *handle, double cfl, int64_t steps);
  * CUDA stream (cudaStream_t), for callers that keep data on the device. */
 int wasl_gpu_state_device(wasl_gpu *handle, double **device_pointer);
 int wasl_gpu_stream(wasl_gpu *handle, void **stream);
+
+/* Measurement hooks: profile_begin zeroes the launch counter and brackets
+ * every following stage kernel with CUDA events on the handle's stream;
+ * profile_end synchronizes and returns the summed stage-kernel time (ms), the
+ * number of stage kernels timed, and all kernels launched since begin. */
+int wasl_gpu_profile_begin(wasl_gpu *handle);
+int wasl_gpu_profile_end(wasl_gpu *handle, double *stage_kernel_ms, int64_t *stage_kernels,
+                         int64_t *kernel_launches);
 
 /* Restart files with the fields of the reference Checkpoint
  * (cpp/include/wasl/io/checkpoint.hpp:17-29) in a portable binary container

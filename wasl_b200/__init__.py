@@ -63,6 +63,7 @@ SIGNATURES = {
     "wasl_gpu_config_default": (None, [C.POINTER(Config)]),
     "wasl_gpu_create": (C.c_int, [C.POINTER(Config), C.c_int64, _i64, _d, C.c_int64, _i64,
                                   C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
+    "wasl_gpu_form_supported": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int]),
     "wasl_gpu_destroy": (None, [C.c_void_p]),
     "wasl_gpu_last_error": (C.c_char_p, [C.c_void_p]),
     "wasl_gpu_sizes": (C.c_int, [C.c_void_p, _i64, _i64, C.POINTER(C.c_int),
@@ -70,6 +71,10 @@ SIGNATURES = {
     "wasl_gpu_element_vertices": (C.c_int, [C.c_void_p, _d, C.c_int64]),
     "wasl_gpu_set_state": (C.c_int, [C.c_void_p, _d, C.c_int64]),
     "wasl_gpu_get_state": (C.c_int, [C.c_void_p, _d, C.c_int64]),
+    "wasl_gpu_rule_points": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
+    "wasl_gpu_quadrature": (C.c_int, [C.c_void_p, C.c_int, _d, _d, _d]),
+    "wasl_gpu_project": (C.c_int, [C.c_void_p, C.c_int, _d, C.c_int64]),
+    "wasl_gpu_evaluate": (C.c_int, [C.c_void_p, C.c_int, _d, C.c_int64]),
     "wasl_gpu_stable_dt": (C.c_int, [C.c_void_p, C.c_double, _d]),
     "wasl_gpu_step": (C.c_int, [C.c_void_p, C.c_double]),
     "wasl_gpu_limit": (C.c_int, [C.c_void_p]),
@@ -80,6 +85,8 @@ SIGNATURES = {
     "wasl_gpu_advance": (C.c_int, [C.c_void_p, C.c_double, C.c_int64]),
     "wasl_gpu_state_device": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "wasl_gpu_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "wasl_gpu_profile_begin": (C.c_int, [C.c_void_p]),
+    "wasl_gpu_profile_end": (C.c_int, [C.c_void_p, _d, _i64, _i64]),
     "wasl_gpu_write_checkpoint": (C.c_int, [C.c_void_p, C.c_char_p, C.c_double, C.c_uint64,
                                             C.c_char_p]),
     "wasl_gpu_read_checkpoint": (C.c_int, [C.c_void_p, C.c_char_p, _d,
@@ -101,6 +108,14 @@ def library(path: str = LIB_PATH):
         fn.argtypes = args
     _lib = lib
     return lib
+
+
+def form_available(precision: str, dimensions: int = 2, equation: str = "euler",
+                   polynomial_order: int = 2) -> bool:
+    """Whether the library implements a precision form for this case."""
+    return bool(library().wasl_gpu_form_supported(
+        PRECISIONS[precision], dimensions, EULER if equation == "euler" else SCALAR_ADVECTION,
+        polynomial_order))
 
 
 def _ptr(a, t=_d):
@@ -186,11 +201,42 @@ class Solver:
         self._check(self._lib.wasl_gpu_get_state(self._h, _ptr(c), c.size))
         return c
 
+    def get_state_into(self, out: np.ndarray):
+        """Copy the state into a caller-owned contiguous float64 array (e.g. pinned)."""
+        assert out.dtype == np.float64 and out.flags.c_contiguous and out.size == self.state_size
+        self._check(self._lib.wasl_gpu_get_state(self._h, _ptr(out), out.size))
+
     def vertices(self) -> np.ndarray:
         per = 6 if self.config.dimensions == 2 else 2
         v = np.empty(self.elements * per)
         self._check(self._lib.wasl_gpu_element_vertices(self._h, _ptr(v), v.size))
         return v.reshape(self.elements, per)
+
+    # ---- quadrature, projection, evaluation ------------------------------------
+    def rule_points(self, rule_order: int) -> int:
+        n = C.c_int()
+        self._check(self._lib.wasl_gpu_rule_points(self._h, rule_order, C.byref(n)))
+        return n.value
+
+    def quadrature(self, rule_order: int):
+        """Physical points and weights [element][point]: (x, y, w) (y None in 1D)."""
+        Q = self.rule_points(rule_order)
+        x, w = np.empty((self.elements, Q)), np.empty((self.elements, Q))
+        y = np.empty((self.elements, Q)) if self.config.dimensions == 2 else None
+        self._check(self._lib.wasl_gpu_quadrature(self._h, rule_order, _ptr(x),
+                                                  _ptr(y) if y is not None else None, _ptr(w)))
+        return x, y, w
+
+    def project(self, rule_order: int, values):
+        """Set the state to the L2 projection of values [element][point][variable]."""
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        self._check(self._lib.wasl_gpu_project(self._h, rule_order, _ptr(v), v.size))
+
+    def evaluate(self, rule_order: int) -> np.ndarray:
+        Q = self.rule_points(rule_order)
+        v = np.empty((self.elements, Q, self.variables))
+        self._check(self._lib.wasl_gpu_evaluate(self._h, rule_order, _ptr(v), v.size))
+        return v
 
     # ---- stepping -----------------------------------------------------------
     def stable_dt(self, cfl: float) -> float:
@@ -234,6 +280,16 @@ class Solver:
         s = C.c_void_p()
         self._check(self._lib.wasl_gpu_stream(self._h, C.byref(s)))
         return s.value or 0
+
+    # ---- measurement ------------------------------------------------------------
+    def profile_begin(self):
+        self._check(self._lib.wasl_gpu_profile_begin(self._h))
+
+    def profile_end(self):
+        """(summed stage-kernel ms, stage kernels timed, kernels launched)."""
+        ms, k, n = C.c_double(), C.c_int64(), C.c_int64()
+        self._check(self._lib.wasl_gpu_profile_end(self._h, C.byref(ms), C.byref(k), C.byref(n)))
+        return ms.value, k.value, n.value
 
     # ---- restart files ----------------------------------------------------------
     def write_checkpoint(self, path, time, step, prepared_mesh=""):

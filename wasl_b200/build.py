@@ -33,6 +33,7 @@ SOURCES = {
     "mesh.cpp": [],
     "tables.cpp": [],
     "capi.cpp": [],
+    "profiling.cpp": [],
 }
 HEADERS = [f for f in os.listdir(CSRC) if f.endswith((".hpp", ".cuh", ".h"))]
 

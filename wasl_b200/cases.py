@@ -1,0 +1,156 @@
+"""Seeded synthetic workloads (initial data and exact solutions).
+
+Each workload builds the mesh with ``meshgen``, projects its initial data with
+the solver's own L2 projection (the rule the reference's initial state uses:
+order max(p, 5) on triangles, 7 Gauss points on lines), and knows its exact
+solution where one exists.  No public dataset is involved.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import meshgen
+
+GAMMA = 1.4
+
+
+def conserved(rho, u, v, p, gamma=GAMMA):
+    """cpp/include/wasl/equations/euler/primitive.hpp:10-17, elementwise."""
+    rho, u, v, p = (np.asarray(a, dtype=np.float64) for a in (rho, u, v, p))
+    kinetic = 0.5 * rho * (u * u + v * v)
+    return np.stack(np.broadcast_arrays(rho, rho * u, rho * v, p / (gamma - 1.0) + kinetic),
+                    axis=-1)
+
+
+# ---- isentropic vortex on a periodic square -------------------------------------
+
+class IsentropicVortex:
+    """Shu's isentropic vortex of strength eps advected with (u0, v0) over the
+    periodic square [0, L]^2; the exact solution is the translated initial
+    field."""
+
+    def __init__(self, strength=5.0, center=(5.0, 5.0), velocity=(1.0, 1.0), length=10.0,
+                 gamma=GAMMA):
+        self.eps, self.center, self.velocity = strength, center, velocity
+        self.length, self.gamma = length, gamma
+
+    def primitive(self, x, y, t=0.0):
+        L = self.length
+        xc = self.center[0] + self.velocity[0] * t
+        yc = self.center[1] + self.velocity[1] * t
+        dx = np.mod(x - xc + 0.5 * L, L) - 0.5 * L
+        dy = np.mod(y - yc + 0.5 * L, L) - 0.5 * L
+        r2 = dx * dx + dy * dy
+        g = self.gamma
+        bump = np.exp(0.5 * (1.0 - r2))
+        du = -self.eps / (2.0 * math.pi) * bump * dy
+        dv = self.eps / (2.0 * math.pi) * bump * dx
+        temperature = 1.0 - (g - 1.0) * self.eps ** 2 / (8.0 * g * math.pi ** 2) * bump * bump
+        rho = temperature ** (1.0 / (g - 1.0))
+        return rho, self.velocity[0] + du, self.velocity[1] + dv, rho * temperature
+
+    def conserved(self, x, y, t=0.0):
+        return conserved(*self.primitive(x, y, t), gamma=self.gamma)
+
+
+def vortex_mesh(n=256, seed=2025):
+    """n x n quads on [0,10]^2, random diagonals, interior jitter +-0.15h."""
+    return meshgen.jittered_box(n, 0.0, 10.0, 0.0, 10.0, jitter=0.15, seed=seed)
+
+
+def project_initial(solver, field, rule_order=None):
+    """Project field(x, y) -> [..., 4] conserved values onto the solver's modes."""
+    p = solver.config.polynomial_order
+    rule = max(p, 5) if rule_order is None else rule_order
+    x, y, _ = solver.quadrature(rule)
+    solver.project(rule, field(x, y))
+
+
+def l1_density_error(solver, exact, rule_order=5):
+    """Integral of |rho_h - rho_exact| with the order-5 triangle rule
+    (the measure of cpp/tests/dg/euler_triangle_residual_test.cpp:161-183)."""
+    x, y, w = solver.quadrature(rule_order)
+    rho_h = solver.evaluate(rule_order)[..., 0]
+    return float(np.sum(w * np.abs(rho_h - exact(x, y)[..., 0])))
+
+
+# ---- Riemann problems ----------------------------------------------------------------
+
+def random_state(rng):
+    """rho in [0.1,1.5], p in [0.02,1.5], |u|,|v| <= 1.2."""
+    return (rng.uniform(0.1, 1.5), rng.uniform(-1.2, 1.2), rng.uniform(-1.2, 1.2),
+            rng.uniform(0.02, 1.5))
+
+
+class QuadrantRiemann:
+    """Seeded four-quadrant Riemann problem on [0,1]^2."""
+
+    def __init__(self, seed=3, gamma=GAMMA):
+        rng = np.random.Generator(np.random.PCG64(seed))
+        self.states = np.array([conserved(*random_state(rng), gamma=gamma) for _ in range(4)])
+
+    def conserved(self, x, y, t=0.0):
+        q = (x >= 0.5).astype(int) + 2 * (y >= 0.5).astype(int)
+        return self.states[q]
+
+
+class PlanarRiemann:
+    """Two seeded states split by a line through (cx, cy) at a random angle."""
+
+    def __init__(self, seed=0, gamma=GAMMA):
+        rng = np.random.Generator(np.random.PCG64(seed))
+        self.left = conserved(*random_state(rng), gamma=gamma)
+        self.right = conserved(*random_state(rng), gamma=gamma)
+        self.angle = rng.uniform(0.0, 2.0 * math.pi)
+        self.cx, self.cy = rng.uniform(0.3, 0.7, size=2)
+
+    def conserved(self, x, y, t=0.0):
+        side = (x - self.cx) * math.cos(self.angle) + (y - self.cy) * math.sin(self.angle) >= 0.0
+        return np.where(side[..., None], self.right, self.left)
+
+
+class ShockVortex:
+    """Stationary Mach 1.1 normal shock at x=0.5 on [0,2]x[0,1]: supersonic
+    upstream flow (rho=1, p=1) on the left, the Rankine-Hugoniot state on the
+    right, and an isentropic vortex of seeded strength in [0.2, 0.4] (radius
+    0.05) centred at (0.25, 0.5) in the upstream flow."""
+
+    def __init__(self, seed=0, mach=1.1, gamma=GAMMA):
+        rng = np.random.Generator(np.random.PCG64(seed))
+        self.strength = rng.uniform(0.2, 0.4)
+        g = gamma
+        self.gamma = g
+        # upstream (left of the shock, moving right at Mach 1.1)
+        rho_u, p_u = 1.0, 1.0
+        c_u = math.sqrt(g * p_u / rho_u)
+        u_u = mach * c_u
+        # stationary normal shock relations
+        m2 = mach * mach
+        rho_d = rho_u * (g + 1.0) * m2 / ((g - 1.0) * m2 + 2.0)
+        p_d = p_u * (2.0 * g * m2 - (g - 1.0)) / (g + 1.0)
+        u_d = u_u * rho_u / rho_d
+        self.upstream = (rho_u, u_u, 0.0, p_u)
+        self.downstream = (rho_d, u_d, 0.0, p_d)
+
+    def primitive(self, x, y):
+        rho_u, u_u, _, p_u = self.upstream
+        g = self.gamma
+        dx, dy = x - 0.25, y - 0.5
+        r2 = (dx * dx + dy * dy) / 0.05 ** 2
+        bump = np.exp(0.5 * (1.0 - r2))
+        eps = self.strength
+        c = math.sqrt(g * p_u / rho_u)
+        du = -eps * c * bump * dy / 0.05
+        dv = eps * c * bump * dx / 0.05
+        t_ratio = 1.0 - (g - 1.0) * eps ** 2 / (2.0 * g) * bump * bump
+        rho = rho_u * t_ratio ** (1.0 / (g - 1.0))
+        p = p_u * t_ratio ** (g / (g - 1.0))
+        left = x < 0.5
+        rho_d, u_d, _, p_d = self.downstream
+        return (np.where(left, rho, rho_d), np.where(left, u_u + du, u_d),
+                np.where(left, dv, 0.0), np.where(left, p, p_d))
+
+    def conserved(self, x, y, t=0.0):
+        return conserved(*self.primitive(x, y), gamma=self.gamma)

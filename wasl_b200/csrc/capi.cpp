@@ -12,9 +12,18 @@
 namespace wasl_b200 {
 std::unique_ptr<Solver> make_euler_tri_solver(const wasl_gpu_config &cfg, TriTopology &&topo);
 
+bool form_supported(int precision, int dimensions, int equation, int p) {
+  if (dimensions == 2 && equation == WASL_EULER)
+    return precision == WASL_PLAIN_FP64 && p >= 0 && p <= 3;
+  return false;
+}
+
 std::unique_ptr<Solver> make_solver(const wasl_gpu_config &cfg, std::int64_t node_count,
                                     const std::int64_t *node_tags, const double *coordinates,
                                     std::int64_t element_count, const std::int64_t *element_nodes) {
+  if (!form_supported(cfg.precision, cfg.dimensions, cfg.equation, cfg.polynomial_order))
+    throw SolverError(WASL_ERR_ARGUMENT,
+                      "unsupported combination of dimension, equation, order and precision");
   if (cfg.dimensions == 2 && cfg.equation == WASL_EULER)
     return make_euler_tri_solver(cfg, build_triangle_topology(node_count, node_tags, coordinates,
                                                               element_count, element_nodes));
@@ -83,6 +92,10 @@ void wasl_gpu_config_default(wasl_gpu_config *c) {
   c->density_floor = 1e-10;
   c->pressure_floor = 1e-10;
   c->precision = WASL_PLAIN_FP64;
+}
+
+int wasl_gpu_form_supported(int precision, int dimensions, int equation, int p) {
+  return wasl_b200::form_supported(precision, dimensions, equation, p) ? 1 : 0;
 }
 
 int wasl_gpu_create(const wasl_gpu_config *config, int64_t node_count, const int64_t *node_tags,
@@ -154,6 +167,40 @@ int wasl_gpu_get_state(wasl_gpu *h, double *c, int64_t count) {
   return guarded(h, [&] {
     need(c && count == state_count(h), "state: coefficient count does not match the layout");
     h->solver->get_state(c);
+  });
+}
+
+int wasl_gpu_rule_points(const wasl_gpu *h, int rule_order, int *points) {
+  return guarded(const_cast<wasl_gpu *>(h), [&] {
+    need(points && rule_order >= 0 && rule_order <= 6, "quadrature: rule order must be 0..6");
+    *points = h->solver->rule_points(rule_order);
+  });
+}
+
+int wasl_gpu_quadrature(const wasl_gpu *h, int rule_order, double *x, double *y, double *w) {
+  return guarded(const_cast<wasl_gpu *>(h), [&] {
+    need(x && rule_order >= 0 && rule_order <= 6, "quadrature: rule order must be 0..6");
+    h->solver->quadrature(rule_order, x, y, w);
+  });
+}
+
+int wasl_gpu_project(wasl_gpu *h, int rule_order, const double *values, int64_t count) {
+  return guarded(h, [&] {
+    need(values && rule_order >= 0 && rule_order <= 6, "projection: rule order must be 0..6");
+    need(count == h->solver->elements() * h->solver->rule_points(rule_order) *
+                      h->solver->variables(),
+         "projection: value count must be elements x points x variables");
+    h->solver->project(rule_order, values);
+  });
+}
+
+int wasl_gpu_evaluate(wasl_gpu *h, int rule_order, double *values, int64_t count) {
+  return guarded(h, [&] {
+    need(values && rule_order >= 0 && rule_order <= 6, "evaluation: rule order must be 0..6");
+    need(count == h->solver->elements() * h->solver->rule_points(rule_order) *
+                      h->solver->variables(),
+         "evaluation: value count must be elements x points x variables");
+    h->solver->evaluate(rule_order, values);
   });
 }
 
@@ -233,6 +280,25 @@ int wasl_gpu_stream(wasl_gpu *h, void **s) {
   return guarded(h, [&] {
     need(s != nullptr, "null pointer");
     *s = reinterpret_cast<void *>(h->solver->stream());
+  });
+}
+
+int wasl_gpu_profile_begin(wasl_gpu *h) {
+  return guarded(h, [&] { h->solver->profile_begin(); });
+}
+
+int wasl_gpu_profile_end(wasl_gpu *h, double *stage_ms, int64_t *stage_kernels,
+                         int64_t *launches) {
+  return guarded(h, [&] {
+    double ms = 0.0;
+    std::int64_t k = 0, n = 0;
+    h->solver->profile_end(ms, k, n);
+    if (stage_ms)
+      *stage_ms = ms;
+    if (stage_kernels)
+      *stage_kernels = k;
+    if (launches)
+      *launches = n;
   });
 }
 

@@ -191,6 +191,57 @@ public:
     }
   }
 
+  int rule_points(int rule_order) const override { return (rule_order + 1) * (rule_order + 1); }
+
+  void quadrature(int rule_order, double *x, double *y, double *w) const override {
+    const Rule2D rule = triangle_rule(rule_order);
+    const int Q = rule.size();
+    for (std::int64_t e = 0; e < ne_; ++e) {
+      const TriMap &m = mesh_.maps[e];
+      const double jac = std::fabs(m.jacobian_determinant());
+      for (int q = 0; q < Q; ++q) {
+        m.to_physical(rule.xi[q], rule.eta[q], x[e * Q + q], y[e * Q + q]);
+        if (w)
+          w[e * Q + q] = rule.w[q] * jac;
+      }
+    }
+  }
+
+  void project(int rule_order, const double *values) override {
+    const Rule2D rule = triangle_rule(rule_order);
+    const int Q = rule.size();
+    std::vector<std::vector<double>> basis(Q);
+    for (int q = 0; q < Q; ++q)
+      basis[q] = dubiner(rule.xi[q], rule.eta[q], p_);
+    std::vector<double> c(static_cast<std::size_t>(4) * M_ * ne_, 0.0);
+    for (std::int64_t e = 0; e < ne_; ++e)
+      for (int q = 0; q < Q; ++q) {
+        const double *val = values + (e * Q + q) * 4;
+        for (int v = 0; v < 4; ++v)
+          for (int m = 0; m < M_; ++m)
+            c[(static_cast<std::int64_t>(v) * M_ + m) * ne_ + e] += rule.w[q] * val[v] * basis[q][m];
+      }
+    set_state(c.data());
+  }
+
+  void evaluate(int rule_order, double *values) override {
+    const Rule2D rule = triangle_rule(rule_order);
+    const int Q = rule.size();
+    std::vector<double> c(static_cast<std::size_t>(4) * M_ * ne_);
+    get_state(c.data());
+    std::vector<std::vector<double>> basis(Q);
+    for (int q = 0; q < Q; ++q)
+      basis[q] = dubiner(rule.xi[q], rule.eta[q], p_);
+    for (std::int64_t e = 0; e < ne_; ++e)
+      for (int q = 0; q < Q; ++q)
+        for (int v = 0; v < 4; ++v) {
+          double s = 0.0;
+          for (int m = 0; m < M_; ++m)
+            s += c[(static_cast<std::int64_t>(v) * M_ + m) * ne_ + e] * basis[q][m];
+          values[(e * Q + q) * 4 + v] = s;
+        }
+  }
+
   void set_state(const double *host) override {
     cuda_check(cudaMemcpyAsync(d_u_.get(), host, d_u_.size() * sizeof(double),
                                cudaMemcpyHostToDevice, stream_),
@@ -223,6 +274,7 @@ public:
 
   double stable_dt(double cfl) override {
     launch_cfl(cfl_args(cfl), stream_);
+    count_launches(3);
     cuda_check(cudaMemcpyAsync(scratch_.words, d_cfl_.get(), 8 * sizeof(unsigned long long),
                                cudaMemcpyDeviceToHost, stream_),
                "cfl result");
@@ -262,12 +314,14 @@ public:
     sa.troubled_count = d_count_.get();
     launch_sense_f64(M_, sa, stream_);
     launch_limit_f64(M_, 3, limit_args(d_u_.get()), stream_);
+    count_launches(3);
     check_error();
   }
 
   void advance(double cfl, std::int64_t steps) override {
     for (std::int64_t n = 0; n < steps; ++n) {
       launch_cfl(cfl_args(cfl), stream_);
+      count_launches(3);
       enqueue_step();
     }
     check_error();
@@ -325,9 +379,14 @@ private:
       a.flags = d_flags_.get() + k * ne_;
       if (limiting_)
         cuda_check(cudaMemsetAsync(d_count_.get(), 0, sizeof(std::int32_t), stream_), "count");
+      stage_begin();
       launch_euler_tri_stage_f64(p_, a, stream_);
-      if (limiting_)
+      stage_end();
+      count_launches(1);
+      if (limiting_) {
         launch_limit_f64(M_, 3, limit_args(outs[k]), stream_);
+        count_launches(2);
+      }
     }
     cuda_check(cudaGetLastError(), "stage launch");
   }

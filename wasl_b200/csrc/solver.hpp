@@ -58,7 +58,7 @@ private:
 
 class Solver {
 public:
-  virtual ~Solver() = default;
+  virtual ~Solver();
   virtual std::int64_t elements() const = 0;
   virtual std::int64_t faces() const = 0;
   virtual int modes() const = 0;
@@ -73,10 +73,35 @@ public:
   virtual void flags(std::uint8_t *out) = 0;
   virtual void mass_energy(double &mass, double &energy) = 0;
   virtual double *state_device() = 0;
+  // Quadrature of rule order r on every element: physical points and weights
+  // (reference weight x |det J|), packed [element][point].
+  virtual int rule_points(int rule_order) const = 0;
+  virtual void quadrature(int rule_order, double *x, double *y, double *w) const = 0;
+  // L2 projection of point values [element][point][variable] onto the modes,
+  // stored as the state (cpp/include/wasl/dg/l2_projection.hpp:36-76).
+  virtual void project(int rule_order, const double *values) = 0;
+  // The state evaluated at the rule's points, [element][point][variable].
+  virtual void evaluate(int rule_order, double *values) = 0;
   cudaStream_t stream() const { return stream_; }
 
+  // Kernel accounting for measurement: every launch is counted; while
+  // profiling, each stage kernel is bracketed by CUDA events on the stream it
+  // is launched on.
+  void profile_begin();
+  void profile_end(double &stage_ms, std::int64_t &stage_kernels, std::int64_t &launches);
+
 protected:
+  void count_launches(std::int64_t n) { launches_ += n; }
+  void stage_begin();
+  void stage_end();
+
   cudaStream_t stream_ = nullptr;
+
+private:
+  bool profiling_ = false;
+  std::int64_t launches_ = 0;
+  std::vector<cudaEvent_t> events_;
+  std::size_t events_used_ = 0;
 };
 
 std::unique_ptr<Solver> make_solver(const wasl_gpu_config &config, std::int64_t node_count,
