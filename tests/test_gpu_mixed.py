@@ -1,0 +1,92 @@
+"""The mixed-precision form: same discretization as the plain FP64 path, FP32
+only on high-mode perturbations.  Checked against the plain path (tolerances
+stated per test), for free-stream preservation, and for conservation."""
+import numpy as np
+import pytest
+
+import wasl_b200
+from golden.make_golden import seeded_state
+from wasl_b200 import cases, meshgen
+
+pytestmark = pytest.mark.gpu
+
+
+def pair(arrays, p, **kw):
+    return (wasl_b200.Solver(*arrays, polynomial_order=p, precision="plain", **kw),
+            wasl_b200.Solver(*arrays, polynomial_order=p, precision="mixed", **kw))
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_uniform_flow_stays_uniform(p):
+    """A constant state is preserved to FP64 round-off: the FP32 part sees dU = 0."""
+    arrays = meshgen.jittered_box(16, jitter=0.15, seed=p)
+    plain, mixed = pair(arrays, p)
+    with plain, mixed:
+        state = np.zeros((4, mixed.modes, mixed.elements))
+        state[:, 0] = np.sqrt(2) * np.array([1.0, 0.3, -0.2, 2.6])[:, None]
+        mixed.set_state(state.ravel())
+        for _ in range(20):
+            mixed.step(mixed.stable_dt(0.2))
+        out = mixed.get_state().reshape(state.shape)
+    assert np.max(np.abs(out - state)) <= 2e-13
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_one_step_close_to_plain(p):
+    """|mixed - plain| after one step, relative to the step's change: <= 1e-6."""
+    arrays = meshgen.jittered_box(24, jitter=0.15, seed=10 + p)
+    plain, mixed = pair(arrays, p)
+    with plain, mixed:
+        c = seeded_state(plain.elements, p, 31 + p, amplitude=0.02)
+        plain.set_state(c)
+        mixed.set_state(c)
+        dt = plain.stable_dt(0.15)
+        assert dt == mixed.stable_dt(0.15)
+        plain.step(dt)
+        mixed.step(dt)
+        a, b = plain.get_state(), mixed.get_state()
+    change = np.max(np.abs(a - c))
+    assert np.max(np.abs(a - b)) <= 1e-6 * change
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_mass_and_energy_conserved(p):
+    arrays = meshgen.jittered_box(16, jitter=0.15, seed=4)
+    with wasl_b200.Solver(*arrays, polynomial_order=p, precision="mixed") as g:
+        g.set_state(seeded_state(g.elements, p, 9, amplitude=0.02))
+        m0, e0 = g.mass_energy()
+        for _ in range(50):
+            g.step(g.stable_dt(0.15))
+        m1, e1 = g.mass_energy()
+    assert abs(m1 - m0) <= 1e-13 * abs(m0)
+    assert abs(e1 - e0) <= 1e-13 * abs(e0)
+
+
+def test_vortex_accuracy_matches_plain():
+    """Isentropic vortex on a 64x64-quad mesh to t=0.5: the mixed form's L1
+    density error is within 1.5x of the plain FP64 path's."""
+    vortex = cases.IsentropicVortex()
+    arrays = cases.vortex_mesh(64, seed=7)
+    errors = {}
+    for form in ("plain", "mixed"):
+        with wasl_b200.Solver(*arrays, polynomial_order=2, precision=form) as g:
+            cases.project_initial(g, vortex.conserved)
+            steps, t = g.run(0.15, 0.0, 0.5)
+            errors[form] = cases.l1_density_error(g, lambda x, y: vortex.conserved(x, y, t))
+    assert errors["mixed"] <= 1.5 * errors["plain"]
+
+
+def test_limited_mixed_runs_quadrant_riemann():
+    """Limiter and positivity on the mixed form: physical averages throughout."""
+    arrays = meshgen.jittered_box(32, jitter=0.15, seed=3)
+    problem = cases.QuadrantRiemann(seed=3)
+    with wasl_b200.Solver(*arrays, polynomial_order=2, precision="mixed", limiting=True,
+                          boundary="transmissive") as g:
+        cases.project_initial(g, problem.conserved)
+        g.limit()
+        m0, _ = g.mass_energy()
+        g.run(0.1, 0.0, 0.05)
+        flags = g.flags()
+        state = g.get_state().reshape(4, g.modes, g.elements)
+    assert flags.sum() > 0
+    assert np.all(state[0, 0] > 0)

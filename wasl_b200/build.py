@@ -29,6 +29,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", f"-I{INCLUDE}", f"-I{CSRC}",
 # file -> extra flags
 SOURCES = {
     "euler_tri_f64.cu": ["--fmad=false"],
+    "euler_tri_mixed.cu": [],
     "euler_tri_solver.cu": [],
     "mesh.cpp": [],
     "tables.cpp": [],

@@ -14,7 +14,8 @@ std::unique_ptr<Solver> make_euler_tri_solver(const wasl_gpu_config &cfg, TriTop
 
 bool form_supported(int precision, int dimensions, int equation, int p) {
   if (dimensions == 2 && equation == WASL_EULER)
-    return precision == WASL_PLAIN_FP64 && p >= 0 && p <= 3;
+    return (precision == WASL_PLAIN_FP64 && p >= 0 && p <= 3) ||
+           (precision == WASL_MIXED && p >= 1 && p <= 3);
   return false;
 }
 

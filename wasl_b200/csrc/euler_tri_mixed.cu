@@ -1,0 +1,515 @@
+// Mixed-precision 2D Euler SSP-RK3 stage (the fast form).
+//
+// Same discretization as the plain path (order-(p+2) volume rule, HLLC faces,
+// SSP-RK3), arranged so that FP32 only ever carries small quantities:
+//   * each element's state is split into its cell average U_bar = c0 phi0
+//     (FP64) and the high-mode part dU(x) = sum_{m>=1} c_m phi_m(x) (FP32);
+//   * for the high modes the element's own mean flux F(U_bar) drops out: its
+//     volume term F(U_bar) . sum_q w grad(phi_m) equals its face term
+//     F(U_bar) . sum_faces w phi_m n (divergence theorem; both rules are exact
+//     for these degrees), so only perturbations remain:
+//       volume  dF = F(U_bar + dU) - F(U_bar), evaluated in perturbation form
+//               (every term proportional to dU) and projected through the
+//               contravariant fluxes G_xi = w (b_y dF_x - b_x dF_y),
+//               G_eta = w (a_x dF_y - a_y dF_x);
+//       faces   HLLC(U_L, U_R).n - F(U_bar).n, from an HLLC written in
+//               perturbation form around the face's left mean;
+//     all in FP32 with FMA;
+//   * mode 0 (the cell averages) takes the full face value, the left mean's
+//     normal flux in FP64 plus the FP32 perturbation, computed identically by
+//     both sides of a face, so mass, momentum and energy are conserved to FP64
+//     round-off and a uniform state stays exactly uniform;
+//   * the residual scaling and the Shu-Osher combination are FP64.
+// The plain kernels (euler_tri_f64.cu) remain the bit-consistent drop-in.
+#include <stdexcept>
+
+#include "euler_device.cuh"
+#include "kernels.hpp"
+#include "tri_tables.hpp"
+
+namespace wasl_b200 {
+
+// FP32 volume tables for modes 1..M-1 plus FP64 column sums of the reference
+// gradients (sigma_m = sum_q w_q D_m(q)).
+template <int P> struct MixedVolume {
+  static constexpr int M = TriShape<P>::M, QV = TriShape<P>::QV, H = M - 1;
+  float phi[QV][H > 0 ? H : 1];
+  float dxi[QV][H > 0 ? H : 1];
+  float deta[QV][H > 0 ? H : 1];
+  float w[QV];
+  double wsum[3]; // FP64 sum of the reference edge weights of each local edge
+};
+
+__constant__ MixedVolume<1> c_mix1;
+__constant__ MixedVolume<2> c_mix2;
+__constant__ MixedVolume<3> c_mix3;
+
+template <int P> __device__ __forceinline__ const MixedVolume<P> &mixed_table();
+template <> __device__ __forceinline__ const MixedVolume<1> &mixed_table<1>() { return c_mix1; }
+template <> __device__ __forceinline__ const MixedVolume<2> &mixed_table<2>() { return c_mix2; }
+template <> __device__ __forceinline__ const MixedVolume<3> &mixed_table<3>() { return c_mix3; }
+
+// Primitive values of a cell average, FP64, with one reciprocal.
+struct MeanState {
+  double rho, mx, my, e, u, v, p, h; // h = E + p
+};
+
+__device__ __forceinline__ MeanState mean_state(double gamma, const double *s) {
+  MeanState m;
+  m.rho = s[0];
+  m.mx = s[1];
+  m.my = s[2];
+  m.e = s[3];
+  const double inv = 1.0 / s[0];
+  m.u = s[1] * inv;
+  m.v = s[2] * inv;
+  m.p = (gamma - 1.0) * (s[3] - 0.5 * (s[1] * m.u + s[2] * m.v));
+  m.h = s[3] + m.p;
+  return m;
+}
+
+// Physical flux of a cell average along n, FP64.
+__device__ __forceinline__ void mean_normal_flux(const MeanState &m, double nx, double ny,
+                                                 double *f) {
+  const double un = m.u * nx + m.v * ny;
+  f[0] = m.rho * un;
+  f[1] = m.mx * un + m.p * nx;
+  f[2] = m.my * un + m.p * ny;
+  f[3] = m.h * un;
+}
+
+// HLLC in FP64 with shared reciprocals: the flux of hllc() with fewer divisions.
+__device__ __forceinline__ void hllc_fast(double gamma, const double *l, const double *r, double nx,
+                                          double ny, double *f) {
+  const double il = 1.0 / l[0], ir = 1.0 / r[0];
+  const double lu = l[1] * il, lv = l[2] * il, ru = r[1] * ir, rv = r[2] * ir;
+  const double lp = (gamma - 1.0) * (l[3] - 0.5 * (l[1] * lu + l[2] * lv));
+  const double rp = (gamma - 1.0) * (r[3] - 0.5 * (r[1] * ru + r[2] * rv));
+  const double lun = lu * nx + lv * ny, run = ru * nx + rv * ny;
+  const double lc = sqrt(gamma * lp * il), rc = sqrt(gamma * rp * ir);
+  const double sl = fmin(lun - lc, run - rc);
+  const double sr = fmax(lun + lc, run + rc);
+  if (sl >= 0.0) {
+    f[0] = l[0] * lun;
+    f[1] = l[1] * lun + lp * nx;
+    f[2] = l[2] * lun + lp * ny;
+    f[3] = (l[3] + lp) * lun;
+    return;
+  }
+  if (sr <= 0.0) {
+    f[0] = r[0] * run;
+    f[1] = r[1] * run + rp * nx;
+    f[2] = r[2] * run + rp * ny;
+    f[3] = (r[3] + rp) * run;
+    return;
+  }
+  const double dl = l[0] * (sl - lun), dr = r[0] * (sr - run);
+  const double contact = (rp - lp + lun * dl - run * dr) / (dl - dr);
+  const bool left = contact >= 0.0;
+  const double *s = left ? l : r;
+  const double is = left ? il : ir;
+  const double un = left ? lun : run, ps = left ? lp : rp, wave = left ? sl : sr;
+  const double vx = left ? lu : ru, vy = left ? lv : rv;
+  const double d = s[0] * (wave - un);
+  const double rho_star = d / (wave - contact);
+  const double shift = contact - un;
+  const double e_star = s[3] * is + shift * (contact + ps / d);
+  f[0] = s[0] * un + wave * (rho_star - s[0]);
+  f[1] = s[1] * un + ps * nx + wave * (rho_star * (vx + shift * nx) - s[1]);
+  f[2] = s[2] * un + ps * ny + wave * (rho_star * (vy + shift * ny) - s[2]);
+  f[3] = (s[3] + ps) * un + wave * (rho_star * e_star - s[3]);
+}
+
+// A reference state (a cell average) in FP32 for the perturbation formulas.
+struct Ref32 {
+  float rho, u, v, e, h, mx, my, p;
+};
+
+__device__ __forceinline__ Ref32 ref32(const MeanState &m) {
+  return {static_cast<float>(m.rho), static_cast<float>(m.u), static_cast<float>(m.v),
+          static_cast<float>(m.e),   static_cast<float>(m.h), static_cast<float>(m.mx),
+          static_cast<float>(m.my),  static_cast<float>(m.p)};
+}
+
+// The state U_bar + d along n: primitive values and the normal-flux change
+// dFn = F(U_bar + d).n - F(U_bar).n, every term proportional to d.
+struct Side32 {
+  float rho, inv, u, v, p, un, dun, e, c, dfn[4];
+};
+
+__device__ __forceinline__ Side32 perturbed_side(const Ref32 &b, const float *d, float g1,
+                                                 float gamma, float nx, float ny) {
+  Side32 s;
+  s.rho = b.rho + d[0];
+  s.inv = __frcp_rn(s.rho);
+  const float du = (d[1] - b.u * d[0]) * s.inv;
+  const float dv = (d[2] - b.v * d[0]) * s.inv;
+  s.u = b.u + du;
+  s.v = b.v + dv;
+  const float dmu = b.mx * du + d[1] * s.u + b.my * dv + d[2] * s.v;
+  const float dp = g1 * (d[3] - 0.5f * dmu);
+  s.p = b.p + dp;
+  s.e = b.e + d[3];
+  s.dun = du * nx + dv * ny;
+  s.un = s.u * nx + s.v * ny;
+  s.c = sqrtf(fmaxf(gamma * s.p * s.inv, 0.0f));
+  s.dfn[0] = d[1] * nx + d[2] * ny;
+  s.dfn[1] = b.mx * s.dun + d[1] * s.un + dp * nx;
+  s.dfn[2] = b.my * s.dun + d[2] * s.un + dp * ny;
+  s.dfn[3] = b.h * s.dun + (d[3] + dp) * s.un;
+  return s;
+}
+
+// HLLC(U_bar + dl, U_bar + dr).n - F(U_bar).n in perturbation form: the wave
+// speeds and branch are those of the HLLC flux (cpp/include/wasl/flux/hllc.hpp:40-74);
+// the star-state jumps are rewritten so that no O(1) terms cancel:
+//   S* - u_L = (dp - rho_R (S_R - u_R) du_n) / D,
+//   rho* - rho_K = rho_K (S* - u_K) / (S_K - S*).
+__device__ __forceinline__ void hllc_perturbed(const Ref32 &b, const float *dl, const float *dr,
+                                               float g1, float gamma, float nx, float ny,
+                                               float *f) {
+  const Side32 L = perturbed_side(b, dl, g1, gamma, nx, ny);
+  const Side32 R = perturbed_side(b, dr, g1, gamma, nx, ny);
+  const float sl = fminf(L.un - L.c, R.un - R.c);
+  const float sr = fmaxf(L.un + L.c, R.un + R.c);
+  if (sl >= 0.0f) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+      f[v] = L.dfn[v];
+    return;
+  }
+  if (sr <= 0.0f) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+      f[v] = R.dfn[v];
+    return;
+  }
+  const float dpress = (R.p - b.p) - (L.p - b.p);
+  const float dn = R.dun - L.dun;
+  const float den = L.rho * (sl - L.un) - R.rho * (sr - R.un);
+  const float sigma_l = (dpress - R.rho * (sr - R.un) * dn) / den; // S* - u_L
+  const float star = L.un + sigma_l;
+  const bool left = star >= 0.0f;
+  const Side32 &K = left ? L : R;
+  const float wave = left ? sl : sr;
+  const float sigma = left ? sigma_l : sigma_l - dn; // S* - u_K
+  const float drho = K.rho * sigma / (wave - star);
+  const float rho_star = K.rho + drho;
+  const float jump[4] = {
+      drho, drho * K.u + rho_star * sigma * nx, drho * K.v + rho_star * sigma * ny,
+      drho * K.e * K.inv + rho_star * sigma * (star + K.p / (K.rho * (wave - K.un)))};
+#pragma unroll
+  for (int v = 0; v < 4; ++v)
+    f[v] = K.dfn[v] + wave * jump[v];
+}
+
+template <int P>
+__global__ void __launch_bounds__(128) euler_tri_stage_mixed(const StageArgs a) {
+  using S = TriShape<P>;
+  constexpr int M = S::M, QV = S::QV, QF = S::QF, H = M - 1;
+  constexpr double phi0 = 0.70710678118654752440; // 1/sqrt(2), the constant mode
+  const std::int64_t ne = a.mesh.ne;
+  const std::int64_t e = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= ne)
+    return;
+  const double *__restrict__ in = a.in;
+  const MixedVolume<P> &T = mixed_table<P>();
+  const FaceTable<P, float> *__restrict__ F = static_cast<const FaceTable<P, float> *>(a.face_table);
+  const double gamma = a.gamma;
+  const float gamma32 = static_cast<float>(gamma), g1 = static_cast<float>(gamma - 1.0);
+
+  double mean[4];
+  float ch[4][H];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    mean[v] = in[(static_cast<std::int64_t>(v) * M) * ne + e] * phi0;
+#pragma unroll
+    for (int m = 0; m < H; ++m)
+      ch[v][m] = static_cast<float>(in[(static_cast<std::int64_t>(v) * M + m + 1) * ne + e]);
+  }
+  const double *__restrict__ geo = a.mesh.geo;
+  const MeanState mb = mean_state(gamma, mean);
+  const Ref32 bb = ref32(mb);
+
+  // Volume term of the high modes: the element's own mean flux cancels
+  // against its faces (divergence theorem, both rules exact), leaving the
+  // perturbation flux dF.  The 1/2 of the scaled gradient is folded into w.
+  float racc[4][H];
+#pragma unroll
+  for (int v = 0; v < 4; ++v)
+#pragma unroll
+    for (int m = 0; m < H; ++m)
+      racc[v][m] = 0.0f;
+  {
+    const float fax = static_cast<float>(geo[e]), fay = static_cast<float>(geo[ne + e]);
+    const float fbx = static_cast<float>(geo[2 * ne + e]), fby = static_cast<float>(geo[3 * ne + e]);
+#pragma unroll 1
+    for (int q = 0; q < QV; ++q) {
+      float d[4];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        float s = 0.0f;
+#pragma unroll
+        for (int m = 0; m < H; ++m)
+          s = fmaf(ch[v][m], T.phi[q][m], s);
+        d[v] = s;
+      }
+      const float inv = __frcp_rn(bb.rho + d[0]);
+      const float du = (d[1] - bb.u * d[0]) * inv;
+      const float dv = (d[2] - bb.v * d[0]) * inv;
+      const float uu = bb.u + du, vv = bb.v + dv;
+      const float dmu = bb.mx * du + d[1] * uu + bb.my * dv + d[2] * vv;
+      const float dp = g1 * (d[3] - 0.5f * dmu);
+      const float dep = d[3] + dp;
+      const float fx[4] = {d[1], bb.mx * du + d[1] * uu + dp, bb.my * du + d[2] * uu,
+                           bb.h * du + dep * uu};
+      const float fy[4] = {d[2], bb.mx * dv + d[1] * vv, bb.my * dv + d[2] * vv + dp,
+                           bb.h * dv + dep * vv};
+      const float w = T.w[q];
+      const float wby = w * fby, wbx = w * fbx, wax = w * fax, way = w * fay;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const float gxi = wby * fx[v] - wbx * fy[v];
+        const float geta = wax * fy[v] - way * fx[v];
+#pragma unroll
+        for (int m = 0; m < H; ++m)
+          racc[v][m] = fmaf(T.dxi[q][m], gxi, fmaf(T.deta[q][m], geta, racc[v][m]));
+      }
+    }
+  }
+
+  // Faces.  The flux of each face is evaluated around its left element's mean
+  // (both sides compute the same numbers); mode 0 takes the full FP64 face
+  // value so the two sides' contributions cancel exactly.
+  double r0[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 1
+  for (int k = 0; k < 3; ++k) {
+    const std::int32_t nb = a.mesh.slot_nbr[k * ne + e];
+    const unsigned code = a.mesh.slot_code[k * ne + e];
+    const double nx = a.mesh.slot_geo[(3 * k) * ne + e];
+    const double ny = a.mesh.slot_geo[(3 * k + 1) * ne + e];
+    const double scale = a.mesh.slot_geo[(3 * k + 2) * ne + e];
+    const float nxf = static_cast<float>(nx), nyf = static_cast<float>(ny);
+    const bool self_left = code & 1u;
+    const int le = (code >> 1) & 3u, re = (code >> 3) & 3u, flip = (code >> 5) & 1u;
+    const float(*lb)[M] = F->lb[le];
+    const float(*rb)[M] = F->rb[(le * 3 + re) * 2 + flip];
+    const float(*own)[M] = self_left ? lb : rb;
+    const float(*oth)[M] = self_left ? rb : lb;
+    double nmean[4] = {mean[0], mean[1], mean[2], mean[3]};
+    float nh[4][H];
+    if (nb >= 0) {
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        nmean[v] = __ldg(in + (static_cast<std::int64_t>(v) * M) * ne + nb) * phi0;
+#pragma unroll
+        for (int m = 0; m < H; ++m)
+          nh[v][m] = static_cast<float>(__ldg(in + (static_cast<std::int64_t>(v) * M + m + 1) * ne + nb));
+      }
+    }
+    // Left-element reference state and its mean normal flux (FP64).
+    const MeanState ml = self_left ? mb : mean_state(gamma, nmean);
+    const Ref32 ref = self_left ? bb : ref32(ml);
+    double fln[4];
+    mean_normal_flux(ml, nx, ny, fln);
+    // The jump of means, right minus left, and for a right-side element the
+    // change of reference from the left mean to its own.
+    float jump[4], shift[4];
+    if (self_left) {
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        jump[v] = static_cast<float>(nmean[v] - mean[v]);
+        shift[v] = 0.0f;
+      }
+    } else {
+      double fon[4];
+      mean_normal_flux(mb, nx, ny, fon);
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        jump[v] = static_cast<float>(mean[v] - nmean[v]);
+        shift[v] = static_cast<float>(fln[v] - fon[v]);
+      }
+    }
+    const float fscale = static_cast<float>(scale);
+    float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    const bool periodic_boundary = nb < 0 && a.mesh.boundary != 3;
+    double exact[4] = {0.0, 0.0, 0.0, 0.0}; // FP64 face value of a periodic boundary face
+#pragma unroll 1
+    for (int q = 0; q < QF; ++q) {
+      float dl[4], dr[4], f[4];
+      // trace perturbations of the left and the right side
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        float so = 0.0f, sn = 0.0f;
+#pragma unroll
+        for (int m = 0; m < H; ++m) {
+          so = fmaf(ch[v][m], own[q][m + 1], so);
+          if (nb >= 0)
+            sn = fmaf(nh[v][m], oth[q][m + 1], sn);
+        }
+        if (self_left) {
+          dl[v] = so;
+          dr[v] = jump[v] + sn;
+        } else {
+          dl[v] = sn;
+          dr[v] = jump[v] + so;
+        }
+      }
+      if (nb < 0) {
+        if (a.mesh.boundary == 3) {
+#pragma unroll
+          for (int v = 0; v < 4; ++v)
+            dr[v] = dl[v];
+        } else {
+          // The partner face across the period is evaluated by the donor as
+          // its own boundary face; both sides therefore take mode 0 from an
+          // FP64 HLLC on FP64 traces, so their contributions cancel to FP64
+          // round-off as in the plain path.
+          const std::int64_t point = static_cast<std::int64_t>(-nb - 1) * QF + q;
+          const std::int64_t d = a.mesh.donor[point];
+          const double *db = a.mesh.donor_basis + point * M;
+          const FaceTable<P, double> *F64 = static_cast<const FaceTable<P, double> *>(a.face_table64);
+          double us[4], ud[4], fx[4];
+#pragma unroll
+          for (int v = 0; v < 4; ++v) {
+            double s = 0.0, o = 0.0;
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+              s += __ldg(in + (static_cast<std::int64_t>(v) * M + m) * ne + d) * db[m];
+              o += in[(static_cast<std::int64_t>(v) * M + m) * ne + e] * F64->lb[le][q][m];
+            }
+            ud[v] = s;
+            us[v] = o;
+            dr[v] = static_cast<float>(s - mean[v]);
+          }
+          hllc_fast(gamma, us, ud, nx, ny, fx);
+#pragma unroll
+          for (int v = 0; v < 4; ++v)
+            exact[v] += F64->ew[le][q] * fx[v];
+        }
+      }
+      hllc_perturbed(ref, dl, dr, g1, gamma32, nxf, nyf, f);
+      const float w = F->ew[le][q];
+      const float wsc = (self_left ? -w : w) * fscale;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        acc[v] = fmaf(w, f[v], acc[v]);
+        const float value = wsc * (f[v] + shift[v]);
+#pragma unroll
+        for (int m = 0; m < H; ++m)
+          racc[v][m] = fmaf(value, own[q][m + 1], racc[v][m]);
+      }
+    }
+    const double sgn = self_left ? -1.0 : 1.0;
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+      r0[v] += sgn * scale * phi0 *
+               (periodic_boundary ? exact[v] : fln[v] * T.wsum[le] + static_cast<double>(acc[v]));
+  }
+
+  const double inv = geo[4 * ne + e];
+  const double dt = *a.dt;
+  double rho[M];
+#pragma unroll
+  for (int v = 0; v < 4; ++v)
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const std::int64_t idx = (static_cast<std::int64_t>(v) * M + m) * ne + e;
+      const double cur = in[idx];
+      const double rr = (m == 0 ? r0[v] : static_cast<double>(racc[v][m > 0 ? m - 1 : 0])) * inv;
+      double o;
+      if (a.stage == 0)
+        o = cur + dt * rr;
+      else if (a.stage == 1)
+        o = 0.75 * a.u0[idx] + 0.25 * (cur + dt * rr);
+      else
+        o = (1.0 / 3.0) * a.u0[idx] + (2.0 / 3.0) * (cur + dt * rr);
+      a.out[idx] = o;
+      if (v == 0)
+        rho[m] = o;
+    }
+
+  if (a.sense) {
+    double total = 0.0, high = 0.0;
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      total += rho[m] * rho[m];
+      if (m >= a.highest_degree_begin)
+        high += rho[m] * rho[m];
+    }
+    const bool troubled = !(total == 0.0 || high / total <= a.threshold);
+    a.flags[e] = troubled ? 1 : 0;
+    const unsigned active = __activemask();
+    const unsigned ballot = __ballot_sync(active, troubled);
+    if (ballot) {
+      const int lane = threadIdx.x & 31;
+      const int leader = __ffs(ballot) - 1;
+      int base = 0;
+      if (lane == leader)
+        base = atomicAdd(a.troubled_count, __popc(ballot));
+      base = __shfl_sync(active, base, leader);
+      if (troubled)
+        a.troubled[base + __popc(ballot & ((1u << lane) - 1u))] = static_cast<std::int32_t>(e);
+    }
+  }
+}
+
+namespace {
+
+void check(cudaError_t rc, const char *what) {
+  if (rc != cudaSuccess)
+    throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(rc));
+}
+
+template <int P> void upload_mixed(const void *symbol) {
+  static MixedVolume<P> t;
+  static VolumeTable<P, double> d;
+  fill_volume_table<P, double>(d);
+  constexpr int M = TriShape<P>::M, QV = TriShape<P>::QV;
+  for (int q = 0; q < QV; ++q) {
+    for (int m = 1; m < M; ++m) {
+      t.phi[q][m - 1] = static_cast<float>(d.phi[q][m]);
+      t.dxi[q][m - 1] = static_cast<float>(d.dxi[q][m]);
+      t.deta[q][m - 1] = static_cast<float>(d.deta[q][m]);
+    }
+    t.w[q] = static_cast<float>(0.5 * d.w[q]);
+  }
+  static FaceTable<P, double> f;
+  fill_face_table<P, double>(f);
+  for (int le = 0; le < 3; ++le) {
+    double sum = 0.0;
+    for (int q = 0; q < TriShape<P>::QF; ++q)
+      sum += f.ew[le][q];
+    t.wsum[le] = sum;
+  }
+  check(cudaMemcpyToSymbol(symbol, &t, sizeof(t)), "upload mixed volume table");
+}
+
+template <int P> void stage_mixed(const StageArgs &a, cudaStream_t s) {
+  const unsigned blocks = static_cast<unsigned>((a.mesh.ne + 127) / 128);
+  euler_tri_stage_mixed<P><<<blocks, 128, 0, s>>>(a);
+}
+
+} // namespace
+
+bool euler_tri_mixed_supported(int p) { return p >= 1 && p <= 3; }
+
+void upload_euler_tri_tables_mixed(int p) {
+  switch (p) {
+  case 1: upload_mixed<1>(reinterpret_cast<const void *>(&c_mix1)); break;
+  case 2: upload_mixed<2>(reinterpret_cast<const void *>(&c_mix2)); break;
+  case 3: upload_mixed<3>(reinterpret_cast<const void *>(&c_mix3)); break;
+  default: throw std::invalid_argument("mixed form: polynomial order must be 1..3");
+  }
+}
+
+void launch_euler_tri_stage_mixed(int p, const StageArgs &a, cudaStream_t s) {
+  switch (p) {
+  case 1: stage_mixed<1>(a, s); break;
+  case 2: stage_mixed<2>(a, s); break;
+  case 3: stage_mixed<3>(a, s); break;
+  default: throw std::invalid_argument("mixed form: polynomial order must be 1..3");
+  }
+}
+
+} // namespace wasl_b200

@@ -67,6 +67,8 @@ public:
         M_(tri_modes(cfg.polynomial_order)) {
     if (!euler_tri_order_supported(p_))
       throw SolverError(WASL_ERR_ARGUMENT, "2D Euler: polynomial order must be 0..3");
+    if (cfg.precision == WASL_MIXED && !euler_tri_mixed_supported(p_))
+      throw SolverError(WASL_ERR_ARGUMENT, "2D Euler mixed form: polynomial order must be 1..3");
     if (cfg.precision != WASL_PLAIN_FP64 && cfg.precision != WASL_MIXED)
       throw SolverError(WASL_ERR_ARGUMENT, "unknown precision form");
     cuda_check(cudaSetDevice(cfg.device), "cudaSetDevice");
@@ -142,10 +144,17 @@ public:
       d_donor_.upload(donors, stream_);
       d_donor_basis_.upload(donor_basis, stream_);
     }
-    upload_euler_tri_tables_f64(p_);
-    std::vector<unsigned char> table(euler_tri_face_table_bytes(p_, false));
-    fill_euler_tri_face_table(p_, false, table.data());
+    mixed_ = cfg.precision == WASL_MIXED;
+    if (mixed_)
+      upload_euler_tri_tables_mixed(p_);
+    else
+      upload_euler_tri_tables_f64(p_);
+    std::vector<unsigned char> table(euler_tri_face_table_bytes(p_, mixed_));
+    fill_euler_tri_face_table(p_, mixed_, table.data());
     d_face_table_.upload(table, stream_);
+    std::vector<unsigned char> table64(euler_tri_face_table_bytes(p_, false));
+    fill_euler_tri_face_table(p_, false, table64.data());
+    d_face_table64_.upload(table64, stream_);
 
     limiting_ = cfg.limiting && p_ > 0;
     if (limiting_) {
@@ -362,6 +371,7 @@ private:
     a.mesh.donor_basis = d_donor_basis_.get();
     a.mesh.boundary = boundary_;
     a.face_table = d_face_table_.get();
+    a.face_table64 = d_face_table64_.get();
     a.dt = d_dt_.get();
     a.gamma = cfg_.heat_capacity_ratio;
     a.sense = limiting_ ? 1 : 0;
@@ -380,7 +390,10 @@ private:
       if (limiting_)
         cuda_check(cudaMemsetAsync(d_count_.get(), 0, sizeof(std::int32_t), stream_), "count");
       stage_begin();
-      launch_euler_tri_stage_f64(p_, a, stream_);
+      if (mixed_)
+        launch_euler_tri_stage_mixed(p_, a, stream_);
+      else
+        launch_euler_tri_stage_f64(p_, a, stream_);
       stage_end();
       count_launches(1);
       if (limiting_) {
@@ -438,6 +451,7 @@ private:
   std::int64_t ne_ = 0;
   int boundary_ = 0;
   bool limiting_ = false;
+  bool mixed_ = false;
   double length_ = 0.0;
   LimiterStencil stencil_;
   PinnedScratch scratch_;
@@ -445,7 +459,7 @@ private:
       d_normal_y_, d_check_, d_limited_, d_u_, d_e_, d_s_, d_dt_;
   DeviceArray<std::int32_t> d_slot_nbr_, d_donor_, d_neighbors_, d_troubled_, d_count_;
   DeviceArray<std::uint8_t> d_slot_code_, d_flags_;
-  DeviceArray<unsigned char> d_face_table_;
+  DeviceArray<unsigned char> d_face_table_, d_face_table64_;
   DeviceArray<unsigned long long> d_error_, d_cfl_;
 };
 

@@ -36,7 +36,8 @@ struct TriMeshView {
 // evaluates the modal-decay sensor on `out` and appends troubled elements.
 struct StageArgs {
   TriMeshView mesh;
-  const void *face_table = nullptr; // FaceTable<P, real> in device memory
+  const void *face_table = nullptr;   // FaceTable<P, real> in device memory
+  const void *face_table64 = nullptr; // FaceTable<P, double> (the mixed form's FP64 boundary terms)
   const double *in = nullptr;
   const double *u0 = nullptr;
   double *out = nullptr;
@@ -101,6 +102,9 @@ void upload_euler_tri_tables_f64(int p);
 std::size_t euler_tri_face_table_bytes(int p, bool fp32);
 void fill_euler_tri_face_table(int p, bool fp32, void *host_buffer);
 void launch_euler_tri_stage_f64(int p, const StageArgs &a, cudaStream_t stream);
+bool euler_tri_mixed_supported(int p);
+void upload_euler_tri_tables_mixed(int p);
+void launch_euler_tri_stage_mixed(int p, const StageArgs &a, cudaStream_t stream);
 void launch_limit_f64(int M, int NB, const LimitArgs &a, cudaStream_t stream);
 void launch_sense_f64(int M, const SenseArgs &a, cudaStream_t stream);
 void launch_cfl(const CflArgs &a, cudaStream_t stream);
