@@ -203,11 +203,189 @@ __device__ __forceinline__ void hllc_perturbed(const Ref32 &b, const float *dl, 
     f[v] = K.dfn[v] + wave * jump[v];
 }
 
+// FP64 mode-0 values of periodic boundary faces, one thread per boundary face:
+// value[v][b] = sum_q w_q HLLC(U_own, U_donor).n at the face's edge points,
+// from FP64 traces.  The partner face across the period is evaluated the same
+// way by its own element, so the two contributions cancel to FP64 round-off
+// as in the plain path.
+template <int P> __global__ void boundary_mode0(const StageArgs a) {
+  using S = TriShape<P>;
+  constexpr int M = S::M, QF = S::QF;
+  const std::int64_t b = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (b >= a.boundary.count)
+    return;
+  const std::int64_t ne = a.mesh.ne;
+  const std::int64_t e = a.boundary.element[b];
+  const int le = a.boundary.local_edge[b];
+  const double nx = a.boundary.normal[b], ny = a.boundary.normal[a.boundary.count + b];
+  const FaceTable<P, double> *F = static_cast<const FaceTable<P, double> *>(a.face_table64);
+  const double *__restrict__ in = a.in;
+  double sum[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int q = 0; q < QF; ++q) {
+    const std::int64_t point = b * QF + q;
+    const std::int64_t d = a.mesh.donor[point];
+    const double *db = a.mesh.donor_basis + point * M;
+    double us[4], ud[4], f[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      double s = 0.0, o = 0.0;
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        s += in[(static_cast<std::int64_t>(v) * M + m) * ne + d] * db[m];
+        o += in[(static_cast<std::int64_t>(v) * M + m) * ne + e] * F->lb[le][q][m];
+      }
+      ud[v] = s;
+      us[v] = o;
+    }
+    hllc_fast(a.gamma, us, ud, nx, ny, f);
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+      sum[v] += F->ew[le][q] * f[v];
+  }
+#pragma unroll
+  for (int v = 0; v < 4; ++v)
+    a.boundary.value[v * a.boundary.count + b] = sum[v];
+}
+
+// Per-face record written by the face kernel and gathered by the element
+// kernel: the HLLC perturbation at each edge point (around the left mean),
+// the change of reference from the left to the right mean, and the full FP64
+// face value that mode 0 takes (both sides read the same numbers).
+template <int P> struct FaceRecord {
+  float dflux[TriShape<P>::QF][4];
+  float shift[4];
+  double mode0[4];
+};
+
 template <int P>
-__global__ void __launch_bounds__(128) euler_tri_stage_mixed(const StageArgs a) {
+__global__ void __launch_bounds__(128) euler_tri_faces_mixed(const StageArgs a) {
+  using S = TriShape<P>;
+  constexpr int M = S::M, QF = S::QF, H = M - 1;
+  constexpr double phi0 = 0.70710678118654752440;
+  const std::int64_t nf = a.faces.count;
+  const std::int64_t f = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (f >= nf)
+    return;
+  const std::int64_t ne = a.mesh.ne;
+  const double *__restrict__ in = a.in;
+  const FaceTable<P, float> *__restrict__ F = static_cast<const FaceTable<P, float> *>(a.face_table);
+  const MixedVolume<P> &T = mixed_table<P>();
+  const double gamma = a.gamma;
+  const float gamma32 = static_cast<float>(gamma), g1 = static_cast<float>(gamma - 1.0);
+  const std::int32_t L = a.faces.left[f], R = a.faces.right[f];
+  const unsigned code = a.faces.code[f];
+  if (code & 0x80u) // the far copy of a paired periodic face: evaluated with its partner
+    return;
+  const int le = (code >> 1) & 3u, re = (code >> 3) & 3u, flip = (code >> 5) & 1u;
+  const double nx = a.faces.normal[f], ny = a.faces.normal[nf + f];
+  const float nxf = static_cast<float>(nx), nyf = static_cast<float>(ny);
+
+  double lmean[4], rmean[4];
+  float lh[4][H], rh[4][H];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    lmean[v] = __ldg(in + (static_cast<std::int64_t>(v) * M) * ne + L) * phi0;
+#pragma unroll
+    for (int m = 0; m < H; ++m)
+      lh[v][m] = static_cast<float>(__ldg(in + (static_cast<std::int64_t>(v) * M + m + 1) * ne + L));
+  }
+  const bool interior = R >= 0;
+  const bool paired = !interior && a.boundary.paired;
+  if (paired) {
+    const std::int64_t d = a.mesh.donor[static_cast<std::int64_t>(-R - 1) * QF];
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+      rmean[v] = __ldg(in + (static_cast<std::int64_t>(v) * M) * ne + d) * phi0;
+  }
+  if (interior) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      rmean[v] = __ldg(in + (static_cast<std::int64_t>(v) * M) * ne + R) * phi0;
+#pragma unroll
+      for (int m = 0; m < H; ++m)
+        rh[v][m] = static_cast<float>(__ldg(in + (static_cast<std::int64_t>(v) * M + m + 1) * ne + R));
+    }
+  }
+  const MeanState ml = mean_state(gamma, lmean);
+  const Ref32 ref = ref32(ml);
+  double fln[4];
+  mean_normal_flux(ml, nx, ny, fln);
+  FaceRecord<P> rec;
+  float jump[4];
+  if (interior || paired) {
+    const MeanState mr = mean_state(gamma, rmean);
+    double frn[4];
+    mean_normal_flux(mr, nx, ny, frn);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      jump[v] = interior ? static_cast<float>(rmean[v] - lmean[v]) : 0.0f;
+      rec.shift[v] = static_cast<float>(fln[v] - frn[v]);
+    }
+  } else {
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      jump[v] = 0.0f;
+      rec.shift[v] = 0.0f;
+    }
+  }
+  const float(*lb)[M] = F->lb[le];
+  const float(*rb)[M] = F->rb[(le * 3 + re) * 2 + flip];
+  float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+  for (int q = 0; q < QF; ++q) {
+    float dl[4], dr[4], fl[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      float sl = 0.0f, sr = 0.0f;
+#pragma unroll
+      for (int m = 0; m < H; ++m) {
+        sl = fmaf(lh[v][m], lb[q][m + 1], sl);
+        if (interior)
+          sr = fmaf(rh[v][m], rb[q][m + 1], sr);
+      }
+      dl[v] = sl;
+      dr[v] = jump[v] + sr;
+    }
+    if (!interior) {
+      if (a.mesh.boundary == 3) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+          dr[v] = dl[v];
+      } else {
+        const std::int64_t point = static_cast<std::int64_t>(-R - 1) * QF + q;
+        const std::int64_t d = a.mesh.donor[point];
+        const double *db = a.mesh.donor_basis + point * M;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          double s = 0.0;
+#pragma unroll
+          for (int m = 0; m < M; ++m)
+            s += __ldg(in + (static_cast<std::int64_t>(v) * M + m) * ne + d) * db[m];
+          dr[v] = static_cast<float>(s - lmean[v]);
+        }
+      }
+    }
+    hllc_perturbed(ref, dl, dr, g1, gamma32, nxf, nyf, fl);
+    const float w = F->ew[le][q];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      rec.dflux[q][v] = fl[v];
+      acc[v] = fmaf(w, fl[v], acc[v]);
+    }
+  }
+  const bool periodic_boundary = !interior && a.mesh.boundary != 3 && !paired;
+#pragma unroll
+  for (int v = 0; v < 4; ++v)
+    rec.mode0[v] = periodic_boundary ? a.boundary.value[v * a.boundary.count + (-R - 1)]
+                                     : fln[v] * T.wsum[le] + static_cast<double>(acc[v]);
+  static_cast<FaceRecord<P> *>(a.faces.record)[f] = rec;
+}
+
+template <int P>
+__global__ void __launch_bounds__(128) euler_tri_elements_mixed(const StageArgs a) {
   using S = TriShape<P>;
   constexpr int M = S::M, QV = S::QV, QF = S::QF, H = M - 1;
-  constexpr double phi0 = 0.70710678118654752440; // 1/sqrt(2), the constant mode
+  constexpr double phi0 = 0.70710678118654752440;
   const std::int64_t ne = a.mesh.ne;
   const std::int64_t e = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (e >= ne)
@@ -215,8 +393,10 @@ __global__ void __launch_bounds__(128) euler_tri_stage_mixed(const StageArgs a) 
   const double *__restrict__ in = a.in;
   const MixedVolume<P> &T = mixed_table<P>();
   const FaceTable<P, float> *__restrict__ F = static_cast<const FaceTable<P, float> *>(a.face_table);
+  const FaceRecord<P> *__restrict__ records = static_cast<const FaceRecord<P> *>(a.faces.record);
   const double gamma = a.gamma;
-  const float gamma32 = static_cast<float>(gamma), g1 = static_cast<float>(gamma - 1.0);
+  const float g1 = static_cast<float>(gamma - 1.0);
+  static_assert(sizeof(FaceRecord<P>) % 16 == 0, "face records are copied in 16-byte chunks");
 
   double mean[4];
   float ch[4][H];
@@ -228,8 +408,25 @@ __global__ void __launch_bounds__(128) euler_tri_stage_mixed(const StageArgs a) 
       ch[v][m] = static_cast<float>(in[(static_cast<std::int64_t>(v) * M + m + 1) * ne + e]);
   }
   const double *__restrict__ geo = a.mesh.geo;
-  const MeanState mb = mean_state(gamma, mean);
-  const Ref32 bb = ref32(mb);
+  const Ref32 bb = ref32(mean_state(gamma, mean));
+
+  // Stage this element's three face records into shared memory now; the
+  // copies complete while the volume term is computed.
+  __shared__ __align__(16) FaceRecord<P> staged[3][128];
+  std::int32_t staged_face[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    staged_face[k] = a.faces.slot_face[k * ne + e];
+    const char *src = reinterpret_cast<const char *>(records + staged_face[k]);
+    char *dst = reinterpret_cast<char *>(&staged[k][threadIdx.x]);
+    const unsigned sdst = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+#pragma unroll
+    for (int c = 0; c < static_cast<int>(sizeof(FaceRecord<P>)) / 16; ++c)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sdst + 16 * c),
+                   "l"(src + 16 * c)
+                   : "memory");
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
 
   // Volume term of the high modes: the element's own mean flux cancels
   // against its faces (divergence theorem, both rules exact), leaving the
@@ -243,7 +440,7 @@ __global__ void __launch_bounds__(128) euler_tri_stage_mixed(const StageArgs a) 
   {
     const float fax = static_cast<float>(geo[e]), fay = static_cast<float>(geo[ne + e]);
     const float fbx = static_cast<float>(geo[2 * ne + e]), fby = static_cast<float>(geo[3 * ne + e]);
-#pragma unroll 1
+#pragma unroll 5
     for (int q = 0; q < QV; ++q) {
       float d[4];
 #pragma unroll
@@ -278,123 +475,28 @@ __global__ void __launch_bounds__(128) euler_tri_stage_mixed(const StageArgs a) 
     }
   }
 
-  // Faces.  The flux of each face is evaluated around its left element's mean
-  // (both sides compute the same numbers); mode 0 takes the full FP64 face
-  // value so the two sides' contributions cancel exactly.
+  // Gather the three faces, in ascending face index, from the staged records.
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
   double r0[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll 1
   for (int k = 0; k < 3; ++k) {
-    const std::int32_t nb = a.mesh.slot_nbr[k * ne + e];
     const unsigned code = a.mesh.slot_code[k * ne + e];
-    const double nx = a.mesh.slot_geo[(3 * k) * ne + e];
-    const double ny = a.mesh.slot_geo[(3 * k + 1) * ne + e];
     const double scale = a.mesh.slot_geo[(3 * k + 2) * ne + e];
-    const float nxf = static_cast<float>(nx), nyf = static_cast<float>(ny);
     const bool self_left = code & 1u;
     const int le = (code >> 1) & 3u, re = (code >> 3) & 3u, flip = (code >> 5) & 1u;
-    const float(*lb)[M] = F->lb[le];
-    const float(*rb)[M] = F->rb[(le * 3 + re) * 2 + flip];
-    const float(*own)[M] = self_left ? lb : rb;
-    const float(*oth)[M] = self_left ? rb : lb;
-    double nmean[4] = {mean[0], mean[1], mean[2], mean[3]};
-    float nh[4][H];
-    if (nb >= 0) {
-#pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        nmean[v] = __ldg(in + (static_cast<std::int64_t>(v) * M) * ne + nb) * phi0;
-#pragma unroll
-        for (int m = 0; m < H; ++m)
-          nh[v][m] = static_cast<float>(__ldg(in + (static_cast<std::int64_t>(v) * M + m + 1) * ne + nb));
-      }
-    }
-    // Left-element reference state and its mean normal flux (FP64).
-    const MeanState ml = self_left ? mb : mean_state(gamma, nmean);
-    const Ref32 ref = self_left ? bb : ref32(ml);
-    double fln[4];
-    mean_normal_flux(ml, nx, ny, fln);
-    // The jump of means, right minus left, and for a right-side element the
-    // change of reference from the left mean to its own.
-    float jump[4], shift[4];
-    if (self_left) {
-#pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        jump[v] = static_cast<float>(nmean[v] - mean[v]);
-        shift[v] = 0.0f;
-      }
-    } else {
-      double fon[4];
-      mean_normal_flux(mb, nx, ny, fon);
-#pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        jump[v] = static_cast<float>(mean[v] - nmean[v]);
-        shift[v] = static_cast<float>(fln[v] - fon[v]);
-      }
-    }
+    const float(*own)[M] = self_left ? F->lb[le] : F->rb[(le * 3 + re) * 2 + flip];
+    if (code & 0x40u) // far side of a paired periodic face: the donor basis is this element's
+      own = reinterpret_cast<const float(*)[M]>(
+          a.boundary.basis32 + static_cast<std::int64_t>(-a.faces.right[staged_face[k]] - 1) * QF * M);
+    const FaceRecord<P> &rec = staged[k][threadIdx.x];
     const float fscale = static_cast<float>(scale);
-    float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-    const bool periodic_boundary = nb < 0 && a.mesh.boundary != 3;
-    double exact[4] = {0.0, 0.0, 0.0, 0.0}; // FP64 face value of a periodic boundary face
-#pragma unroll 1
+#pragma unroll
     for (int q = 0; q < QF; ++q) {
-      float dl[4], dr[4], f[4];
-      // trace perturbations of the left and the right side
-#pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        float so = 0.0f, sn = 0.0f;
-#pragma unroll
-        for (int m = 0; m < H; ++m) {
-          so = fmaf(ch[v][m], own[q][m + 1], so);
-          if (nb >= 0)
-            sn = fmaf(nh[v][m], oth[q][m + 1], sn);
-        }
-        if (self_left) {
-          dl[v] = so;
-          dr[v] = jump[v] + sn;
-        } else {
-          dl[v] = sn;
-          dr[v] = jump[v] + so;
-        }
-      }
-      if (nb < 0) {
-        if (a.mesh.boundary == 3) {
-#pragma unroll
-          for (int v = 0; v < 4; ++v)
-            dr[v] = dl[v];
-        } else {
-          // The partner face across the period is evaluated by the donor as
-          // its own boundary face; both sides therefore take mode 0 from an
-          // FP64 HLLC on FP64 traces, so their contributions cancel to FP64
-          // round-off as in the plain path.
-          const std::int64_t point = static_cast<std::int64_t>(-nb - 1) * QF + q;
-          const std::int64_t d = a.mesh.donor[point];
-          const double *db = a.mesh.donor_basis + point * M;
-          const FaceTable<P, double> *F64 = static_cast<const FaceTable<P, double> *>(a.face_table64);
-          double us[4], ud[4], fx[4];
-#pragma unroll
-          for (int v = 0; v < 4; ++v) {
-            double s = 0.0, o = 0.0;
-#pragma unroll
-            for (int m = 0; m < M; ++m) {
-              s += __ldg(in + (static_cast<std::int64_t>(v) * M + m) * ne + d) * db[m];
-              o += in[(static_cast<std::int64_t>(v) * M + m) * ne + e] * F64->lb[le][q][m];
-            }
-            ud[v] = s;
-            us[v] = o;
-            dr[v] = static_cast<float>(s - mean[v]);
-          }
-          hllc_fast(gamma, us, ud, nx, ny, fx);
-#pragma unroll
-          for (int v = 0; v < 4; ++v)
-            exact[v] += F64->ew[le][q] * fx[v];
-        }
-      }
-      hllc_perturbed(ref, dl, dr, g1, gamma32, nxf, nyf, f);
       const float w = F->ew[le][q];
       const float wsc = (self_left ? -w : w) * fscale;
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
-        acc[v] = fmaf(w, f[v], acc[v]);
-        const float value = wsc * (f[v] + shift[v]);
+        const float value = wsc * (self_left ? rec.dflux[q][v] : rec.dflux[q][v] + rec.shift[v]);
 #pragma unroll
         for (int m = 0; m < H; ++m)
           racc[v][m] = fmaf(value, own[q][m + 1], racc[v][m]);
@@ -403,8 +505,7 @@ __global__ void __launch_bounds__(128) euler_tri_stage_mixed(const StageArgs a) 
     const double sgn = self_left ? -1.0 : 1.0;
 #pragma unroll
     for (int v = 0; v < 4; ++v)
-      r0[v] += sgn * scale * phi0 *
-               (periodic_boundary ? exact[v] : fln[v] * T.wsum[le] + static_cast<double>(acc[v]));
+      r0[v] += sgn * scale * phi0 * rec.mode0[v];
   }
 
   const double inv = geo[4 * ne + e];
@@ -486,13 +587,24 @@ template <int P> void upload_mixed(const void *symbol) {
 }
 
 template <int P> void stage_mixed(const StageArgs &a, cudaStream_t s) {
-  const unsigned blocks = static_cast<unsigned>((a.mesh.ne + 127) / 128);
-  euler_tri_stage_mixed<P><<<blocks, 128, 0, s>>>(a);
+  if (a.boundary.count > 0 && a.mesh.boundary != 3 && !a.boundary.paired)
+    boundary_mode0<P><<<static_cast<unsigned>((a.boundary.count + 127) / 128), 128, 0, s>>>(a);
+  euler_tri_faces_mixed<P><<<static_cast<unsigned>((a.faces.count + 127) / 128), 128, 0, s>>>(a);
+  euler_tri_elements_mixed<P><<<static_cast<unsigned>((a.mesh.ne + 127) / 128), 128, 0, s>>>(a);
 }
 
 } // namespace
 
 bool euler_tri_mixed_supported(int p) { return p >= 1 && p <= 3; }
+
+std::size_t euler_tri_mixed_face_record_bytes(int p) {
+  switch (p) {
+  case 1: return sizeof(FaceRecord<1>);
+  case 2: return sizeof(FaceRecord<2>);
+  case 3: return sizeof(FaceRecord<3>);
+  default: throw std::invalid_argument("mixed form: polynomial order must be 1..3");
+  }
+}
 
 void upload_euler_tri_tables_mixed(int p) {
   switch (p) {

@@ -8,6 +8,7 @@
 #include <array>
 #include <cmath>
 #include <cstring>
+#include <map>
 
 #include "basis.hpp"
 #include "kernels.hpp"
@@ -101,9 +102,15 @@ public:
     std::vector<std::uint8_t> slot_code(3 * ne_);
     std::vector<double> slot_geo(9 * ne_);
     std::vector<int> fill(ne_, 0);
+    std::vector<std::int32_t> slot_face(3 * ne_), face_right(nf), left_slot(nf, 0);
+    std::vector<std::uint8_t> face_code(nf);
+    std::vector<double> face_normal(2 * nf);
     std::vector<std::int32_t> donors;
     std::vector<double> donor_basis;
     std::int32_t boundary_index = 0;
+    std::vector<std::int32_t> bnd_element;
+    std::vector<std::uint8_t> bnd_edge;
+    std::vector<double> bnd_nx, bnd_ny;
     for (std::int64_t f = 0; f < nf; ++f) { // ascending face index = slot order
       const std::int32_t L = mesh_.face_left[f], R = mesh_.face_right[f];
       const unsigned le = mesh_.face_left_edge[f], re = mesh_.face_right_edge[f];
@@ -112,6 +119,10 @@ public:
       std::int32_t right_slot_value = R;
       if (R < 0) {
         right_slot_value = -(boundary_index + 1);
+        bnd_element.push_back(L);
+        bnd_edge.push_back(static_cast<std::uint8_t>(le));
+        bnd_nx.push_back(mesh_.face_nx[f]);
+        bnd_ny.push_back(mesh_.face_ny[f]);
         if (boundary_ == WASL_PERIODIC)
           for (int q = 0; q < QF; ++q) {
             donors.push_back(trace.donors[f * QF + q]);
@@ -120,8 +131,14 @@ public:
           }
         ++boundary_index;
       }
+      face_right[f] = right_slot_value;
+      face_code[f] = static_cast<std::uint8_t>(shared | 1u);
+      face_normal[f] = mesh_.face_nx[f];
+      face_normal[nf + f] = mesh_.face_ny[f];
+      left_slot[f] = fill[L];
       auto put = [&](std::int32_t e, std::int32_t other, unsigned code) {
         const int k = fill[e]++;
+        slot_face[k * ne_ + e] = static_cast<std::int32_t>(f);
         slot_nbr[k * ne_ + e] = other;
         slot_code[k * ne_ + e] = static_cast<std::uint8_t>(code);
         slot_geo[(3 * k) * ne_ + e] = mesh_.face_nx[f];
@@ -136,6 +153,25 @@ public:
       if (fill[e] != 3)
         throw SolverError(WASL_ERR_RUNTIME, "triangle mesh: element without three faces");
 
+    boundary_count_ = boundary_index;
+    if (boundary_count_ > 0) {
+      d_bnd_element_.upload(bnd_element, stream_);
+      d_bnd_edge_.upload(bnd_edge, stream_);
+      bnd_nx.insert(bnd_nx.end(), bnd_ny.begin(), bnd_ny.end());
+      d_bnd_normal_.upload(bnd_nx, stream_);
+      d_bnd_value_.resize(static_cast<std::size_t>(4) * boundary_count_);
+    }
+    if (cfg.precision == WASL_MIXED && boundary_ == WASL_PERIODIC && boundary_index > 0)
+      paired_ = pair_periodic_faces(QF, donors, donor_basis, face_code, slot_face, slot_code,
+                                    slot_geo, left_slot);
+    if (cfg.precision == WASL_MIXED) {
+      d_face_left_.upload(mesh_.face_left, stream_);
+      d_face_right_.upload(face_right, stream_);
+      d_face_code_.upload(face_code, stream_);
+      d_face_normal_.upload(face_normal, stream_);
+      d_slot_face_.upload(slot_face, stream_);
+      d_face_record_.resize(euler_tri_mixed_face_record_bytes(p_) * nf);
+    }
     d_geo_.upload(geo, stream_);
     d_slot_nbr_.upload(slot_nbr, stream_);
     d_slot_code_.upload(slot_code, stream_);
@@ -370,6 +406,20 @@ private:
     a.mesh.donor = d_donor_.get();
     a.mesh.donor_basis = d_donor_basis_.get();
     a.mesh.boundary = boundary_;
+    a.boundary.count = boundary_count_;
+    a.boundary.element = d_bnd_element_.get();
+    a.boundary.local_edge = d_bnd_edge_.get();
+    a.boundary.normal = d_bnd_normal_.get();
+    a.boundary.value = d_bnd_value_.get();
+    a.boundary.paired = paired_ ? 1 : 0;
+    a.boundary.basis32 = d_basis32_.get();
+    a.faces.count = mesh_.face_count();
+    a.faces.left = d_face_left_.get();
+    a.faces.right = d_face_right_.get();
+    a.faces.code = d_face_code_.get();
+    a.faces.normal = d_face_normal_.get();
+    a.faces.record = d_face_record_.get();
+    a.faces.slot_face = d_slot_face_.get();
     a.face_table = d_face_table_.get();
     a.face_table64 = d_face_table64_.get();
     a.dt = d_dt_.get();
@@ -395,13 +445,68 @@ private:
       else
         launch_euler_tri_stage_f64(p_, a, stream_);
       stage_end();
-      count_launches(1);
+      count_launches(mixed_ ? (boundary_count_ > 0 && boundary_ != WASL_TRANSMISSIVE && !paired_ ? 3 : 2)
+                            : 1);
       if (limiting_) {
         launch_limit_f64(M_, 3, limit_args(outs[k]), stream_);
         count_launches(2);
       }
     }
     cuda_check(cudaGetLastError(), "stage launch");
+  }
+
+  // The mixed form evaluates each periodic face pair once, as one face
+  // between the two elements: the lower-numbered face of the pair is kept
+  // (its element is the left side, the donor the right), the other is
+  // skipped by the face kernel and its element reads the kept face's record
+  // with the donor basis as its own.  Requires every boundary face to have a
+  // single donor whose boundary face points back; otherwise the solver keeps
+  // the FP64 boundary-face kernel.
+  bool pair_periodic_faces(int QF, const std::vector<std::int32_t> &donors,
+                           const std::vector<double> &donor_basis,
+                           std::vector<std::uint8_t> &face_code, std::vector<std::int32_t> &slot_face,
+                           std::vector<std::uint8_t> &slot_code, std::vector<double> &slot_geo,
+                           const std::vector<std::int32_t> &left_slot) {
+    std::vector<std::int64_t> bface;
+    for (std::int64_t f = 0; f < mesh_.face_count(); ++f)
+      if (mesh_.face_right[f] < 0)
+        bface.push_back(f);
+    const std::size_t nb = bface.size();
+    std::vector<std::int32_t> bdonor(nb);
+    std::map<std::pair<std::int32_t, std::int32_t>, std::vector<std::size_t>> by_pair;
+    for (std::size_t b = 0; b < nb; ++b) {
+      bdonor[b] = donors[b * QF];
+      for (int q = 1; q < QF; ++q)
+        if (donors[b * QF + q] != bdonor[b])
+          return false;
+      by_pair[{mesh_.face_left[bface[b]], bdonor[b]}].push_back(b);
+    }
+    std::vector<std::size_t> partner(nb);
+    for (std::size_t b = 0; b < nb; ++b) {
+      const auto it = by_pair.find({bdonor[b], mesh_.face_left[bface[b]]});
+      if (it == by_pair.end() || it->second.size() != 1)
+        return false;
+      partner[b] = it->second[0];
+      if (partner[b] == b)
+        return false;
+    }
+    for (std::size_t b = 0; b < nb; ++b)
+      if (partner[partner[b]] != b)
+        return false;
+    for (std::size_t b = 0; b < nb; ++b) {
+      const std::int64_t f = bface[b], c = bface[partner[b]];
+      if (f < c)
+        continue; // f is the kept face of its pair
+      face_code[f] |= 0x80u;
+      const std::int32_t e = mesh_.face_left[f];
+      const std::int64_t k = left_slot[f];
+      slot_face[k * ne_ + e] = static_cast<std::int32_t>(c);
+      slot_code[k * ne_ + e] = static_cast<std::uint8_t>((mesh_.face_left_edge[c] << 1) | 0x40u);
+      slot_geo[(3 * k + 2) * ne_ + e] = mesh_.face_scale[c];
+    }
+    std::vector<float> basis32(donor_basis.begin(), donor_basis.end());
+    d_basis32_.upload(basis32, stream_);
+    return true;
   }
 
   LimitArgs limit_args(double *state) {
@@ -450,11 +555,20 @@ private:
   int p_, M_;
   std::int64_t ne_ = 0;
   int boundary_ = 0;
+  std::int64_t boundary_count_ = 0;
   bool limiting_ = false;
   bool mixed_ = false;
+  bool paired_ = false;
+  DeviceArray<float> d_basis32_;
   double length_ = 0.0;
   LimiterStencil stencil_;
   PinnedScratch scratch_;
+  DeviceArray<double> d_bnd_normal_, d_bnd_value_, d_face_normal_;
+  DeviceArray<std::int32_t> d_face_left_, d_face_right_, d_slot_face_;
+  DeviceArray<std::uint8_t> d_face_code_;
+  DeviceArray<unsigned char> d_face_record_;
+  DeviceArray<std::int32_t> d_bnd_element_;
+  DeviceArray<std::uint8_t> d_bnd_edge_;
   DeviceArray<double> d_geo_, d_slot_geo_, d_donor_basis_, d_transforms_, d_normal_x_,
       d_normal_y_, d_check_, d_limited_, d_u_, d_e_, d_s_, d_dt_;
   DeviceArray<std::int32_t> d_slot_nbr_, d_donor_, d_neighbors_, d_troubled_, d_count_;

@@ -28,6 +28,36 @@ struct TriMeshView {
   int boundary = 0; // 0 periodic, 3 transmissive (the owner's own trace)
 };
 
+// Boundary faces in boundary index order (the slots' -(b+1) numbering):
+// owning element, its local edge, normal [2][count], and a scratch value
+// buffer [4][count] (the mixed form's FP64 mode-0 face values).
+struct BoundaryView {
+  std::int64_t count = 0;
+  const std::int32_t *element = nullptr;
+  const std::uint8_t *local_edge = nullptr;
+  const double *normal = nullptr;
+  double *value = nullptr;
+  // Periodic faces paired across the period (the mixed form evaluates each
+  // pair once): the FP32 donor basis [count][QF][M] at the canonical face's
+  // points, used by the element on the far side as its own basis.
+  int paired = 0;
+  const float *basis32 = nullptr;
+};
+
+// Faces in global face order for the face-centric mixed kernels: left and
+// right element (-(b+1) for boundary face b), code (bits as slot_code),
+// normal [2][count], per-face record scratch, and each element's face index
+// per slot [3][ne].
+struct FaceView {
+  std::int64_t count = 0;
+  const std::int32_t *left = nullptr;
+  const std::int32_t *right = nullptr;
+  const std::uint8_t *code = nullptr;
+  const double *normal = nullptr;
+  void *record = nullptr;
+  const std::int32_t *slot_face = nullptr;
+};
+
 // One SSP-RK3 stage: residual of `in`, then
 //   stage 0: out = in + dt r
 //   stage 1: out = 0.75 u0 + 0.25 (in + dt r)
@@ -36,6 +66,8 @@ struct TriMeshView {
 // evaluates the modal-decay sensor on `out` and appends troubled elements.
 struct StageArgs {
   TriMeshView mesh;
+  BoundaryView boundary;
+  FaceView faces;
   const void *face_table = nullptr;   // FaceTable<P, real> in device memory
   const void *face_table64 = nullptr; // FaceTable<P, double> (the mixed form's FP64 boundary terms)
   const double *in = nullptr;
@@ -104,6 +136,7 @@ void fill_euler_tri_face_table(int p, bool fp32, void *host_buffer);
 void launch_euler_tri_stage_f64(int p, const StageArgs &a, cudaStream_t stream);
 bool euler_tri_mixed_supported(int p);
 void upload_euler_tri_tables_mixed(int p);
+std::size_t euler_tri_mixed_face_record_bytes(int p);
 void launch_euler_tri_stage_mixed(int p, const StageArgs &a, cudaStream_t stream);
 void launch_limit_f64(int M, int NB, const LimitArgs &a, cudaStream_t stream);
 void launch_sense_f64(int M, const SenseArgs &a, cudaStream_t stream);
