@@ -163,6 +163,26 @@ int wasl_gpu_write_checkpoint(wasl_gpu *handle, const char *path, double time, u
                               const char *prepared_mesh);
 int wasl_gpu_read_checkpoint(wasl_gpu *handle, const char *path, double *time, uint64_t *step);
 
+/* The CFL time step of a device-resident 2D/1D Euler state, computed without
+ * allocating anything.  No counterpart in the reference: it is an entry point
+ * for callers that cannot call cudaMalloc (an application whose device memory
+ * is owned by its own pool allocator, or a latency-critical loop that cannot
+ * take cudaMalloc's implicit device synchronization).  `state` is
+ * U[variable][mode][element] in device memory, `length` the mesh's smallest
+ * altitude (or length in 1D), `dt` one double of device memory that receives
+ * cfl * length / (max |u|+c over cell averages * (2p+1)), or 0 when that speed
+ * is 0; `stream` a cudaStream_t (NULL: the default stream).  The reduction's
+ * scratch is a fixed 128 KiB array that every GPU loading the library holds
+ * until exit: element_count above 33,554,432 is rejected.  Every call shares
+ * that array, so calls whose kernels overlap on one GPU race.  The first call
+ * on a device looks up the array's address with that device current; make it
+ * before any stream capture.  The call synchronizes `stream` to return a
+ * status: WASL_ERR_NONPHYSICAL for a non-physical cell average, with the
+ * message in `error`. */
+int wasl_cfl_dt_static(const double *state, int64_t element_count, int mode_count, int dimensions,
+                       int polynomial_order, double gamma, double cfl, double length, double *dt,
+                       void *stream, char *error, size_t error_length);
+
 #ifdef __cplusplus
 }
 #endif

@@ -91,6 +91,9 @@ SIGNATURES = {
                                             C.c_char_p]),
     "wasl_gpu_read_checkpoint": (C.c_int, [C.c_void_p, C.c_char_p, _d,
                                            C.POINTER(C.c_uint64)]),
+    "wasl_cfl_dt_static": (C.c_int, [C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int,
+                                     C.c_double, C.c_double, C.c_double, C.c_void_p,
+                                     C.c_void_p, C.c_char_p, C.c_size_t]),
 }
 
 

@@ -35,6 +35,7 @@ SOURCES = {
     "tables.cpp": [],
     "capi.cpp": [],
     "profiling.cpp": [],
+    "cfl_static.cu": [],
 }
 HEADERS = [f for f in os.listdir(CSRC) if f.endswith((".hpp", ".cuh", ".h"))]
 
