@@ -172,35 +172,29 @@ __device__ __forceinline__ void hllc_perturbed(const Ref32 &b, const float *dl, 
   const Side32 R = perturbed_side(b, dr, g1, gamma, nx, ny);
   const float sl = fminf(L.un - L.c, R.un - R.c);
   const float sr = fmaxf(L.un + L.c, R.un + R.c);
-  if (sl >= 0.0f) {
-#pragma unroll
-    for (int v = 0; v < 4; ++v)
-      f[v] = L.dfn[v];
-    return;
-  }
-  if (sr <= 0.0f) {
-#pragma unroll
-    for (int v = 0; v < 4; ++v)
-      f[v] = R.dfn[v];
-    return;
-  }
+  // The star states are evaluated unconditionally and the supersonic cases
+  // selected afterwards, so a warp never diverges on the flow regime.
   const float dpress = (R.p - b.p) - (L.p - b.p);
   const float dn = R.dun - L.dun;
   const float den = L.rho * (sl - L.un) - R.rho * (sr - R.un);
   const float sigma_l = (dpress - R.rho * (sr - R.un) * dn) / den; // S* - u_L
   const float star = L.un + sigma_l;
   const bool left = star >= 0.0f;
-  const Side32 &K = left ? L : R;
+  const float krho = left ? L.rho : R.rho, ku = left ? L.u : R.u, kv = left ? L.v : R.v;
+  const float ke = left ? L.e : R.e, kinv = left ? L.inv : R.inv, kp = left ? L.p : R.p;
+  const float kun = left ? L.un : R.un;
   const float wave = left ? sl : sr;
   const float sigma = left ? sigma_l : sigma_l - dn; // S* - u_K
-  const float drho = K.rho * sigma / (wave - star);
-  const float rho_star = K.rho + drho;
-  const float jump[4] = {
-      drho, drho * K.u + rho_star * sigma * nx, drho * K.v + rho_star * sigma * ny,
-      drho * K.e * K.inv + rho_star * sigma * (star + K.p / (K.rho * (wave - K.un)))};
+  const float drho = krho * sigma / (wave - star);
+  const float rho_star = krho + drho;
+  const float t = rho_star * sigma;
+  const float jump[4] = {drho, drho * ku + t * nx, drho * kv + t * ny,
+                         drho * ke * kinv + t * (star + kp / (krho * (wave - kun)))};
 #pragma unroll
-  for (int v = 0; v < 4; ++v)
-    f[v] = K.dfn[v] + wave * jump[v];
+  for (int v = 0; v < 4; ++v) {
+    const float starf = (left ? L.dfn[v] : R.dfn[v]) + wave * jump[v];
+    f[v] = sl >= 0.0f ? L.dfn[v] : (sr <= 0.0f ? R.dfn[v] : starf);
+  }
 }
 
 // FP64 mode-0 values of periodic boundary faces, one thread per boundary face:
@@ -262,13 +256,22 @@ __global__ void __launch_bounds__(128) euler_tri_faces_mixed(const StageArgs a) 
   using S = TriShape<P>;
   constexpr int M = S::M, QF = S::QF, H = M - 1;
   constexpr double phi0 = 0.70710678118654752440;
+  // The edge tables, shared by the block.
+  __shared__ FaceTable<P, float> table;
+  {
+    const float *src = static_cast<const float *>(a.face_table);
+    float *dst = reinterpret_cast<float *>(&table);
+    for (int i = threadIdx.x; i < static_cast<int>(sizeof(table) / sizeof(float)); i += blockDim.x)
+      dst[i] = src[i];
+  }
+  __syncthreads();
   const std::int64_t nf = a.faces.count;
   const std::int64_t f = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (f >= nf)
     return;
   const std::int64_t ne = a.mesh.ne;
   const double *__restrict__ in = a.in;
-  const FaceTable<P, float> *__restrict__ F = static_cast<const FaceTable<P, float> *>(a.face_table);
+  const FaceTable<P, float> *F = &table;
   const MixedVolume<P> &T = mixed_table<P>();
   const double gamma = a.gamma;
   const float gamma32 = static_cast<float>(gamma), g1 = static_cast<float>(gamma - 1.0);
