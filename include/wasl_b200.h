@@ -20,9 +20,19 @@
  *   write_checkpoint/read_checkpoint cpp/include/wasl/io/checkpoint_file.hpp:9-11
  *                                                -> wasl_gpu_write_checkpoint / _read_checkpoint
  *   case setup (mesh, stencil, periodic trace)   cpp/src/case/euler_triangle.cpp:16-25,
- *                                                cpp/src/case/euler_line.cpp:14-22 -> wasl_gpu_create
- *   coarse FFI run_euler_case / run_scalar_advection_case
- *                                  crates/wasl-bridge/include/bridge.hpp:13-32 -> wasl_run_case
+ *                                                cpp/src/case/euler_line.cpp:14-22,
+ *                                                cpp/src/case/scalar_advection_line.cpp:11-19,
+ *                                                cpp/src/case/scalar_advection_triangle.cpp:16-30
+ *                                                -> wasl_gpu_create
+ *
+ * Solvers behind one handle (wasl_gpu_form_supported tells which forms exist):
+ *   2D Euler, triangles P0-P3: plain FP64 (bit-identical) and the mixed form (P1-P3);
+ *   2D scalar advection, triangles P0-P3, periodic: plain FP64;
+ *   1D Euler and 1D scalar advection, lines P0-P6: plain FP64.
+ * Line elements are stored in the reference's order (sorted by left end);
+ * triangles keep the caller's order.  Scalar states use the checkpoint layout
+ * [mode][element] (cpp/src/case/scalar_coefficient_layout.cpp transposes the
+ * reference's solver layout [element][mode] into it).
  */
 #ifndef WASL_B200_H
 #define WASL_B200_H
@@ -57,7 +67,7 @@ typedef struct {
   double velocity_x;         /* scalar advection: wavespeed (1D) / velocity (2D) */
   double velocity_y;
   int boundary_left;         /* 1D: left end kind; 2D: every boundary (periodic/transmissive) */
-  int boundary_right;        /* 1D: right end kind */
+  int boundary_right;        /* 1D: right end kind (transmissive on a line is outflow) */
   double inflow_left;        /* 1D scalar inflow values */
   double inflow_right;
   int limiting;              /* Euler: modal-decay + characteristic WENO + positivity */

@@ -141,7 +141,7 @@ class Oracle:
         L.wo_euler_tri_step.argtypes = [tm, C.POINTER(WoEulerTriSetup), C.c_double, C.c_int,
                                         C.c_double, _d, _u8]
         L.wo_euler_line_step.argtypes = [lm, C.c_int, C.c_int, st, C.c_double, C.c_double,
-                                         C.c_double, C.c_double, C.c_int, C.c_double, _d]
+                                         C.c_double, C.c_double, C.c_int, C.c_double, _d, _u8]
         L.wo_scalar_line_step.argtypes = [lm, C.c_int, C.c_double, C.c_int, C.c_double,
                                           C.c_double, C.c_int, C.c_double, _d]
         L.wo_scalar_tri_step.argtypes = [tm, _i32, _d, C.c_double, C.c_double, C.c_int,
@@ -409,12 +409,18 @@ class OracleLineMesh:
         return self.lib.wo_line_advection_cfl(self.ptr, a, p, cfl)
 
     def euler_step(self, gamma, p, dt, c, left_kind=0, right_kind=0, stencil=None,
-                   threshold=1e-3, density_floor=1e-10, pressure_floor=1e-10):
+                   threshold=1e-3, density_floor=1e-10, pressure_floor=1e-10,
+                   return_flags=False):
+        """In place on c; with return_flags the troubled sets [stage][element]."""
         st = C.pointer(stencil.s) if stencil is not None else None
+        flags = np.zeros(3 * self.ne, dtype=np.uint8)
         rc = self.lib.wo_euler_line_step(self.ptr, left_kind, right_kind, st, threshold,
-                                         density_floor, pressure_floor, gamma, p, dt, _p(c))
+                                         density_floor, pressure_floor, gamma, p, dt, _p(c),
+                                         _p(flags, _u8))
         if rc != 0:
             raise ValueError("Euler line step failed")
+        if return_flags:
+            return flags.reshape(3, self.ne)
 
     def scalar_step(self, a, p, dt, c, lk=0, lv=0.0, rk=0, rv=0.0):
         self.lib.wo_scalar_line_step(self.ptr, lk, lv, rk, rv, a, p, dt, _p(c))

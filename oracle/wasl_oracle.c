@@ -1871,7 +1871,8 @@ done:
 
 int wo_euler_line_step(const wo_line_mesh *mesh, int left_kind, int right_kind,
                        const wo_stencil *stencil, double threshold, double density_floor,
-                       double pressure_floor, double gamma, int p, double dt, double *c) {
+                       double pressure_floor, double gamma, int p, double dt, double *c,
+                       uint8_t *flags) {
   const int M = wo_line_modes(p);
   const size_t n = 4 * (size_t)M * (size_t)mesh->element_count;
   double *rhs = (double *)malloc(sizeof(double) * n);
@@ -1896,7 +1897,7 @@ int wo_euler_line_step(const wo_line_mesh *mesh, int left_kind, int right_kind,
         c[i] = (1.0 / 3.0) * c[i] + (2.0 / 3.0) * (stage[i] + dt * rhs[i]);
     if (stencil &&
         (rc = wo_limit_euler(stencil, gamma, threshold, density_floor, pressure_floor, states[k],
-                             NULL, NULL)) != 0)
+                             flags ? flags + k * mesh->element_count : NULL, NULL)) != 0)
       break;
   }
   free(rhs);

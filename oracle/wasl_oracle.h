@@ -185,10 +185,11 @@ typedef struct {
  * troubled set of each of the three stages, packed [stage][element]. */
 int wo_euler_tri_step(const wo_tri_mesh *mesh, const wo_euler_tri_setup *setup, double gamma,
                       int p, double dt, double *coefficients, uint8_t *flags);
+/* flags (optional, [stage][element]) as for wo_euler_tri_step. */
 int wo_euler_line_step(const wo_line_mesh *mesh, int left_kind, int right_kind,
                        const wo_stencil *stencil, double threshold, double density_floor,
                        double pressure_floor, double gamma, int p, double dt,
-                       double *coefficients);
+                       double *coefficients, uint8_t *flags);
 void wo_scalar_line_step(const wo_line_mesh *mesh, int left_kind, double left_value,
                          int right_kind, double right_value, double wavespeed, int p, double dt,
                          double *coefficients);

@@ -33,6 +33,10 @@ SOURCES = {
     # division/square root and flushed denormals cost nothing in accuracy.
     "euler_tri_mixed.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
     "euler_tri_solver.cu": [],
+    "line_f64.cu": ["--fmad=false"],
+    "scalar_tri_f64.cu": ["--fmad=false"],
+    "line_solver.cu": [],
+    "scalar_tri_solver.cu": [],
     "mesh.cpp": [],
     "tables.cpp": [],
     "capi.cpp": [],

@@ -76,6 +76,42 @@ def l1_density_error(solver, exact, rule_order=5):
     return float(np.sum(w * np.abs(rho_h - exact(x, y)[..., 0])))
 
 
+# ---- 1D periodic advection -------------------------------------------------------------
+
+class AdvectedPulse:
+    """u0 = sin(2 pi x) + exp(-300 (x - 0.5)^2) on the periodic unit line,
+    advected with speed a; the exact solution is the translated initial data."""
+
+    def __init__(self, speed=1.0):
+        self.speed = speed
+
+    def value(self, x, t=0.0):
+        y = np.mod(np.asarray(x, dtype=np.float64) - self.speed * t, 1.0)
+        return np.sin(2.0 * math.pi * y) + np.exp(-300.0 * (y - 0.5) ** 2)
+
+
+def advection_line_mesh(n=400, seed=2024):
+    """n cells on [0,1], interior nodes moved uniformly within +-0.2h."""
+    return meshgen.jittered_line(n, 0.0, 1.0, jitter=0.2, seed=seed)
+
+
+def project_line(solver, field, points=7):
+    """Project field(x) -> [..., variables] with the 7-point Gauss rule
+    (cpp/src/case/initial_state.cpp:16-29)."""
+    x, _, _ = solver.quadrature(points - 1)
+    values = np.asarray(field(x), dtype=np.float64)
+    if values.ndim == 2:
+        values = values[..., None]
+    solver.project(points - 1, values)
+
+
+def l1_line_error(solver, exact, points=7):
+    """Integral of |u_h - u_exact| (first variable) with a Gauss rule."""
+    x, _, w = solver.quadrature(points - 1)
+    u_h = solver.evaluate(points - 1)[..., 0]
+    return float(np.sum(w * np.abs(u_h - exact(x))))
+
+
 # ---- Riemann problems ----------------------------------------------------------------
 
 def random_state(rng):

@@ -11,11 +11,19 @@
 
 namespace wasl_b200 {
 std::unique_ptr<Solver> make_euler_tri_solver(const wasl_gpu_config &cfg, TriTopology &&topo);
+std::unique_ptr<Solver> make_scalar_tri_solver(const wasl_gpu_config &cfg, TriTopology &&topo);
+std::unique_ptr<Solver> make_line_solver(const wasl_gpu_config &cfg, LineTopology &&topo);
 
 bool form_supported(int precision, int dimensions, int equation, int p) {
+  if (equation != WASL_EULER && equation != WASL_SCALAR_ADVECTION)
+    return false;
   if (dimensions == 2 && equation == WASL_EULER)
     return (precision == WASL_PLAIN_FP64 && p >= 0 && p <= 3) ||
            (precision == WASL_MIXED && p >= 1 && p <= 3);
+  if (dimensions == 2)
+    return precision == WASL_PLAIN_FP64 && p >= 0 && p <= 3;
+  if (dimensions == 1)
+    return precision == WASL_PLAIN_FP64 && p >= 0 && p <= 6;
   return false;
 }
 
@@ -25,10 +33,15 @@ std::unique_ptr<Solver> make_solver(const wasl_gpu_config &cfg, std::int64_t nod
   if (!form_supported(cfg.precision, cfg.dimensions, cfg.equation, cfg.polynomial_order))
     throw SolverError(WASL_ERR_ARGUMENT,
                       "unsupported combination of dimension, equation, order and precision");
-  if (cfg.dimensions == 2 && cfg.equation == WASL_EULER)
-    return make_euler_tri_solver(cfg, build_triangle_topology(node_count, node_tags, coordinates,
-                                                              element_count, element_nodes));
-  throw SolverError(WASL_ERR_ARGUMENT, "unsupported dimension/equation combination");
+  if (cfg.dimensions == 2) {
+    TriTopology topo =
+        build_triangle_topology(node_count, node_tags, coordinates, element_count, element_nodes);
+    if (cfg.equation == WASL_EULER)
+      return make_euler_tri_solver(cfg, std::move(topo));
+    return make_scalar_tri_solver(cfg, std::move(topo));
+  }
+  return make_line_solver(cfg, build_line_topology(node_count, node_tags, coordinates,
+                                                   element_count, element_nodes));
 }
 } // namespace wasl_b200
 

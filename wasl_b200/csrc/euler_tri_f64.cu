@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(128) euler_tri_stage_f64(const StageArgs a) {
 
   // Mass inverse and the Shu-Osher combination.
   const double inv = geo[4 * ne + e];
-  const double dt = *a.dt;
+  const double dt = a.dt ? *a.dt : a.dt_value;
   double rho[M];
 #pragma unroll
   for (int v = 0; v < 4; ++v)
@@ -558,6 +558,9 @@ void launch_limit_f64(int M, int NB, const LimitArgs &a, cudaStream_t s) {
   WASL_LIMIT(2, 2)
   WASL_LIMIT(3, 2)
   WASL_LIMIT(4, 2)
+  WASL_LIMIT(5, 2)
+  WASL_LIMIT(6, 2)
+  WASL_LIMIT(7, 2)
 #undef WASL_LIMIT
   throw std::invalid_argument("limiter: unsupported mode count");
 }

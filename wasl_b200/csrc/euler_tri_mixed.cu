@@ -512,7 +512,7 @@ __global__ void __launch_bounds__(128) euler_tri_elements_mixed(const StageArgs 
   }
 
   const double inv = geo[4 * ne + e];
-  const double dt = *a.dt;
+  const double dt = a.dt ? *a.dt : a.dt_value;
   double rho[M];
 #pragma unroll
   for (int v = 0; v < 4; ++v)

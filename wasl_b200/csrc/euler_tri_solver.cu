@@ -23,33 +23,24 @@ void cuda_check(cudaError_t rc, const char *what) {
     throw SolverError(WASL_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(rc));
 }
 
-namespace {
-
-// Pinned host scratch for the few scalars a step exchanges with the device.
-struct PinnedScratch {
-  double *dt = nullptr;
-  unsigned long long *words = nullptr; // error word + CFL result (8)
-  PinnedScratch() {
-    cuda_check(cudaMallocHost(reinterpret_cast<void **>(&dt), sizeof(double)), "pinned");
-    cuda_check(cudaMallocHost(reinterpret_cast<void **>(&words), 16 * sizeof(unsigned long long)),
-               "pinned");
-  }
-  ~PinnedScratch() {
-    cudaFreeHost(dt);
-    cudaFreeHost(words);
-  }
-};
-
 double bits_to_double(unsigned long long b) {
   double d;
   std::memcpy(&d, &b, sizeof(d));
   return d;
 }
 
-} // namespace
+void throw_device_error(unsigned long long word) {
+  if (!word)
+    return;
+  const int code = static_cast<int>(word >> 56);
+  const long long element = static_cast<long long>(word & 0xffffffffffffffULL);
+  if (code == 1)
+    throw SolverError(WASL_ERR_NONPHYSICAL, "simulation: Euler cell average is not physical"
+                                            " (element " + std::to_string(element) + ")");
+  throw SolverError(WASL_ERR_FLOOR, "Euler positivity limiter: cell average is below a floor"
+                                    " (element " + std::to_string(element) + ")");
+}
 
-// Host evaluation of one cell-average wave speed with the C library's hypot,
-// as cfl_timestep.cpp:33-47 computes it.
 double host_cell_speed(double gamma, const double *mode0, int dimensions) {
   const double scale = 1.0 / std::sqrt(2.0);
   const double s[4] = {scale * mode0[0], scale * mode0[1], scale * mode0[2], scale * mode0[3]};
@@ -88,80 +79,22 @@ public:
     if (has_boundary && boundary_ == WASL_PERIODIC)
       trace = periodic_trace(mesh_, p_);
 
-    // Element geometry [5][ne] and the three face slots of each element.
-    std::vector<double> geo(5 * ne_);
-    for (std::int64_t e = 0; e < ne_; ++e) {
-      const TriMap &m = mesh_.maps[e];
-      geo[e] = m.ax();
-      geo[ne_ + e] = m.ay();
-      geo[2 * ne_ + e] = m.bx();
-      geo[3 * ne_ + e] = m.by();
-      geo[4 * ne_ + e] = 1.0 / m.jacobian_determinant();
-    }
-    std::vector<std::int32_t> slot_nbr(3 * ne_);
-    std::vector<std::uint8_t> slot_code(3 * ne_);
-    std::vector<double> slot_geo(9 * ne_);
-    std::vector<int> fill(ne_, 0);
-    std::vector<std::int32_t> slot_face(3 * ne_), face_right(nf), left_slot(nf, 0);
-    std::vector<std::uint8_t> face_code(nf);
-    std::vector<double> face_normal(2 * nf);
-    std::vector<std::int32_t> donors;
-    std::vector<double> donor_basis;
-    std::int32_t boundary_index = 0;
-    std::vector<std::int32_t> bnd_element;
-    std::vector<std::uint8_t> bnd_edge;
-    std::vector<double> bnd_nx, bnd_ny;
-    for (std::int64_t f = 0; f < nf; ++f) { // ascending face index = slot order
-      const std::int32_t L = mesh_.face_left[f], R = mesh_.face_right[f];
-      const unsigned le = mesh_.face_left_edge[f], re = mesh_.face_right_edge[f];
-      const unsigned flip = mesh_.face_flip[f];
-      const unsigned shared = (le << 1) | (re << 3) | (flip << 5);
-      std::int32_t right_slot_value = R;
-      if (R < 0) {
-        right_slot_value = -(boundary_index + 1);
-        bnd_element.push_back(L);
-        bnd_edge.push_back(static_cast<std::uint8_t>(le));
-        bnd_nx.push_back(mesh_.face_nx[f]);
-        bnd_ny.push_back(mesh_.face_ny[f]);
-        if (boundary_ == WASL_PERIODIC)
-          for (int q = 0; q < QF; ++q) {
-            donors.push_back(trace.donors[f * QF + q]);
-            donor_basis.insert(donor_basis.end(), trace.basis.begin() + (f * QF + q) * M_,
-                               trace.basis.begin() + (f * QF + q + 1) * M_);
-          }
-        ++boundary_index;
-      }
-      face_right[f] = right_slot_value;
-      face_code[f] = static_cast<std::uint8_t>(shared | 1u);
-      face_normal[f] = mesh_.face_nx[f];
-      face_normal[nf + f] = mesh_.face_ny[f];
-      left_slot[f] = fill[L];
-      auto put = [&](std::int32_t e, std::int32_t other, unsigned code) {
-        const int k = fill[e]++;
-        slot_face[k * ne_ + e] = static_cast<std::int32_t>(f);
-        slot_nbr[k * ne_ + e] = other;
-        slot_code[k * ne_ + e] = static_cast<std::uint8_t>(code);
-        slot_geo[(3 * k) * ne_ + e] = mesh_.face_nx[f];
-        slot_geo[(3 * k + 1) * ne_ + e] = mesh_.face_ny[f];
-        slot_geo[(3 * k + 2) * ne_ + e] = mesh_.face_scale[f];
-      };
-      put(L, right_slot_value, shared | 1u);
-      if (R >= 0)
-        put(R, L, shared);
-    }
-    for (std::int64_t e = 0; e < ne_; ++e)
-      if (fill[e] != 3)
-        throw SolverError(WASL_ERR_RUNTIME, "triangle mesh: element without three faces");
-
-    boundary_count_ = boundary_index;
+    TriSlots t = build_tri_slots(mesh_, boundary_ == WASL_PERIODIC && has_boundary ? &trace : nullptr,
+                                 QF, M_);
+    boundary_count_ = t.boundary_count;
     if (boundary_count_ > 0) {
-      d_bnd_element_.upload(bnd_element, stream_);
-      d_bnd_edge_.upload(bnd_edge, stream_);
-      bnd_nx.insert(bnd_nx.end(), bnd_ny.begin(), bnd_ny.end());
-      d_bnd_normal_.upload(bnd_nx, stream_);
+      d_bnd_element_.upload(t.bnd_element, stream_);
+      d_bnd_edge_.upload(t.bnd_edge, stream_);
+      d_bnd_normal_.upload(t.bnd_normal, stream_);
       d_bnd_value_.resize(static_cast<std::size_t>(4) * boundary_count_);
     }
-    if (cfg.precision == WASL_MIXED && boundary_ == WASL_PERIODIC && boundary_index > 0)
+    std::vector<std::int32_t> &donors = t.donors;
+    std::vector<double> &donor_basis = t.donor_basis;
+    std::vector<double> &geo = t.geo, &slot_geo = t.slot_geo, &face_normal = t.face_normal;
+    std::vector<std::int32_t> &slot_nbr = t.slot_nbr, &slot_face = t.slot_face,
+                              &face_right = t.face_right, &left_slot = t.left_slot;
+    std::vector<std::uint8_t> &slot_code = t.slot_code, &face_code = t.face_code;
+    if (cfg.precision == WASL_MIXED && boundary_ == WASL_PERIODIC && boundary_count_ > 0)
       paired_ = pair_periodic_faces(QF, donors, donor_basis, face_code, slot_face, slot_code,
                                     slot_geo, left_slot);
     if (cfg.precision == WASL_MIXED) {
@@ -336,11 +269,7 @@ public:
   }
 
   void step(double dt) override {
-    *scratch_.dt = dt;
-    cuda_check(cudaMemcpyAsync(d_dt_.get(), scratch_.dt, sizeof(double), cudaMemcpyHostToDevice,
-                               stream_),
-               "dt");
-    enqueue_step();
+    enqueue_step(nullptr, dt);
     if (limiting_)
       check_error();
   }
@@ -367,7 +296,7 @@ public:
     for (std::int64_t n = 0; n < steps; ++n) {
       launch_cfl(cfl_args(cfl), stream_);
       count_launches(3);
-      enqueue_step();
+      enqueue_step(d_dt_.get(), 0.0);
     }
     check_error();
   }
@@ -396,7 +325,9 @@ public:
   }
 
 private:
-  void enqueue_step() {
+  // One step with dt read from device memory (dt_device, written by the CFL
+  // kernels) or, when dt_device is null, passed by value.
+  void enqueue_step(const double *dt_device, double dt_value) {
     StageArgs a;
     a.mesh.ne = ne_;
     a.mesh.geo = d_geo_.get();
@@ -422,7 +353,8 @@ private:
     a.faces.slot_face = d_slot_face_.get();
     a.face_table = d_face_table_.get();
     a.face_table64 = d_face_table64_.get();
-    a.dt = d_dt_.get();
+    a.dt = dt_device;
+    a.dt_value = dt_value;
     a.gamma = cfg_.heat_capacity_ratio;
     a.sense = limiting_ ? 1 : 0;
     a.threshold = cfg_.sensor_threshold;
@@ -541,13 +473,7 @@ private:
     if (!word)
       return;
     cuda_check(cudaMemsetAsync(d_error_.get(), 0, sizeof(unsigned long long), stream_), "memset");
-    const int code = static_cast<int>(word >> 56);
-    const long long element = static_cast<long long>(word & 0xffffffffffffffULL);
-    if (code == 1)
-      throw SolverError(WASL_ERR_NONPHYSICAL, "simulation: Euler cell average is not physical"
-                                              " (element " + std::to_string(element) + ")");
-    throw SolverError(WASL_ERR_FLOOR, "Euler positivity limiter: cell average is below a floor"
-                                      " (element " + std::to_string(element) + ")");
+    throw_device_error(word);
   }
 
   wasl_gpu_config cfg_;

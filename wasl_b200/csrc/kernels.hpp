@@ -73,8 +73,10 @@ struct StageArgs {
   const double *in = nullptr;
   const double *u0 = nullptr;
   double *out = nullptr;
-  const double *dt = nullptr; // device scalar
+  const double *dt = nullptr; // device scalar, or null: dt_value
+  double dt_value = 0.0;
   double gamma = 1.4;
+  double velocity_x = 0.0, velocity_y = 0.0; // scalar advection velocity
   int stage = 0;
   int sense = 0;
   double threshold = 1e-3;
@@ -128,6 +130,54 @@ struct CflArgs {
   double *dt = nullptr;                 // device dt written by the final kernel
   unsigned long long *error = nullptr;
 };
+
+// Reference-line tables of the 1D kernels: orthonormal Legendre modes and
+// their derivatives at the Gauss points of the residual's rule (p+1 points
+// for Euler, line_residual.hpp:29; max(1, p) for scalar advection,
+// scalar_advection/line_residual.hpp:40-42), the weights, and the modes at
+// the ends xi = -1 (lb) and xi = +1 (rb).  Passed by value.
+struct LineTable {
+  static constexpr int kMaxPoints = 8, kMaxModes = 8;
+  double phi[kMaxPoints][kMaxModes];
+  double dphi[kMaxPoints][kMaxModes];
+  double w[kMaxPoints];
+  double lb[kMaxModes], rb[kMaxModes];
+};
+
+// One SSP-RK3 stage on a line mesh (elements sorted left to right: element e
+// has face e on its left and face e+1 on its right).  State [variable][mode]
+// [element] with 4 Euler variables or 1 scalar.  End kinds as enum
+// wasl_boundary (periodic, inflow (scalar only), outflow).
+struct LineStageArgs {
+  std::int64_t ne = 0;
+  const double *inv_jacobian = nullptr; // [ne] 1 / ((x_right - x_left) / 2)
+  const double *in = nullptr;
+  const double *u0 = nullptr;
+  double *out = nullptr;
+  const double *dt = nullptr; // device scalar, or null: dt_value
+  double dt_value = 0.0;
+  double gamma = 1.4;
+  double speed = 0.0;         // scalar wavespeed
+  int left_kind = 0, right_kind = 0;
+  double left_value = 0.0, right_value = 0.0;
+  int stage = 0;
+  int sense = 0;
+  double threshold = 1e-3;
+  int highest_degree_begin = 0;
+  std::uint8_t *flags = nullptr;
+  std::int32_t *troubled = nullptr;
+  std::int32_t *troubled_count = nullptr;
+  LineTable table;
+};
+
+bool line_order_supported(int p); // 0..6
+void fill_line_table(int p, int points, LineTable &table);
+void launch_line_stage_f64(int variables, int p, const LineStageArgs &a, cudaStream_t stream);
+
+// 2D scalar advection (constant velocity a.velocity_x/y) on the triangle
+// slots of StageArgs; state [mode][element].
+void upload_scalar_tri_tables(int p);
+void launch_scalar_tri_stage_f64(int p, const StageArgs &a, cudaStream_t stream);
 
 bool euler_tri_order_supported(int p);
 void upload_euler_tri_tables_f64(int p);

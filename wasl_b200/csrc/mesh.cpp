@@ -563,6 +563,74 @@ LimiterStencil line_stencil(const LineTopology &mesh, int p, bool periodic) {
   return s;
 }
 
+TriSlots build_tri_slots(const TriTopology &mesh, const PeriodicTrace *trace, int QF, int M) {
+  const std::int64_t ne = mesh.element_count, nf = mesh.face_count();
+  TriSlots t;
+  t.geo.resize(5 * ne);
+  for (std::int64_t e = 0; e < ne; ++e) {
+    const TriMap &m = mesh.maps[e];
+    t.geo[e] = m.ax();
+    t.geo[ne + e] = m.ay();
+    t.geo[2 * ne + e] = m.bx();
+    t.geo[3 * ne + e] = m.by();
+    t.geo[4 * ne + e] = 1.0 / m.jacobian_determinant();
+  }
+  t.slot_nbr.resize(3 * ne);
+  t.slot_code.resize(3 * ne);
+  t.slot_geo.resize(9 * ne);
+  t.slot_face.resize(3 * ne);
+  t.face_right.resize(nf);
+  t.left_slot.assign(nf, 0);
+  t.face_code.resize(nf);
+  t.face_normal.resize(2 * nf);
+  std::vector<int> fill(ne, 0);
+  std::vector<double> bny;
+  for (std::int64_t f = 0; f < nf; ++f) {
+    const std::int32_t L = mesh.face_left[f], R = mesh.face_right[f];
+    const unsigned le = mesh.face_left_edge[f], re = mesh.face_right_edge[f];
+    const unsigned shared = (le << 1) | (re << 3) | (static_cast<unsigned>(mesh.face_flip[f]) << 5);
+    std::int32_t right = R;
+    if (R < 0) {
+      right = -static_cast<std::int32_t>(t.boundary_count + 1);
+      t.bnd_element.push_back(L);
+      t.bnd_edge.push_back(static_cast<std::uint8_t>(le));
+      t.bnd_normal.push_back(mesh.face_nx[f]);
+      bny.push_back(mesh.face_ny[f]);
+      if (trace)
+        for (int q = 0; q < QF; ++q) {
+          t.donors.push_back(trace->donors[f * QF + q]);
+          t.donor_basis.insert(t.donor_basis.end(), trace->basis.begin() + (f * QF + q) * M,
+                               trace->basis.begin() + (f * QF + q + 1) * M);
+        }
+      ++t.boundary_count;
+    }
+    t.face_right[f] = right;
+    t.face_code[f] = static_cast<std::uint8_t>(shared | 1u);
+    t.face_normal[f] = mesh.face_nx[f];
+    t.face_normal[nf + f] = mesh.face_ny[f];
+    t.left_slot[f] = fill[L];
+    auto put = [&](std::int32_t e, std::int32_t other, unsigned code) {
+      const int k = fill[e]++;
+      if (k >= 3)
+        throw std::runtime_error("triangle mesh: element with more than three faces");
+      t.slot_face[k * ne + e] = static_cast<std::int32_t>(f);
+      t.slot_nbr[k * ne + e] = other;
+      t.slot_code[k * ne + e] = static_cast<std::uint8_t>(code);
+      t.slot_geo[(3 * k) * ne + e] = mesh.face_nx[f];
+      t.slot_geo[(3 * k + 1) * ne + e] = mesh.face_ny[f];
+      t.slot_geo[(3 * k + 2) * ne + e] = mesh.face_scale[f];
+    };
+    put(L, right, shared | 1u);
+    if (R >= 0)
+      put(R, L, shared);
+  }
+  for (std::int64_t e = 0; e < ne; ++e)
+    if (fill[e] != 3)
+      throw std::runtime_error("triangle mesh: element without three faces");
+  t.bnd_normal.insert(t.bnd_normal.end(), bny.begin(), bny.end());
+  return t;
+}
+
 double minimum_altitude(const TriTopology &mesh) {
   double result = std::numeric_limits<double>::max();
   for (const auto &m : mesh.maps) {

@@ -78,6 +78,32 @@ struct PeriodicTrace {
 };
 PeriodicTrace periodic_trace(const TriTopology &mesh, int p);
 
+// The face slots and boundary lists the triangle stage kernels read, built in
+// ascending global face index (the reference's flux summation order):
+//   geo [5][ne]: ax, ay, bx, by (the affine map's columns), 1/det(J);
+//   slot_nbr/slot_code/slot_face [3][ne], slot_geo [3][3][ne] (normal x, y,
+//   edge scale); code bit 0: this element is the face's left side, bits 1-2
+//   left local edge, bits 3-4 right local edge, bit 5 orientation flip;
+//   face_right [face]: the right element, or -(b+1) for boundary face b;
+//   boundary lists in boundary order, with each boundary face's periodic
+//   donors [b][QF] and donor basis [b][QF][M] when a trace is given.
+struct TriSlots {
+  std::vector<double> geo;
+  std::vector<std::int32_t> slot_nbr, slot_face;
+  std::vector<std::uint8_t> slot_code;
+  std::vector<double> slot_geo;
+  std::vector<std::int32_t> face_right, left_slot;
+  std::vector<std::uint8_t> face_code;
+  std::vector<double> face_normal;        // [2][face]
+  std::vector<std::int32_t> bnd_element;
+  std::vector<std::uint8_t> bnd_edge;
+  std::vector<double> bnd_normal;         // [2][boundary]
+  std::vector<std::int32_t> donors;
+  std::vector<double> donor_basis;
+  std::int64_t boundary_count = 0;
+};
+TriSlots build_tri_slots(const TriTopology &mesh, const PeriodicTrace *trace, int QF, int M);
+
 // Immediate-neighbour limiter stencil (cpp/include/wasl/limiting/euler_limiter_stencil.hpp:19-50).
 struct LimiterStencil {
   int mode_count = 0;

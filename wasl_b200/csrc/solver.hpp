@@ -56,6 +56,29 @@ private:
   std::size_t n_ = 0;
 };
 
+// Pinned host scratch for the few scalars a step exchanges with the device.
+struct PinnedScratch {
+  unsigned long long *words = nullptr; // [0..7] CFL result, [8] error word
+  PinnedScratch() {
+    cuda_check(cudaMallocHost(reinterpret_cast<void **>(&words), 16 * sizeof(unsigned long long)),
+               "pinned");
+  }
+  ~PinnedScratch() { cudaFreeHost(words); }
+  PinnedScratch(const PinnedScratch &) = delete;
+  PinnedScratch &operator=(const PinnedScratch &) = delete;
+};
+
+double bits_to_double(unsigned long long bits);
+
+// One cell-average wave speed |u| + c (hypot(u, v) + c in 2D) evaluated on the
+// host with the C library's functions, as cpp/src/time/cfl_timestep.cpp:33-47
+// computes it; mode0 holds the four mode-0 coefficients.
+double host_cell_speed(double gamma, const double *mode0, int dimensions);
+
+// Throws the SolverError a device error word stands for (code in the top
+// byte, element index below); returns if the word is zero.
+void throw_device_error(unsigned long long word);
+
 class Solver {
 public:
   virtual ~Solver();
