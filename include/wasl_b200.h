@@ -76,6 +76,8 @@ typedef struct {
   double pressure_floor;     /* default 1e-10 */
   int precision;             /* enum wasl_precision */
   int device;                /* CUDA device ordinal */
+  int volume_rule_order;     /* mixed form: order r of the collapsed (r+1)^2-point volume
+                                rule, p..p+2; 0 = p+2, the reference residual's rule */
 } wasl_gpu_config;
 
 /* Fill the reference's defaults (crates/wasl-bridge/src/config.rs:87-104). */

@@ -1,6 +1,8 @@
-"""The mixed-precision form: same discretization as the plain FP64 path, FP32
-only on high-mode perturbations.  Checked against the plain path (tolerances
-stated per test), for free-stream preservation, and for conservation."""
+"""The mixed-precision form: the plain FP64 path's discretization with FP32
+only on high-mode perturbations, and optionally a lower-order collapsed volume
+rule (order p..p+2; the reference's residual uses p+2).  Checked against the
+plain path (tolerances stated per test), for free-stream preservation, and for
+conservation."""
 import numpy as np
 import pytest
 
@@ -16,11 +18,11 @@ def pair(arrays, p, **kw):
             wasl_b200.Solver(*arrays, polynomial_order=p, precision="mixed", **kw))
 
 
-@pytest.mark.parametrize("p", [1, 2, 3])
-def test_uniform_flow_stays_uniform(p):
+@pytest.mark.parametrize("p,rule", [(p, r) for p in (1, 2, 3) for r in (0, p, p + 1)])
+def test_uniform_flow_stays_uniform(p, rule):
     """A constant state is preserved to FP64 round-off: the FP32 part sees dU = 0."""
     arrays = meshgen.jittered_box(16, jitter=0.15, seed=p)
-    plain, mixed = pair(arrays, p)
+    plain, mixed = pair(arrays, p, volume_rule_order=rule)
     with plain, mixed:
         state = np.zeros((4, mixed.modes, mixed.elements))
         state[:, 0] = np.sqrt(2) * np.array([1.0, 0.3, -0.2, 2.6])[:, None]
@@ -49,10 +51,11 @@ def test_one_step_close_to_plain(p):
     assert np.max(np.abs(a - b)) <= 1e-6 * change
 
 
-@pytest.mark.parametrize("p", [1, 2, 3])
-def test_mass_and_energy_conserved(p):
+@pytest.mark.parametrize("p,rule", [(p, r) for p in (1, 2, 3) for r in (0, p)])
+def test_mass_and_energy_conserved(p, rule):
     arrays = meshgen.jittered_box(16, jitter=0.15, seed=4)
-    with wasl_b200.Solver(*arrays, polynomial_order=p, precision="mixed") as g:
+    with wasl_b200.Solver(*arrays, polynomial_order=p, precision="mixed",
+                          volume_rule_order=rule) as g:
         g.set_state(seeded_state(g.elements, p, 9, amplitude=0.02))
         m0, e0 = g.mass_energy()
         for _ in range(50):
@@ -62,18 +65,26 @@ def test_mass_and_energy_conserved(p):
     assert abs(e1 - e0) <= 1e-13 * abs(e0)
 
 
-def test_vortex_accuracy_matches_plain():
+@pytest.mark.parametrize("p,rule", [(2, 0), (2, 2), (3, 3)])
+def test_vortex_accuracy_matches_plain(p, rule):
     """Isentropic vortex on a 64x64-quad mesh to t=0.5: the mixed form's L1
     density error is within 1.5x of the plain FP64 path's."""
     vortex = cases.IsentropicVortex()
     arrays = cases.vortex_mesh(64, seed=7)
     errors = {}
     for form in ("plain", "mixed"):
-        with wasl_b200.Solver(*arrays, polynomial_order=2, precision=form) as g:
+        with wasl_b200.Solver(*arrays, polynomial_order=p, precision=form,
+                              volume_rule_order=rule if form == "mixed" else 0) as g:
             cases.project_initial(g, vortex.conserved)
             steps, t = g.run(0.15, 0.0, 0.5)
             errors[form] = cases.l1_density_error(g, lambda x, y: vortex.conserved(x, y, t))
     assert errors["mixed"] <= 1.5 * errors["plain"]
+
+
+def test_rule_order_out_of_range_is_rejected():
+    arrays = meshgen.jittered_box(4, jitter=0.1, seed=1)
+    with pytest.raises(wasl_b200.WaslError, match="volume rule"):
+        wasl_b200.Solver(*arrays, polynomial_order=2, precision="mixed", volume_rule_order=5)
 
 
 def test_limited_mixed_runs_quadrant_riemann():

@@ -50,6 +50,7 @@ class Config(C.Structure):
         ("inflow_left", C.c_double), ("inflow_right", C.c_double), ("limiting", C.c_int),
         ("sensor_threshold", C.c_double), ("density_floor", C.c_double),
         ("pressure_floor", C.c_double), ("precision", C.c_int), ("device", C.c_int),
+        ("volume_rule_order", C.c_int),
     ]
 
 
@@ -138,7 +139,7 @@ class Solver:
                  equation="euler", polynomial_order=2, gamma=1.4, velocity=(0.0, 0.0),
                  boundary="periodic", boundary_right=None, inflow=(0.0, 0.0), limiting=False,
                  sensor_threshold=1e-3, density_floor=1e-10, pressure_floor=1e-10,
-                 precision="plain", device=0):
+                 precision="plain", device=0, volume_rule_order=0):
         lib = library()
         cfg = default_config()
         cfg.dimensions = dimensions
@@ -155,6 +156,7 @@ class Solver:
         cfg.pressure_floor = pressure_floor
         cfg.precision = PRECISIONS[precision]
         cfg.device = device
+        cfg.volume_rule_order = volume_rule_order
         self.config = cfg
         tags = np.ascontiguousarray(node_tags, dtype=np.int64)
         coords = np.ascontiguousarray(node_coordinates, dtype=np.float64)

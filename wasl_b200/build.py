@@ -23,7 +23,7 @@ LIB = os.path.join(HERE, "libwasl_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-COMMON = ["-O3", "-std=c++17", "-lineinfo", f"-I{INCLUDE}", f"-I{CSRC}",
+COMMON = ["-O3", "-std=c++20", "-lineinfo", f"-I{INCLUDE}", f"-I{CSRC}",
           "-Xcompiler", "-fPIC,-ffp-contract=off", "--expt-relaxed-constexpr"]
 
 # file -> extra flags

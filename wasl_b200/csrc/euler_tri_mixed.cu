@@ -29,25 +29,19 @@
 
 namespace wasl_b200 {
 
-// FP32 volume tables for modes 1..M-1 plus FP64 column sums of the reference
-// gradients (sigma_m = sum_q w_q D_m(q)).
-template <int P> struct MixedVolume {
-  static constexpr int M = TriShape<P>::M, QV = TriShape<P>::QV, H = M - 1;
+// FP32 volume tables for modes 1..M-1 on the collapsed rule of order R
+// ((R+1)^2 points, exact to degree 2R; the reference residual uses R = p+2).
+template <int P, int R> struct MixedVolume {
+  static constexpr int M = TriShape<P>::M, QV = (R + 1) * (R + 1), H = M - 1;
   float phi[QV][H > 0 ? H : 1];
   float dxi[QV][H > 0 ? H : 1];
   float deta[QV][H > 0 ? H : 1];
   float w[QV];
-  double wsum[3]; // FP64 sum of the reference edge weights of each local edge
 };
 
-__constant__ MixedVolume<1> c_mix1;
-__constant__ MixedVolume<2> c_mix2;
-__constant__ MixedVolume<3> c_mix3;
-
-template <int P> __device__ __forceinline__ const MixedVolume<P> &mixed_table();
-template <> __device__ __forceinline__ const MixedVolume<1> &mixed_table<1>() { return c_mix1; }
-template <> __device__ __forceinline__ const MixedVolume<2> &mixed_table<2>() { return c_mix2; }
-template <> __device__ __forceinline__ const MixedVolume<3> &mixed_table<3>() { return c_mix3; }
+template <int P, int R> __constant__ MixedVolume<P, R> c_mix;
+// FP64 sum of the reference edge weights of each local edge.
+template <int P> __constant__ double c_edge_wsum[3];
 
 // Primitive values of a cell average, FP64, with one reciprocal.
 struct MeanState {
@@ -272,7 +266,6 @@ __global__ void __launch_bounds__(128) euler_tri_faces_mixed(const StageArgs a) 
   const std::int64_t ne = a.mesh.ne;
   const double *__restrict__ in = a.in;
   const FaceTable<P, float> *F = &table;
-  const MixedVolume<P> &T = mixed_table<P>();
   const double gamma = a.gamma;
   const float gamma32 = static_cast<float>(gamma), g1 = static_cast<float>(gamma - 1.0);
   const std::int32_t L = a.faces.left[f], R = a.faces.right[f];
@@ -380,21 +373,21 @@ __global__ void __launch_bounds__(128) euler_tri_faces_mixed(const StageArgs a) 
 #pragma unroll
   for (int v = 0; v < 4; ++v)
     rec.mode0[v] = periodic_boundary ? a.boundary.value[v * a.boundary.count + (-R - 1)]
-                                     : fln[v] * T.wsum[le] + static_cast<double>(acc[v]);
+                                     : fln[v] * c_edge_wsum<P>[le] + static_cast<double>(acc[v]);
   static_cast<FaceRecord<P> *>(a.faces.record)[f] = rec;
 }
 
-template <int P>
+template <int P, int R>
 __global__ void __launch_bounds__(128) euler_tri_elements_mixed(const StageArgs a) {
   using S = TriShape<P>;
-  constexpr int M = S::M, QV = S::QV, QF = S::QF, H = M - 1;
+  constexpr int M = S::M, QV = MixedVolume<P, R>::QV, QF = S::QF, H = M - 1;
   constexpr double phi0 = 0.70710678118654752440;
   const std::int64_t ne = a.mesh.ne;
   const std::int64_t e = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (e >= ne)
     return;
   const double *__restrict__ in = a.in;
-  const MixedVolume<P> &T = mixed_table<P>();
+  const MixedVolume<P, R> &T = c_mix<P, R>;
   const FaceTable<P, float> *__restrict__ F = static_cast<const FaceTable<P, float> *>(a.face_table);
   const FaceRecord<P> *__restrict__ records = static_cast<const FaceRecord<P> *>(a.faces.record);
   const double gamma = a.gamma;
@@ -565,40 +558,76 @@ void check(cudaError_t rc, const char *what) {
     throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(rc));
 }
 
-template <int P> void upload_mixed(const void *symbol) {
-  static MixedVolume<P> t;
-  static VolumeTable<P, double> d;
-  fill_volume_table<P, double>(d);
-  constexpr int M = TriShape<P>::M, QV = TriShape<P>::QV;
+template <int P, int R> void upload_mixed() {
+  static MixedVolume<P, R> t;
+  constexpr int M = TriShape<P>::M, QV = MixedVolume<P, R>::QV;
+  const Rule2D rule = triangle_rule(R);
+  std::vector<double> gx, ge;
   for (int q = 0; q < QV; ++q) {
+    const auto b = dubiner(rule.xi[q], rule.eta[q], P);
+    dubiner_gradient(rule.xi[q], rule.eta[q], P, gx, ge);
     for (int m = 1; m < M; ++m) {
-      t.phi[q][m - 1] = static_cast<float>(d.phi[q][m]);
-      t.dxi[q][m - 1] = static_cast<float>(d.dxi[q][m]);
-      t.deta[q][m - 1] = static_cast<float>(d.deta[q][m]);
+      t.phi[q][m - 1] = static_cast<float>(b[m]);
+      t.dxi[q][m - 1] = static_cast<float>(gx[m]);
+      t.deta[q][m - 1] = static_cast<float>(ge[m]);
     }
-    t.w[q] = static_cast<float>(0.5 * d.w[q]);
+    t.w[q] = static_cast<float>(0.5 * rule.w[q]);
   }
+  check(cudaMemcpyToSymbol(c_mix<P, R>, &t, sizeof(t)), "upload mixed volume table");
   static FaceTable<P, double> f;
   fill_face_table<P, double>(f);
+  double wsum[3];
   for (int le = 0; le < 3; ++le) {
     double sum = 0.0;
     for (int q = 0; q < TriShape<P>::QF; ++q)
       sum += f.ew[le][q];
-    t.wsum[le] = sum;
+    wsum[le] = sum;
   }
-  check(cudaMemcpyToSymbol(symbol, &t, sizeof(t)), "upload mixed volume table");
+  check(cudaMemcpyToSymbol(c_edge_wsum<P>, wsum, sizeof(wsum)), "upload edge weight sums");
 }
 
-template <int P> void stage_mixed(const StageArgs &a, cudaStream_t s) {
+template <int P, int R> void stage_mixed(const StageArgs &a, cudaStream_t s) {
   if (a.boundary.count > 0 && a.mesh.boundary != 3 && !a.boundary.paired)
     boundary_mode0<P><<<static_cast<unsigned>((a.boundary.count + 127) / 128), 128, 0, s>>>(a);
   euler_tri_faces_mixed<P><<<static_cast<unsigned>((a.faces.count + 127) / 128), 128, 0, s>>>(a);
-  euler_tri_elements_mixed<P><<<static_cast<unsigned>((a.mesh.ne + 127) / 128), 128, 0, s>>>(a);
+  euler_tri_elements_mixed<P, R>
+      <<<static_cast<unsigned>((a.mesh.ne + 127) / 128), 128, 0, s>>>(a);
+}
+
+// Op<P, R>::run(args...) for a supported (p, rule order) pair.
+template <int P, int R> struct UploadMixed {
+  static void run() { upload_mixed<P, R>(); }
+};
+template <int P, int R> struct StageMixed {
+  static void run(const StageArgs &a, cudaStream_t s) { stage_mixed<P, R>(a, s); }
+};
+
+template <template <int, int> class Op, typename... A> void dispatch_mixed(int p, int rule, A &&...args) {
+  if (rule == 0)
+    rule = p + 2;
+  switch (p * 10 + rule) {
+  case 11: Op<1, 1>::run(args...); break;
+  case 12: Op<1, 2>::run(args...); break;
+  case 13: Op<1, 3>::run(args...); break;
+  case 22: Op<2, 2>::run(args...); break;
+  case 23: Op<2, 3>::run(args...); break;
+  case 24: Op<2, 4>::run(args...); break;
+  case 33: Op<3, 3>::run(args...); break;
+  case 34: Op<3, 4>::run(args...); break;
+  case 35: Op<3, 5>::run(args...); break;
+  default:
+    throw std::invalid_argument("mixed form: polynomial order must be 1..3 and the volume rule"
+                                " order p..p+2");
+  }
 }
 
 } // namespace
 
-bool euler_tri_mixed_supported(int p) { return p >= 1 && p <= 3; }
+bool euler_tri_mixed_supported(int p, int rule) {
+  if (rule == 0)
+    rule = p + 2;
+  return p >= 1 && p <= 3 && rule >= p && rule <= p + 2;
+}
 
 std::size_t euler_tri_mixed_face_record_bytes(int p) {
   switch (p) {
@@ -609,22 +638,12 @@ std::size_t euler_tri_mixed_face_record_bytes(int p) {
   }
 }
 
-void upload_euler_tri_tables_mixed(int p) {
-  switch (p) {
-  case 1: upload_mixed<1>(reinterpret_cast<const void *>(&c_mix1)); break;
-  case 2: upload_mixed<2>(reinterpret_cast<const void *>(&c_mix2)); break;
-  case 3: upload_mixed<3>(reinterpret_cast<const void *>(&c_mix3)); break;
-  default: throw std::invalid_argument("mixed form: polynomial order must be 1..3");
-  }
+void upload_euler_tri_tables_mixed(int p, int rule) {
+  dispatch_mixed<UploadMixed>(p, rule);
 }
 
-void launch_euler_tri_stage_mixed(int p, const StageArgs &a, cudaStream_t s) {
-  switch (p) {
-  case 1: stage_mixed<1>(a, s); break;
-  case 2: stage_mixed<2>(a, s); break;
-  case 3: stage_mixed<3>(a, s); break;
-  default: throw std::invalid_argument("mixed form: polynomial order must be 1..3");
-  }
+void launch_euler_tri_stage_mixed(int p, int rule, const StageArgs &a, cudaStream_t s) {
+  dispatch_mixed<StageMixed>(p, rule, a, s);
 }
 
 } // namespace wasl_b200

@@ -59,8 +59,9 @@ public:
         M_(tri_modes(cfg.polynomial_order)) {
     if (!euler_tri_order_supported(p_))
       throw SolverError(WASL_ERR_ARGUMENT, "2D Euler: polynomial order must be 0..3");
-    if (cfg.precision == WASL_MIXED && !euler_tri_mixed_supported(p_))
-      throw SolverError(WASL_ERR_ARGUMENT, "2D Euler mixed form: polynomial order must be 1..3");
+    if (cfg.precision == WASL_MIXED && !euler_tri_mixed_supported(p_, cfg.volume_rule_order))
+      throw SolverError(WASL_ERR_ARGUMENT, "2D Euler mixed form: polynomial order must be 1..3"
+                                           " and the volume rule order p..p+2");
     if (cfg.precision != WASL_PLAIN_FP64 && cfg.precision != WASL_MIXED)
       throw SolverError(WASL_ERR_ARGUMENT, "unknown precision form");
     cuda_check(cudaSetDevice(cfg.device), "cudaSetDevice");
@@ -115,7 +116,7 @@ public:
     }
     mixed_ = cfg.precision == WASL_MIXED;
     if (mixed_)
-      upload_euler_tri_tables_mixed(p_);
+      upload_euler_tri_tables_mixed(p_, cfg.volume_rule_order);
     else
       upload_euler_tri_tables_f64(p_);
     std::vector<unsigned char> table(euler_tri_face_table_bytes(p_, mixed_));
@@ -373,7 +374,7 @@ private:
         cuda_check(cudaMemsetAsync(d_count_.get(), 0, sizeof(std::int32_t), stream_), "count");
       stage_begin();
       if (mixed_)
-        launch_euler_tri_stage_mixed(p_, a, stream_);
+        launch_euler_tri_stage_mixed(p_, cfg_.volume_rule_order, a, stream_);
       else
         launch_euler_tri_stage_f64(p_, a, stream_);
       stage_end();

@@ -184,10 +184,12 @@ void upload_euler_tri_tables_f64(int p);
 std::size_t euler_tri_face_table_bytes(int p, bool fp32);
 void fill_euler_tri_face_table(int p, bool fp32, void *host_buffer);
 void launch_euler_tri_stage_f64(int p, const StageArgs &a, cudaStream_t stream);
-bool euler_tri_mixed_supported(int p);
-void upload_euler_tri_tables_mixed(int p);
+// The mixed form's volume rule: the collapsed rule of order `rule` (p..p+2;
+// 0 means p+2, the reference residual's rule).
+bool euler_tri_mixed_supported(int p, int rule);
+void upload_euler_tri_tables_mixed(int p, int rule);
 std::size_t euler_tri_mixed_face_record_bytes(int p);
-void launch_euler_tri_stage_mixed(int p, const StageArgs &a, cudaStream_t stream);
+void launch_euler_tri_stage_mixed(int p, int rule, const StageArgs &a, cudaStream_t stream);
 void launch_limit_f64(int M, int NB, const LimitArgs &a, cudaStream_t stream);
 void launch_sense_f64(int M, const SenseArgs &a, cudaStream_t stream);
 void launch_cfl(const CflArgs &a, cudaStream_t stream);
