@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--p", type=int, default=2)
     ap.add_argument("--rule", type=int, default=None,
                     help="mixed form's volume rule order (default p; the reference uses p+2)")
+    ap.add_argument("--kernel", type=int, default=0,
+                    help="mixed form's kernel: 0 autotuned, 1 face-centric, 2+s tile shape s")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -134,7 +136,8 @@ def build_solver(args, form, device):
     arrays = cases.vortex_mesh(args.n)
     vortex = cases.IsentropicVortex()
     g = wasl_b200.Solver(*arrays, polynomial_order=args.p, precision=form, device=device,
-                         volume_rule_order=rule_order(args, form))
+                         volume_rule_order=rule_order(args, form),
+                         mixed_kernel=args.kernel if form == "mixed" else 0)
     cases.project_initial(g, vortex.conserved)
     return g, vortex
 
@@ -294,6 +297,7 @@ def ours(args, rank, world, local_rank):
                    "form": "plain-fp64" if form == "plain" else "mixed-precision",
                    "volume_rule": (f"collapsed order {rule_order(args, form) or args.p + 2}"
                                    f" ({((rule_order(args, form) or args.p + 2) + 1) ** 2} points)"),
+                   "kernel": kernel_description(g.tuning()),
                    "elements": g.elements, "dof": dofs, "parallelism": f"replicas x{world}",
                    "l2": "flushed between timed steps (256 MiB write)"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
@@ -324,6 +328,19 @@ def ours(args, rank, world, local_rank):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def kernel_description(tuning):
+    choice, ms = tuning
+    names = ["face-centric (face + element kernels)", "tile 128 el/CTA, <=128 regs",
+             "tile 128 el/CTA, uncapped regs", "tile 256 el/CTA, <=128 regs",
+             "tile 64 el/CTA, <=128 regs"]
+    if choice < 0:
+        return {"name": "single stage kernel"}
+    out = {"name": names[choice] if choice < len(names) else str(choice)}
+    if ms:
+        out["autotuned_stage_ms"] = {names[i]: round(t, 5) for i, t in enumerate(ms)}
+    return out
 
 
 def stream_of(g, torch):

@@ -78,6 +78,9 @@ typedef struct {
   int device;                /* CUDA device ordinal */
   int volume_rule_order;     /* mixed form: order r of the collapsed (r+1)^2-point volume
                                 rule, p..p+2; 0 = p+2, the reference residual's rule */
+  int mixed_kernel;          /* mixed form: 0 autotuned; 1 face-centric kernels (face pass
+                                + element pass); 2 + s the fused tile kernel in launch
+                                shape s (0..3, see wasl_gpu_tuning) */
 } wasl_gpu_config;
 
 /* Fill the reference's defaults (crates/wasl-bridge/src/config.rs:87-104). */
@@ -154,6 +157,16 @@ int wasl_gpu_run(wasl_gpu *handle, double cfl, double start_time, double end_tim
 /* Device-resident fast path: `steps` steps with the CFL step computed on the
  * device each step, no host synchronization (capturable in a CUDA graph). */
 int wasl_gpu_advance(wasl_gpu *handle, double cfl, int64_t steps);
+
+/* The mixed form's kernel in use: 0 face-centric kernels, 1 + s the fused
+ * tile kernel in launch shape s (0: 128 elements per CTA at <= 128 registers
+ * a thread; 1: 128, no register cap; 2: 256 at <= 128; 3: 64 at <= 128);
+ * -1 for forms with a single kernel or before the first step.  When the
+ * choice was autotuned (mixed_kernel 0: every variant timed on the solver's
+ * own state before its first step, the fastest kept for the process per
+ * polynomial order, rule order and mesh size class), `ms` receives up to
+ * `capacity` per-variant stage times and `count` their number. */
+int wasl_gpu_tuning(const wasl_gpu *handle, int *choice, double *ms, int capacity, int *count);
 
 /* Device pointer of the state U[variable][mode][element] and the handle's
  * CUDA stream (cudaStream_t), for callers that keep data on the device. */

@@ -12,6 +12,9 @@ from wasl_b200 import cases, meshgen
 
 pytestmark = pytest.mark.gpu
 
+# mixed_kernel: 1 face-centric kernels, 2 + s the fused tile kernel in shape s.
+KERNELS = [1, 2, 3, 4, 5]
+
 
 def pair(arrays, p, **kw):
     return (wasl_b200.Solver(*arrays, polynomial_order=p, precision="plain", **kw),
@@ -51,11 +54,14 @@ def test_one_step_close_to_plain(p):
     assert np.max(np.abs(a - b)) <= 1e-6 * change
 
 
-@pytest.mark.parametrize("p,rule", [(p, r) for p in (1, 2, 3) for r in (0, p)])
-def test_mass_and_energy_conserved(p, rule):
+@pytest.mark.parametrize("p,rule,kernel", [(p, r, k) for p in (1, 2, 3) for r in (0, p)
+                                           for k in (1, 2)] + [(2, 2, k) for k in (3, 4, 5)])
+def test_mass_and_energy_conserved(p, rule, kernel):
+    """Periodic faces paired, interior faces evaluated by both sides with the
+    same instructions: totals conserved to FP64 round-off."""
     arrays = meshgen.jittered_box(16, jitter=0.15, seed=4)
     with wasl_b200.Solver(*arrays, polynomial_order=p, precision="mixed",
-                          volume_rule_order=rule) as g:
+                          volume_rule_order=rule, mixed_kernel=kernel) as g:
         g.set_state(seeded_state(g.elements, p, 9, amplitude=0.02))
         m0, e0 = g.mass_energy()
         for _ in range(50):
@@ -101,3 +107,56 @@ def test_limited_mixed_runs_quadrant_riemann():
         state = g.get_state().reshape(4, g.modes, g.elements)
     assert flags.sum() > 0
     assert np.all(state[0, 0] > 0)
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+@pytest.mark.parametrize("kernel", [2, 3, 4, 5])
+@pytest.mark.parametrize("boundary", ["periodic", "transmissive"])
+def test_tile_kernel_matches_face_centric(p, kernel, boundary):
+    """The fused tile kernel computes the face-centric form's arithmetic (up
+    to FP32 contraction order): after three steps the states differ by at most
+    1e-6 of the change the steps made."""
+    arrays = meshgen.jittered_box(20, jitter=0.15, seed=20 + p)
+    c = seeded_state(2 * 20 * 20, p, 40 + p, amplitude=0.02)
+    out = {}
+    for k in (1, kernel):
+        with wasl_b200.Solver(*arrays, polynomial_order=p, precision="mixed", mixed_kernel=k,
+                              boundary=boundary) as g:
+            g.set_state(c)
+            for _ in range(3):
+                g.step(g.stable_dt(0.15))
+            out[k] = g.get_state()
+            assert g.tuning()[0] == k - 1
+    change = np.max(np.abs(out[1] - c))
+    assert np.max(np.abs(out[kernel] - out[1])) <= 1e-6 * change
+
+
+def test_uniform_flow_tile_transmissive():
+    arrays = meshgen.jittered_box(12, jitter=0.15, seed=5)
+    with wasl_b200.Solver(*arrays, polynomial_order=2, precision="mixed", mixed_kernel=2,
+                          boundary="transmissive") as g:
+        state = np.zeros((4, g.modes, g.elements))
+        state[:, 0] = np.sqrt(2) * np.array([0.8, -0.2, 0.5, 2.0])[:, None]
+        g.set_state(state.ravel())
+        for _ in range(10):
+            g.step(g.stable_dt(0.2))
+        out = g.get_state().reshape(state.shape)
+    assert np.max(np.abs(out - state)) <= 2e-13
+
+
+def test_autotuner_times_every_variant():
+    """mixed_kernel 0: the first step times the face-centric kernels and every
+    tile shape and keeps the fastest; later solvers of the same class reuse it."""
+    arrays = cases.vortex_mesh(32, seed=3)
+    vortex = cases.IsentropicVortex()
+    with wasl_b200.Solver(*arrays, polynomial_order=2, precision="mixed") as g:
+        assert g.tuning()[0] == -1
+        cases.project_initial(g, vortex.conserved)
+        g.step(g.stable_dt(0.15))
+        choice, ms = g.tuning()
+    assert len(ms) == 5 and all(t > 0 for t in ms)
+    assert 0 <= choice < 5 and ms[choice] == min(ms)
+    with wasl_b200.Solver(*arrays, polynomial_order=2, precision="mixed") as g:
+        cases.project_initial(g, vortex.conserved)
+        g.step(g.stable_dt(0.15))
+        assert g.tuning() == (choice, ms)

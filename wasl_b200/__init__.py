@@ -50,7 +50,7 @@ class Config(C.Structure):
         ("inflow_left", C.c_double), ("inflow_right", C.c_double), ("limiting", C.c_int),
         ("sensor_threshold", C.c_double), ("density_floor", C.c_double),
         ("pressure_floor", C.c_double), ("precision", C.c_int), ("device", C.c_int),
-        ("volume_rule_order", C.c_int),
+        ("volume_rule_order", C.c_int), ("mixed_kernel", C.c_int),
     ]
 
 
@@ -86,6 +86,8 @@ SIGNATURES = {
     "wasl_gpu_advance": (C.c_int, [C.c_void_p, C.c_double, C.c_int64]),
     "wasl_gpu_state_device": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "wasl_gpu_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "wasl_gpu_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), _d, C.c_int,
+                                  C.POINTER(C.c_int)]),
     "wasl_gpu_profile_begin": (C.c_int, [C.c_void_p]),
     "wasl_gpu_profile_end": (C.c_int, [C.c_void_p, _d, _i64, _i64]),
     "wasl_gpu_write_checkpoint": (C.c_int, [C.c_void_p, C.c_char_p, C.c_double, C.c_uint64,
@@ -139,7 +141,7 @@ class Solver:
                  equation="euler", polynomial_order=2, gamma=1.4, velocity=(0.0, 0.0),
                  boundary="periodic", boundary_right=None, inflow=(0.0, 0.0), limiting=False,
                  sensor_threshold=1e-3, density_floor=1e-10, pressure_floor=1e-10,
-                 precision="plain", device=0, volume_rule_order=0):
+                 precision="plain", device=0, volume_rule_order=0, mixed_kernel=0):
         lib = library()
         cfg = default_config()
         cfg.dimensions = dimensions
@@ -157,6 +159,7 @@ class Solver:
         cfg.precision = PRECISIONS[precision]
         cfg.device = device
         cfg.volume_rule_order = volume_rule_order
+        cfg.mixed_kernel = mixed_kernel
         self.config = cfg
         tags = np.ascontiguousarray(node_tags, dtype=np.int64)
         coords = np.ascontiguousarray(node_coordinates, dtype=np.float64)
@@ -287,6 +290,14 @@ class Solver:
         return s.value or 0
 
     # ---- measurement ------------------------------------------------------------
+    def tuning(self):
+        """(kernel choice, per-variant stage ms) of the mixed form; see wasl_gpu_tuning."""
+        choice, count = C.c_int(), C.c_int()
+        ms = np.zeros(16)
+        self._check(self._lib.wasl_gpu_tuning(self._h, C.byref(choice), _ptr(ms), len(ms),
+                                              C.byref(count)))
+        return choice.value, ms[:count.value].tolist()
+
     def profile_begin(self):
         self._check(self._lib.wasl_gpu_profile_begin(self._h))
 

@@ -42,6 +42,7 @@ SOURCES = {
     "capi.cpp": [],
     "profiling.cpp": [],
     "cfl_static.cu": [],
+    "autotune.cpp": [],
 }
 HEADERS = [f for f in os.listdir(CSRC) if f.endswith((".hpp", ".cuh", ".h"))]
 

@@ -297,6 +297,15 @@ int wasl_gpu_stream(wasl_gpu *h, void **s) {
   });
 }
 
+int wasl_gpu_tuning(const wasl_gpu *h, int *choice, double *ms, int capacity, int *count) {
+  return guarded(const_cast<wasl_gpu *>(h), [&] {
+    need(choice && count && (ms || capacity <= 0), "tuning: null output");
+    int n = 0;
+    *choice = h->solver->kernel_choice(ms, capacity, n);
+    *count = n;
+  });
+}
+
 int wasl_gpu_profile_begin(wasl_gpu *h) {
   return guarded(h, [&] { h->solver->profile_begin(); });
 }

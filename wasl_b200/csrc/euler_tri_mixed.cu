@@ -43,7 +43,10 @@ template <int P, int R> __constant__ MixedVolume<P, R> c_mix;
 // FP64 sum of the reference edge weights of each local edge.
 template <int P> __constant__ double c_edge_wsum[3];
 
-// Primitive values of a cell average, FP64, with one reciprocal.
+// Primitive values of a cell average, FP64, with one reciprocal.  Written
+// with explicit round-to-nearest operations (no multiply-add contraction), so
+// every call site produces the same bits: the two sides of a face evaluate it
+// independently in the tile kernel and must agree exactly.
 struct MeanState {
   double rho, mx, my, e, u, v, p, h; // h = E + p
 };
@@ -55,21 +58,22 @@ __device__ __forceinline__ MeanState mean_state(double gamma, const double *s) {
   m.my = s[2];
   m.e = s[3];
   const double inv = 1.0 / s[0];
-  m.u = s[1] * inv;
-  m.v = s[2] * inv;
-  m.p = (gamma - 1.0) * (s[3] - 0.5 * (s[1] * m.u + s[2] * m.v));
-  m.h = s[3] + m.p;
+  m.u = __dmul_rn(s[1], inv);
+  m.v = __dmul_rn(s[2], inv);
+  const double kinetic = __dmul_rn(0.5, __dadd_rn(__dmul_rn(s[1], m.u), __dmul_rn(s[2], m.v)));
+  m.p = __dmul_rn(gamma - 1.0, __dsub_rn(s[3], kinetic));
+  m.h = __dadd_rn(s[3], m.p);
   return m;
 }
 
-// Physical flux of a cell average along n, FP64.
+// Physical flux of a cell average along n, FP64 (explicit rounding as above).
 __device__ __forceinline__ void mean_normal_flux(const MeanState &m, double nx, double ny,
                                                  double *f) {
-  const double un = m.u * nx + m.v * ny;
-  f[0] = m.rho * un;
-  f[1] = m.mx * un + m.p * nx;
-  f[2] = m.my * un + m.p * ny;
-  f[3] = m.h * un;
+  const double un = __dadd_rn(__dmul_rn(m.u, nx), __dmul_rn(m.v, ny));
+  f[0] = __dmul_rn(m.rho, un);
+  f[1] = __dadd_rn(__dmul_rn(m.mx, un), __dmul_rn(m.p, nx));
+  f[2] = __dadd_rn(__dmul_rn(m.my, un), __dmul_rn(m.p, ny));
+  f[3] = __dmul_rn(m.h, un);
 }
 
 // HLLC in FP64 with shared reciprocals: the flux of hllc() with fewer divisions.
@@ -551,6 +555,301 @@ __global__ void __launch_bounds__(128) euler_tri_elements_mixed(const StageArgs 
   }
 }
 
+// FP32 trace of high modes h at one edge point: sum_m h[v][m] basis[m+1],
+// with explicit fused multiply-adds so both sides of a face get the same bits.
+template <int P>
+__device__ __forceinline__ void high_trace(const float (&h)[4][TriShape<P>::M - 1],
+                                           const float *basis, float *out) {
+  constexpr int H = TriShape<P>::M - 1;
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    float s = 0.0f;
+#pragma unroll
+    for (int m = 0; m < H; ++m)
+      s = fmaf(h[v][m], basis[m + 1], s);
+    out[v] = s;
+  }
+}
+
+// The fused mixed stage on a tile of TILE consecutive elements per CTA.
+// The tile's state is staged in shared memory (FP64 means, FP32 high modes)
+// with asynchronous copies; each thread then computes its element's volume
+// term and all three of its faces, reading a neighbour inside the tile from
+// shared memory and one outside it from global memory (L2).  Each face is
+// evaluated by both of its elements with the same instructions on the same
+// inputs (the HLLC perturbation is always taken around the face's left mean),
+// so the two mode-0 contributions cancel exactly, as in the face-centric form.
+// MINB: resident CTAs per SM the register budget is sized for (1: no cap).
+template <int P, int R, int TILE, int MINB>
+__global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_mixed(const StageArgs a) {
+  using S = TriShape<P>;
+  constexpr int M = S::M, QV = MixedVolume<P, R>::QV, QF = S::QF, H = M - 1;
+  constexpr double phi0 = 0.70710678118654752440;
+  __shared__ FaceTable<P, float> table;
+  // The tile's FP64 state, row v M + m (dynamic shared memory, 4 M TILE doubles).
+  extern __shared__ __align__(16) double tile_state[];
+  double(*sstate)[TILE] = reinterpret_cast<double(*)[TILE]>(tile_state);
+
+  std::int64_t first, count;
+  int case_id = 0;
+  if (a.work) {
+    const TileWork w = a.work[blockIdx.x];
+    first = w.first;
+    count = w.count;
+    case_id = w.case_id;
+  } else {
+    first = static_cast<std::int64_t>(blockIdx.x) * TILE;
+    count = a.mesh.ne - first < TILE ? a.mesh.ne - first : TILE;
+  }
+  const int t = threadIdx.x;
+  const bool active = t < count;
+  const std::int64_t ne = a.mesh.ne;
+  const std::int64_t e = first + t;
+  const double *__restrict__ in = a.in;
+
+  // Stage this tile's state (asynchronous 8-byte copies, coalesced per row)
+  // and the face tables.
+  if (active) {
+    const unsigned base = static_cast<unsigned>(__cvta_generic_to_shared(&sstate[0][t]));
+#pragma unroll
+    for (int r = 0; r < 4 * M; ++r)
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(base + r * TILE * 8),
+                   "l"(in + r * ne + e)
+                   : "memory");
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  {
+    const float *src = static_cast<const float *>(a.face_table);
+    float *dst = reinterpret_cast<float *>(&table);
+    for (int i = t; i < static_cast<int>(sizeof(table) / sizeof(float)); i += TILE)
+      dst[i] = src[i];
+  }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncthreads();
+  if (!active)
+    return;
+  double mean[4];
+  float ch[4][H];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    mean[v] = sstate[v * M][t] * phi0;
+#pragma unroll
+    for (int m = 0; m < H; ++m)
+      ch[v][m] = static_cast<float>(sstate[v * M + m + 1][t]);
+  }
+
+  const MixedVolume<P, R> &T = c_mix<P, R>;
+  const double gamma = a.gamma;
+  const float gamma32 = static_cast<float>(gamma), g1 = static_cast<float>(gamma - 1.0);
+  const double *__restrict__ geo = a.mesh.geo;
+  const MeanState own = mean_state(gamma, mean);
+  const Ref32 bb = ref32(own);
+
+  // Volume term of the high modes (perturbation flux, as in the element kernel).
+  float racc[4][H];
+#pragma unroll
+  for (int v = 0; v < 4; ++v)
+#pragma unroll
+    for (int m = 0; m < H; ++m)
+      racc[v][m] = 0.0f;
+  {
+    const float fax = static_cast<float>(geo[e]), fay = static_cast<float>(geo[ne + e]);
+    const float fbx = static_cast<float>(geo[2 * ne + e]), fby = static_cast<float>(geo[3 * ne + e]);
+#pragma unroll 3
+    for (int q = 0; q < QV; ++q) {
+      float d[4];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        float s = 0.0f;
+#pragma unroll
+        for (int m = 0; m < H; ++m)
+          s = fmaf(ch[v][m], T.phi[q][m], s);
+        d[v] = s;
+      }
+      const float inv = __frcp_rn(bb.rho + d[0]);
+      const float du = (d[1] - bb.u * d[0]) * inv;
+      const float dv = (d[2] - bb.v * d[0]) * inv;
+      const float uu = bb.u + du, vv = bb.v + dv;
+      const float dmu = bb.mx * du + d[1] * uu + bb.my * dv + d[2] * vv;
+      const float dp = g1 * (d[3] - 0.5f * dmu);
+      const float dep = d[3] + dp;
+      const float fx[4] = {d[1], bb.mx * du + d[1] * uu + dp, bb.my * du + d[2] * uu,
+                           bb.h * du + dep * uu};
+      const float fy[4] = {d[2], bb.mx * dv + d[1] * vv, bb.my * dv + d[2] * vv + dp,
+                           bb.h * dv + dep * vv};
+      const float w = T.w[q];
+      const float wby = w * fby, wbx = w * fbx, wax = w * fax, way = w * fay;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const float gxi = wby * fx[v] - wbx * fy[v];
+        const float geta = wax * fy[v] - way * fx[v];
+#pragma unroll
+        for (int m = 0; m < H; ++m)
+          racc[v][m] = fmaf(T.dxi[q][m], gxi, fmaf(T.deta[q][m], geta, racc[v][m]));
+      }
+    }
+  }
+
+  // The three faces, in the element's slot order.
+  double r0[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 1
+  for (int k = 0; k < 3; ++k) {
+    const std::int64_t slot = k * ne + e;
+    const unsigned code = a.tile.code[slot];
+    const std::int32_t nb = a.tile.nbr[slot];
+    const bool self_left = code & 1u;
+    const int le = (code >> 1) & 3u, re = (code >> 3) & 3u, flip = (code >> 5) & 1u;
+    const double nx = a.mesh.slot_geo[(3 * k) * ne + e];
+    const double ny = a.mesh.slot_geo[(3 * k + 1) * ne + e];
+    const double scale = a.mesh.slot_geo[(3 * k + 2) * ne + e];
+    const float *lb = &table.lb[le][0][0];
+    const float *rb = &table.rb[(le * 3 + re) * 2 + flip][0][0];
+    const float *own_basis = self_left ? lb : rb;
+    const float *other_basis = self_left ? rb : lb;
+    if (code & 0xC0u) {
+      const float *periodic = a.boundary.basis32 + static_cast<std::int64_t>(a.tile.aux[slot]) * QF * M;
+      if (code & 0x40u)
+        own_basis = periodic;
+      else
+        other_basis = periodic;
+    }
+    // The element across the face: its mean and high modes.
+    double nmean[4] = {0.0, 0.0, 0.0, 0.0};
+    float nh[4][H];
+    const bool boundary = nb < 0;
+    if (!boundary) {
+      const std::int64_t local = nb - first;
+      if (local >= 0 && local < count) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          nmean[v] = sstate[v * M][local] * phi0;
+#pragma unroll
+          for (int m = 0; m < H; ++m)
+            nh[v][m] = static_cast<float>(sstate[v * M + m + 1][local]);
+        }
+      } else {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          const double *row = in + static_cast<std::int64_t>(v) * M * ne + nb;
+          nmean[v] = __ldg(row) * phi0;
+#pragma unroll
+          for (int m = 0; m < H; ++m)
+            nh[v][m] = static_cast<float>(__ldg(row + (m + 1) * ne));
+        }
+      }
+    }
+    // The face's left state is the reference of the perturbation form.
+    MeanState ml;
+    if (self_left)
+      ml = own;
+    else
+      ml = mean_state(gamma, nmean);
+    const Ref32 ref = ref32(ml);
+    double fln[4];
+    mean_normal_flux(ml, nx, ny, fln);
+    float jump[4], shift[4];
+    if (boundary) {
+#pragma unroll
+      for (int v = 0; v < 4; ++v)
+        jump[v] = shift[v] = 0.0f;
+    } else {
+#pragma unroll
+      for (int v = 0; v < 4; ++v)
+        jump[v] = static_cast<float>(self_left ? nmean[v] - mean[v] : mean[v] - nmean[v]);
+      if (!self_left) {
+        double frn[4];
+        mean_normal_flux(own, nx, ny, frn);
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+          shift[v] = static_cast<float>(fln[v] - frn[v]);
+      }
+    }
+    const float nxf = static_cast<float>(nx), nyf = static_cast<float>(ny);
+    const float fscale = static_cast<float>(scale);
+    float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int q = 0; q < QF; ++q) {
+      float to[4], tn[4], dl[4], dr[4], fl[4];
+      high_trace<P>(ch, own_basis + q * M, to);
+      if (boundary) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+          dl[v] = dr[v] = to[v];
+      } else {
+        high_trace<P>(nh, other_basis + q * M, tn);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          dl[v] = self_left ? to[v] : tn[v];
+          dr[v] = jump[v] + (self_left ? tn[v] : to[v]);
+        }
+      }
+      hllc_perturbed(ref, dl, dr, g1, gamma32, nxf, nyf, fl);
+      const float w = table.ew[le][q];
+      const float wsc = (self_left ? -w : w) * fscale;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        acc[v] = fmaf(w, fl[v], acc[v]);
+        const float value = wsc * (self_left ? fl[v] : fl[v] + shift[v]);
+#pragma unroll
+        for (int m = 0; m < H; ++m)
+          racc[v][m] = fmaf(value, own_basis[q * M + m + 1], racc[v][m]);
+      }
+    }
+    const double sgn = self_left ? -1.0 : 1.0;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const double mode0 = fln[v] * c_edge_wsum<P>[le] + static_cast<double>(acc[v]);
+      r0[v] += sgn * scale * phi0 * mode0;
+    }
+  }
+
+  const double inv = geo[4 * ne + e];
+  const double dt = a.case_dt ? a.case_dt[case_id] : (a.dt ? *a.dt : a.dt_value);
+  double rho[M];
+#pragma unroll
+  for (int v = 0; v < 4; ++v)
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const std::int64_t idx = (static_cast<std::int64_t>(v) * M + m) * ne + e;
+      const double cur = sstate[v * M + m][t];
+      const double rr = (m == 0 ? r0[v] : static_cast<double>(racc[v][m > 0 ? m - 1 : 0])) * inv;
+      double o;
+      if (a.stage == 0)
+        o = cur + dt * rr;
+      else if (a.stage == 1)
+        o = 0.75 * a.u0[idx] + 0.25 * (cur + dt * rr);
+      else
+        o = (1.0 / 3.0) * a.u0[idx] + (2.0 / 3.0) * (cur + dt * rr);
+      a.out[idx] = o;
+      if (v == 0)
+        rho[m] = o;
+    }
+
+  if (a.sense) {
+    double total = 0.0, high = 0.0;
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      total += rho[m] * rho[m];
+      if (m >= a.highest_degree_begin)
+        high += rho[m] * rho[m];
+    }
+    const bool troubled = !(total == 0.0 || high / total <= a.threshold);
+    a.flags[e] = troubled ? 1 : 0;
+    const unsigned active_mask = __activemask();
+    const unsigned ballot = __ballot_sync(active_mask, troubled);
+    if (ballot) {
+      const int lane = threadIdx.x & 31;
+      const int leader = __ffs(ballot) - 1;
+      int base = 0;
+      if (lane == leader)
+        base = atomicAdd(a.troubled_count, __popc(ballot));
+      base = __shfl_sync(active_mask, base, leader);
+      if (troubled)
+        a.troubled[base + __popc(ballot & ((1u << lane) - 1u))] = static_cast<std::int32_t>(e);
+    }
+  }
+}
+
 namespace {
 
 void check(cudaError_t rc, const char *what) {
@@ -593,6 +892,45 @@ template <int P, int R> void stage_mixed(const StageArgs &a, cudaStream_t s) {
   euler_tri_elements_mixed<P, R>
       <<<static_cast<unsigned>((a.mesh.ne + 127) / 128), 128, 0, s>>>(a);
 }
+
+template <int P, int R, int TILE, int MINB> void stage_tile(const StageArgs &a, cudaStream_t s) {
+  const std::size_t smem = sizeof(double) * 4 * TriShape<P>::M * TILE;
+  // Static (face table) plus dynamic shared memory above the default 48 KiB
+  // needs the opt-in attribute, set once per device.
+  if (smem + sizeof(FaceTable<P, float>) > 48 * 1024) {
+    static bool opted_in[64] = {};
+    int device = 0;
+    check(cudaGetDevice(&device), "cudaGetDevice");
+    if (device >= 64 || !opted_in[device]) {
+      check(cudaFuncSetAttribute(euler_tri_tile_mixed<P, R, TILE, MINB>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)),
+            "tile kernel shared memory");
+      if (device < 64)
+        opted_in[device] = true;
+    }
+  }
+  const std::int64_t blocks = a.work ? a.work_count : (a.mesh.ne + TILE - 1) / TILE;
+  if (blocks > 0)
+    euler_tri_tile_mixed<P, R, TILE, MINB><<<static_cast<unsigned>(blocks), TILE, smem, s>>>(a);
+}
+
+// Launch shapes of the tile kernel (elements per CTA, register budget):
+//   0: 128 elements, <= 128 registers (4 CTAs / 16 warps per SM)
+//   1: 128 elements, no register cap
+//   2: 256 elements, <= 128 registers (2 CTAs per SM)
+//   3:  64 elements, <= 128 registers (8 CTAs per SM)
+template <int P, int R> struct StageTile {
+  static void run(int shape, const StageArgs &a, cudaStream_t s) {
+    switch (shape) {
+    case 0: stage_tile<P, R, 128, 4>(a, s); break;
+    case 1: stage_tile<P, R, 128, 1>(a, s); break;
+    case 2: stage_tile<P, R, 256, 2>(a, s); break;
+    case 3: stage_tile<P, R, 64, 8>(a, s); break;
+    default: throw std::invalid_argument("tile kernel: unknown launch shape");
+    }
+  }
+};
 
 // Op<P, R>::run(args...) for a supported (p, rule order) pair.
 template <int P, int R> struct UploadMixed {
@@ -640,6 +978,17 @@ std::size_t euler_tri_mixed_face_record_bytes(int p) {
 
 void upload_euler_tri_tables_mixed(int p, int rule) {
   dispatch_mixed<UploadMixed>(p, rule);
+}
+
+int euler_tri_tile_shapes() { return 4; }
+
+int euler_tri_tile_elements(int shape) {
+  static const int elements[4] = {128, 128, 256, 64};
+  return shape >= 0 && shape < 4 ? elements[shape] : 0;
+}
+
+void launch_euler_tri_stage_tile(int p, int rule, int shape, const StageArgs &a, cudaStream_t s) {
+  dispatch_mixed<StageTile>(p, rule, shape, a, s);
 }
 
 void launch_euler_tri_stage_mixed(int p, int rule, const StageArgs &a, cudaStream_t s) {

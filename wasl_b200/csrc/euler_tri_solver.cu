@@ -10,6 +10,7 @@
 #include <cstring>
 #include <map>
 
+#include "autotune.hpp"
 #include "basis.hpp"
 #include "kernels.hpp"
 #include "mesh.hpp"
@@ -99,6 +100,14 @@ public:
       paired_ = pair_periodic_faces(QF, donors, donor_basis, face_code, slot_face, slot_code,
                                     slot_geo, left_slot);
     if (cfg.precision == WASL_MIXED) {
+      if (cfg.mixed_kernel < 0 || cfg.mixed_kernel > 1 + euler_tri_tile_shapes())
+        throw SolverError(WASL_ERR_ARGUMENT, "2D Euler mixed form: unknown kernel choice");
+      tile_ok_ = boundary_count_ == 0 || boundary_ == WASL_TRANSMISSIVE || paired_;
+      if (cfg.mixed_kernel >= 2 && !tile_ok_)
+        throw SolverError(WASL_ERR_ARGUMENT, "2D Euler mixed form: the tile kernel needs"
+                                             " transmissive or paired periodic boundaries");
+      if (tile_ok_)
+        build_tile_slots(t, QF);
       d_face_left_.upload(mesh_.face_left, stream_);
       d_face_right_.upload(face_right, stream_);
       d_face_code_.upload(face_code, stream_);
@@ -115,6 +124,8 @@ public:
       d_donor_basis_.upload(donor_basis, stream_);
     }
     mixed_ = cfg.precision == WASL_MIXED;
+    if (mixed_ && cfg.mixed_kernel >= 1)
+      kernel_ = cfg.mixed_kernel - 1;
     if (mixed_)
       upload_euler_tri_tables_mixed(p_, cfg.volume_rule_order);
     else
@@ -302,6 +313,13 @@ public:
     check_error();
   }
 
+  int kernel_choice(double *ms, int capacity, int &count) override {
+    count = static_cast<int>(tuning_.ms.size());
+    for (int i = 0; i < count && i < capacity; ++i)
+      ms[i] = tuning_.ms[i];
+    return mixed_ ? kernel_ : -1;
+  }
+
   void flags(std::uint8_t *out) override {
     cuda_check(cudaMemcpyAsync(out, d_flags_.get(), 3 * ne_, cudaMemcpyDeviceToHost, stream_),
                "flags");
@@ -354,6 +372,9 @@ private:
     a.faces.slot_face = d_slot_face_.get();
     a.face_table = d_face_table_.get();
     a.face_table64 = d_face_table64_.get();
+    a.tile.nbr = d_tile_nbr_.get();
+    a.tile.code = d_tile_code_.get();
+    a.tile.aux = d_tile_aux_.get();
     a.dt = dt_device;
     a.dt_value = dt_value;
     a.gamma = cfg_.heat_capacity_ratio;
@@ -362,6 +383,8 @@ private:
     a.highest_degree_begin = stencil_.highest_degree_begin;
     a.troubled = d_troubled_.get();
     a.troubled_count = d_count_.get();
+    if (mixed_ && kernel_ < 0)
+      tune_mixed(a);
     double *ins[3] = {d_u_.get(), d_e_.get(), d_s_.get()};
     double *outs[3] = {d_e_.get(), d_s_.get(), d_u_.get()};
     for (int k = 0; k < 3; ++k) {
@@ -374,18 +397,89 @@ private:
         cuda_check(cudaMemsetAsync(d_count_.get(), 0, sizeof(std::int32_t), stream_), "count");
       stage_begin();
       if (mixed_)
-        launch_euler_tri_stage_mixed(p_, cfg_.volume_rule_order, a, stream_);
-      else
+        launch_mixed(a);
+      else {
         launch_euler_tri_stage_f64(p_, a, stream_);
+        count_launches(1);
+      }
       stage_end();
-      count_launches(mixed_ ? (boundary_count_ > 0 && boundary_ != WASL_TRANSMISSIVE && !paired_ ? 3 : 2)
-                            : 1);
       if (limiting_) {
         launch_limit_f64(M_, 3, limit_args(outs[k]), stream_);
         count_launches(2);
       }
     }
     cuda_check(cudaGetLastError(), "stage launch");
+  }
+
+  // kernel_: 0 face-centric kernels, 1 + s the tile kernel in shape s.
+  void launch_mixed(const StageArgs &a) {
+    if (kernel_ == 0) {
+      launch_euler_tri_stage_mixed(p_, cfg_.volume_rule_order, a, stream_);
+      count_launches(boundary_count_ > 0 && boundary_ != WASL_TRANSMISSIVE && !paired_ ? 3 : 2);
+    } else {
+      launch_euler_tri_stage_tile(p_, cfg_.volume_rule_order, kernel_ - 1, a, stream_);
+      count_launches(1);
+    }
+  }
+
+  // Times every kernel choice on a first-stage evaluation of the current
+  // state into scratch (u^n is read, not written; sensing off) and keeps the
+  // fastest, per polynomial order, rule order and mesh size class.
+  void tune_mixed(StageArgs a) {
+    const int variants = tile_ok_ ? 1 + euler_tri_tile_shapes() : 1;
+    a.stage = 0;
+    a.in = d_u_.get();
+    a.u0 = d_u_.get();
+    a.out = d_e_.get();
+    a.sense = 0;
+    a.dt = nullptr;
+    a.dt_value = 0.0;
+    const std::string key = "euler_tri_mixed/p" + std::to_string(p_) + "/rule" +
+                            std::to_string(cfg_.volume_rule_order ? cfg_.volume_rule_order : p_ + 2) +
+                            "/bnd" + std::to_string(boundary_count_ > 0 ? boundary_ : -1) +
+                            "/size" + std::to_string(size_class(ne_));
+    tuning_ = autotune(key, variants, [&](int i) {
+      kernel_ = i;
+      launch_mixed(a);
+    }, stream_);
+    kernel_ = tuning_.choice;
+  }
+
+  // Element-centric slots of the tile kernel (kernels.hpp TileSlots), from
+  // the face slots after periodic pairing.
+  void build_tile_slots(const TriSlots &t, int QF) {
+    std::vector<std::int32_t> nbr(3 * ne_), aux(3 * ne_, 0);
+    std::vector<std::uint8_t> code(3 * ne_);
+    for (int k = 0; k < 3; ++k)
+      for (std::int64_t e = 0; e < ne_; ++e) {
+        const std::int64_t slot = k * ne_ + e;
+        const std::int64_t f = t.slot_face[slot];
+        const std::int32_t L = mesh_.face_left[f], R = t.face_right[f];
+        const unsigned bits = (static_cast<unsigned>(mesh_.face_left_edge[f]) << 1) |
+                              (static_cast<unsigned>(mesh_.face_right_edge[f]) << 3) |
+                              (static_cast<unsigned>(mesh_.face_flip[f]) << 5);
+        const bool left = L == e;
+        if (R >= 0) {
+          nbr[slot] = left ? R : L;
+          code[slot] = static_cast<std::uint8_t>(bits | (left ? 1u : 0u));
+        } else if (boundary_ == WASL_TRANSMISSIVE) {
+          nbr[slot] = -1;
+          code[slot] = static_cast<std::uint8_t>(bits | 1u);
+        } else {
+          const std::int32_t b = -R - 1;
+          aux[slot] = b;
+          if (left) {
+            nbr[slot] = t.donors[static_cast<std::size_t>(b) * QF];
+            code[slot] = static_cast<std::uint8_t>(bits | 1u | 0x80u);
+          } else {
+            nbr[slot] = L;
+            code[slot] = static_cast<std::uint8_t>(bits | 0x40u);
+          }
+        }
+      }
+    d_tile_nbr_.upload(nbr, stream_);
+    d_tile_code_.upload(code, stream_);
+    d_tile_aux_.upload(aux, stream_);
   }
 
   // The mixed form evaluates each periodic face pair once, as one face
@@ -435,6 +529,8 @@ private:
       const std::int64_t k = left_slot[f];
       slot_face[k * ne_ + e] = static_cast<std::int32_t>(c);
       slot_code[k * ne_ + e] = static_cast<std::uint8_t>((mesh_.face_left_edge[c] << 1) | 0x40u);
+      slot_geo[(3 * k) * ne_ + e] = mesh_.face_nx[c];
+      slot_geo[(3 * k + 1) * ne_ + e] = mesh_.face_ny[c];
       slot_geo[(3 * k + 2) * ne_ + e] = mesh_.face_scale[c];
     }
     std::vector<float> basis32(donor_basis.begin(), donor_basis.end());
@@ -486,6 +582,11 @@ private:
   bool limiting_ = false;
   bool mixed_ = false;
   bool paired_ = false;
+  bool tile_ok_ = false;
+  int kernel_ = -1; // mixed form: -1 not chosen yet, 0 face-centric, 1 + s tile shape s
+  TuneResult tuning_;
+  DeviceArray<std::int32_t> d_tile_nbr_, d_tile_aux_;
+  DeviceArray<std::uint8_t> d_tile_code_;
   DeviceArray<float> d_basis32_;
   double length_ = 0.0;
   LimiterStencil stencil_;

@@ -58,6 +58,27 @@ struct FaceView {
   const std::int32_t *slot_face = nullptr;
 };
 
+// Element-centric slots of the fused tile kernel, [3][ne] each, in the
+// element's face order: the element across the face (-1 on a transmissive
+// boundary face, whose exterior is the element's own trace), a code byte as
+// slot_code (bit 0 this element is the face's left side, bits 1-2 left local
+// edge, bits 3-4 right local edge, bit 5 orientation flip) plus bit 6 "this
+// element's basis on the face is the periodic table row aux" and bit 7 "the
+// other element's basis is the periodic table row aux", and aux (the row of
+// BoundaryView::basis32 for paired periodic faces).  The normal and edge
+// scale of the face are slot_geo's.
+struct TileSlots {
+  const std::int32_t *nbr = nullptr;
+  const std::uint8_t *code = nullptr;
+  const std::int32_t *aux = nullptr;
+};
+
+// One entry of a tile work list: elements [first, first + count) of one case
+// (count <= the kernel's tile size), and the case whose dt applies.
+struct TileWork {
+  std::int32_t first = 0, count = 0, case_id = 0, pad = 0;
+};
+
 // One SSP-RK3 stage: residual of `in`, then
 //   stage 0: out = in + dt r
 //   stage 1: out = 0.75 u0 + 0.25 (in + dt r)
@@ -84,6 +105,12 @@ struct StageArgs {
   std::uint8_t *flags = nullptr;       // [ne]
   std::int32_t *troubled = nullptr;    // [ne] compacted list
   std::int32_t *troubled_count = nullptr;
+  // Fused tile kernel: slots, and an optional work list (null: tile b covers
+  // elements [b T, b T + T)) with per-case time steps (null: dt / dt_value).
+  TileSlots tile;
+  const TileWork *work = nullptr;
+  std::int64_t work_count = 0;
+  const double *case_dt = nullptr;
 };
 
 // Limiter over the compacted troubled list (cpp/src/limiting/euler_modal_limiter.cpp:70-98).
@@ -190,6 +217,15 @@ bool euler_tri_mixed_supported(int p, int rule);
 void upload_euler_tri_tables_mixed(int p, int rule);
 std::size_t euler_tri_mixed_face_record_bytes(int p);
 void launch_euler_tri_stage_mixed(int p, int rule, const StageArgs &a, cudaStream_t stream);
+// The fused tile form of the mixed stage: one kernel per stage.  `shape`
+// (0 .. euler_tri_tile_shapes()-1) picks elements per CTA and the register
+// budget; with a work list there is one CTA per entry (count <= the shape's
+// elements), else ceil(ne / elements) CTAs.  Requires transmissive
+// boundaries or paired periodic faces.
+int euler_tri_tile_shapes();
+int euler_tri_tile_elements(int shape);
+void launch_euler_tri_stage_tile(int p, int rule, int shape, const StageArgs &a,
+                                 cudaStream_t stream);
 void launch_limit_f64(int M, int NB, const LimitArgs &a, cudaStream_t stream);
 void launch_sense_f64(int M, const SenseArgs &a, cudaStream_t stream);
 void launch_cfl(const CflArgs &a, cudaStream_t stream);

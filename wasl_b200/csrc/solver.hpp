@@ -106,6 +106,14 @@ public:
   // The state evaluated at the rule's points, [element][point][variable].
   virtual void evaluate(int rule_order, double *values) = 0;
   cudaStream_t stream() const { return stream_; }
+  // The kernel variant in use (-1: the form has one kernel) and, when it was
+  // autotuned, the timed mean of every variant (count of them in `count`).
+  virtual int kernel_choice(double *ms, int capacity, int &count) {
+    (void)ms;
+    (void)capacity;
+    count = 0;
+    return -1;
+  }
 
   // Kernel accounting for measurement: every launch is counted; while
   // profiling, each stage kernel is bracketed by CUDA events on the stream it
