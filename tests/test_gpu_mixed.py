@@ -160,3 +160,25 @@ def test_autotuner_times_every_variant():
         cases.project_initial(g, vortex.conserved)
         g.step(g.stable_dt(0.15))
         assert g.tuning() == (choice, ms)
+
+
+@pytest.mark.parametrize("kernel", [1, 2, 5])
+def test_fused_cfl_speed_matches_cfl_kernels(kernel):
+    """advance() with the tile kernel reduces the next step's CFL speed inside
+    the last stage; the trajectory is bit-identical to one whose every dt comes
+    from the standalone CFL kernels (set_state in between forces them)."""
+    arrays = cases.vortex_mesh(24, seed=5)
+    vortex = cases.IsentropicVortex()
+    out = []
+    for fused in (True, False):
+        with wasl_b200.Solver(*arrays, polynomial_order=2, precision="mixed",
+                              mixed_kernel=kernel) as g:
+            cases.project_initial(g, vortex.conserved)
+            if fused:
+                g.advance(0.15, 6)
+            else:
+                for _ in range(6):
+                    g.advance(0.15, 1)
+                    g.set_state(g.get_state())
+            out.append(g.get_state())
+    assert np.array_equal(out[0], out[1])

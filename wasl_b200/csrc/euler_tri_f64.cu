@@ -498,6 +498,21 @@ __global__ void cfl_finish(const CflArgs a) {
     *a.dt = dt;
 }
 
+// dt from a reduced speed word per case (the finish step of the CFL kernels),
+// then the word is zeroed for the next reduction.
+__global__ void dt_from_speed(std::int64_t cases, unsigned long long *speed, double cfl,
+                              const double *length, const int *p, double length_all, int p_all,
+                              double *dt) {
+  const std::int64_t c = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (c >= cases)
+    return;
+  const double v = __longlong_as_double(static_cast<long long>(speed[c]));
+  const double h = length ? length[c] : length_all;
+  const int order = p ? p[c] : p_all;
+  dt[c] = v > 0.0 ? cfl * h / (v * (2 * order + 1)) : 0.0;
+  speed[c] = 0ULL;
+}
+
 // ---- host launchers -------------------------------------------------------------
 
 namespace {
@@ -578,6 +593,13 @@ void launch_sense_f64(int M, const SenseArgs &a, cudaStream_t s) {
   case 10: sense_f64<10><<<blocks, 256, 0, s>>>(a); break;
   default: throw std::invalid_argument("sensor: unsupported mode count");
   }
+}
+
+void launch_dt_from_speed(std::int64_t cases, unsigned long long *speed, double cfl,
+                          const double *length, const int *p, double length_all, int p_all,
+                          double *dt, cudaStream_t s) {
+  dt_from_speed<<<static_cast<unsigned>((cases + 255) / 256), 256, 0, s>>>(
+      cases, speed, cfl, length, p, length_all, p_all, dt);
 }
 
 void launch_cfl(const CflArgs &a, cudaStream_t s) {

@@ -805,7 +805,7 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_mixed(const StageAr
 
   const double inv = geo[4 * ne + e];
   const double dt = a.case_dt ? a.case_dt[case_id] : (a.dt ? *a.dt : a.dt_value);
-  double rho[M];
+  double rho[M], avg[4];
 #pragma unroll
   for (int v = 0; v < 4; ++v)
 #pragma unroll
@@ -823,7 +823,32 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_mixed(const StageAr
       a.out[idx] = o;
       if (v == 0)
         rho[m] = o;
+      if (m == 0)
+        avg[v] = o;
     }
+
+  if (a.speed_max) {
+    // The next step's CFL speed from this stage's cell averages.
+    const double scale = 1.0 / sqrt(2.0);
+    const double sa[4] = {scale * avg[0], scale * avg[1], scale * avg[2], scale * avg[3]};
+    const Prim<double> pv = primitive(gamma, sa);
+    unsigned long long best = 0;
+    if (sa[0] > 0.0 && pv.p > 0.0)
+      best = __double_as_longlong(hypot(pv.vx, pv.vy) + sound_speed(gamma, pv));
+    else
+      raise_error(a.error, kNonPhysicalAverage, e);
+    // Warp max over the active lanes (a prefix of the warp: lanes past the
+    // tile's end returned), then one atomic per warp.
+    const unsigned mask = __activemask();
+    const int lane = threadIdx.x & 31;
+    for (int off = 16; off > 0; off >>= 1) {
+      const unsigned long long o = __shfl_down_sync(mask, best, off);
+      if (lane + off < 32 && ((mask >> (lane + off)) & 1u) && o > best)
+        best = o;
+    }
+    if (lane == __ffs(mask) - 1)
+      atomicMax(a.speed_max + case_id, best);
+  }
 
   if (a.sense) {
     double total = 0.0, high = 0.0;

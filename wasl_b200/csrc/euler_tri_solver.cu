@@ -155,6 +155,7 @@ public:
       b->resize(static_cast<std::size_t>(4) * M_ * ne_);
     cuda_check(cudaMemsetAsync(d_u_.get(), 0, d_u_.size() * sizeof(double), stream_), "memset");
     d_error_.resize(1);
+    d_speed_.resize(1);
     d_cfl_.resize(8);
     d_dt_.resize(1);
     cuda_check(cudaMemsetAsync(d_error_.get(), 0, sizeof(unsigned long long), stream_), "memset");
@@ -233,6 +234,7 @@ public:
   }
 
   void set_state(const double *host) override {
+    speed_ready_ = false;
     cuda_check(cudaMemcpyAsync(d_u_.get(), host, d_u_.size() * sizeof(double),
                                cudaMemcpyHostToDevice, stream_),
                "set_state");
@@ -281,12 +283,14 @@ public:
   }
 
   void step(double dt) override {
+    speed_ready_ = false;
     enqueue_step(nullptr, dt);
     if (limiting_)
       check_error();
   }
 
   void limit() override {
+    speed_ready_ = false;
     if (!limiting_)
       return;
     cuda_check(cudaMemsetAsync(d_count_.get(), 0, sizeof(std::int32_t), stream_), "count");
@@ -304,11 +308,27 @@ public:
     check_error();
   }
 
+  // Device-resident steps.  With the tile kernel and no limiter, the last
+  // stage of each step also reduces the next step's CFL speed, so a step
+  // after the first needs one small kernel for dt instead of the three CFL
+  // kernels and their pass over the state.
   void advance(double cfl, std::int64_t steps) override {
     for (std::int64_t n = 0; n < steps; ++n) {
-      launch_cfl(cfl_args(cfl), stream_);
-      count_launches(3);
+      if (speed_ready_) {
+        launch_dt_from_speed(1, d_speed_.get(), cfl, nullptr, nullptr, length_, p_, d_dt_.get(),
+                             stream_);
+        count_launches(1);
+      } else {
+        launch_cfl(cfl_args(cfl), stream_);
+        count_launches(3);
+      }
+      fused_speed_ = mixed_ && !limiting_;
+      if (fused_speed_ && !speed_ready_)
+        cuda_check(cudaMemsetAsync(d_speed_.get(), 0, sizeof(unsigned long long), stream_),
+                   "speed reset");
       enqueue_step(d_dt_.get(), 0.0);
+      speed_ready_ = fused_speed_ && kernel_ >= 1;
+      fused_speed_ = false;
     }
     check_error();
   }
@@ -395,6 +415,8 @@ private:
       a.flags = d_flags_.get() + k * ne_;
       if (limiting_)
         cuda_check(cudaMemsetAsync(d_count_.get(), 0, sizeof(std::int32_t), stream_), "count");
+      a.speed_max = fused_speed_ && k == 2 && kernel_ >= 1 ? d_speed_.get() : nullptr;
+      a.error = d_error_.get();
       stage_begin();
       if (mixed_)
         launch_mixed(a);
@@ -583,6 +605,9 @@ private:
   bool mixed_ = false;
   bool paired_ = false;
   bool tile_ok_ = false;
+  bool fused_speed_ = false; // this step's last stage reduces the next CFL speed
+  bool speed_ready_ = false; // d_speed_ holds the current state's CFL speed
+  DeviceArray<unsigned long long> d_speed_;
   int kernel_ = -1; // mixed form: -1 not chosen yet, 0 face-centric, 1 + s tile shape s
   TuneResult tuning_;
   DeviceArray<std::int32_t> d_tile_nbr_, d_tile_aux_;

@@ -111,6 +111,11 @@ struct StageArgs {
   const TileWork *work = nullptr;
   std::int64_t work_count = 0;
   const double *case_dt = nullptr;
+  // Tile kernel, last stage: the largest cell-average wave speed |u| + c of
+  // `out` (the CFL kernels' formula) is max-reduced into speed_max[case] as
+  // FP64 bits, and a non-physical average sets the error word.
+  unsigned long long *speed_max = nullptr;
+  unsigned long long *error = nullptr;
 };
 
 // Limiter over the compacted troubled list (cpp/src/limiting/euler_modal_limiter.cpp:70-98).
@@ -229,5 +234,11 @@ void launch_euler_tri_stage_tile(int p, int rule, int shape, const StageArgs &a,
 void launch_limit_f64(int M, int NB, const LimitArgs &a, cudaStream_t stream);
 void launch_sense_f64(int M, const SenseArgs &a, cudaStream_t stream);
 void launch_cfl(const CflArgs &a, cudaStream_t stream);
+// dt[c] = cfl length[c] / (speed (2 p[c] + 1)) from the speeds the tile
+// kernel reduced (0 where the speed is 0), then the speed words are zeroed;
+// `cases` entries, length/p may be per case (arrays) or shared (count 1).
+void launch_dt_from_speed(std::int64_t cases, unsigned long long *speed, double cfl,
+                          const double *length, const int *p, double length_all, int p_all,
+                          double *dt, cudaStream_t stream);
 
 } // namespace wasl_b200
