@@ -188,6 +188,77 @@ int wasl_gpu_write_checkpoint(wasl_gpu *handle, const char *path, double time, u
                               const char *prepared_mesh);
 int wasl_gpu_read_checkpoint(wasl_gpu *handle, const char *path, double *time, uint64_t *step);
 
+/* ---- Batched 2D Euler (the mixed form) --------------------------------------
+ * Many independent triangle meshes of uneven size and polynomial order (1-3)
+ * advanced together: cases of one order share one launch of the fused tile
+ * kernel per stage over a work list of element tiles (tiles never straddle
+ * cases, each carries its case's own CFL time step), and a step (per-case CFL,
+ * three stages, stage limiter) is captured once in a CUDA graph and replayed.
+ * No counterpart in the reference, which runs one case per process
+ * (cpp/src/case/serial_case_runner.cpp:117-149); each case behaves as that
+ * loop's case with the mixed form's arithmetic. */
+typedef struct wasl_batch wasl_batch;
+
+typedef struct {
+  double heat_capacity_ratio;
+  int boundary;              /* WASL_PERIODIC (faces must pair) or WASL_TRANSMISSIVE */
+  int limiting;              /* modal-decay sensor + characteristic WENO + positivity */
+  double sensor_threshold;
+  double density_floor;
+  double pressure_floor;
+  int reduced_volume_rule;   /* 1: volume rule order p; 0: p+2 (the reference's rule) */
+  int tile_shape;            /* 0 autotuned per polynomial order; 1 + s launch shape s */
+  int use_graph;             /* 1: capture the step in a CUDA graph and replay it */
+  int device;
+} wasl_batch_config;
+
+void wasl_batch_config_default(wasl_batch_config *config);
+
+/* Cases are given back to back: orders[c], node_counts[c] node tags and
+ * [node][2] coordinates, element_counts[c] triangles ([element][3] node tags). */
+int wasl_batch_create(const wasl_batch_config *config, int64_t case_count, const int *orders,
+                      const int64_t *node_counts, const int64_t *node_tags,
+                      const double *node_coordinates, const int64_t *element_counts,
+                      const int64_t *element_nodes, wasl_batch **handle, char *error,
+                      size_t error_length);
+void wasl_batch_destroy(wasl_batch *handle);
+const char *wasl_batch_last_error(const wasl_batch *handle);
+
+/* Totals over all cases, and one case's elements and modes per variable. */
+int wasl_batch_sizes(const wasl_batch *handle, int64_t *cases, int64_t *elements, int64_t *dof);
+int wasl_batch_case_size(const wasl_batch *handle, int64_t case_index, int64_t *elements,
+                         int *modes);
+
+/* One case's state U[variable][mode][element] (FP64, that case's elements). */
+int wasl_batch_set_state(wasl_batch *handle, int64_t case_index, const double *coefficients,
+                         int64_t count);
+int wasl_batch_get_state(wasl_batch *handle, int64_t case_index, double *coefficients,
+                         int64_t count);
+
+/* Quadrature and L2 projection of one case, as wasl_gpu_quadrature and
+ * wasl_gpu_project. */
+int wasl_batch_quadrature(const wasl_batch *handle, int64_t case_index, int rule_order, double *x,
+                          double *y, double *weights);
+int wasl_batch_project(wasl_batch *handle, int64_t case_index, int rule_order,
+                       const double *values, int64_t count);
+
+/* `steps` SSP-RK3 steps of every case, each with its own CFL time step
+ * cfl h_c / ((|u| + c)_max,c (2 p_c + 1)).  Synchronizes to report errors. */
+int wasl_batch_advance(wasl_batch *handle, double cfl, int64_t steps);
+
+/* Per case: time advanced since creation, and the last step's dt. */
+int wasl_batch_times(wasl_batch *handle, double *time, double *dt, int64_t count);
+
+/* The tile shape chosen for the cases of order p (-1 if none), and the timed
+ * mean stage time of every shape when it was autotuned. */
+int wasl_batch_tuning(const wasl_batch *handle, int polynomial_order, int *choice, double *ms,
+                      int capacity, int *count);
+
+/* Kernels enqueued per step, whether steps replay a CUDA graph, all kernels
+ * launched so far, and the handle's CUDA stream (cudaStream_t). */
+int wasl_batch_launches(const wasl_batch *handle, int64_t *per_step, int *graph, int64_t *total);
+int wasl_batch_stream(wasl_batch *handle, void **stream);
+
 /* The CFL time step of a device-resident 2D/1D Euler state, computed without
  * allocating anything.  No counterpart in the reference: it is an entry point
  * for callers that cannot call cudaMalloc (an application whose device memory

@@ -54,6 +54,15 @@ class Config(C.Structure):
     ]
 
 
+class BatchConfig(C.Structure):
+    _fields_ = [
+        ("heat_capacity_ratio", C.c_double), ("boundary", C.c_int), ("limiting", C.c_int),
+        ("sensor_threshold", C.c_double), ("density_floor", C.c_double),
+        ("pressure_floor", C.c_double), ("reduced_volume_rule", C.c_int),
+        ("tile_shape", C.c_int), ("use_graph", C.c_int), ("device", C.c_int),
+    ]
+
+
 _d = C.POINTER(C.c_double)
 _i64 = C.POINTER(C.c_int64)
 _u8 = C.POINTER(C.c_uint8)
@@ -88,6 +97,24 @@ SIGNATURES = {
     "wasl_gpu_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "wasl_gpu_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), _d, C.c_int,
                                   C.POINTER(C.c_int)]),
+    "wasl_batch_config_default": (None, [C.POINTER(BatchConfig)]),
+    "wasl_batch_create": (C.c_int, [C.POINTER(BatchConfig), C.c_int64, C.POINTER(C.c_int), _i64,
+                                    _i64, _d, _i64, _i64, C.POINTER(C.c_void_p), C.c_char_p,
+                                    C.c_size_t]),
+    "wasl_batch_destroy": (None, [C.c_void_p]),
+    "wasl_batch_last_error": (C.c_char_p, [C.c_void_p]),
+    "wasl_batch_sizes": (C.c_int, [C.c_void_p, _i64, _i64, _i64]),
+    "wasl_batch_case_size": (C.c_int, [C.c_void_p, C.c_int64, _i64, C.POINTER(C.c_int)]),
+    "wasl_batch_set_state": (C.c_int, [C.c_void_p, C.c_int64, _d, C.c_int64]),
+    "wasl_batch_get_state": (C.c_int, [C.c_void_p, C.c_int64, _d, C.c_int64]),
+    "wasl_batch_quadrature": (C.c_int, [C.c_void_p, C.c_int64, C.c_int, _d, _d, _d]),
+    "wasl_batch_project": (C.c_int, [C.c_void_p, C.c_int64, C.c_int, _d, C.c_int64]),
+    "wasl_batch_advance": (C.c_int, [C.c_void_p, C.c_double, C.c_int64]),
+    "wasl_batch_times": (C.c_int, [C.c_void_p, _d, _d, C.c_int64]),
+    "wasl_batch_tuning": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), _d, C.c_int,
+                                    C.POINTER(C.c_int)]),
+    "wasl_batch_launches": (C.c_int, [C.c_void_p, _i64, C.POINTER(C.c_int), _i64]),
+    "wasl_batch_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "wasl_gpu_profile_begin": (C.c_int, [C.c_void_p]),
     "wasl_gpu_profile_end": (C.c_int, [C.c_void_p, _d, _i64, _i64]),
     "wasl_gpu_write_checkpoint": (C.c_int, [C.c_void_p, C.c_char_p, C.c_double, C.c_uint64,
@@ -317,3 +344,121 @@ class Solver:
         self._check(self._lib.wasl_gpu_read_checkpoint(self._h, os.fsencode(path), C.byref(t),
                                                        C.byref(s)))
         return t.value, s.value
+
+
+class Batch:
+    """Many independent 2D Euler cases (triangle meshes, orders 1-3) advanced
+    together in the mixed form (wasl_batch_* in include/wasl_b200.h).
+
+    ``cases`` is a list of ``(node_tags, node_coordinates, element_nodes,
+    polynomial_order)``.
+    """
+
+    def __init__(self, cases, *, gamma=1.4, boundary="transmissive", limiting=False,
+                 sensor_threshold=1e-3, density_floor=1e-10, pressure_floor=1e-10,
+                 reduced_volume_rule=True, tile_shape=0, use_graph=True, device=0):
+        lib = library()
+        cfg = BatchConfig()
+        lib.wasl_batch_config_default(C.byref(cfg))
+        cfg.heat_capacity_ratio = gamma
+        cfg.boundary = BOUNDARY_KINDS[boundary]
+        cfg.limiting = 1 if limiting else 0
+        cfg.sensor_threshold = sensor_threshold
+        cfg.density_floor = density_floor
+        cfg.pressure_floor = pressure_floor
+        cfg.reduced_volume_rule = 1 if reduced_volume_rule else 0
+        cfg.tile_shape = tile_shape
+        cfg.use_graph = 1 if use_graph else 0
+        cfg.device = device
+        self.config = cfg
+        orders = np.array([c[3] for c in cases], dtype=np.int32)
+        node_counts = np.array([len(c[0]) for c in cases], dtype=np.int64)
+        elem_counts = np.array([len(c[2]) for c in cases], dtype=np.int64)
+        tags = np.ascontiguousarray(np.concatenate([np.asarray(c[0], np.int64) for c in cases]))
+        xy = np.ascontiguousarray(np.concatenate([np.asarray(c[1], np.float64) for c in cases]))
+        tris = np.ascontiguousarray(np.concatenate([np.asarray(c[2], np.int64) for c in cases]))
+        err = C.create_string_buffer(1024)
+        h = C.c_void_p()
+        rc = lib.wasl_batch_create(C.byref(cfg), len(cases),
+                                   orders.ctypes.data_as(C.POINTER(C.c_int)),
+                                   _ptr(node_counts, _i64), _ptr(tags, _i64), _ptr(xy),
+                                   _ptr(elem_counts, _i64), _ptr(tris, _i64), C.byref(h), err,
+                                   len(err))
+        if rc != 0:
+            raise WaslError(rc, err.value.decode())
+        self._lib, self._h = lib, h
+        n, ne, dof = C.c_int64(), C.c_int64(), C.c_int64()
+        self._check(lib.wasl_batch_sizes(h, C.byref(n), C.byref(ne), C.byref(dof)))
+        self.cases, self.elements, self.dof = n.value, ne.value, dof.value
+        self.orders = orders.tolist()
+
+    def _check(self, rc):
+        if rc != 0:
+            raise WaslError(rc, self._lib.wasl_batch_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.wasl_batch_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        self.close()
+
+    def case_size(self, c):
+        ne, nm = C.c_int64(), C.c_int()
+        self._check(self._lib.wasl_batch_case_size(self._h, c, C.byref(ne), C.byref(nm)))
+        return ne.value, nm.value
+
+    def set_state(self, c, coefficients):
+        a = np.ascontiguousarray(coefficients, dtype=np.float64).ravel()
+        self._check(self._lib.wasl_batch_set_state(self._h, c, _ptr(a), a.size))
+
+    def get_state(self, c):
+        ne, nm = self.case_size(c)
+        out = np.empty(4 * nm * ne)
+        self._check(self._lib.wasl_batch_get_state(self._h, c, _ptr(out), out.size))
+        return out
+
+    def quadrature(self, c, rule_order):
+        ne, _ = self.case_size(c)
+        q = (rule_order + 1) ** 2
+        x, y, w = (np.empty((ne, q)) for _ in range(3))
+        self._check(self._lib.wasl_batch_quadrature(self._h, c, rule_order, _ptr(x), _ptr(y),
+                                                    _ptr(w)))
+        return x, y, w
+
+    def project(self, c, rule_order, values):
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        self._check(self._lib.wasl_batch_project(self._h, c, rule_order, _ptr(a), a.size))
+
+    def advance(self, cfl, steps):
+        self._check(self._lib.wasl_batch_advance(self._h, cfl, steps))
+
+    def times(self):
+        t, dt = np.empty(self.cases), np.empty(self.cases)
+        self._check(self._lib.wasl_batch_times(self._h, _ptr(t), _ptr(dt), self.cases))
+        return t, dt
+
+    def tuning(self, polynomial_order):
+        choice, count = C.c_int(), C.c_int()
+        ms = np.zeros(16)
+        self._check(self._lib.wasl_batch_tuning(self._h, polynomial_order, C.byref(choice),
+                                                _ptr(ms), len(ms), C.byref(count)))
+        return choice.value, ms[:count.value].tolist()
+
+    def launches(self):
+        per_step, graph, total = C.c_int64(), C.c_int(), C.c_int64()
+        self._check(self._lib.wasl_batch_launches(self._h, C.byref(per_step), C.byref(graph),
+                                                  C.byref(total)))
+        return per_step.value, bool(graph.value), total.value
+
+    def stream_handle(self) -> int:
+        s = C.c_void_p()
+        self._check(self._lib.wasl_batch_stream(self._h, C.byref(s)))
+        return s.value or 0

@@ -43,6 +43,9 @@ SOURCES = {
     "profiling.cpp": [],
     "cfl_static.cu": [],
     "autotune.cpp": [],
+    "tri_setup.cpp": [],
+    "batch_solver.cu": [],
+    "capi_batch.cpp": [],
 }
 HEADERS = [f for f in os.listdir(CSRC) if f.endswith((".hpp", ".cuh", ".h"))]
 

@@ -190,3 +190,31 @@ class ShockVortex:
 
     def conserved(self, x, y, t=0.0):
         return conserved(*self.primitive(x, y), gamma=self.gamma)
+
+
+# ---- batched cases ---------------------------------------------------------------------
+
+def batched_riemann_cases(count, seed=4, min_triangles=2_000, max_triangles=128_000,
+                          orders=(1, 2, 3)):
+    """Independent planar two-state Riemann problems on [0,1]^2: per case a
+    triangle count drawn log-uniformly in [min, max] (n x n quads, n =
+    round(sqrt(count / 2)), jittered +-0.15h), an order drawn from `orders`,
+    and seeded states.  Returns [(node_tags, coordinates, triangles, p,
+    problem)]."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for c in range(count):
+        triangles = math.exp(rng.uniform(math.log(min_triangles), math.log(max_triangles)))
+        n = max(2, int(round(math.sqrt(triangles / 2.0))))
+        p = int(rng.choice(orders))
+        case_seed = int(rng.integers(1 << 31))
+        arrays = meshgen.jittered_box(n, 0.0, 1.0, 0.0, 1.0, jitter=0.15, seed=case_seed)
+        out.append((*arrays, p, PlanarRiemann(seed=case_seed)))
+    return out
+
+
+def project_batch_case(batch, c, field, p):
+    """Project field(x, y) -> [..., 4] onto case c of a Batch (rule max(p, 5))."""
+    rule = max(p, 5)
+    x, y, _ = batch.quadrature(c, rule)
+    batch.project(c, rule, field(x, y))

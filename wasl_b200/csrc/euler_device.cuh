@@ -33,6 +33,23 @@ template <typename T> __device__ __forceinline__ T sound_speed(T gamma, const Pr
   return sqrt(gamma * v.p / v.rho);
 }
 
+// The CFL wave speed |u| + c (hypot(u, v) + c in 2D) of a cell average s
+// (cpp/src/time/cfl_timestep.cpp:33-47), with the operations of primitive()
+// and sound_speed() written as explicitly rounded steps, so kernels compiled
+// with and without multiply-add contraction compute the same bits.  physical
+// is false for a non-positive density or pressure.
+__device__ __forceinline__ double cfl_speed(double gamma, const double *s, int dimensions,
+                                            bool &physical) {
+  const double inv = 1.0 / s[0];
+  const double vx = __dmul_rn(s[1], inv);
+  const double vy = __dmul_rn(s[2], inv);
+  const double ke = __dmul_rn(0.5, __dadd_rn(__dmul_rn(s[1], vx), __dmul_rn(s[2], vy)));
+  const double p = __dmul_rn(gamma - 1.0, __dsub_rn(s[3], ke));
+  physical = s[0] > 0.0 && p > 0.0;
+  const double velocity = dimensions == 1 ? fabs(vx) : hypot(vx, vy);
+  return __dadd_rn(velocity, sqrt(__dmul_rn(gamma, p) / s[0]));
+}
+
 // Both physical flux components from one primitive evaluation.
 template <typename T>
 __device__ __forceinline__ void flux_xy(T gamma, const T *s, T *fx, T *fy) {

@@ -436,10 +436,7 @@ __device__ __forceinline__ double cell_speed(const CflArgs &a, std::int64_t e, b
   const std::int64_t plane = static_cast<std::int64_t>(a.M) * a.ne;
   const double s[4] = {scale * a.state[e], scale * a.state[plane + e],
                        scale * a.state[2 * plane + e], scale * a.state[3 * plane + e]};
-  physical = s[0] > 0.0 && primitive(a.gamma, s).p > 0.0;
-  const Prim<double> v = primitive(a.gamma, s);
-  const double velocity = a.dimensions == 1 ? fabs(v.vx) : hypot(v.vx, v.vy);
-  return velocity + sound_speed(a.gamma, v);
+  return cfl_speed(a.gamma, s, a.dimensions, physical);
 }
 
 __global__ void cfl_max(const CflArgs a) {
@@ -502,14 +499,17 @@ __global__ void cfl_finish(const CflArgs a) {
 // then the word is zeroed for the next reduction.
 __global__ void dt_from_speed(std::int64_t cases, unsigned long long *speed, double cfl,
                               const double *length, const int *p, double length_all, int p_all,
-                              double *dt) {
+                              double *dt, double *elapsed) {
   const std::int64_t c = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (c >= cases)
     return;
   const double v = __longlong_as_double(static_cast<long long>(speed[c]));
   const double h = length ? length[c] : length_all;
   const int order = p ? p[c] : p_all;
-  dt[c] = v > 0.0 ? cfl * h / (v * (2 * order + 1)) : 0.0;
+  const double step = v > 0.0 ? cfl * h / (v * (2 * order + 1)) : 0.0;
+  dt[c] = step;
+  if (elapsed)
+    elapsed[c] += step;
   speed[c] = 0ULL;
 }
 
@@ -597,9 +597,9 @@ void launch_sense_f64(int M, const SenseArgs &a, cudaStream_t s) {
 
 void launch_dt_from_speed(std::int64_t cases, unsigned long long *speed, double cfl,
                           const double *length, const int *p, double length_all, int p_all,
-                          double *dt, cudaStream_t s) {
+                          double *dt, double *elapsed, cudaStream_t s) {
   dt_from_speed<<<static_cast<unsigned>((cases + 255) / 256), 256, 0, s>>>(
-      cases, speed, cfl, length, p, length_all, p_all, dt);
+      cases, speed, cfl, length, p, length_all, p_all, dt, elapsed);
 }
 
 void launch_cfl(const CflArgs &a, cudaStream_t s) {

@@ -830,11 +830,13 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_mixed(const StageAr
   if (a.speed_max) {
     // The next step's CFL speed from this stage's cell averages.
     const double scale = 1.0 / sqrt(2.0);
-    const double sa[4] = {scale * avg[0], scale * avg[1], scale * avg[2], scale * avg[3]};
-    const Prim<double> pv = primitive(gamma, sa);
+    const double sa[4] = {__dmul_rn(scale, avg[0]), __dmul_rn(scale, avg[1]),
+                          __dmul_rn(scale, avg[2]), __dmul_rn(scale, avg[3])};
+    bool physical = true;
+    const double speed = cfl_speed(gamma, sa, 2, physical);
     unsigned long long best = 0;
-    if (sa[0] > 0.0 && pv.p > 0.0)
-      best = __double_as_longlong(hypot(pv.vx, pv.vy) + sound_speed(gamma, pv));
+    if (physical)
+      best = __double_as_longlong(speed);
     else
       raise_error(a.error, kNonPhysicalAverage, e);
     // Warp max over the active lanes (a prefix of the warp: lanes past the
@@ -873,6 +875,39 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_mixed(const StageAr
         a.troubled[base + __popc(ballot & ((1u << lane) - 1u))] = static_cast<std::int32_t>(e);
     }
   }
+}
+
+// Per-case CFL speed over a tile work list: the largest cell-average wave
+// speed |u| + c of each case (the CFL kernels' formula), max-reduced as FP64
+// bits into speed[case]; a non-physical average sets the error word.
+__global__ void batch_speed(const double *state, std::int64_t ne, int M, double gamma,
+                            const TileWork *work, unsigned long long *speed,
+                            unsigned long long *error) {
+  const TileWork w = work[blockIdx.x];
+  const int lane = threadIdx.x & 31;
+  unsigned long long best = 0;
+  for (int i = threadIdx.x; i < w.count; i += blockDim.x) {
+    const std::int64_t e = w.first + i;
+    const double scale = 1.0 / sqrt(2.0);
+    const std::int64_t plane = static_cast<std::int64_t>(M) * ne;
+    const double s[4] = {__dmul_rn(scale, state[e]), __dmul_rn(scale, state[plane + e]),
+                         __dmul_rn(scale, state[2 * plane + e]),
+                         __dmul_rn(scale, state[3 * plane + e])};
+    bool physical = true;
+    const double speed = cfl_speed(gamma, s, 2, physical);
+    if (physical) {
+      const unsigned long long bits = __double_as_longlong(speed);
+      best = bits > best ? bits : best;
+    } else {
+      raise_error(error, kNonPhysicalAverage, e);
+    }
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    const unsigned long long o = __shfl_down_sync(0xffffffffu, best, off);
+    best = o > best ? o : best;
+  }
+  if (lane == 0 && best)
+    atomicMax(speed + w.case_id, best);
 }
 
 namespace {
@@ -918,26 +953,34 @@ template <int P, int R> void stage_mixed(const StageArgs &a, cudaStream_t s) {
       <<<static_cast<unsigned>((a.mesh.ne + 127) / 128), 128, 0, s>>>(a);
 }
 
+template <int P, int TILE> constexpr std::size_t tile_smem() {
+  return sizeof(double) * 4 * TriShape<P>::M * TILE;
+}
+
+// Static (face table) plus dynamic shared memory above the default 48 KiB
+// needs the opt-in attribute, set once per device (and before any capture).
+template <int P, int R, int TILE, int MINB> void tile_opt_in() {
+  if (tile_smem<P, TILE>() + sizeof(FaceTable<P, float>) <= 48 * 1024)
+    return;
+  static bool opted_in[64] = {};
+  int device = 0;
+  check(cudaGetDevice(&device), "cudaGetDevice");
+  if (device < 64 && opted_in[device])
+    return;
+  check(cudaFuncSetAttribute(euler_tri_tile_mixed<P, R, TILE, MINB>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(tile_smem<P, TILE>())),
+        "tile kernel shared memory");
+  if (device < 64)
+    opted_in[device] = true;
+}
+
 template <int P, int R, int TILE, int MINB> void stage_tile(const StageArgs &a, cudaStream_t s) {
-  const std::size_t smem = sizeof(double) * 4 * TriShape<P>::M * TILE;
-  // Static (face table) plus dynamic shared memory above the default 48 KiB
-  // needs the opt-in attribute, set once per device.
-  if (smem + sizeof(FaceTable<P, float>) > 48 * 1024) {
-    static bool opted_in[64] = {};
-    int device = 0;
-    check(cudaGetDevice(&device), "cudaGetDevice");
-    if (device >= 64 || !opted_in[device]) {
-      check(cudaFuncSetAttribute(euler_tri_tile_mixed<P, R, TILE, MINB>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem)),
-            "tile kernel shared memory");
-      if (device < 64)
-        opted_in[device] = true;
-    }
-  }
+  tile_opt_in<P, R, TILE, MINB>();
   const std::int64_t blocks = a.work ? a.work_count : (a.mesh.ne + TILE - 1) / TILE;
   if (blocks > 0)
-    euler_tri_tile_mixed<P, R, TILE, MINB><<<static_cast<unsigned>(blocks), TILE, smem, s>>>(a);
+    euler_tri_tile_mixed<P, R, TILE, MINB>
+        <<<static_cast<unsigned>(blocks), TILE, tile_smem<P, TILE>(), s>>>(a);
 }
 
 // Launch shapes of the tile kernel (elements per CTA, register budget):
@@ -954,6 +997,15 @@ template <int P, int R> struct StageTile {
     case 3: stage_tile<P, R, 64, 8>(a, s); break;
     default: throw std::invalid_argument("tile kernel: unknown launch shape");
     }
+  }
+};
+
+template <int P, int R> struct PrepareTile {
+  static void run() {
+    tile_opt_in<P, R, 128, 4>();
+    tile_opt_in<P, R, 128, 1>();
+    tile_opt_in<P, R, 256, 2>();
+    tile_opt_in<P, R, 64, 8>();
   }
 };
 
@@ -1012,8 +1064,18 @@ int euler_tri_tile_elements(int shape) {
   return shape >= 0 && shape < 4 ? elements[shape] : 0;
 }
 
+void prepare_euler_tri_stage_tile(int p, int rule) { dispatch_mixed<PrepareTile>(p, rule); }
+
 void launch_euler_tri_stage_tile(int p, int rule, int shape, const StageArgs &a, cudaStream_t s) {
   dispatch_mixed<StageTile>(p, rule, shape, a, s);
+}
+
+void launch_batch_speed(const double *state, std::int64_t ne, int M, double gamma,
+                        const TileWork *work, std::int64_t work_count, unsigned long long *speed,
+                        unsigned long long *error, cudaStream_t s) {
+  if (work_count > 0)
+    batch_speed<<<static_cast<unsigned>(work_count), 128, 0, s>>>(state, ne, M, gamma, work, speed,
+                                                                  error);
 }
 
 void launch_euler_tri_stage_mixed(int p, int rule, const StageArgs &a, cudaStream_t s) {

@@ -15,6 +15,7 @@
 #include "kernels.hpp"
 #include "mesh.hpp"
 #include "solver.hpp"
+#include "tri_setup.hpp"
 #include "tri_tables.hpp"
 
 namespace wasl_b200 {
@@ -94,11 +95,14 @@ public:
     std::vector<double> &donor_basis = t.donor_basis;
     std::vector<double> &geo = t.geo, &slot_geo = t.slot_geo, &face_normal = t.face_normal;
     std::vector<std::int32_t> &slot_nbr = t.slot_nbr, &slot_face = t.slot_face,
-                              &face_right = t.face_right, &left_slot = t.left_slot;
+                              &face_right = t.face_right;
     std::vector<std::uint8_t> &slot_code = t.slot_code, &face_code = t.face_code;
-    if (cfg.precision == WASL_MIXED && boundary_ == WASL_PERIODIC && boundary_count_ > 0)
-      paired_ = pair_periodic_faces(QF, donors, donor_basis, face_code, slot_face, slot_code,
-                                    slot_geo, left_slot);
+    if (cfg.precision == WASL_MIXED && boundary_ == WASL_PERIODIC && boundary_count_ > 0) {
+      std::vector<float> basis32;
+      paired_ = pair_periodic_faces(mesh_, QF, t, basis32);
+      if (paired_)
+        d_basis32_.upload(basis32, stream_);
+    }
     if (cfg.precision == WASL_MIXED) {
       if (cfg.mixed_kernel < 0 || cfg.mixed_kernel > 1 + euler_tri_tile_shapes())
         throw SolverError(WASL_ERR_ARGUMENT, "2D Euler mixed form: unknown kernel choice");
@@ -106,8 +110,12 @@ public:
       if (cfg.mixed_kernel >= 2 && !tile_ok_)
         throw SolverError(WASL_ERR_ARGUMENT, "2D Euler mixed form: the tile kernel needs"
                                              " transmissive or paired periodic boundaries");
-      if (tile_ok_)
-        build_tile_slots(t, QF);
+      if (tile_ok_) {
+        const TileSlotArrays ts = build_tile_slots(mesh_, t, boundary_, QF);
+        d_tile_nbr_.upload(ts.nbr, stream_);
+        d_tile_code_.upload(ts.code, stream_);
+        d_tile_aux_.upload(ts.aux, stream_);
+      }
       d_face_left_.upload(mesh_.face_left, stream_);
       d_face_right_.upload(face_right, stream_);
       d_face_code_.upload(face_code, stream_);
@@ -185,52 +193,17 @@ public:
   int rule_points(int rule_order) const override { return (rule_order + 1) * (rule_order + 1); }
 
   void quadrature(int rule_order, double *x, double *y, double *w) const override {
-    const Rule2D rule = triangle_rule(rule_order);
-    const int Q = rule.size();
-    for (std::int64_t e = 0; e < ne_; ++e) {
-      const TriMap &m = mesh_.maps[e];
-      const double jac = std::fabs(m.jacobian_determinant());
-      for (int q = 0; q < Q; ++q) {
-        m.to_physical(rule.xi[q], rule.eta[q], x[e * Q + q], y[e * Q + q]);
-        if (w)
-          w[e * Q + q] = rule.w[q] * jac;
-      }
-    }
+    tri_quadrature(mesh_, rule_order, x, y, w);
   }
 
   void project(int rule_order, const double *values) override {
-    const Rule2D rule = triangle_rule(rule_order);
-    const int Q = rule.size();
-    std::vector<std::vector<double>> basis(Q);
-    for (int q = 0; q < Q; ++q)
-      basis[q] = dubiner(rule.xi[q], rule.eta[q], p_);
-    std::vector<double> c(static_cast<std::size_t>(4) * M_ * ne_, 0.0);
-    for (std::int64_t e = 0; e < ne_; ++e)
-      for (int q = 0; q < Q; ++q) {
-        const double *val = values + (e * Q + q) * 4;
-        for (int v = 0; v < 4; ++v)
-          for (int m = 0; m < M_; ++m)
-            c[(static_cast<std::int64_t>(v) * M_ + m) * ne_ + e] += rule.w[q] * val[v] * basis[q][m];
-      }
-    set_state(c.data());
+    set_state(tri_project(mesh_, p_, 4, rule_order, values).data());
   }
 
   void evaluate(int rule_order, double *values) override {
-    const Rule2D rule = triangle_rule(rule_order);
-    const int Q = rule.size();
     std::vector<double> c(static_cast<std::size_t>(4) * M_ * ne_);
     get_state(c.data());
-    std::vector<std::vector<double>> basis(Q);
-    for (int q = 0; q < Q; ++q)
-      basis[q] = dubiner(rule.xi[q], rule.eta[q], p_);
-    for (std::int64_t e = 0; e < ne_; ++e)
-      for (int q = 0; q < Q; ++q)
-        for (int v = 0; v < 4; ++v) {
-          double s = 0.0;
-          for (int m = 0; m < M_; ++m)
-            s += c[(static_cast<std::int64_t>(v) * M_ + m) * ne_ + e] * basis[q][m];
-          values[(e * Q + q) * 4 + v] = s;
-        }
+    tri_evaluate(mesh_, p_, 4, rule_order, c.data(), values);
   }
 
   void set_state(const double *host) override {
@@ -316,7 +289,7 @@ public:
     for (std::int64_t n = 0; n < steps; ++n) {
       if (speed_ready_) {
         launch_dt_from_speed(1, d_speed_.get(), cfl, nullptr, nullptr, length_, p_, d_dt_.get(),
-                             stream_);
+                             nullptr, stream_);
         count_launches(1);
       } else {
         launch_cfl(cfl_args(cfl), stream_);
@@ -465,99 +438,6 @@ private:
       launch_mixed(a);
     }, stream_);
     kernel_ = tuning_.choice;
-  }
-
-  // Element-centric slots of the tile kernel (kernels.hpp TileSlots), from
-  // the face slots after periodic pairing.
-  void build_tile_slots(const TriSlots &t, int QF) {
-    std::vector<std::int32_t> nbr(3 * ne_), aux(3 * ne_, 0);
-    std::vector<std::uint8_t> code(3 * ne_);
-    for (int k = 0; k < 3; ++k)
-      for (std::int64_t e = 0; e < ne_; ++e) {
-        const std::int64_t slot = k * ne_ + e;
-        const std::int64_t f = t.slot_face[slot];
-        const std::int32_t L = mesh_.face_left[f], R = t.face_right[f];
-        const unsigned bits = (static_cast<unsigned>(mesh_.face_left_edge[f]) << 1) |
-                              (static_cast<unsigned>(mesh_.face_right_edge[f]) << 3) |
-                              (static_cast<unsigned>(mesh_.face_flip[f]) << 5);
-        const bool left = L == e;
-        if (R >= 0) {
-          nbr[slot] = left ? R : L;
-          code[slot] = static_cast<std::uint8_t>(bits | (left ? 1u : 0u));
-        } else if (boundary_ == WASL_TRANSMISSIVE) {
-          nbr[slot] = -1;
-          code[slot] = static_cast<std::uint8_t>(bits | 1u);
-        } else {
-          const std::int32_t b = -R - 1;
-          aux[slot] = b;
-          if (left) {
-            nbr[slot] = t.donors[static_cast<std::size_t>(b) * QF];
-            code[slot] = static_cast<std::uint8_t>(bits | 1u | 0x80u);
-          } else {
-            nbr[slot] = L;
-            code[slot] = static_cast<std::uint8_t>(bits | 0x40u);
-          }
-        }
-      }
-    d_tile_nbr_.upload(nbr, stream_);
-    d_tile_code_.upload(code, stream_);
-    d_tile_aux_.upload(aux, stream_);
-  }
-
-  // The mixed form evaluates each periodic face pair once, as one face
-  // between the two elements: the lower-numbered face of the pair is kept
-  // (its element is the left side, the donor the right), the other is
-  // skipped by the face kernel and its element reads the kept face's record
-  // with the donor basis as its own.  Requires every boundary face to have a
-  // single donor whose boundary face points back; otherwise the solver keeps
-  // the FP64 boundary-face kernel.
-  bool pair_periodic_faces(int QF, const std::vector<std::int32_t> &donors,
-                           const std::vector<double> &donor_basis,
-                           std::vector<std::uint8_t> &face_code, std::vector<std::int32_t> &slot_face,
-                           std::vector<std::uint8_t> &slot_code, std::vector<double> &slot_geo,
-                           const std::vector<std::int32_t> &left_slot) {
-    std::vector<std::int64_t> bface;
-    for (std::int64_t f = 0; f < mesh_.face_count(); ++f)
-      if (mesh_.face_right[f] < 0)
-        bface.push_back(f);
-    const std::size_t nb = bface.size();
-    std::vector<std::int32_t> bdonor(nb);
-    std::map<std::pair<std::int32_t, std::int32_t>, std::vector<std::size_t>> by_pair;
-    for (std::size_t b = 0; b < nb; ++b) {
-      bdonor[b] = donors[b * QF];
-      for (int q = 1; q < QF; ++q)
-        if (donors[b * QF + q] != bdonor[b])
-          return false;
-      by_pair[{mesh_.face_left[bface[b]], bdonor[b]}].push_back(b);
-    }
-    std::vector<std::size_t> partner(nb);
-    for (std::size_t b = 0; b < nb; ++b) {
-      const auto it = by_pair.find({bdonor[b], mesh_.face_left[bface[b]]});
-      if (it == by_pair.end() || it->second.size() != 1)
-        return false;
-      partner[b] = it->second[0];
-      if (partner[b] == b)
-        return false;
-    }
-    for (std::size_t b = 0; b < nb; ++b)
-      if (partner[partner[b]] != b)
-        return false;
-    for (std::size_t b = 0; b < nb; ++b) {
-      const std::int64_t f = bface[b], c = bface[partner[b]];
-      if (f < c)
-        continue; // f is the kept face of its pair
-      face_code[f] |= 0x80u;
-      const std::int32_t e = mesh_.face_left[f];
-      const std::int64_t k = left_slot[f];
-      slot_face[k * ne_ + e] = static_cast<std::int32_t>(c);
-      slot_code[k * ne_ + e] = static_cast<std::uint8_t>((mesh_.face_left_edge[c] << 1) | 0x40u);
-      slot_geo[(3 * k) * ne_ + e] = mesh_.face_nx[c];
-      slot_geo[(3 * k + 1) * ne_ + e] = mesh_.face_ny[c];
-      slot_geo[(3 * k + 2) * ne_ + e] = mesh_.face_scale[c];
-    }
-    std::vector<float> basis32(donor_basis.begin(), donor_basis.end());
-    d_basis32_.upload(basis32, stream_);
-    return true;
   }
 
   LimitArgs limit_args(double *state) {

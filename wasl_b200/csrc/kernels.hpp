@@ -227,18 +227,27 @@ void launch_euler_tri_stage_mixed(int p, int rule, const StageArgs &a, cudaStrea
 // budget; with a work list there is one CTA per entry (count <= the shape's
 // elements), else ceil(ne / elements) CTAs.  Requires transmissive
 // boundaries or paired periodic faces.
+// Largest cell-average wave speed per case over a tile work list (blocks of
+// 128 threads; tiles of any size), max-reduced into speed[case].
+void launch_batch_speed(const double *state, std::int64_t ne, int M, double gamma,
+                        const TileWork *work, std::int64_t work_count, unsigned long long *speed,
+                        unsigned long long *error, cudaStream_t stream);
 int euler_tri_tile_shapes();
 int euler_tri_tile_elements(int shape);
 void launch_euler_tri_stage_tile(int p, int rule, int shape, const StageArgs &a,
                                  cudaStream_t stream);
+// Sets the tile kernels' launch attributes on the current device (call
+// before capturing launches in a graph).
+void prepare_euler_tri_stage_tile(int p, int rule);
 void launch_limit_f64(int M, int NB, const LimitArgs &a, cudaStream_t stream);
 void launch_sense_f64(int M, const SenseArgs &a, cudaStream_t stream);
 void launch_cfl(const CflArgs &a, cudaStream_t stream);
-// dt[c] = cfl length[c] / (speed (2 p[c] + 1)) from the speeds the tile
-// kernel reduced (0 where the speed is 0), then the speed words are zeroed;
-// `cases` entries, length/p may be per case (arrays) or shared (count 1).
+// dt[c] = cfl length[c] / (speed (2 p[c] + 1)) from reduced speeds (0 where
+// the speed is 0), added to elapsed[c] when elapsed is not null; then the
+// speed words are zeroed.  length/p are per-case arrays, or null for the
+// shared length_all/p_all.
 void launch_dt_from_speed(std::int64_t cases, unsigned long long *speed, double cfl,
                           const double *length, const int *p, double length_all, int p_all,
-                          double *dt, cudaStream_t stream);
+                          double *dt, double *elapsed, cudaStream_t stream);
 
 } // namespace wasl_b200
