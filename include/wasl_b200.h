@@ -81,6 +81,9 @@ typedef struct {
   int mixed_kernel;          /* mixed form: 0 autotuned; 1 face-centric kernels (face pass
                                 + element pass); 2 + s the fused tile kernel in launch
                                 shape s (0..3, see wasl_gpu_tuning) */
+  int positivity_all;        /* with limiting: 1 applies the positivity limiter to every
+                                element, not only troubled ones (not the reference's
+                                behaviour, cpp/src/limiting/euler_modal_limiter.cpp:81-96) */
 } wasl_gpu_config;
 
 /* Fill the reference's defaults (crates/wasl-bridge/src/config.rs:87-104). */
@@ -210,6 +213,7 @@ typedef struct {
   int tile_shape;            /* 0 autotuned per polynomial order; 1 + s launch shape s */
   int use_graph;             /* 1: capture the step in a CUDA graph and replay it */
   int device;
+  int positivity_all;        /* with limiting: positivity limiter on every element */
 } wasl_batch_config;
 
 void wasl_batch_config_default(wasl_batch_config *config);
@@ -241,6 +245,11 @@ int wasl_batch_quadrature(const wasl_batch *handle, int64_t case_index, int rule
                           double *y, double *weights);
 int wasl_batch_project(wasl_batch *handle, int64_t case_index, int rule_order,
                        const double *values, int64_t count);
+
+/* The stage limiter applied to every case's current state, as the reference
+ * applies it to the projected initial state (cpp/src/case/euler_triangle.cpp:33-37).
+ * No-op without limiting. */
+int wasl_batch_limit(wasl_batch *handle);
 
 /* `steps` SSP-RK3 steps of every case, each with its own CFL time step
  * cfl h_c / ((|u| + c)_max,c (2 p_c + 1)).  Synchronizes to report errors. */

@@ -129,3 +129,36 @@ def test_bad_arguments_rejected():
     with wasl_b200.Batch([s[:4] for s in specs]) as b:
         with pytest.raises(wasl_b200.WaslError, match="out of range"):
             b.get_state(5)
+
+
+def test_batch_limit_matches_single_case_limit():
+    """wasl_batch_limit applies the same stage limiter as wasl_gpu_limit."""
+    specs = small_cases(13, count=4)
+    with wasl_b200.Batch([s[:4] for s in specs], limiting=True) as b:
+        for c, s in enumerate(specs):
+            cases.project_batch_case(b, c, s[4].conserved, s[3])
+        b.limit()
+        got = [b.get_state(c) for c in range(len(specs))]
+    for c, s in enumerate(specs):
+        with wasl_b200.Solver(*s[:3], polynomial_order=s[3], precision="mixed",
+                              volume_rule_order=s[3], boundary="transmissive", limiting=True) as g:
+            cases.project_initial(g, s[4].conserved)
+            g.limit()
+            assert np.array_equal(got[c], g.get_state()), f"case {c} differs"
+
+
+def test_batched_riemann_runs_with_always_on_positivity():
+    """The batched workload's configuration (limiter on, positivity on every
+    element, initial limiting) on a few small seeded cases: 30 steps, every
+    case advances and stays physical."""
+    specs = cases.batched_riemann_cases(6, seed=21, min_triangles=200, max_triangles=3000)
+    with wasl_b200.Batch([s[:4] for s in specs], limiting=True, positivity_all=True) as b:
+        for c, s in enumerate(specs):
+            cases.project_batch_case(b, c, s[4].conserved, s[3])
+        b.limit()
+        b.advance(0.1, 30)
+        time, dt = b.times()
+        assert np.all(time > 0) and np.all(dt > 0)
+        for c in range(len(specs)):
+            ne, nm = b.case_size(c)
+            assert np.all(b.get_state(c).reshape(4, nm, ne)[0, 0] > 0)

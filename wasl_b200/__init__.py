@@ -51,6 +51,7 @@ class Config(C.Structure):
         ("sensor_threshold", C.c_double), ("density_floor", C.c_double),
         ("pressure_floor", C.c_double), ("precision", C.c_int), ("device", C.c_int),
         ("volume_rule_order", C.c_int), ("mixed_kernel", C.c_int),
+        ("positivity_all", C.c_int),
     ]
 
 
@@ -60,6 +61,7 @@ class BatchConfig(C.Structure):
         ("sensor_threshold", C.c_double), ("density_floor", C.c_double),
         ("pressure_floor", C.c_double), ("reduced_volume_rule", C.c_int),
         ("tile_shape", C.c_int), ("use_graph", C.c_int), ("device", C.c_int),
+        ("positivity_all", C.c_int),
     ]
 
 
@@ -109,6 +111,7 @@ SIGNATURES = {
     "wasl_batch_get_state": (C.c_int, [C.c_void_p, C.c_int64, _d, C.c_int64]),
     "wasl_batch_quadrature": (C.c_int, [C.c_void_p, C.c_int64, C.c_int, _d, _d, _d]),
     "wasl_batch_project": (C.c_int, [C.c_void_p, C.c_int64, C.c_int, _d, C.c_int64]),
+    "wasl_batch_limit": (C.c_int, [C.c_void_p]),
     "wasl_batch_advance": (C.c_int, [C.c_void_p, C.c_double, C.c_int64]),
     "wasl_batch_times": (C.c_int, [C.c_void_p, _d, _d, C.c_int64]),
     "wasl_batch_tuning": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), _d, C.c_int,
@@ -168,7 +171,8 @@ class Solver:
                  equation="euler", polynomial_order=2, gamma=1.4, velocity=(0.0, 0.0),
                  boundary="periodic", boundary_right=None, inflow=(0.0, 0.0), limiting=False,
                  sensor_threshold=1e-3, density_floor=1e-10, pressure_floor=1e-10,
-                 precision="plain", device=0, volume_rule_order=0, mixed_kernel=0):
+                 precision="plain", device=0, volume_rule_order=0, mixed_kernel=0,
+                 positivity_all=False):
         lib = library()
         cfg = default_config()
         cfg.dimensions = dimensions
@@ -187,6 +191,7 @@ class Solver:
         cfg.device = device
         cfg.volume_rule_order = volume_rule_order
         cfg.mixed_kernel = mixed_kernel
+        cfg.positivity_all = 1 if positivity_all else 0
         self.config = cfg
         tags = np.ascontiguousarray(node_tags, dtype=np.int64)
         coords = np.ascontiguousarray(node_coordinates, dtype=np.float64)
@@ -356,7 +361,8 @@ class Batch:
 
     def __init__(self, cases, *, gamma=1.4, boundary="transmissive", limiting=False,
                  sensor_threshold=1e-3, density_floor=1e-10, pressure_floor=1e-10,
-                 reduced_volume_rule=True, tile_shape=0, use_graph=True, device=0):
+                 reduced_volume_rule=True, tile_shape=0, use_graph=True, device=0,
+                 positivity_all=False):
         lib = library()
         cfg = BatchConfig()
         lib.wasl_batch_config_default(C.byref(cfg))
@@ -370,6 +376,7 @@ class Batch:
         cfg.tile_shape = tile_shape
         cfg.use_graph = 1 if use_graph else 0
         cfg.device = device
+        cfg.positivity_all = 1 if positivity_all else 0
         self.config = cfg
         orders = np.array([c[3] for c in cases], dtype=np.int32)
         node_counts = np.array([len(c[0]) for c in cases], dtype=np.int64)
@@ -436,6 +443,11 @@ class Batch:
     def project(self, c, rule_order, values):
         a = np.ascontiguousarray(values, dtype=np.float64)
         self._check(self._lib.wasl_batch_project(self._h, c, rule_order, _ptr(a), a.size))
+
+    def limit(self):
+        """The stage limiter on every case's current state (as the reference
+        limits the projected initial state)."""
+        self._check(self._lib.wasl_batch_limit(self._h))
 
     def advance(self, cfl, steps):
         self._check(self._lib.wasl_batch_advance(self._h, cfl, steps))

@@ -120,12 +120,44 @@ def random_state(rng):
             rng.uniform(0.02, 1.5))
 
 
+def star_pressure(left, right, nx, ny, gamma=GAMMA):
+    """Two-rarefaction estimate of the star pressure of the 1D Riemann problem
+    between primitive states (rho, u, v, p) along the normal (nx, ny) (Toro,
+    Riemann Solvers and Numerical Methods, eq. 9.32); <= 0 when the exact
+    solution contains vacuum (u_R - u_L >= 2 (c_L + c_R) / (gamma - 1))."""
+    rl, ul, vl, pl = left
+    rr, ur, vr, pr = right
+    cl, cr = math.sqrt(gamma * pl / rl), math.sqrt(gamma * pr / rr)
+    z = (gamma - 1.0) / (2.0 * gamma)
+    numerator = cl + cr - 0.5 * (gamma - 1.0) * ((ur - ul) * nx + (vr - vl) * ny)
+    if numerator <= 0.0:
+        return 0.0
+    return (numerator / (cl / pl ** z + cr / pr ** z)) ** (1.0 / z)
+
+
+def resolvable(left, right, nx, ny, gamma=GAMMA, fraction=0.1):
+    """Whether the interface's star pressure is at least `fraction` of the
+    smaller initial pressure: the discontinuous Galerkin method with density
+    and pressure floors (the reference's limiter included) cannot follow a
+    flow into vacuum, so seeded problems that would open one are redrawn."""
+    return star_pressure(left, right, nx, ny, gamma) >= fraction * min(left[3], right[3])
+
+
 class QuadrantRiemann:
-    """Seeded four-quadrant Riemann problem on [0,1]^2."""
+    """Seeded four-quadrant Riemann problem on [0,1]^2 (states redrawn until
+    every interface between neighbouring quadrants is resolvable)."""
 
     def __init__(self, seed=3, gamma=GAMMA):
         rng = np.random.Generator(np.random.PCG64(seed))
-        self.states = np.array([conserved(*random_state(rng), gamma=gamma) for _ in range(4)])
+        while True:
+            prim = [random_state(rng) for _ in range(4)]
+            # quadrants 0 (SW), 1 (SE), 2 (NW), 3 (NE)
+            if (resolvable(prim[0], prim[1], 1, 0, gamma) and resolvable(prim[2], prim[3], 1, 0, gamma)
+                    and resolvable(prim[0], prim[2], 0, 1, gamma)
+                    and resolvable(prim[1], prim[3], 0, 1, gamma)):
+                break
+        self.primitive_states = prim
+        self.states = np.array([conserved(*s, gamma=gamma) for s in prim])
 
     def conserved(self, x, y, t=0.0):
         q = (x >= 0.5).astype(int) + 2 * (y >= 0.5).astype(int)
@@ -133,14 +165,20 @@ class QuadrantRiemann:
 
 
 class PlanarRiemann:
-    """Two seeded states split by a line through (cx, cy) at a random angle."""
+    """Two seeded states split by a line through (cx, cy) at a random angle
+    (states redrawn until the interface is resolvable)."""
 
     def __init__(self, seed=0, gamma=GAMMA):
         rng = np.random.Generator(np.random.PCG64(seed))
-        self.left = conserved(*random_state(rng), gamma=gamma)
-        self.right = conserved(*random_state(rng), gamma=gamma)
         self.angle = rng.uniform(0.0, 2.0 * math.pi)
         self.cx, self.cy = rng.uniform(0.3, 0.7, size=2)
+        nx, ny = math.cos(self.angle), math.sin(self.angle)
+        while True:
+            left, right = random_state(rng), random_state(rng)
+            if resolvable(left, right, nx, ny, gamma):
+                break
+        self.left = conserved(*left, gamma=gamma)
+        self.right = conserved(*right, gamma=gamma)
 
     def conserved(self, x, y, t=0.0):
         side = (x - self.cx) * math.cos(self.angle) + (y - self.cy) * math.sin(self.angle) >= 0.0

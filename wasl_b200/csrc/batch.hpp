@@ -35,6 +35,7 @@ public:
   void quadrature(std::int64_t c, int rule, double *x, double *y, double *w) const;
   void project(std::int64_t c, int rule, const double *values);
   void advance(double cfl, std::int64_t steps);
+  void limit();
   void times(double *time, double *dt);
   int tuning(int p, double *ms, int capacity, int &count) const;
   cudaStream_t stream() const { return stream_; }

@@ -349,6 +349,9 @@ LimitArgs BatchSolver::limit_args(const Group &g, double *state) const {
   l.pressure_floor = cfg_.pressure_floor;
   l.limited = g.limited.get();
   l.error = d_error_.get();
+  l.positivity_all = cfg_.positivity_all ? 1 : 0;
+  l.flags = g.flags.get();
+  l.relative_floor = kMixedRelativeFloor;
   return l;
 }
 
@@ -394,7 +397,7 @@ void BatchSolver::enqueue_step(double cfl) {
       ++launches_per_step_;
       if (cfg_.limiting) {
         launch_limit_f64(g.M, 3, limit_args(g, a.out), stream_);
-        launches_per_step_ += 2;
+        launches_per_step_ += cfg_.positivity_all ? 3 : 2;
       }
     }
 }
@@ -428,6 +431,28 @@ void BatchSolver::advance(double cfl, std::int64_t steps) {
       enqueue_step(cfl);
   }
   launches_ += launches_per_step_ * steps;
+  check_error();
+}
+
+void BatchSolver::limit() {
+  if (!cfg_.limiting)
+    return;
+  for (auto &gp : groups_) {
+    Group &g = *gp;
+    if (g.p == 0)
+      continue;
+    cuda_check(cudaMemsetAsync(g.count.get(), 0, sizeof(std::int32_t), stream_), "count");
+    SenseArgs sa;
+    sa.ne = g.ne;
+    sa.state = g.u.get();
+    sa.threshold = cfg_.sensor_threshold;
+    sa.highest_degree_begin = g.highest_degree_begin;
+    sa.flags = g.flags.get();
+    sa.troubled = g.troubled.get();
+    sa.troubled_count = g.count.get();
+    launch_sense_f64(g.M, sa, stream_);
+    launch_limit_f64(g.M, 3, limit_args(g, g.u.get()), stream_);
+  }
   check_error();
 }
 

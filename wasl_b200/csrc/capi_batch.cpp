@@ -151,6 +151,10 @@ int wasl_batch_project(wasl_batch *h, int64_t c, int rule_order, const double *v
   });
 }
 
+int wasl_batch_limit(wasl_batch *h) {
+  return guarded(h, [&] { h->solver->limit(); });
+}
+
 int wasl_batch_advance(wasl_batch *h, double cfl, int64_t steps) {
   return guarded(h, [&] {
     need(cfl > 0.0 && steps >= 0, "batch advance: cfl must be positive and steps non-negative");

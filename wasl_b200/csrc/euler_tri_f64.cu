@@ -250,6 +250,89 @@ template <int M> __device__ __forceinline__ double smoothness(const double *c) {
   return value;
 }
 
+// The positivity limiter on one element's modes lim[4 M]
+// (cpp/include/wasl/limiting/positivity/euler_positivity.hpp:44-102): density
+// scaled toward the mean to keep rho >= floor at every check point, then the
+// pressure factor found by 64 bisection steps per violating point; a mean
+// below a floor sets the error word instead.
+template <int M>
+__device__ __forceinline__ void positivity_limit(const LimitArgs &a, double *lim, std::int64_t e) {
+  const double inv_root2 = 1.0 / sqrt(2.0);
+  const double pavg[4] = {lim[0] * inv_root2, lim[M] * inv_root2, lim[2 * M] * inv_root2,
+                          lim[3 * M] * inv_root2};
+  if (pavg[0] <= a.density_floor || primitive(a.gamma, pavg).p <= a.pressure_floor) {
+    raise_error(a.error, kBelowFloor, e);
+    return;
+  }
+  // Check-point floors: the absolute floors, raised to a fraction of the mean
+  // density and energy when relative_floor > 0 (forms whose fluxes evaluate
+  // point states in FP32, which resolves them only to ~1e-7 of the mean).
+  const double rf = a.relative_floor > 0.0 ? fmax(a.density_floor, a.relative_floor * pavg[0])
+                                           : a.density_floor;
+  const double pf = a.relative_floor > 0.0 ? fmax(a.pressure_floor, a.relative_floor * pavg[3])
+                                           : a.pressure_floor;
+  double dscale = 1.0;
+  for (int pt = 0; pt < a.check_points; ++pt) {
+    const double *b = a.check_basis + pt * M;
+    double rho = 0.0;
+    for (int m = 0; m < M; ++m)
+      rho += lim[m] * b[m];
+    if (rho < rf)
+      dscale = smin(dscale, (pavg[0] - rf) / (pavg[0] - rho));
+  }
+  for (int v = 0; v < 4; ++v)
+    for (int m = 1; m < M; ++m)
+      lim[v * M + m] *= dscale;
+  double pscale = 1.0;
+  for (int pt = 0; pt < a.check_points; ++pt) {
+    const double *b = a.check_basis + pt * M;
+    double s[4];
+    for (int v = 0; v < 4; ++v) {
+      double acc = 0.0;
+      for (int m = 0; m < M; ++m)
+        acc += lim[v * M + m] * b[m];
+      s[v] = acc;
+    }
+    if (primitive(a.gamma, s).p >= pf)
+      continue;
+    double lower = 0.0, upper = 1.0;
+    for (int it = 0; it < 64; ++it) {
+      const double middle = 0.5 * (lower + upper);
+      double x[4];
+      for (int v = 0; v < 4; ++v)
+        x[v] = pavg[v] + middle * (s[v] - pavg[v]);
+      if (primitive(a.gamma, x).p >= pf)
+        lower = middle;
+      else
+        upper = middle;
+    }
+    pscale = smin(pscale, lower);
+  }
+  for (int v = 0; v < 4; ++v)
+    for (int m = 1; m < M; ++m)
+      lim[v * M + m] *= pscale;
+}
+
+// The positivity limiter on every element the sensor did not flag (flags[e]
+// == 0), in place: the always-on positivity of the non-reference forms (the
+// reference limits positivity in troubled cells only,
+// cpp/src/limiting/euler_modal_limiter.cpp:81-96).
+template <int M> __global__ void positivity_rest(const LimitArgs a) {
+  for (std::int64_t e = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < a.ne;
+       e += static_cast<std::int64_t>(gridDim.x) * blockDim.x) {
+    if (a.flags && a.flags[e])
+      continue;
+    double lim[4 * M];
+#pragma unroll
+    for (int i = 0; i < 4 * M; ++i)
+      lim[i] = a.state[i * a.ne + e];
+    positivity_limit<M>(a, lim, e);
+#pragma unroll
+    for (int i = 0; i < 4 * M; ++i)
+      a.state[i * a.ne + e] = lim[i];
+  }
+}
+
 template <int M, int NB>
 __global__ void __launch_bounds__(64) limit_f64(const LimitArgs a) {
   const int count = *a.troubled_count;
@@ -342,55 +425,7 @@ __global__ void __launch_bounds__(64) limit_f64(const LimitArgs a) {
     for (int v = 0; v < 4; ++v)
       lim[v * M] = target[v * M];
 
-    // Positivity (limiting/positivity/euler_positivity.hpp:63-102).
-    const double inv_root2 = 1.0 / sqrt(2.0);
-    const double pavg[4] = {lim[0] * inv_root2, lim[M] * inv_root2, lim[2 * M] * inv_root2,
-                            lim[3 * M] * inv_root2};
-    const double rf = a.density_floor, pf = a.pressure_floor;
-    if (pavg[0] <= rf || primitive(a.gamma, pavg).p <= pf) {
-      raise_error(a.error, kBelowFloor, e);
-    } else {
-      double dscale = 1.0;
-      for (int pt = 0; pt < a.check_points; ++pt) {
-        const double *b = a.check_basis + pt * M;
-        double rho = 0.0;
-        for (int m = 0; m < M; ++m)
-          rho += lim[m] * b[m];
-        if (rho < rf)
-          dscale = smin(dscale, (pavg[0] - rf) / (pavg[0] - rho));
-      }
-      for (int v = 0; v < 4; ++v)
-        for (int m = 1; m < M; ++m)
-          lim[v * M + m] *= dscale;
-      double pscale = 1.0;
-      for (int pt = 0; pt < a.check_points; ++pt) {
-        const double *b = a.check_basis + pt * M;
-        double s[4];
-        for (int v = 0; v < 4; ++v) {
-          double acc = 0.0;
-          for (int m = 0; m < M; ++m)
-            acc += lim[v * M + m] * b[m];
-          s[v] = acc;
-        }
-        if (primitive(a.gamma, s).p >= pf)
-          continue;
-        double lower = 0.0, upper = 1.0;
-        for (int it = 0; it < 64; ++it) {
-          const double middle = 0.5 * (lower + upper);
-          double x[4];
-          for (int v = 0; v < 4; ++v)
-            x[v] = pavg[v] + middle * (s[v] - pavg[v]);
-          if (primitive(a.gamma, x).p >= pf)
-            lower = middle;
-          else
-            upper = middle;
-        }
-        pscale = smin(pscale, lower);
-      }
-      for (int v = 0; v < 4; ++v)
-        for (int m = 1; m < M; ++m)
-          lim[v * M + m] *= pscale;
-    }
+    positivity_limit<M>(a, lim, e);
     double *dst = a.limited + static_cast<std::int64_t>(k) * 4 * M;
     for (int i = 0; i < 4 * M; ++i)
       dst[i] = lim[i];
@@ -560,11 +595,14 @@ void launch_euler_tri_stage_f64(int p, const StageArgs &a, cudaStream_t s) {
 void launch_limit_f64(int M, int NB, const LimitArgs &a, cudaStream_t s) {
   const unsigned blocks = static_cast<unsigned>(std::min<std::int64_t>((a.ne + 63) / 64, 148 * 16));
   const unsigned sblocks = static_cast<unsigned>(std::min<std::int64_t>((a.ne + 255) / 256, 148 * 8));
+  const unsigned pblocks = static_cast<unsigned>(std::min<std::int64_t>((a.ne + 127) / 128, 148 * 16));
 #define WASL_LIMIT(MM, NN)                                                                     \
   if (M == MM && NB == NN) {                                                                   \
     limit_f64<MM, NN><<<blocks, 64, 0, s>>>(a);                                                \
     scatter_limited<MM><<<sblocks, 256, 0, s>>>(a.state, a.ne, a.troubled, a.troubled_count,   \
                                                  a.limited);                                   \
+    if (a.positivity_all)                                                                      \
+      positivity_rest<MM><<<pblocks, 128, 0, s>>>(a);                                          \
     return;                                                                                    \
   }
   WASL_LIMIT(3, 3)

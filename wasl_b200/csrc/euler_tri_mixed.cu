@@ -135,10 +135,17 @@ struct Side32 {
   float rho, inv, u, v, p, un, dun, e, c, dfn[4];
 };
 
+// Smallest point density FP32 works with, as a fraction of the mean: the
+// positivity limiter keeps point values above its floors in FP64, but near
+// vacuum mean + perturbation can round to zero or below in FP32; there the
+// density used for velocities and sound speed is clamped to this fraction of
+// the mean (and the pressure to zero), which changes nothing elsewhere.
+constexpr float kVacuumFraction = 1e-6f;
+
 __device__ __forceinline__ Side32 perturbed_side(const Ref32 &b, const float *d, float g1,
                                                  float gamma, float nx, float ny) {
   Side32 s;
-  s.rho = b.rho + d[0];
+  s.rho = fmaxf(b.rho + d[0], kVacuumFraction * b.rho);
   s.inv = __frcp_rn(s.rho);
   const float du = (d[1] - b.u * d[0]) * s.inv;
   const float dv = (d[2] - b.v * d[0]) * s.inv;
@@ -174,7 +181,9 @@ __device__ __forceinline__ void hllc_perturbed(const Ref32 &b, const float *dl, 
   // selected afterwards, so a warp never diverges on the flow regime.
   const float dpress = (R.p - b.p) - (L.p - b.p);
   const float dn = R.dun - L.dun;
-  const float den = L.rho * (sl - L.un) - R.rho * (sr - R.un);
+  // den <= 0 always (sl <= u_L - c_L, sr >= u_R + c_R); it is zero only when
+  // both sound speeds vanish, which FP32 rounding can produce near vacuum.
+  const float den = fminf(L.rho * (sl - L.un) - R.rho * (sr - R.un), -1e-30f);
   const float sigma_l = (dpress - R.rho * (sr - R.un) * dn) / den; // S* - u_L
   const float star = L.un + sigma_l;
   const bool left = star >= 0.0f;
@@ -183,11 +192,15 @@ __device__ __forceinline__ void hllc_perturbed(const Ref32 &b, const float *dl, 
   const float kun = left ? L.un : R.un;
   const float wave = left ? sl : sr;
   const float sigma = left ? sigma_l : sigma_l - dn; // S* - u_K
-  const float drho = krho * sigma / (wave - star);
+  // S_K - S* and S_K - u_K keep their sign (negative on the left, positive
+  // on the right) and stay off zero in the FP32 near-vacuum corner case.
+  const float wave_gap = left ? fminf(wave - star, -1e-30f) : fmaxf(wave - star, 1e-30f);
+  const float kun_gap = left ? fminf(wave - kun, -1e-30f) : fmaxf(wave - kun, 1e-30f);
+  const float drho = krho * sigma / wave_gap;
   const float rho_star = krho + drho;
   const float t = rho_star * sigma;
   const float jump[4] = {drho, drho * ku + t * nx, drho * kv + t * ny,
-                         drho * ke * kinv + t * (star + kp / (krho * (wave - kun)))};
+                         drho * ke * kinv + t * (star + kp / (krho * kun_gap))};
 #pragma unroll
   for (int v = 0; v < 4; ++v) {
     const float starf = (left ? L.dfn[v] : R.dfn[v]) + wave * jump[v];
@@ -451,7 +464,7 @@ __global__ void __launch_bounds__(128) euler_tri_elements_mixed(const StageArgs 
           s = fmaf(ch[v][m], T.phi[q][m], s);
         d[v] = s;
       }
-      const float inv = __frcp_rn(bb.rho + d[0]);
+      const float inv = __frcp_rn(fmaxf(bb.rho + d[0], kVacuumFraction * bb.rho));
       const float du = (d[1] - bb.u * d[0]) * inv;
       const float dv = (d[2] - bb.v * d[0]) * inv;
       const float uu = bb.u + du, vv = bb.v + dv;
@@ -666,7 +679,7 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_mixed(const StageAr
           s = fmaf(ch[v][m], T.phi[q][m], s);
         d[v] = s;
       }
-      const float inv = __frcp_rn(bb.rho + d[0]);
+      const float inv = __frcp_rn(fmaxf(bb.rho + d[0], kVacuumFraction * bb.rho));
       const float du = (d[1] - bb.u * d[0]) * inv;
       const float dv = (d[2] - bb.v * d[0]) * inv;
       const float uu = bb.u + du, vv = bb.v + dv;

@@ -276,8 +276,8 @@ public:
     sa.troubled = d_troubled_.get();
     sa.troubled_count = d_count_.get();
     launch_sense_f64(M_, sa, stream_);
-    launch_limit_f64(M_, 3, limit_args(d_u_.get()), stream_);
-    count_launches(3);
+    launch_limit_f64(M_, 3, limit_args(d_u_.get(), d_flags_.get()), stream_);
+    count_launches(cfg_.positivity_all ? 4 : 3);
     check_error();
   }
 
@@ -399,8 +399,8 @@ private:
       }
       stage_end();
       if (limiting_) {
-        launch_limit_f64(M_, 3, limit_args(outs[k]), stream_);
-        count_launches(2);
+        launch_limit_f64(M_, 3, limit_args(outs[k], d_flags_.get() + k * ne_), stream_);
+        count_launches(cfg_.positivity_all ? 3 : 2);
       }
     }
     cuda_check(cudaGetLastError(), "stage launch");
@@ -440,8 +440,11 @@ private:
     kernel_ = tuning_.choice;
   }
 
-  LimitArgs limit_args(double *state) {
+  LimitArgs limit_args(double *state, const std::uint8_t *flags) {
     LimitArgs l;
+    l.positivity_all = cfg_.positivity_all ? 1 : 0;
+    l.flags = flags;
+    l.relative_floor = mixed_ ? kMixedRelativeFloor : 0.0;
     l.ne = ne_;
     l.state = state;
     l.troubled = d_troubled_.get();

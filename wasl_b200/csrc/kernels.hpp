@@ -132,7 +132,20 @@ struct LimitArgs {
   double gamma = 1.4, density_floor = 1e-10, pressure_floor = 1e-10;
   double *limited = nullptr;                 // [ne][4][M] scratch, by list position
   unsigned long long *error = nullptr;
+  // Always-on positivity (not the reference's behaviour): after the troubled
+  // cells, the positivity limiter also runs on every element with flags[e]
+  // == 0.  The launch then counts three kernels instead of two.
+  int positivity_all = 0;
+  const std::uint8_t *flags = nullptr;
+  // > 0: the check-point floors become max(floor, relative_floor x mean
+  // density) and max(floor, relative_floor x mean energy) (the mixed form).
+  double relative_floor = 0.0;
 };
+
+// The mixed form's positivity check-point floors relative to the mean: FP32
+// resolves a point state to ~6e-8 of the mean, so point densities and
+// pressures are kept at least 1e-5 of the mean density and energy.
+constexpr double kMixedRelativeFloor = 1e-5;
 
 // Modal-decay sensor on the density modes of `state` (modal_decay.hpp:23-33).
 struct SenseArgs {
