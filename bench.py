@@ -500,6 +500,7 @@ def batched(args, rank, world, local_rank):
     torch.cuda.synchronize()
     e2e_ms = start.elapsed_time(end) / e2e_steps
     times, dts = b.times()
+    status = b.status()
     peaks, peak_kind = measured_peaks()
     per_step_bytes = 3.0 * (BYTES_PER_DOF * b.dof + BYTES_PER_ELEMENT * b.elements)
     achieved = per_step_bytes / (ms * 1e-3 / args.steps) / 1e9
@@ -532,6 +533,9 @@ def batched(args, rank, world, local_rank):
         "gpu_launches": per_step * args.steps,
         "clocks": clocks,
         "simulated_time": {"min": float(times.min()), "max": float(times.max())},
+        "failed_cases": {"count": int((status != 0).sum()),
+                         "cases": [int(c) for c in np.nonzero(status)[0][:20]],
+                         "note": "a failed case is frozen (dt 0) and still swept by every launch"},
     }
     b.close()
     if dist:

@@ -252,8 +252,16 @@ int wasl_batch_project(wasl_batch *handle, int64_t case_index, int rule_order,
 int wasl_batch_limit(wasl_batch *handle);
 
 /* `steps` SSP-RK3 steps of every case, each with its own CFL time step
- * cfl h_c / ((|u| + c)_max,c (2 p_c + 1)).  Synchronizes to report errors. */
+ * cfl h_c / ((|u| + c)_max,c (2 p_c + 1)).  A case that fails (a non-physical
+ * cell average, or a mean below a positivity floor) is frozen (dt 0 from then
+ * on) and recorded in wasl_batch_status; the other cases go on, and the call
+ * still returns 0.  Synchronizes to report CUDA errors. */
 int wasl_batch_advance(wasl_batch *handle, double cfl, int64_t steps);
+
+/* Per case: 0, or the failure that froze it: 1 a non-physical cell average
+ * (cpp/src/time/cfl_timestep.cpp:39-40), 2 a positivity mean below a floor
+ * (cpp/include/wasl/limiting/positivity/euler_positivity.hpp:74-75). */
+int wasl_batch_status(wasl_batch *handle, int *status, int64_t count);
 
 /* Per case: time advanced since creation, and the last step's dt. */
 int wasl_batch_times(wasl_batch *handle, double *time, double *dt, int64_t count);

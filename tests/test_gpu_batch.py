@@ -108,18 +108,32 @@ def test_batch_autotunes_each_order_and_conserves():
                 area * before)
 
 
-def test_nonphysical_case_reported():
+@pytest.mark.parametrize("limiting", [False, True])
+def test_failed_case_is_frozen_and_the_rest_go_on(limiting):
+    """A case with a non-physical cell average (made on the host) is frozen
+    and reported; the other cases advance exactly as in a batch without it."""
     specs = small_cases(5, count=3)
-    with wasl_b200.Batch([s[:4] for s in specs]) as b:
-        for c, s in enumerate(specs):
-            cases.project_batch_case(b, c, smooth_field, s[3])
-        ne, nm = b.case_size(1)
-        state = b.get_state(1).reshape(4, nm, ne)
-        state[0, 0, ne // 2] = -0.5  # a negative cell-average density, made on the host
-        b.set_state(1, state)
-        with pytest.raises(wasl_b200.WaslError, match="not physical") as err:
-            b.advance(0.1, 1)
-        assert err.value.status == -4
+    states = {}
+    for bad in (True, False):
+        with wasl_b200.Batch([s[:4] for s in specs], limiting=limiting, tile_shape=1) as b:
+            for c, s in enumerate(specs):
+                cases.project_batch_case(b, c, smooth_field, s[3])
+            if bad:
+                ne, nm = b.case_size(1)
+                state = b.get_state(1).reshape(4, nm, ne)
+                state[0, 0, ne // 2] = -0.5  # a negative cell-average density
+                b.set_state(1, state)
+            b.advance(0.1, 3)
+            status = b.status()
+            time, _ = b.times()
+            states[bad] = [b.get_state(c) for c in (0, 2)]
+            if bad:
+                assert status.tolist() == [0, 1, 0]
+                assert time[1] == 0.0 and time[0] > 0 and time[2] > 0
+            else:
+                assert not status.any()
+    for a, b_ in zip(states[True], states[False]):
+        assert np.array_equal(a, b_)
 
 
 def test_bad_arguments_rejected():

@@ -114,6 +114,7 @@ SIGNATURES = {
     "wasl_batch_limit": (C.c_int, [C.c_void_p]),
     "wasl_batch_advance": (C.c_int, [C.c_void_p, C.c_double, C.c_int64]),
     "wasl_batch_times": (C.c_int, [C.c_void_p, _d, _d, C.c_int64]),
+    "wasl_batch_status": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.c_int64]),
     "wasl_batch_tuning": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), _d, C.c_int,
                                     C.POINTER(C.c_int)]),
     "wasl_batch_launches": (C.c_int, [C.c_void_p, _i64, C.POINTER(C.c_int), _i64]),
@@ -456,6 +457,14 @@ class Batch:
         t, dt = np.empty(self.cases), np.empty(self.cases)
         self._check(self._lib.wasl_batch_times(self._h, _ptr(t), _ptr(dt), self.cases))
         return t, dt
+
+    def status(self):
+        """Per case: 0, or 1 (non-physical average) / 2 (mean below a floor)
+        for a case that failed and was frozen."""
+        out = np.zeros(self.cases, dtype=np.int32)
+        self._check(self._lib.wasl_batch_status(self._h, out.ctypes.data_as(C.POINTER(C.c_int)),
+                                                self.cases))
+        return out
 
     def tuning(self, polynomial_order):
         choice, count = C.c_int(), C.c_int()

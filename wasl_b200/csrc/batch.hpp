@@ -37,6 +37,7 @@ public:
   void advance(double cfl, std::int64_t steps);
   void limit();
   void times(double *time, double *dt);
+  void status(int *out);
   int tuning(int p, double *ms, int capacity, int &count) const;
   cudaStream_t stream() const { return stream_; }
   std::int64_t launches_per_step() const { return launches_per_step_; }
@@ -54,7 +55,7 @@ private:
     TuneResult tuning;
     int highest_degree_begin = 0, check_points = 0;
     DeviceArray<double> u, e, s, geo, slot_geo, transforms, normal_x, normal_y, check, limited;
-    DeviceArray<std::int32_t> tile_nbr, tile_aux, neighbors, troubled, count;
+    DeviceArray<std::int32_t> tile_nbr, tile_aux, neighbors, troubled, count, element_case;
     DeviceArray<std::uint8_t> tile_code, flags;
     DeviceArray<float> basis32;
     DeviceArray<unsigned char> face_table;
@@ -79,7 +80,7 @@ private:
   std::vector<TriTopology> meshes_; // maps only, for quadrature and projection
   std::int64_t total_elements_ = 0, total_dof_ = 0;
   DeviceArray<double> d_length_, d_dt_, d_time_;
-  DeviceArray<int> d_p_;
+  DeviceArray<int> d_p_, d_status_;
   DeviceArray<unsigned long long> d_speed_, d_error_;
   bool tuned_ = false;
   cudaGraphExec_t graph_exec_ = nullptr;

@@ -180,6 +180,12 @@ BatchSolver::BatchSolver(const wasl_batch_config &cfg, std::int64_t case_count, 
       lengths[c] = cs.length;
       case_p[c] = p;
     }
+    std::vector<std::int32_t> element_case(ne);
+    for (std::int64_t c : members)
+      std::fill(element_case.begin() + case_offset_[c],
+                element_case.begin() + case_offset_[c] + setup[c].mesh.element_count,
+                static_cast<std::int32_t>(c));
+    g->element_case.upload(element_case, stream_);
     g->geo.upload(geo, stream_);
     g->slot_geo.upload(slot_geo, stream_);
     g->tile_nbr.upload(nbr, stream_);
@@ -242,6 +248,8 @@ BatchSolver::BatchSolver(const wasl_batch_config &cfg, std::int64_t case_count, 
   d_time_.resize(case_count);
   d_speed_.resize(case_count);
   d_error_.resize(1);
+  d_status_.resize(case_count);
+  cuda_check(cudaMemsetAsync(d_status_.get(), 0, case_count * sizeof(int), stream_), "memset");
   cuda_check(cudaMemsetAsync(d_dt_.get(), 0, case_count * sizeof(double), stream_), "memset");
   cuda_check(cudaMemsetAsync(d_time_.get(), 0, case_count * sizeof(double), stream_), "memset");
   cuda_check(cudaMemsetAsync(d_speed_.get(), 0, case_count * sizeof(unsigned long long), stream_),
@@ -352,6 +360,8 @@ LimitArgs BatchSolver::limit_args(const Group &g, double *state) const {
   l.positivity_all = cfg_.positivity_all ? 1 : 0;
   l.flags = g.flags.get();
   l.relative_floor = kMixedRelativeFloor;
+  l.case_status = d_status_.get();
+  l.element_case = g.element_case.get();
   return l;
 }
 
@@ -382,10 +392,11 @@ void BatchSolver::enqueue_step(double cfl) {
   for (auto &gp : groups_) {
     const Group &g = *gp;
     launch_batch_speed(g.u.get(), g.ne, g.M, cfg_.heat_capacity_ratio, g.work[g.shape].get(),
-                       g.work_count[g.shape], d_speed_.get(), d_error_.get(), stream_);
+                       g.work_count[g.shape], d_speed_.get(), d_error_.get(), d_status_.get(),
+                       stream_);
   }
   launch_dt_from_speed(cases_, d_speed_.get(), cfl, d_length_.get(), d_p_.get(), 0.0, 0,
-                       d_dt_.get(), d_time_.get(), stream_);
+                       d_dt_.get(), d_time_.get(), d_status_.get(), stream_);
   launches_per_step_ = static_cast<std::int64_t>(groups_.size()) + 1;
   for (int k = 0; k < 3; ++k)
     for (auto &gp : groups_) {
@@ -467,6 +478,13 @@ void BatchSolver::check_error() {
     // The element index is the group's; name the case it belongs to.
     throw_device_error(word);
   }
+}
+
+void BatchSolver::status(int *out) {
+  cuda_check(cudaMemcpyAsync(out, d_status_.get(), cases_ * sizeof(int), cudaMemcpyDeviceToHost,
+                             stream_),
+             "status");
+  cuda_check(cudaStreamSynchronize(stream_), "status");
 }
 
 void BatchSolver::times(double *time, double *dt) {

@@ -162,6 +162,13 @@ int wasl_batch_advance(wasl_batch *h, double cfl, int64_t steps) {
   });
 }
 
+int wasl_batch_status(wasl_batch *h, int *status, int64_t count) {
+  return guarded(h, [&] {
+    need(status && count == h->solver->cases(), "batch status: count must be the number of cases");
+    h->solver->status(status);
+  });
+}
+
 int wasl_batch_times(wasl_batch *h, double *time, double *dt, int64_t count) {
   return guarded(h, [&] {
     need(count == h->solver->cases(), "batch times: count must be the number of cases");

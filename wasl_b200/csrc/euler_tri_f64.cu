@@ -260,8 +260,12 @@ __device__ __forceinline__ void positivity_limit(const LimitArgs &a, double *lim
   const double inv_root2 = 1.0 / sqrt(2.0);
   const double pavg[4] = {lim[0] * inv_root2, lim[M] * inv_root2, lim[2 * M] * inv_root2,
                           lim[3 * M] * inv_root2};
-  if (pavg[0] <= a.density_floor || primitive(a.gamma, pavg).p <= a.pressure_floor) {
-    raise_error(a.error, kBelowFloor, e);
+  if (!(pavg[0] > a.density_floor && primitive(a.gamma, pavg).p > a.pressure_floor)) {
+    // (a NaN mean fails too) - recorded against its case when cases are tracked
+    if (a.case_status)
+      atomicCAS(a.case_status + a.element_case[e], 0, static_cast<int>(kBelowFloor));
+    else
+      raise_error(a.error, kBelowFloor, e);
     return;
   }
   // Check-point floors: the absolute floors, raised to a fraction of the mean
@@ -534,14 +538,15 @@ __global__ void cfl_finish(const CflArgs a) {
 // then the word is zeroed for the next reduction.
 __global__ void dt_from_speed(std::int64_t cases, unsigned long long *speed, double cfl,
                               const double *length, const int *p, double length_all, int p_all,
-                              double *dt, double *elapsed) {
+                              double *dt, double *elapsed, const int *status) {
   const std::int64_t c = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (c >= cases)
     return;
   const double v = __longlong_as_double(static_cast<long long>(speed[c]));
   const double h = length ? length[c] : length_all;
   const int order = p ? p[c] : p_all;
-  const double step = v > 0.0 ? cfl * h / (v * (2 * order + 1)) : 0.0;
+  // A failed case is frozen: dt 0.
+  const double step = v > 0.0 && !(status && status[c]) ? cfl * h / (v * (2 * order + 1)) : 0.0;
   dt[c] = step;
   if (elapsed)
     elapsed[c] += step;
@@ -635,9 +640,9 @@ void launch_sense_f64(int M, const SenseArgs &a, cudaStream_t s) {
 
 void launch_dt_from_speed(std::int64_t cases, unsigned long long *speed, double cfl,
                           const double *length, const int *p, double length_all, int p_all,
-                          double *dt, double *elapsed, cudaStream_t s) {
+                          double *dt, double *elapsed, const int *status, cudaStream_t s) {
   dt_from_speed<<<static_cast<unsigned>((cases + 255) / 256), 256, 0, s>>>(
-      cases, speed, cfl, length, p, length_all, p_all, dt, elapsed);
+      cases, speed, cfl, length, p, length_all, p_all, dt, elapsed, status);
 }
 
 void launch_cfl(const CflArgs &a, cudaStream_t s) {

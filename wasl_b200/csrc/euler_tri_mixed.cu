@@ -895,7 +895,7 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_mixed(const StageAr
 // bits into speed[case]; a non-physical average sets the error word.
 __global__ void batch_speed(const double *state, std::int64_t ne, int M, double gamma,
                             const TileWork *work, unsigned long long *speed,
-                            unsigned long long *error) {
+                            unsigned long long *error, int *status) {
   const TileWork w = work[blockIdx.x];
   const int lane = threadIdx.x & 31;
   unsigned long long best = 0;
@@ -911,6 +911,8 @@ __global__ void batch_speed(const double *state, std::int64_t ne, int M, double 
     if (physical) {
       const unsigned long long bits = __double_as_longlong(speed);
       best = bits > best ? bits : best;
+    } else if (status) {
+      atomicCAS(status + w.case_id, 0, static_cast<int>(kNonPhysicalAverage));
     } else {
       raise_error(error, kNonPhysicalAverage, e);
     }
@@ -1085,10 +1087,10 @@ void launch_euler_tri_stage_tile(int p, int rule, int shape, const StageArgs &a,
 
 void launch_batch_speed(const double *state, std::int64_t ne, int M, double gamma,
                         const TileWork *work, std::int64_t work_count, unsigned long long *speed,
-                        unsigned long long *error, cudaStream_t s) {
+                        unsigned long long *error, int *status, cudaStream_t s) {
   if (work_count > 0)
     batch_speed<<<static_cast<unsigned>(work_count), 128, 0, s>>>(state, ne, M, gamma, work, speed,
-                                                                  error);
+                                                                  error, status);
 }
 
 void launch_euler_tri_stage_mixed(int p, int rule, const StageArgs &a, cudaStream_t s) {

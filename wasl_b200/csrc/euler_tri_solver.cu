@@ -289,7 +289,7 @@ public:
     for (std::int64_t n = 0; n < steps; ++n) {
       if (speed_ready_) {
         launch_dt_from_speed(1, d_speed_.get(), cfl, nullptr, nullptr, length_, p_, d_dt_.get(),
-                             nullptr, stream_);
+                             nullptr, nullptr, stream_);
         count_launches(1);
       } else {
         launch_cfl(cfl_args(cfl), stream_);

@@ -140,6 +140,10 @@ struct LimitArgs {
   // > 0: the check-point floors become max(floor, relative_floor x mean
   // density) and max(floor, relative_floor x mean energy) (the mixed form).
   double relative_floor = 0.0;
+  // Batched solves: a mean below a floor is recorded as case_status[case of
+  // e] (first error only) instead of in the error word.
+  int *case_status = nullptr;
+  const std::int32_t *element_case = nullptr;
 };
 
 // The mixed form's positivity check-point floors relative to the mean: FP32
@@ -244,7 +248,7 @@ void launch_euler_tri_stage_mixed(int p, int rule, const StageArgs &a, cudaStrea
 // 128 threads; tiles of any size), max-reduced into speed[case].
 void launch_batch_speed(const double *state, std::int64_t ne, int M, double gamma,
                         const TileWork *work, std::int64_t work_count, unsigned long long *speed,
-                        unsigned long long *error, cudaStream_t stream);
+                        unsigned long long *error, int *status, cudaStream_t stream);
 int euler_tri_tile_shapes();
 int euler_tri_tile_elements(int shape);
 void launch_euler_tri_stage_tile(int p, int rule, int shape, const StageArgs &a,
@@ -256,11 +260,11 @@ void launch_limit_f64(int M, int NB, const LimitArgs &a, cudaStream_t stream);
 void launch_sense_f64(int M, const SenseArgs &a, cudaStream_t stream);
 void launch_cfl(const CflArgs &a, cudaStream_t stream);
 // dt[c] = cfl length[c] / (speed (2 p[c] + 1)) from reduced speeds (0 where
-// the speed is 0), added to elapsed[c] when elapsed is not null; then the
-// speed words are zeroed.  length/p are per-case arrays, or null for the
-// shared length_all/p_all.
+// the speed is 0 or status[c] is non-zero), added to elapsed[c] when elapsed
+// is not null; then the speed words are zeroed.  length/p are per-case
+// arrays, or null for the shared length_all/p_all; status may be null.
 void launch_dt_from_speed(std::int64_t cases, unsigned long long *speed, double cfl,
                           const double *length, const int *p, double length_all, int p_all,
-                          double *dt, double *elapsed, cudaStream_t stream);
+                          double *dt, double *elapsed, const int *status, cudaStream_t stream);
 
 } // namespace wasl_b200
