@@ -54,11 +54,12 @@ private:
     int shape = 0;
     TuneResult tuning;
     int highest_degree_begin = 0, check_points = 0;
-    DeviceArray<double> u, e, s, geo, slot_geo, transforms, normal_x, normal_y, check, limited;
-    DeviceArray<std::int32_t> tile_nbr, tile_aux, neighbors, troubled, count, element_case;
+    DeviceArray<double> u, e, s, geo, slot_geo, transforms, normal_x, normal_y, check, limited,
+        basis64;
+    DeviceArray<std::int32_t> tile_nbr, tile_aux, neighbors, troubled, count, element_case, rough;
     DeviceArray<std::uint8_t> tile_code, flags;
     DeviceArray<float> basis32;
-    DeviceArray<unsigned char> face_table;
+    DeviceArray<unsigned char> face_table, face_table64;
     std::array<DeviceArray<TileWork>, 4> work;
     std::array<std::int64_t, 4> work_count{};
   };

@@ -150,7 +150,7 @@ BatchSolver::BatchSolver(const wasl_batch_config &cfg, std::int64_t case_count, 
     std::vector<std::int32_t> nbr(3 * ne), aux(3 * ne), neighbors;
     std::vector<std::uint8_t> code(3 * ne);
     std::vector<float> basis32;
-    std::vector<double> transforms, nx, ny;
+    std::vector<double> basis64, transforms, nx, ny;
     for (std::int64_t c : members) {
       const CaseSetup &cs = setup[c];
       const std::int64_t n = cs.mesh.element_count, off = case_offset_[c];
@@ -166,6 +166,8 @@ BatchSolver::BatchSolver(const wasl_batch_config &cfg, std::int64_t case_count, 
       place_rows(aux, ca, 3, n, off, ne);
       place_rows(code, cs.tile.code, 3, n, off, ne);
       append(basis32, cs.basis32);
+      if (!cs.basis32.empty())
+        append(basis64, cs.slots.donor_basis);
       nb += static_cast<std::int64_t>(cs.basis32.size()) / (QF * M);
       if (cfg.limiting) {
         std::vector<std::int32_t> sn = cs.stencil.neighbors;
@@ -191,11 +193,16 @@ BatchSolver::BatchSolver(const wasl_batch_config &cfg, std::int64_t case_count, 
     g->tile_nbr.upload(nbr, stream_);
     g->tile_aux.upload(aux, stream_);
     g->tile_code.upload(code, stream_);
-    if (!basis32.empty())
+    if (!basis32.empty()) {
       g->basis32.upload(basis32, stream_);
+      g->basis64.upload(basis64, stream_);
+    }
     std::vector<unsigned char> table(euler_tri_face_table_bytes(p, true));
     fill_euler_tri_face_table(p, true, table.data());
     g->face_table.upload(table, stream_);
+    std::vector<unsigned char> table64(euler_tri_face_table_bytes(p, false));
+    fill_euler_tri_face_table(p, false, table64.data());
+    g->face_table64.upload(table64, stream_);
     upload_euler_tri_tables_mixed(p, g->rule);
     prepare_euler_tri_stage_tile(p, g->rule);
     if (cfg.limiting) {
@@ -214,6 +221,8 @@ BatchSolver::BatchSolver(const wasl_batch_config &cfg, std::int64_t case_count, 
     }
     for (auto *b : {&g->u, &g->e, &g->s})
       b->resize(static_cast<std::size_t>(4) * M * ne);
+    if (cfg.limiting)
+      g->rough.resize(ne + 1); // rough list, then its count
     cuda_check(cudaMemsetAsync(g->u.get(), 0, g->u.size() * sizeof(double), stream_), "memset");
     // Work lists, one per tile size of the launch shapes.
     for (int shape = 0; shape < euler_tri_tile_shapes(); ++shape) {
@@ -316,10 +325,16 @@ StageArgs BatchSolver::stage_args(const Group &g, int stage) const {
   a.mesh.slot_geo = g.slot_geo.get();
   a.mesh.boundary = cfg_.boundary;
   a.boundary.basis32 = g.basis32.get();
+  a.mesh.donor_basis = g.basis64.get();
   a.face_table = g.face_table.get();
+  a.face_table64 = g.face_table64.get();
   a.tile.nbr = g.tile_nbr.get();
   a.tile.code = g.tile_code.get();
   a.tile.aux = g.tile_aux.get();
+  // FP64 face islands at discontinuities (the rough pass), with the limiter.
+  a.rough = cfg_.limiting ? g.rough.get() : nullptr;
+  a.rough_count = a.rough ? g.rough.get() + g.ne : nullptr;
+  a.element_case = g.element_case.get();
   a.work = g.work[g.shape].get();
   a.work_count = g.work_count[g.shape];
   a.case_dt = d_dt_.get();
@@ -405,7 +420,7 @@ void BatchSolver::enqueue_step(double cfl) {
         cuda_check(cudaMemsetAsync(g.count.get(), 0, sizeof(std::int32_t), stream_), "count");
       const StageArgs a = stage_args(g, k);
       launch_euler_tri_stage_tile(g.p, g.rule, g.shape, a, stream_);
-      ++launches_per_step_;
+      launches_per_step_ += a.rough ? 2 : 1;
       if (cfg_.limiting) {
         launch_limit_f64(g.M, 3, limit_args(g, a.out), stream_);
         launches_per_step_ += cfg_.positivity_all ? 3 : 2;

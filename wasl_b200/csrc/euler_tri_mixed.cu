@@ -584,6 +584,62 @@ __device__ __forceinline__ void high_trace(const float (&h)[4][TriShape<P>::M - 
   }
 }
 
+// Relative jump of density or energy between two cell means above which a
+// face is evaluated in FP64: near discontinuities the perturbations are as
+// large as the means and FP32 point states lose the positivity margins the
+// limiter keeps in FP64.
+constexpr double kFp64Jump = 0.05;
+
+__device__ __forceinline__ bool mean_jump(double rho_a, double rho_b, double e_a, double e_b) {
+  return fabs(rho_a - rho_b) > kFp64Jump * fmin(rho_a, rho_b) ||
+         fabs(e_a - e_b) > kFp64Jump * fmin(e_a, e_b);
+}
+
+// One face in FP64 (the mixed form's islands): traces of both elements from
+// their FP64 coefficients (rows stride apart) and the FP64 face tables, HLLC
+// in FP64 (reference order of operations up to contraction), then the
+// high-mode perturbations dflux[q][v] = F_q - F(U_L bar).n (FP32) and the
+// full mode-0 value sum_q w_q F_q.  Both elements of a face call it with the
+// same inputs in the same roles, so they get the same bits.
+template <int P>
+__device__ __noinline__ void face_fp64(double gamma, const double *own, std::int64_t own_stride,
+                                       const double *other, std::int64_t other_stride,
+                                       bool boundary, bool self_left, const double *own_basis,
+                                       const double *other_basis, const double *weights,
+                                       double nx, double ny, const double *fln,
+                                       float (*dflux)[4], double *mode0) {
+  constexpr int M = TriShape<P>::M, QF = TriShape<P>::QF;
+#pragma unroll
+  for (int v = 0; v < 4; ++v)
+    mode0[v] = 0.0;
+  for (int q = 0; q < QF; ++q) {
+    double to[4], tn[4], ul[4], ur[4], f[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      double so = 0.0, sn = 0.0;
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        so = fma(own[(v * M + m) * own_stride], own_basis[q * M + m], so);
+        if (!boundary)
+          sn = fma(other[(v * M + m) * other_stride], other_basis[q * M + m], sn);
+      }
+      to[v] = so;
+      tn[v] = sn;
+    }
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      ul[v] = boundary || self_left ? to[v] : tn[v];
+      ur[v] = boundary ? to[v] : (self_left ? tn[v] : to[v]);
+    }
+    hllc_fast(gamma, ul, ur, nx, ny, f);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      dflux[q][v] = static_cast<float>(f[v] - fln[v]);
+      mode0[v] = fma(weights[q], f[v], mode0[v]);
+    }
+  }
+}
+
 // The fused mixed stage on a tile of TILE consecutive elements per CTA.
 // The tile's state is staged in shared memory (FP64 means, FP32 high modes)
 // with asynchronous copies; each thread then computes its element's volume
@@ -593,7 +649,15 @@ __device__ __forceinline__ void high_trace(const float (&h)[4][TriShape<P>::M - 
 // inputs (the HLLC perturbation is always taken around the face's left mean),
 // so the two mode-0 contributions cancel exactly, as in the face-centric form.
 // MINB: resident CTAs per SM the register budget is sized for (1: no cap).
-template <int P, int R, int TILE, int MINB>
+//
+// ROUGH = false: the FP32 pass.  An element with a face across which the two
+// cell means jump (kFp64Jump; a test both elements of the face make alike) is
+// not computed here but appended to the rough list (when a.rough is set).
+// ROUGH = true: the elements of the rough list (one per thread, neighbours
+// read from global memory); faces with a jump are evaluated in FP64
+// (face_fp64), the others with the same FP32 code as the FP32 pass, so both
+// elements of every face still compute the same values.
+template <int P, int R, int TILE, int MINB, bool ROUGH>
 __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_mixed(const StageArgs a) {
   using S = TriShape<P>;
   constexpr int M = S::M, QV = MixedVolume<P, R>::QV, QF = S::QF, H = M - 1;
@@ -603,21 +667,34 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_mixed(const StageAr
   extern __shared__ __align__(16) double tile_state[];
   double(*sstate)[TILE] = reinterpret_cast<double(*)[TILE]>(tile_state);
 
-  std::int64_t first, count;
-  int case_id = 0;
-  if (a.work) {
-    const TileWork w = a.work[blockIdx.x];
-    first = w.first;
-    count = w.count;
-    case_id = w.case_id;
-  } else {
-    first = static_cast<std::int64_t>(blockIdx.x) * TILE;
-    count = a.mesh.ne - first < TILE ? a.mesh.ne - first : TILE;
-  }
   const int t = threadIdx.x;
-  const bool active = t < count;
   const std::int64_t ne = a.mesh.ne;
-  const std::int64_t e = first + t;
+  std::int64_t first = 0, count = 0, e = 0;
+  int case_id = 0;
+  bool active;
+  if (ROUGH) {
+    const std::int64_t list = *a.rough_count;
+    if (static_cast<std::int64_t>(blockIdx.x) * TILE >= list)
+      return; // the whole CTA is past the list (uniform: no barrier reached)
+    const std::int64_t i = static_cast<std::int64_t>(blockIdx.x) * TILE + t;
+    active = i < list;
+    if (active) {
+      e = a.rough[i];
+      case_id = a.element_case ? a.element_case[e] : 0;
+    }
+  } else {
+    if (a.work) {
+      const TileWork w = a.work[blockIdx.x];
+      first = w.first;
+      count = w.count;
+      case_id = w.case_id;
+    } else {
+      first = static_cast<std::int64_t>(blockIdx.x) * TILE;
+      count = a.mesh.ne - first < TILE ? a.mesh.ne - first : TILE;
+    }
+    active = t < count;
+    e = first + t;
+  }
   const double *__restrict__ in = a.in;
 
   // Stage this tile's state (asynchronous 8-byte copies, coalesced per row)
@@ -732,7 +809,7 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_mixed(const StageAr
     const bool boundary = nb < 0;
     if (!boundary) {
       const std::int64_t local = nb - first;
-      if (local >= 0 && local < count) {
+      if (!ROUGH && local >= 0 && local < count) {
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
           nmean[v] = sstate[v * M][local] * phi0;
@@ -750,6 +827,12 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_mixed(const StageAr
             nh[v][m] = static_cast<float>(__ldg(row + (m + 1) * ne));
         }
       }
+    }
+    // FP32 pass: an element with a face across a jump of the means is left
+    // to the rough pass (its work so far is dropped, nothing was written).
+    if (!ROUGH && a.rough && !boundary && mean_jump(nmean[0], mean[0], nmean[3], mean[3])) {
+      a.rough[atomicAdd(a.rough_count, 1)] = static_cast<std::int32_t>(e);
+      return;
     }
     // The face's left state is the reference of the perturbation form.
     MeanState ml;
@@ -779,6 +862,43 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_mixed(const StageAr
     }
     const float nxf = static_cast<float>(nx), nyf = static_cast<float>(ny);
     const float fscale = static_cast<float>(scale);
+    const double sgn = self_left ? -1.0 : 1.0;
+    // Near a discontinuity (symmetric test on the two means): the face in FP64.
+    if (ROUGH && !boundary && mean_jump(nmean[0], mean[0], nmean[3], mean[3])) {
+      const FaceTable<P, double> *T64 = static_cast<const FaceTable<P, double> *>(a.face_table64);
+      const double *lb64 = &T64->lb[le][0][0];
+      const double *rb64 = &T64->rb[(le * 3 + re) * 2 + flip][0][0];
+      const double *own64 = self_left ? lb64 : rb64;
+      const double *other64 = self_left ? rb64 : lb64;
+      if (code & 0xC0u) {
+        const double *periodic =
+            a.mesh.donor_basis + static_cast<std::int64_t>(a.tile.aux[slot]) * QF * M;
+        if (code & 0x40u)
+          own64 = periodic;
+        else
+          other64 = periodic;
+      }
+      float dq[QF][4];
+      double m0[4];
+      face_fp64<P>(gamma, &sstate[0][t], TILE, in + nb, ne, false, self_left, own64, other64,
+                   &T64->ew[le][0], nx, ny, fln, dq, m0);
+#pragma unroll
+      for (int q = 0; q < QF; ++q) {
+        const float w = table.ew[le][q];
+        const float wsc = (self_left ? -w : w) * fscale;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          const float value = wsc * (self_left ? dq[q][v] : dq[q][v] + shift[v]);
+#pragma unroll
+          for (int m = 0; m < H; ++m)
+            racc[v][m] = fmaf(value, own_basis[q * M + m + 1], racc[v][m]);
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < 4; ++v)
+        r0[v] += sgn * scale * phi0 * m0[v];
+      continue;
+    }
     float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
     for (int q = 0; q < QF; ++q) {
@@ -808,7 +928,6 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_mixed(const StageAr
           racc[v][m] = fmaf(value, own_basis[q * M + m + 1], racc[v][m]);
       }
     }
-    const double sgn = self_left ? -1.0 : 1.0;
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
       const double mode0 = fln[v] * c_edge_wsum<P>[le] + static_cast<double>(acc[v]);
@@ -852,17 +971,24 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_mixed(const StageAr
       best = __double_as_longlong(speed);
     else
       raise_error(a.error, kNonPhysicalAverage, e);
-    // Warp max over the active lanes (a prefix of the warp: lanes past the
-    // tile's end returned), then one atomic per warp.
+    // Warp max over whichever lanes are still active (past the tile's end,
+    // or handed to the rough pass, lanes have returned): the 64-bit max of
+    // positive FP64 bits as the max of the high words, then of the low words
+    // among the lanes holding it; one atomic per warp and case.
     const unsigned mask = __activemask();
     const int lane = threadIdx.x & 31;
-    for (int off = 16; off > 0; off >>= 1) {
-      const unsigned long long o = __shfl_down_sync(mask, best, off);
-      if (lane + off < 32 && ((mask >> (lane + off)) & 1u) && o > best)
-        best = o;
-    }
-    if (lane == __ffs(mask) - 1)
+    // (No lane's match set is the whole mask unless all lanes share the case,
+    // so the branch is uniform across the warp.)
+    if (__match_any_sync(mask, case_id) == mask) {
+      const unsigned hi = __reduce_max_sync(mask, static_cast<unsigned>(best >> 32));
+      const unsigned lo = __reduce_max_sync(
+          mask, static_cast<unsigned>(best >> 32) == hi ? static_cast<unsigned>(best) : 0u);
+      if (lane == __ffs(mask) - 1)
+        atomicMax(a.speed_max + case_id, (static_cast<unsigned long long>(hi) << 32) | lo);
+    } else {
+      // Lanes of one warp from different cases (the rough pass of a batch).
       atomicMax(a.speed_max + case_id, best);
+    }
   }
 
   if (a.sense) {
@@ -982,7 +1108,11 @@ template <int P, int R, int TILE, int MINB> void tile_opt_in() {
   check(cudaGetDevice(&device), "cudaGetDevice");
   if (device < 64 && opted_in[device])
     return;
-  check(cudaFuncSetAttribute(euler_tri_tile_mixed<P, R, TILE, MINB>,
+  check(cudaFuncSetAttribute(euler_tri_tile_mixed<P, R, TILE, MINB, false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(tile_smem<P, TILE>())),
+        "tile kernel shared memory");
+  check(cudaFuncSetAttribute(euler_tri_tile_mixed<P, R, TILE, MINB, true>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(tile_smem<P, TILE>())),
         "tile kernel shared memory");
@@ -990,12 +1120,21 @@ template <int P, int R, int TILE, int MINB> void tile_opt_in() {
     opted_in[device] = true;
 }
 
+// The FP32 pass over all tiles, then (with a rough list) the pass over the
+// elements it left, sized for the worst case: its CTAs beyond the list's
+// length return at once.
 template <int P, int R, int TILE, int MINB> void stage_tile(const StageArgs &a, cudaStream_t s) {
   tile_opt_in<P, R, TILE, MINB>();
   const std::int64_t blocks = a.work ? a.work_count : (a.mesh.ne + TILE - 1) / TILE;
-  if (blocks > 0)
-    euler_tri_tile_mixed<P, R, TILE, MINB>
-        <<<static_cast<unsigned>(blocks), TILE, tile_smem<P, TILE>(), s>>>(a);
+  if (blocks <= 0)
+    return;
+  if (a.rough)
+    check(cudaMemsetAsync(a.rough_count, 0, sizeof(std::int32_t), s), "rough count");
+  euler_tri_tile_mixed<P, R, TILE, MINB, false>
+      <<<static_cast<unsigned>(blocks), TILE, tile_smem<P, TILE>(), s>>>(a);
+  if (a.rough)
+    euler_tri_tile_mixed<P, R, TILE, MINB, true>
+        <<<static_cast<unsigned>((a.mesh.ne + TILE - 1) / TILE), TILE, tile_smem<P, TILE>(), s>>>(a);
 }
 
 // Launch shapes of the tile kernel (elements per CTA, register budget):

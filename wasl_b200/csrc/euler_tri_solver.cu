@@ -111,6 +111,8 @@ public:
         throw SolverError(WASL_ERR_ARGUMENT, "2D Euler mixed form: the tile kernel needs"
                                              " transmissive or paired periodic boundaries");
       if (tile_ok_) {
+        if (cfg.limiting)
+          d_rough_.resize(ne_ + 1); // rough list, then its count
         const TileSlotArrays ts = build_tile_slots(mesh_, t, boundary_, QF);
         d_tile_nbr_.upload(ts.nbr, stream_);
         d_tile_code_.upload(ts.code, stream_);
@@ -368,6 +370,9 @@ private:
     a.tile.nbr = d_tile_nbr_.get();
     a.tile.code = d_tile_code_.get();
     a.tile.aux = d_tile_aux_.get();
+    // FP64 face islands at discontinuities (the rough pass), with the limiter.
+    a.rough = limiting_ ? d_rough_.get() : nullptr;
+    a.rough_count = a.rough ? d_rough_.get() + ne_ : nullptr;
     a.dt = dt_device;
     a.dt_value = dt_value;
     a.gamma = cfg_.heat_capacity_ratio;
@@ -413,7 +418,7 @@ private:
       count_launches(boundary_count_ > 0 && boundary_ != WASL_TRANSMISSIVE && !paired_ ? 3 : 2);
     } else {
       launch_euler_tri_stage_tile(p_, cfg_.volume_rule_order, kernel_ - 1, a, stream_);
-      count_launches(1);
+      count_launches(a.rough ? 2 : 1);
     }
   }
 
@@ -421,7 +426,10 @@ private:
   // state into scratch (u^n is read, not written; sensing off) and keeps the
   // fastest, per polynomial order, rule order and mesh size class.
   void tune_mixed(StageArgs a) {
-    const int variants = tile_ok_ ? 1 + euler_tri_tile_shapes() : 1;
+    // With the limiter (flows with discontinuities) only the tile kernel,
+    // whose second pass evaluates faces at discontinuities in FP64, competes.
+    const int base = tile_ok_ && limiting_ ? 1 : 0;
+    const int variants = tile_ok_ ? 1 + euler_tri_tile_shapes() - base : 1;
     a.stage = 0;
     a.in = d_u_.get();
     a.u0 = d_u_.get();
@@ -433,11 +441,14 @@ private:
                             std::to_string(cfg_.volume_rule_order ? cfg_.volume_rule_order : p_ + 2) +
                             "/bnd" + std::to_string(boundary_count_ > 0 ? boundary_ : -1) +
                             "/size" + std::to_string(size_class(ne_));
-    tuning_ = autotune(key, variants, [&](int i) {
-      kernel_ = i;
+    tuning_ = autotune(key + (base ? "/tile-only" : ""), variants, [&](int i) {
+      kernel_ = i + base;
       launch_mixed(a);
     }, stream_);
-    kernel_ = tuning_.choice;
+    if (base)
+      tuning_.ms.insert(tuning_.ms.begin(), 0.0); // face-centric: not timed
+    kernel_ = tuning_.choice + base;
+    tuning_.choice = kernel_;
   }
 
   LimitArgs limit_args(double *state, const std::uint8_t *flags) {
@@ -493,7 +504,7 @@ private:
   DeviceArray<unsigned long long> d_speed_;
   int kernel_ = -1; // mixed form: -1 not chosen yet, 0 face-centric, 1 + s tile shape s
   TuneResult tuning_;
-  DeviceArray<std::int32_t> d_tile_nbr_, d_tile_aux_;
+  DeviceArray<std::int32_t> d_tile_nbr_, d_tile_aux_, d_rough_;
   DeviceArray<std::uint8_t> d_tile_code_;
   DeviceArray<float> d_basis32_;
   double length_ = 0.0;

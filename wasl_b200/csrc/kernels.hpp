@@ -116,6 +116,13 @@ struct StageArgs {
   // FP64 bits, and a non-physical average sets the error word.
   unsigned long long *speed_max = nullptr;
   unsigned long long *error = nullptr;
+  // Tile kernel: elements with a face across which the cell means jump go to
+  // the rough list [ne] (count rough_count) and are computed by the second
+  // pass with FP64 faces; null: one FP32 pass.  element_case [ne] gives the
+  // case (for case_dt) of a rough element; null: case 0.
+  std::int32_t *rough = nullptr;
+  std::int32_t *rough_count = nullptr;
+  const std::int32_t *element_case = nullptr;
 };
 
 // Limiter over the compacted troubled list (cpp/src/limiting/euler_modal_limiter.cpp:70-98).
