@@ -191,6 +191,63 @@ int wasl_gpu_write_checkpoint(wasl_gpu *handle, const char *path, double time, u
                               const char *prepared_mesh);
 int wasl_gpu_read_checkpoint(wasl_gpu *handle, const char *path, double *time, uint64_t *step);
 
+/* ---- Learned troubled-cell indicator -----------------------------------------
+ * A small network (features -> 64 -> 64 -> 1, BF16 weights, FP32 accumulate)
+ * over the normalised density modes of a cell and its three limiter-stencil
+ * neighbours, trained on the flags of the reference modal-decay sensor
+ * (cpp/src/limiting/euler_modal_limiter.cpp:18-24) on the method's own runs.
+ * With it set, each stage's troubled cells are the network's decision where
+ * sigmoid(logit) >= hi or <= lo, and the reference sensor's elsewhere (the
+ * fallback); the limiter then runs as usual.  No counterpart in the reference.
+ * 2D Euler with limiting only. */
+
+/* Features per element for this solver: 4 (M - 1) + 3, padded to 16k. */
+int wasl_gpu_indicator_features(const wasl_gpu *handle, int *features);
+
+/* The current state's features [element][features] and the reference
+ * sensor's flags [element] (training data). */
+int wasl_gpu_indicator_data(wasl_gpu *handle, float *features, uint8_t *labels, int64_t count);
+
+/* Use the network with FP32 weights (wasl_mlp_get_weights layout) and the
+ * confidence band (lo, hi) handed to the reference sensor (lo < 0 and hi > 1:
+ * every cell falls back, which reproduces the reference sensor exactly). */
+int wasl_gpu_set_indicator(wasl_gpu *handle, const float *weights, int64_t count, double lo,
+                           double hi);
+
+/* The network's logits for the current state (the tensor-core inference
+ * kernel), one per element. */
+int wasl_gpu_indicator_logits(wasl_gpu *handle, float *logits, int64_t count);
+
+/* Cell-stage counts since the indicator was set (or last reset): [0] network
+ * troubled, [1] network smooth, [2] fallback to the reference, [3] reference
+ * troubled, [4] missed (reference troubled, decided smooth), [5] false
+ * (reference smooth, decided troubled). */
+int wasl_gpu_indicator_stats(wasl_gpu *handle, uint64_t *stats, int reset);
+
+/* Training on the GPU (the project's own forward/backward and Adam kernels). */
+typedef struct wasl_mlp wasl_mlp;
+int wasl_mlp_create(int features, uint64_t seed, int device, wasl_mlp **handle, char *error,
+                    size_t error_length);
+void wasl_mlp_destroy(wasl_mlp *handle);
+const char *wasl_mlp_last_error(const wasl_mlp *handle);
+int wasl_mlp_parameter_count(const wasl_mlp *handle, int64_t *count);
+/* Training samples [sample][features] and 0/1 labels, copied to the device. */
+int wasl_mlp_set_data(wasl_mlp *handle, const float *features, const uint8_t *labels,
+                      int64_t count);
+/* `steps` Adam steps (lr, beta 0.9/0.999) on mini-batches of `batch` samples
+ * (a multiple of 64) taken in order, cycling; loss: weighted binary
+ * cross-entropy (positives weighted positive_weight), mean of the last batch. */
+int wasl_mlp_train(wasl_mlp *handle, int64_t steps, int64_t batch, double learning_rate,
+                   double positive_weight, double *loss);
+/* The gradient of the mean loss over `count` samples (a multiple of 64) at the
+ * current weights, in the weights' layout, and that loss. */
+int wasl_mlp_gradient(wasl_mlp *handle, const float *features, const uint8_t *labels,
+                      int64_t count, double positive_weight, float *gradient, double *loss);
+int wasl_mlp_predict(wasl_mlp *handle, const float *features, int64_t count, float *logits);
+/* FP32 weights: W1 [64][F], b1 [64], W2 [64][64], b2 [64], w3 [64], b3. */
+int wasl_mlp_get_weights(const wasl_mlp *handle, float *weights, int64_t count);
+int wasl_mlp_set_weights(wasl_mlp *handle, const float *weights, int64_t count);
+
 /* ---- Batched 2D Euler (the mixed form) --------------------------------------
  * Many independent triangle meshes of uneven size and polynomial order (1-3)
  * advanced together: cases of one order share one launch of the fused tile

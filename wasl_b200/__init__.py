@@ -68,6 +68,7 @@ class BatchConfig(C.Structure):
 _d = C.POINTER(C.c_double)
 _i64 = C.POINTER(C.c_int64)
 _u8 = C.POINTER(C.c_uint8)
+_f = C.POINTER(C.c_float)
 _lib = None
 
 # name -> (restype, argtypes), one per declaration in include/wasl_b200.h
@@ -119,6 +120,22 @@ SIGNATURES = {
                                     C.POINTER(C.c_int)]),
     "wasl_batch_launches": (C.c_int, [C.c_void_p, _i64, C.POINTER(C.c_int), _i64]),
     "wasl_batch_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "wasl_gpu_indicator_features": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "wasl_gpu_indicator_data": (C.c_int, [C.c_void_p, _f, _u8, C.c_int64]),
+    "wasl_gpu_set_indicator": (C.c_int, [C.c_void_p, _f, C.c_int64, C.c_double, C.c_double]),
+    "wasl_gpu_indicator_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.c_int]),
+    "wasl_gpu_indicator_logits": (C.c_int, [C.c_void_p, _f, C.c_int64]),
+    "wasl_mlp_create": (C.c_int, [C.c_int, C.c_uint64, C.c_int, C.POINTER(C.c_void_p),
+                                  C.c_char_p, C.c_size_t]),
+    "wasl_mlp_destroy": (None, [C.c_void_p]),
+    "wasl_mlp_last_error": (C.c_char_p, [C.c_void_p]),
+    "wasl_mlp_parameter_count": (C.c_int, [C.c_void_p, _i64]),
+    "wasl_mlp_set_data": (C.c_int, [C.c_void_p, _f, _u8, C.c_int64]),
+    "wasl_mlp_train": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_double, C.c_double, _d]),
+    "wasl_mlp_gradient": (C.c_int, [C.c_void_p, _f, _u8, C.c_int64, C.c_double, _f, _d]),
+    "wasl_mlp_predict": (C.c_int, [C.c_void_p, _f, C.c_int64, _f]),
+    "wasl_mlp_get_weights": (C.c_int, [C.c_void_p, _f, C.c_int64]),
+    "wasl_mlp_set_weights": (C.c_int, [C.c_void_p, _f, C.c_int64]),
     "wasl_gpu_profile_begin": (C.c_int, [C.c_void_p]),
     "wasl_gpu_profile_end": (C.c_int, [C.c_void_p, _d, _i64, _i64]),
     "wasl_gpu_write_checkpoint": (C.c_int, [C.c_void_p, C.c_char_p, C.c_double, C.c_uint64,
@@ -331,6 +348,40 @@ class Solver:
                                               C.byref(count)))
         return choice.value, ms[:count.value].tolist()
 
+    # ---- learned troubled-cell indicator -------------------------------------------
+
+    def indicator_features(self) -> int:
+        n = C.c_int()
+        self._check(self._lib.wasl_gpu_indicator_features(self._h, C.byref(n)))
+        return n.value
+
+    def indicator_data(self):
+        """(features [elements][F] float32, reference flags [elements] uint8) of
+        the current state."""
+        F = self.indicator_features()
+        x = np.empty((self.elements, F), dtype=np.float32)
+        y = np.empty(self.elements, dtype=np.uint8)
+        self._check(self._lib.wasl_gpu_indicator_data(self._h, _ptr(x, _f), _ptr(y, _u8),
+                                                      self.elements))
+        return x, y
+
+    def set_indicator(self, weights, lo=0.1, hi=0.9):
+        w = np.ascontiguousarray(weights, dtype=np.float32)
+        self._check(self._lib.wasl_gpu_set_indicator(self._h, _ptr(w, _f), w.size, lo, hi))
+
+    def indicator_logits(self):
+        z = np.empty(self.elements, dtype=np.float32)
+        self._check(self._lib.wasl_gpu_indicator_logits(self._h, _ptr(z, _f), self.elements))
+        return z
+
+    def indicator_stats(self, reset=False):
+        """dict of cell-stage counts since set (or the last reset)."""
+        s = (C.c_uint64 * 6)()
+        self._check(self._lib.wasl_gpu_indicator_stats(self._h, s, 1 if reset else 0))
+        keys = ["network_troubled", "network_smooth", "fallback", "reference_troubled",
+                "missed", "false"]
+        return dict(zip(keys, [int(v) for v in s]))
+
     def profile_begin(self):
         self._check(self._lib.wasl_gpu_profile_begin(self._h))
 
@@ -483,3 +534,73 @@ class Batch:
         s = C.c_void_p()
         self._check(self._lib.wasl_batch_stream(self._h, C.byref(s)))
         return s.value or 0
+
+
+class Mlp:
+    """The indicator network on the GPU: training (wasl_mlp_*) with the
+    project's own forward/backward and Adam kernels."""
+
+    def __init__(self, features, seed=0, device=0):
+        lib = library()
+        err = C.create_string_buffer(512)
+        h = C.c_void_p()
+        rc = lib.wasl_mlp_create(features, seed, device, C.byref(h), err, len(err))
+        if rc != 0:
+            raise WaslError(rc, err.value.decode())
+        self._lib, self._h, self.features = lib, h, features
+        n = C.c_int64()
+        self._check(lib.wasl_mlp_parameter_count(h, C.byref(n)))
+        self.parameters = n.value
+
+    def _check(self, rc):
+        if rc != 0:
+            raise WaslError(rc, self._lib.wasl_mlp_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.wasl_mlp_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        self.close()
+
+    def set_data(self, features, labels):
+        x = np.ascontiguousarray(features, dtype=np.float32)
+        y = np.ascontiguousarray(labels, dtype=np.uint8)
+        self._check(self._lib.wasl_mlp_set_data(self._h, _ptr(x, _f), _ptr(y, _u8), len(y)))
+
+    def train(self, steps, batch=4096, learning_rate=1e-3, positive_weight=1.0):
+        loss = C.c_double()
+        self._check(self._lib.wasl_mlp_train(self._h, steps, batch, learning_rate,
+                                             positive_weight, C.byref(loss)))
+        return loss.value
+
+    def gradient(self, features, labels, positive_weight=1.0):
+        x = np.ascontiguousarray(features, dtype=np.float32)
+        y = np.ascontiguousarray(labels, dtype=np.uint8)
+        g = np.empty(self.parameters, dtype=np.float32)
+        loss = C.c_double()
+        self._check(self._lib.wasl_mlp_gradient(self._h, _ptr(x, _f), _ptr(y, _u8), len(y),
+                                                positive_weight, _ptr(g, _f), C.byref(loss)))
+        return g, loss.value
+
+    def predict(self, features):
+        x = np.ascontiguousarray(features, dtype=np.float32)
+        z = np.empty(len(x), dtype=np.float32)
+        self._check(self._lib.wasl_mlp_predict(self._h, _ptr(x, _f), len(x), _ptr(z, _f)))
+        return z
+
+    def weights(self):
+        w = np.empty(self.parameters, dtype=np.float32)
+        self._check(self._lib.wasl_mlp_get_weights(self._h, _ptr(w, _f), w.size))
+        return w
+
+    def set_weights(self, weights):
+        w = np.ascontiguousarray(weights, dtype=np.float32)
+        self._check(self._lib.wasl_mlp_set_weights(self._h, _ptr(w, _f), w.size))

@@ -46,6 +46,8 @@ SOURCES = {
     "tri_setup.cpp": [],
     "batch_solver.cu": [],
     "capi_batch.cpp": [],
+    "mlp.cu": [],
+    "mlp_trainer.cpp": [],
 }
 HEADERS = [f for f in os.listdir(CSRC) if f.endswith((".hpp", ".cuh", ".h"))]
 

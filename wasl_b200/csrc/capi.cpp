@@ -306,6 +306,47 @@ int wasl_gpu_tuning(const wasl_gpu *h, int *choice, double *ms, int capacity, in
   });
 }
 
+int wasl_gpu_indicator_features(const wasl_gpu *h, int *features) {
+  return guarded(const_cast<wasl_gpu *>(h), [&] {
+    need(features != nullptr, "indicator features: null output");
+    *features = h->solver->indicator_features();
+  });
+}
+
+int wasl_gpu_indicator_data(wasl_gpu *h, float *features, uint8_t *labels, int64_t count) {
+  return guarded(h, [&] {
+    need(features && labels && count == h->solver->elements(),
+         "indicator data: count must be the number of elements");
+    h->solver->indicator_data(features, labels);
+  });
+}
+
+int wasl_gpu_set_indicator(wasl_gpu *h, const float *weights, int64_t count, double lo,
+                           double hi) {
+  return guarded(h, [&] {
+    need(weights != nullptr, "set indicator: null weights");
+    h->solver->set_indicator(weights, count, lo, hi);
+  });
+}
+
+int wasl_gpu_indicator_logits(wasl_gpu *h, float *logits, int64_t count) {
+  return guarded(h, [&] {
+    need(logits && count == h->solver->elements(),
+         "indicator logits: count must be the number of elements");
+    h->solver->indicator_logits(logits);
+  });
+}
+
+int wasl_gpu_indicator_stats(wasl_gpu *h, uint64_t *stats, int reset) {
+  return guarded(h, [&] {
+    need(stats != nullptr, "indicator stats: null output");
+    unsigned long long s[6];
+    h->solver->indicator_stats(s, reset != 0);
+    for (int i = 0; i < 6; ++i)
+      stats[i] = s[i];
+  });
+}
+
 int wasl_gpu_profile_begin(wasl_gpu *h) {
   return guarded(h, [&] { h->solver->profile_begin(); });
 }

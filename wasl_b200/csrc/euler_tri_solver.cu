@@ -14,6 +14,7 @@
 #include "basis.hpp"
 #include "kernels.hpp"
 #include "mesh.hpp"
+#include "mlp.hpp"
 #include "solver.hpp"
 #include "tri_setup.hpp"
 #include "tri_tables.hpp"
@@ -308,6 +309,86 @@ public:
     check_error();
   }
 
+  int indicator_features() const override {
+    return limiting_ ? mlp_features_for_modes(M_) : 0;
+  }
+
+  void set_indicator(const float *weights, std::int64_t count, double lo, double hi) override {
+    if (!limiting_)
+      throw SolverError(WASL_ERR_ARGUMENT, "learned indicator: needs limiting on and p >= 1");
+    const MlpShape sh = mlp_shape(mlp_features_for_modes(M_));
+    if (count != sh.count)
+      throw SolverError(WASL_ERR_ARGUMENT, "learned indicator: expected " +
+                                               std::to_string(sh.count) + " weights");
+    if (!(lo <= hi))
+      throw SolverError(WASL_ERR_ARGUMENT, "learned indicator: need lo <= hi");
+    d_mlp_.upload(std::vector<float>(weights, weights + count), stream_);
+    d_mlp_stats_.resize(6);
+    cuda_check(cudaMemsetAsync(d_mlp_stats_.get(), 0, 6 * sizeof(unsigned long long), stream_),
+               "stats");
+    mlp_lo_ = lo;
+    mlp_hi_ = hi;
+    cuda_check(cudaStreamSynchronize(stream_), "set indicator");
+  }
+
+  void indicator_data(float *features, std::uint8_t *labels) override {
+    if (!limiting_)
+      throw SolverError(WASL_ERR_ARGUMENT, "learned indicator: needs limiting on and p >= 1");
+    const int F = mlp_features_for_modes(M_);
+    DeviceArray<float> f(static_cast<std::size_t>(ne_) * F);
+    DeviceArray<std::uint8_t> y(ne_);
+    launch_mlp_features(d_u_.get(), ne_, M_, d_neighbors_.get(), F, cfg_.sensor_threshold,
+                        stencil_.highest_degree_begin, f.get(), y.get(), stream_);
+    cuda_check(cudaMemcpyAsync(features, f.get(), sizeof(float) * f.size(), cudaMemcpyDeviceToHost,
+                               stream_),
+               "features");
+    cuda_check(cudaMemcpyAsync(labels, y.get(), ne_, cudaMemcpyDeviceToHost, stream_), "labels");
+    cuda_check(cudaStreamSynchronize(stream_), "indicator data");
+  }
+
+  // The network's logits for the current state, from the inference kernel
+  // (its flags and troubled list go to scratch; the state is untouched).
+  void indicator_logits(float *logits) override {
+    if (d_mlp_.size() == 0)
+      throw SolverError(WASL_ERR_ARGUMENT, "learned indicator: not set");
+    DeviceArray<float> z(ne_);
+    DeviceArray<std::uint8_t> flags(ne_);
+    DeviceArray<std::int32_t> list(ne_ + 1);
+    cuda_check(cudaMemsetAsync(list.get() + ne_, 0, sizeof(std::int32_t), stream_), "count");
+    MlpIndicatorArgs m;
+    m.shape = mlp_shape(mlp_features_for_modes(M_));
+    m.params = d_mlp_.get();
+    m.lo = static_cast<float>(mlp_lo_);
+    m.hi = static_cast<float>(mlp_hi_);
+    m.state = d_u_.get();
+    m.ne = ne_;
+    m.M = M_;
+    m.neighbors = d_neighbors_.get();
+    m.threshold = cfg_.sensor_threshold;
+    m.highest_degree_begin = stencil_.highest_degree_begin;
+    m.flags = flags.get();
+    m.troubled = list.get();
+    m.troubled_count = list.get() + ne_;
+    m.logits = z.get();
+    launch_mlp_indicator(m, stream_);
+    cuda_check(cudaMemcpyAsync(logits, z.get(), sizeof(float) * ne_, cudaMemcpyDeviceToHost,
+                               stream_),
+               "logits");
+    cuda_check(cudaStreamSynchronize(stream_), "indicator logits");
+  }
+
+  void indicator_stats(unsigned long long *stats, bool reset) override {
+    if (d_mlp_.size() == 0)
+      throw SolverError(WASL_ERR_ARGUMENT, "learned indicator: not set");
+    cuda_check(cudaMemcpyAsync(stats, d_mlp_stats_.get(), 6 * sizeof(unsigned long long),
+                               cudaMemcpyDeviceToHost, stream_),
+               "stats");
+    if (reset)
+      cuda_check(cudaMemsetAsync(d_mlp_stats_.get(), 0, 6 * sizeof(unsigned long long), stream_),
+                 "stats");
+    cuda_check(cudaStreamSynchronize(stream_), "stats");
+  }
+
   int kernel_choice(double *ms, int capacity, int &count) override {
     count = static_cast<int>(tuning_.ms.size());
     for (int i = 0; i < count && i < capacity; ++i)
@@ -376,7 +457,8 @@ private:
     a.dt = dt_device;
     a.dt_value = dt_value;
     a.gamma = cfg_.heat_capacity_ratio;
-    a.sense = limiting_ ? 1 : 0;
+    const bool learned = limiting_ && d_mlp_.size() > 0;
+    a.sense = limiting_ && !learned ? 1 : 0;
     a.threshold = cfg_.sensor_threshold;
     a.highest_degree_begin = stencil_.highest_degree_begin;
     a.troubled = d_troubled_.get();
@@ -403,6 +485,25 @@ private:
         count_launches(1);
       }
       stage_end();
+      if (learned) {
+        MlpIndicatorArgs m;
+        m.shape = mlp_shape(mlp_features_for_modes(M_));
+        m.params = d_mlp_.get();
+        m.lo = static_cast<float>(mlp_lo_);
+        m.hi = static_cast<float>(mlp_hi_);
+        m.state = outs[k];
+        m.ne = ne_;
+        m.M = M_;
+        m.neighbors = d_neighbors_.get();
+        m.threshold = cfg_.sensor_threshold;
+        m.highest_degree_begin = stencil_.highest_degree_begin;
+        m.flags = d_flags_.get() + k * ne_;
+        m.troubled = d_troubled_.get();
+        m.troubled_count = d_count_.get();
+        m.stats = d_mlp_stats_.get();
+        launch_mlp_indicator(m, stream_);
+        count_launches(1);
+      }
       if (limiting_) {
         launch_limit_f64(M_, 3, limit_args(outs[k], d_flags_.get() + k * ne_), stream_);
         count_launches(cfg_.positivity_all ? 3 : 2);
@@ -505,6 +606,9 @@ private:
   int kernel_ = -1; // mixed form: -1 not chosen yet, 0 face-centric, 1 + s tile shape s
   TuneResult tuning_;
   DeviceArray<std::int32_t> d_tile_nbr_, d_tile_aux_, d_rough_;
+  DeviceArray<float> d_mlp_; // learned indicator weights (empty: the reference sensor)
+  DeviceArray<unsigned long long> d_mlp_stats_;
+  double mlp_lo_ = 0.1, mlp_hi_ = 0.9;
   DeviceArray<std::uint8_t> d_tile_code_;
   DeviceArray<float> d_basis32_;
   double length_ = 0.0;

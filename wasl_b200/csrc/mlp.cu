@@ -1,0 +1,487 @@
+// The learned troubled-cell indicator: a small MLP over normalised modal
+// coefficients of a cell and its limiter-stencil neighbours, trained on the
+// flags the reference modal-decay sensor (cpp/src/limiting/euler_modal_limiter.cpp:18-24)
+// produces on the method's own runs, with that sensor as the fallback for
+// cells the network is not confident about.
+//
+// Network: x[F] -> 64 (ReLU) -> 64 (ReLU) -> 1 (logit), F = 4 (M - 1) + 3
+// padded to a multiple of 16.  Weights and the two matrix operands (inputs,
+// first hidden layer) are BF16, accumulation and biases FP32; training keeps
+// FP32 master weights and runs the forward pass with the same BF16 rounding
+// the inference kernel applies (gradients pass straight through it).
+//
+// Kernels: features (shared by data collection and inference), the training
+// forward/backward over a block's mini-batch with atomic gradient
+// accumulation, Adam, an FP32 prediction pass, and the inference kernel on
+// the tensor cores (mma.sync m16n8k16 BF16, FP32 accumulate).
+#include <cuda_bf16.h>
+
+#include <stdexcept>
+#include <string>
+
+#include "mlp.hpp"
+
+namespace wasl_b200 {
+
+namespace {
+
+__device__ __forceinline__ float clamp8(float x) { return fminf(fmaxf(x, -8.0f), 8.0f); }
+
+__device__ __forceinline__ float bf16_round(float x) {
+  return __bfloat162float(__float2bfloat16_rn(x));
+}
+
+} // namespace
+
+// Features of element e into x[F] (zero padded): density modes m >= 1 over
+// the mean, for the cell then each stencil neighbour (zeros for a missing
+// one), then neighbour mean / cell mean - 1; every value clamped to [-8, 8].
+__device__ __forceinline__ void mlp_features_of(const double *state, std::int64_t ne, int M,
+                                                const std::int32_t *neighbors, std::int64_t e,
+                                                int F, float *x) {
+  for (int i = 0; i < F; ++i)
+    x[i] = 0.0f;
+  const double c0 = state[e];
+  const double inv = c0 != 0.0 ? 1.0 / c0 : 0.0;
+  for (int m = 1; m < M; ++m)
+    x[m - 1] = clamp8(static_cast<float>(state[m * ne + e] * inv));
+  for (int j = 0; j < 3; ++j) {
+    const std::int32_t nb = neighbors[e * 3 + j];
+    if (nb < 0)
+      continue;
+    const double n0 = state[nb];
+    const double ninv = n0 != 0.0 ? 1.0 / n0 : 0.0;
+    for (int m = 1; m < M; ++m)
+      x[(j + 1) * (M - 1) + m - 1] = clamp8(static_cast<float>(state[m * ne + nb] * ninv));
+    x[4 * (M - 1) + j] = clamp8(static_cast<float>(n0 * inv - 1.0));
+  }
+}
+
+// The reference modal-decay decision on density (modal_decay.hpp:23-33).
+__device__ __forceinline__ bool reference_troubled(const double *state, std::int64_t ne, int M,
+                                                   std::int64_t e, double threshold,
+                                                   int highest_degree_begin) {
+  double total = 0.0, high = 0.0;
+  for (int m = 0; m < M; ++m) {
+    const double value = state[m * ne + e];
+    total += value * value;
+    if (m >= highest_degree_begin)
+      high += value * value;
+  }
+  return !(total == 0.0 || high / total <= threshold);
+}
+
+__global__ void mlp_features_kernel(const double *state, std::int64_t ne, int M,
+                                    const std::int32_t *neighbors, int F, double threshold,
+                                    int highest_degree_begin, float *features,
+                                    std::uint8_t *labels) {
+  const std::int64_t e = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= ne)
+    return;
+  float x[kMlpMaxFeatures];
+  mlp_features_of(state, ne, M, neighbors, e, F, x);
+  for (int i = 0; i < F; ++i)
+    features[e * F + i] = x[i];
+  labels[e] = reference_troubled(state, ne, M, e, threshold, highest_degree_begin) ? 1 : 0;
+}
+
+// ---- training ------------------------------------------------------------------
+
+// One block: kMlpBatch samples [first, first + kMlpBatch) of the data (cyclic),
+// forward with BF16-rounded weights and operands, weighted binary
+// cross-entropy on the logit (positives weighted pos_weight), backward, and
+// the gradient of the summed loss added to grad; the summed loss to loss.
+__global__ void __launch_bounds__(256) mlp_train_kernel(const MlpShape sh, const float *params,
+                                                        const float *features,
+                                                        const std::uint8_t *labels,
+                                                        std::int64_t n, std::int64_t first,
+                                                        float pos_weight, float *grad,
+                                                        double *loss) {
+  constexpr int B = kMlpBatch, Hd = kMlpHidden;
+  const int F = sh.features;
+  extern __shared__ float smem[];
+  float *X = smem;            // [B][F]
+  float *H1 = X + B * F;      // [B][Hd]
+  float *H2 = H1 + B * Hd;    // [B][Hd]
+  float *D2 = H2 + B * Hd;    // [B][Hd] dLoss/d(pre-activation 2)
+  float *D1 = D2 + B * Hd;    // [B][Hd]
+  float *d3 = D1 + B * Hd;    // [B] dLoss/dlogit
+  const float *W1 = params + sh.w1, *b1 = params + sh.b1, *W2 = params + sh.w2,
+              *b2 = params + sh.b2, *w3 = params + sh.w3;
+  const float b3 = params[sh.b3];
+  const std::int64_t base = first + static_cast<std::int64_t>(blockIdx.x) * B;
+  const int t = threadIdx.x;
+  for (int i = t; i < B * F; i += blockDim.x) {
+    const std::int64_t s = (base + i / F) % n;
+    X[i] = bf16_round(features[s * F + i % F]);
+  }
+  __syncthreads();
+  for (int i = t; i < B * Hd; i += blockDim.x) {
+    const int b = i / Hd, j = i % Hd;
+    float acc = b1[j];
+    for (int k = 0; k < F; ++k)
+      acc = fmaf(bf16_round(W1[j * F + k]), X[b * F + k], acc);
+    H1[i] = bf16_round(fmaxf(acc, 0.0f));
+  }
+  __syncthreads();
+  for (int i = t; i < B * Hd; i += blockDim.x) {
+    const int b = i / Hd, j = i % Hd;
+    float acc = b2[j];
+    for (int k = 0; k < Hd; ++k)
+      acc = fmaf(bf16_round(W2[j * Hd + k]), H1[b * Hd + k], acc);
+    H2[i] = fmaxf(acc, 0.0f);
+  }
+  __syncthreads();
+  if (t < B) {
+    float z = b3;
+    for (int k = 0; k < Hd; ++k)
+      z = fmaf(bf16_round(w3[k]), H2[t * Hd + k], z);
+    const std::int64_t s = (base + t) % n;
+    const float y = labels[s] ? 1.0f : 0.0f;
+    const float w = labels[s] ? pos_weight : 1.0f;
+    // loss = w (softplus(z) - y z), stable form; dloss/dz = w (sigmoid(z) - y)
+    const float sp = fmaxf(z, 0.0f) + log1pf(expf(-fabsf(z)));
+    atomicAdd(loss, static_cast<double>(w * (sp - y * z)));
+    d3[t] = w * (1.0f / (1.0f + expf(-z)) - y);
+  }
+  __syncthreads();
+  for (int i = t; i < B * Hd; i += blockDim.x) {
+    const int b = i / Hd, k = i % Hd;
+    D2[i] = H2[i] > 0.0f ? d3[b] * bf16_round(w3[k]) : 0.0f;
+  }
+  __syncthreads();
+  for (int i = t; i < B * Hd; i += blockDim.x) {
+    const int b = i / Hd, j = i % Hd;
+    float acc = 0.0f;
+    for (int k = 0; k < Hd; ++k)
+      acc = fmaf(D2[b * Hd + k], bf16_round(W2[k * Hd + j]), acc);
+    D1[i] = H1[i] > 0.0f ? acc : 0.0f;
+  }
+  __syncthreads();
+  // Weight gradients, one entry per thread and pass, summed over the batch.
+  for (int i = t; i < Hd; i += blockDim.x) {
+    float gw3 = 0.0f, gb2 = 0.0f, gb1 = 0.0f;
+    for (int b = 0; b < B; ++b) {
+      gw3 = fmaf(d3[b], H2[b * Hd + i], gw3);
+      gb2 += D2[b * Hd + i];
+      gb1 += D1[b * Hd + i];
+    }
+    atomicAdd(grad + sh.w3 + i, gw3);
+    atomicAdd(grad + sh.b2 + i, gb2);
+    atomicAdd(grad + sh.b1 + i, gb1);
+  }
+  if (t == 0) {
+    float gb3 = 0.0f;
+    for (int b = 0; b < B; ++b)
+      gb3 += d3[b];
+    atomicAdd(grad + sh.b3, gb3);
+  }
+  for (int i = t; i < Hd * Hd; i += blockDim.x) {
+    const int k = i / Hd, j = i % Hd;
+    float acc = 0.0f;
+    for (int b = 0; b < B; ++b)
+      acc = fmaf(D2[b * Hd + k], H1[b * Hd + j], acc);
+    atomicAdd(grad + sh.w2 + i, acc);
+  }
+  for (int i = t; i < Hd * F; i += blockDim.x) {
+    const int j = i / F, k = i % F;
+    float acc = 0.0f;
+    for (int b = 0; b < B; ++b)
+      acc = fmaf(D1[b * Hd + j], X[b * F + k], acc);
+    atomicAdd(grad + sh.w1 + i, acc);
+  }
+}
+
+// Adam on the FP32 master weights with the summed gradient scaled by
+// `scale` (1 / samples), then the gradient is zeroed.
+__global__ void mlp_adam_kernel(std::int64_t count, float *params, float *grad, float *m1,
+                                float *m2, float lr, float beta1, float beta2, float eps,
+                                float bias1, float bias2, float scale) {
+  const std::int64_t i = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= count)
+    return;
+  const float g = grad[i] * scale;
+  m1[i] = beta1 * m1[i] + (1.0f - beta1) * g;
+  m2[i] = beta2 * m2[i] + (1.0f - beta2) * g * g;
+  params[i] -= lr * (m1[i] / bias1) / (sqrtf(m2[i] / bias2) + eps);
+  grad[i] = 0.0f;
+}
+
+// Logits of samples with the training forward pass (FP32 SIMT, BF16 rounding).
+__global__ void mlp_predict_kernel(const MlpShape sh, const float *params, const float *features,
+                                   std::int64_t n, float *logits) {
+  const std::int64_t s = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (s >= n)
+    return;
+  constexpr int Hd = kMlpHidden;
+  const int F = sh.features;
+  float x[kMlpMaxFeatures], h1[Hd];
+  for (int k = 0; k < F; ++k)
+    x[k] = bf16_round(features[s * F + k]);
+  for (int j = 0; j < Hd; ++j) {
+    float acc = params[sh.b1 + j];
+    for (int k = 0; k < F; ++k)
+      acc = fmaf(bf16_round(params[sh.w1 + j * F + k]), x[k], acc);
+    h1[j] = bf16_round(fmaxf(acc, 0.0f));
+  }
+  float z = params[sh.b3];
+  for (int j = 0; j < Hd; ++j) {
+    float acc = params[sh.b2 + j];
+    for (int k = 0; k < Hd; ++k)
+      acc = fmaf(bf16_round(params[sh.w2 + j * Hd + k]), h1[k], acc);
+    z = fmaf(bf16_round(params[sh.w3 + j]), fmaxf(acc, 0.0f), z);
+  }
+  logits[s] = z;
+}
+
+// ---- inference on the tensor cores ------------------------------------------------
+
+namespace {
+
+__device__ __forceinline__ unsigned pack_bf16(float lo, float hi) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const unsigned *>(&v);
+}
+
+// D = A B + D, A 16x16 row-major BF16 (4 registers), B 16x8 column-major BF16
+// (2 registers), D 16x8 FP32.
+__device__ __forceinline__ void mma_bf16(float *d, const unsigned *a, const unsigned *b) {
+  asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+               "{%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};\n"
+               : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+               : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+} // namespace
+
+// One CTA of 128 threads: 128 elements.  Each thread builds its element's
+// features (BF16 rows in shared memory) and its reference decision; each
+// warp then runs its 32 rows through the network as two 16-row tiles of
+// m16n8k16 MMAs (the first layer's accumulators become the second layer's A
+// fragments in registers), and the last layer as a quad reduction.  A cell is
+// troubled when sigmoid(logit) >= hi, smooth when <= lo, and otherwise takes
+// the reference decision.  Flags and the compacted troubled list as the
+// sensor writes them; counters: [0] network troubled, [1] network smooth,
+// [2] fallback, [3] reference troubled, [4] missed (reference troubled,
+// decided smooth), [5] false (reference smooth, decided troubled).
+template <int KF>
+__global__ void __launch_bounds__(128) mlp_indicator_kernel(const MlpIndicatorArgs a) {
+  constexpr int Hd = kMlpHidden, F = KF * 16, ROW = F + 8; // +8: fewer bank conflicts
+  __shared__ __align__(16) __nv_bfloat16 X[128 * ROW];
+  __shared__ __align__(16) __nv_bfloat16 W1[Hd * ROW];
+  __shared__ __align__(16) __nv_bfloat16 W2[Hd * (Hd + 8)];
+  __shared__ float b1[Hd], b2[Hd], w3[Hd], logit[128];
+  __shared__ unsigned long long counts[6];
+  const int t = threadIdx.x;
+  const float *P = a.params;
+  for (int i = t; i < Hd * F; i += 128)
+    W1[(i / F) * ROW + i % F] = __float2bfloat16_rn(P[a.shape.w1 + i]);
+  for (int i = t; i < Hd * Hd; i += 128)
+    W2[(i / Hd) * (Hd + 8) + i % Hd] = __float2bfloat16_rn(P[a.shape.w2 + i]);
+  for (int i = t; i < Hd; i += 128) {
+    b1[i] = P[a.shape.b1 + i];
+    b2[i] = P[a.shape.b2 + i];
+    w3[i] = bf16_round(P[a.shape.w3 + i]);
+  }
+  if (t < 6)
+    counts[t] = 0;
+  const std::int64_t e = static_cast<std::int64_t>(blockIdx.x) * 128 + t;
+  const bool active = e < a.ne;
+  bool reference = false;
+  {
+    float x[F];
+    if (active) {
+      mlp_features_of(a.state, a.ne, a.M, a.neighbors, e, F, x);
+      reference = reference_troubled(a.state, a.ne, a.M, e, a.threshold, a.highest_degree_begin);
+    } else {
+      for (int i = 0; i < F; ++i)
+        x[i] = 0.0f;
+    }
+    for (int i = 0; i < F; ++i)
+      X[t * ROW + i] = __float2bfloat16_rn(x[i]);
+  }
+  __syncthreads();
+
+  const int warp = t >> 5, lane = t & 31, g = lane >> 2, q = lane & 3;
+  for (int mt = 0; mt < 2; ++mt) {
+    const int row0 = warp * 32 + mt * 16;
+    // Layer 1: 16 rows x 64 outputs, K = F.
+    float h[8][4];
+    for (int nt = 0; nt < 8; ++nt) {
+      const int c = nt * 8 + 2 * q;
+      h[nt][0] = h[nt][2] = b1[c];
+      h[nt][1] = h[nt][3] = b1[c + 1];
+    }
+    for (int kk = 0; kk < KF; ++kk) {
+      unsigned af[4];
+      const __nv_bfloat16 *r0 = X + (row0 + g) * ROW + kk * 16 + 2 * q;
+      const __nv_bfloat16 *r8 = X + (row0 + g + 8) * ROW + kk * 16 + 2 * q;
+      af[0] = *reinterpret_cast<const unsigned *>(r0);
+      af[1] = *reinterpret_cast<const unsigned *>(r8);
+      af[2] = *reinterpret_cast<const unsigned *>(r0 + 8);
+      af[3] = *reinterpret_cast<const unsigned *>(r8 + 8);
+      for (int nt = 0; nt < 8; ++nt) {
+        const __nv_bfloat16 *wb = W1 + (nt * 8 + g) * ROW + kk * 16 + 2 * q;
+        const unsigned bf[2] = {*reinterpret_cast<const unsigned *>(wb),
+                                *reinterpret_cast<const unsigned *>(wb + 8)};
+        mma_bf16(h[nt], af, bf);
+      }
+    }
+    // Layer 2: A fragments straight from layer 1's accumulators (ReLU, BF16).
+    float o[8][4];
+    for (int nt = 0; nt < 8; ++nt) {
+      const int c = nt * 8 + 2 * q;
+      o[nt][0] = o[nt][2] = b2[c];
+      o[nt][1] = o[nt][3] = b2[c + 1];
+    }
+    for (int kk = 0; kk < 4; ++kk) {
+      const float *lo = h[2 * kk], *hi = h[2 * kk + 1];
+      const unsigned af[4] = {pack_bf16(fmaxf(lo[0], 0.0f), fmaxf(lo[1], 0.0f)),
+                              pack_bf16(fmaxf(lo[2], 0.0f), fmaxf(lo[3], 0.0f)),
+                              pack_bf16(fmaxf(hi[0], 0.0f), fmaxf(hi[1], 0.0f)),
+                              pack_bf16(fmaxf(hi[2], 0.0f), fmaxf(hi[3], 0.0f))};
+      for (int nt = 0; nt < 8; ++nt) {
+        const __nv_bfloat16 *wb = W2 + (nt * 8 + g) * (Hd + 8) + kk * 16 + 2 * q;
+        const unsigned bf[2] = {*reinterpret_cast<const unsigned *>(wb),
+                                *reinterpret_cast<const unsigned *>(wb + 8)};
+        mma_bf16(o[nt], af, bf);
+      }
+    }
+    // Layer 3: rows g and g + 8, columns 2q, 2q+1 of each n-tile, then the quad.
+    float z0 = 0.0f, z8 = 0.0f;
+    for (int nt = 0; nt < 8; ++nt) {
+      const int c = nt * 8 + 2 * q;
+      z0 = fmaf(w3[c], fmaxf(o[nt][0], 0.0f), fmaf(w3[c + 1], fmaxf(o[nt][1], 0.0f), z0));
+      z8 = fmaf(w3[c], fmaxf(o[nt][2], 0.0f), fmaf(w3[c + 1], fmaxf(o[nt][3], 0.0f), z8));
+    }
+    z0 += __shfl_xor_sync(0xffffffffu, z0, 1);
+    z0 += __shfl_xor_sync(0xffffffffu, z0, 2);
+    z8 += __shfl_xor_sync(0xffffffffu, z8, 1);
+    z8 += __shfl_xor_sync(0xffffffffu, z8, 2);
+    if (q == 0) {
+      logit[row0 + g] = z0 + P[a.shape.b3];
+      logit[row0 + g + 8] = z8 + P[a.shape.b3];
+    }
+  }
+  __syncthreads();
+
+  if (active) {
+    const float p = 1.0f / (1.0f + expf(-logit[t]));
+    bool troubled;
+    int kind;
+    if (p >= a.hi) {
+      troubled = true;
+      kind = 0;
+    } else if (p <= a.lo) {
+      troubled = false;
+      kind = 1;
+    } else {
+      troubled = reference;
+      kind = 2;
+    }
+    if (a.logits)
+      a.logits[e] = logit[t];
+    a.flags[e] = troubled ? 1 : 0;
+    atomicAdd(&counts[kind], 1ULL);
+    if (reference)
+      atomicAdd(&counts[3], 1ULL);
+    if (reference && !troubled)
+      atomicAdd(&counts[4], 1ULL);
+    if (!reference && troubled)
+      atomicAdd(&counts[5], 1ULL);
+    const unsigned mask = __activemask();
+    const unsigned ballot = __ballot_sync(mask, troubled);
+    if (ballot) {
+      const int leader = __ffs(ballot) - 1;
+      int base = 0;
+      if (lane == leader)
+        base = atomicAdd(a.troubled_count, __popc(ballot));
+      base = __shfl_sync(mask, base, leader);
+      if (troubled)
+        a.troubled[base + __popc(ballot & ((1u << lane) - 1u))] = static_cast<std::int32_t>(e);
+    }
+  }
+  __syncthreads();
+  if (t < 6 && a.stats && counts[t])
+    atomicAdd(a.stats + t, counts[t]);
+}
+
+// ---- host launchers -------------------------------------------------------------
+
+MlpShape mlp_shape(int features) {
+  if (features <= 0 || features % 16 != 0 || features > kMlpMaxFeatures)
+    throw std::invalid_argument("indicator network: features must be a multiple of 16, at most " +
+                                std::to_string(kMlpMaxFeatures));
+  MlpShape s;
+  s.features = features;
+  s.w1 = 0;
+  s.b1 = s.w1 + kMlpHidden * features;
+  s.w2 = s.b1 + kMlpHidden;
+  s.b2 = s.w2 + kMlpHidden * kMlpHidden;
+  s.w3 = s.b2 + kMlpHidden;
+  s.b3 = s.w3 + kMlpHidden;
+  s.count = s.b3 + 1;
+  return s;
+}
+
+int mlp_features_for_modes(int M) {
+  const int raw = 4 * (M - 1) + 3;
+  return (raw + 15) / 16 * 16;
+}
+
+void launch_mlp_features(const double *state, std::int64_t ne, int M,
+                         const std::int32_t *neighbors, int F, double threshold,
+                         int highest_degree_begin, float *features, std::uint8_t *labels,
+                         cudaStream_t s) {
+  if (ne > 0)
+    mlp_features_kernel<<<static_cast<unsigned>((ne + 127) / 128), 128, 0, s>>>(
+        state, ne, M, neighbors, F, threshold, highest_degree_begin, features, labels);
+}
+
+std::size_t mlp_train_smem(int F) {
+  return sizeof(float) * (kMlpBatch * F + 4 * kMlpBatch * kMlpHidden + kMlpBatch);
+}
+
+void launch_mlp_train(const MlpShape &sh, const float *params, const float *features,
+                      const std::uint8_t *labels, std::int64_t n, std::int64_t first,
+                      std::int64_t blocks, float pos_weight, float *grad, double *loss,
+                      cudaStream_t s) {
+  const std::size_t smem = mlp_train_smem(sh.features);
+  cudaError_t rc = cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(smem));
+  if (rc != cudaSuccess)
+    throw std::runtime_error(std::string("indicator training: ") + cudaGetErrorString(rc));
+  if (blocks > 0)
+    mlp_train_kernel<<<static_cast<unsigned>(blocks), 256, smem, s>>>(
+        sh, params, features, labels, n, first, pos_weight, grad, loss);
+}
+
+void launch_mlp_adam(std::int64_t count, float *params, float *grad, float *m1, float *m2,
+                     float lr, float beta1, float beta2, float eps, std::int64_t step, float scale,
+                     cudaStream_t s) {
+  const float bias1 = 1.0f - powf(beta1, static_cast<float>(step));
+  const float bias2 = 1.0f - powf(beta2, static_cast<float>(step));
+  mlp_adam_kernel<<<static_cast<unsigned>((count + 255) / 256), 256, 0, s>>>(
+      count, params, grad, m1, m2, lr, beta1, beta2, eps, bias1, bias2, scale);
+}
+
+void launch_mlp_predict(const MlpShape &sh, const float *params, const float *features,
+                        std::int64_t n, float *logits, cudaStream_t s) {
+  if (n > 0)
+    mlp_predict_kernel<<<static_cast<unsigned>((n + 127) / 128), 128, 0, s>>>(sh, params, features,
+                                                                              n, logits);
+}
+
+void launch_mlp_indicator(const MlpIndicatorArgs &a, cudaStream_t s) {
+  if (a.ne <= 0)
+    return;
+  const unsigned blocks = static_cast<unsigned>((a.ne + 127) / 128);
+  switch (a.shape.features / 16) {
+  case 1: mlp_indicator_kernel<1><<<blocks, 128, 0, s>>>(a); break;
+  case 2: mlp_indicator_kernel<2><<<blocks, 128, 0, s>>>(a); break;
+  case 3: mlp_indicator_kernel<3><<<blocks, 128, 0, s>>>(a); break;
+  default: throw std::invalid_argument("indicator network: unsupported feature count");
+  }
+}
+
+} // namespace wasl_b200

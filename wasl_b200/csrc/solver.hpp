@@ -106,6 +106,24 @@ public:
   // The state evaluated at the rule's points, [element][point][variable].
   virtual void evaluate(int rule_order, double *values) = 0;
   cudaStream_t stream() const { return stream_; }
+  // The learned troubled-cell indicator (2D Euler with limiting only).
+  virtual void set_indicator(const float *weights, std::int64_t count, double lo, double hi) {
+    (void)weights, (void)count, (void)lo, (void)hi;
+    throw SolverError(WASL_ERR_ARGUMENT, "learned indicator: 2D Euler with limiting only");
+  }
+  virtual int indicator_features() const { return 0; }
+  virtual void indicator_data(float *features, std::uint8_t *labels) {
+    (void)features, (void)labels;
+    throw SolverError(WASL_ERR_ARGUMENT, "learned indicator: 2D Euler with limiting only");
+  }
+  virtual void indicator_logits(float *logits) {
+    (void)logits;
+    throw SolverError(WASL_ERR_ARGUMENT, "learned indicator: 2D Euler with limiting only");
+  }
+  virtual void indicator_stats(unsigned long long *stats, bool reset) {
+    (void)stats, (void)reset;
+    throw SolverError(WASL_ERR_ARGUMENT, "learned indicator: 2D Euler with limiting only");
+  }
   // The kernel variant in use (-1: the form has one kernel) and, when it was
   // autotuned, the timed mean of every variant (count of them in `count`).
   virtual int kernel_choice(double *ms, int capacity, int &count) {
