@@ -256,3 +256,99 @@ def project_batch_case(batch, c, field, p):
     rule = max(p, 5)
     x, y, _ = batch.quadrature(c, rule)
     batch.project(c, rule, field(x, y))
+
+
+# ---- exact Riemann solution ------------------------------------------------------------
+
+class ExactRiemann:
+    """Exact solution of the 1D Riemann problem for an ideal gas between
+    primitive states (rho, u, p) (Toro, Riemann Solvers and Numerical Methods
+    for Fluid Dynamics, ch. 4): the star pressure by Newton's method on the
+    sum of the two wave functions, started from the primitive-variable
+    estimate, then each similarity coordinate sampled across the left wave,
+    the contact and the right wave.  Vectorised over samples."""
+
+    def __init__(self, left, right, gamma=GAMMA):
+        self.gamma = g = gamma
+        self.left, self.right = tuple(map(float, left)), tuple(map(float, right))
+        (rl, ul, pl), (rr, ur, pr) = self.left, self.right
+        self.cl, self.cr = math.sqrt(g * pl / rl), math.sqrt(g * pr / rr)
+        if 2.0 * (self.cl + self.cr) / (g - 1.0) <= ur - ul:
+            raise ValueError("exact Riemann solution: the states open a vacuum")
+        p = max(1e-12, 0.5 * (pl + pr) - 0.125 * (ur - ul) * (rl + rr) * (self.cl + self.cr))
+        for _ in range(100):
+            fl, dl = self._wave(p, rl, pl, self.cl)
+            fr, dr = self._wave(p, rr, pr, self.cr)
+            step = (fl + fr + ur - ul) / (dl + dr)
+            p_new = max(1e-14, p - step)
+            if abs(p_new - p) <= 1e-15 * (p_new + p):
+                p = p_new
+                break
+            p = p_new
+        self.p_star = p
+        fl, _ = self._wave(p, rl, pl, self.cl)
+        fr, _ = self._wave(p, rr, pr, self.cr)
+        self.u_star = 0.5 * (ul + ur) + 0.5 * (fr - fl)
+
+    def _wave(self, p, rho, pk, c):
+        """The velocity jump across the wave from pressure pk to p, and its
+        derivative in p (shock for p > pk, rarefaction otherwise)."""
+        g = self.gamma
+        if p > pk:
+            a, b = 2.0 / ((g + 1.0) * rho), (g - 1.0) / (g + 1.0) * pk
+            root = math.sqrt(a / (b + p))
+            return (p - pk) * root, root * (1.0 - 0.5 * (p - pk) / (b + p))
+        ratio = p / pk
+        return (2.0 * c / (g - 1.0) * (ratio ** ((g - 1.0) / (2.0 * g)) - 1.0),
+                ratio ** (-(g + 1.0) / (2.0 * g)) / (rho * c))
+
+    def _side(self, s, state, c, sign):
+        """Samples on one side of the contact; sign +1 left, -1 right (the
+        right side is the left side's mirror image)."""
+        g = self.gamma
+        rho, u, p = state
+        ps, us = self.p_star, self.u_star
+        out_rho, out_u, out_p = (np.full_like(s, rho), np.full_like(s, u), np.full_like(s, p))
+        ratio = ps / p
+        if ps > p:  # shock
+            speed = u - sign * c * math.sqrt((g + 1.0) / (2.0 * g) * ratio + (g - 1.0) / (2.0 * g))
+            behind = sign * (s - speed) > 0.0
+            k = (g - 1.0) / (g + 1.0)
+            out_rho = np.where(behind, rho * (ratio + k) / (k * ratio + 1.0), out_rho)
+            out_u = np.where(behind, us, out_u)
+            out_p = np.where(behind, ps, out_p)
+            return out_rho, out_u, out_p
+        c_star = c * ratio ** ((g - 1.0) / (2.0 * g))
+        head, tail = u - sign * c, us - sign * c_star
+        star = sign * (s - tail) >= 0.0
+        fan = (sign * (s - head) > 0.0) & ~star
+        out_rho = np.where(star, rho * ratio ** (1.0 / g), out_rho)
+        out_u = np.where(star, us, out_u)
+        out_p = np.where(star, ps, out_p)
+        cf = 2.0 / (g + 1.0) * (c + sign * (g - 1.0) / 2.0 * (u - s))
+        uf = 2.0 / (g + 1.0) * (sign * c + (g - 1.0) / 2.0 * u + s)
+        cf = np.maximum(cf, 0.0)
+        out_rho = np.where(fan, rho * (cf / c) ** (2.0 / (g - 1.0)), out_rho)
+        out_u = np.where(fan, uf, out_u)
+        out_p = np.where(fan, p * (cf / c) ** (2.0 * g / (g - 1.0)), out_p)
+        return out_rho, out_u, out_p
+
+    def sample(self, s):
+        """(rho, u, p) at similarity coordinates s = (x - x0) / t."""
+        s = np.asarray(s, dtype=np.float64)
+        left = self._side(s, self.left, self.cl, 1.0)
+        right = self._side(s, self.right, self.cr, -1.0)
+        on_left = s <= self.u_star
+        return tuple(np.where(on_left, a, b) for a, b in zip(left, right))
+
+
+def sod_density_l1(solver, exact, interface=0.5, time=0.2, samples=400):
+    """L1 error of the density cell averages against the exact cell averages
+    (each averaged over `samples` evenly spaced points), on a line mesh."""
+    ends = solver.vertices().reshape(-1, 2)
+    state = solver.get_state().reshape(4, solver.modes, solver.elements)
+    average = state[0, 0] / math.sqrt(2.0)
+    width = ends[:, 1] - ends[:, 0]
+    points = ends[:, :1] + (np.arange(samples) + 0.5)[None, :] / samples * width[:, None]
+    exact_average = exact.sample((points - interface) / time)[0].mean(axis=1)
+    return float(np.sum(width * np.abs(average - exact_average)))
