@@ -62,6 +62,8 @@ def parse():
                          " quadrant: four-quadrant Riemann, 1024x1024 quads, P3, limiter;"
                          " shock-vortex: 2048x1024 quads, P3, learned indicator")
     ap.add_argument("--cases", type=int, default=512, help="batched workload: number of cases")
+    ap.add_argument("--quads", type=int, default=1024,
+                    help="quadrant / shock-vortex workloads: quads per unit side")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -583,12 +585,12 @@ def limited(args, rank, world, local_rank):
     p = 3
     t0 = time.perf_counter()
     if args.workload == "quadrant":
-        arrays = meshgen.jittered_box(1024, jitter=0.15, seed=3)
+        arrays = meshgen.jittered_box(args.quads, jitter=0.15, seed=3)
         problem = cases.QuadrantRiemann(seed=3)
         forms = ("plain", "mixed")
         weights = None
     else:
-        arrays = indicator.shock_vortex_mesh(1024, seed=5)
+        arrays = indicator.shock_vortex_mesh(args.quads, seed=5)
         problem = cases.ShockVortex(seed=5)
         forms = ("mixed",)
         xs, ys = [], []
@@ -637,10 +639,12 @@ def limited(args, rank, world, local_rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": chosen["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
         "data": "synthetic (seeded jittered mesh, projected initial data)",
-        "config": {"workload": (f"four-quadrant Riemann, 1024x1024 quads -> {elements}"
+        "config": {"workload": (f"four-quadrant Riemann, {args.quads}x{args.quads} quads ->"
+                                f" {elements}"
                                 " jittered triangles, P3, transmissive, WENO + positivity,"
                                 " CFL 0.1" if args.workload == "quadrant" else
-                                f"shock-vortex, 2048x1024 quads -> {elements} jittered"
+                                f"shock-vortex, {2 * args.quads}x{args.quads} quads ->"
+                                f" {elements} jittered"
                                 " triangles, P3, transmissive, learned indicator + WENO +"
                                 " positivity on every element, CFL 0.1"),
                    "elements": elements, "dof": dof, "forms": out,
