@@ -55,7 +55,7 @@ private:
     TuneResult tuning;
     int highest_degree_begin = 0, check_points = 0;
     DeviceArray<double> u, e, s, geo, slot_geo, transforms, normal_x, normal_y, check, limited,
-        basis64;
+        basis64, check_bound;
     DeviceArray<std::int32_t> tile_nbr, tile_aux, neighbors, troubled, count, element_case, rough;
     DeviceArray<std::uint8_t> tile_code, flags;
     DeviceArray<float> basis32;

@@ -214,6 +214,7 @@ BatchSolver::BatchSolver(const wasl_batch_config &cfg, std::int64_t case_count, 
       g->normal_x.upload(nx, stream_);
       g->normal_y.upload(ny, stream_);
       g->check.upload(first.check_basis, stream_);
+      g->check_bound.upload(positivity_check_bound(first.check_basis, M), stream_);
       g->limited.resize(static_cast<std::size_t>(ne) * 4 * M);
       g->troubled.resize(ne);
       g->count.resize(1);
@@ -376,6 +377,7 @@ LimitArgs BatchSolver::limit_args(const Group &g, double *state) const {
   l.flags = g.flags.get();
   l.relative_floor = kMixedRelativeFloor;
   l.case_status = d_status_.get();
+  l.check_bound = g.check_bound.get();
   l.element_case = g.element_case.get();
   return l;
 }

@@ -317,10 +317,48 @@ __device__ __forceinline__ void positivity_limit(const LimitArgs &a, double *lim
       lim[v * M + m] *= pscale;
 }
 
+// Whether an element provably keeps density and pressure at or above the
+// check-point floors of positivity_limit at every check point, from bounds
+// on the point values: |sum_{m>=1} c_m phi_m| <= sum_{m>=1} |c_m| max|phi_m|
+// (max over the check points, check_bound), then the pressure's lower bound
+// from the bounds on density, momentum and energy.  Where it holds the limiter
+// would scale by exactly 1, so skipping it gives the same bits.  Small
+// margins cover the rounding of the point sums.
+template <int M> __device__ __forceinline__ bool positivity_clear(const LimitArgs &a,
+                                                                  const double *lim) {
+  const double inv_root2 = 1.0 / sqrt(2.0);
+  const double avg[4] = {lim[0] * inv_root2, lim[M] * inv_root2, lim[2 * M] * inv_root2,
+                         lim[3 * M] * inv_root2};
+  if (!(avg[0] > a.density_floor && primitive(a.gamma, avg).p > a.pressure_floor))
+    return false; // positivity_limit reports it
+  const double rf = a.relative_floor > 0.0 ? fmax(a.density_floor, a.relative_floor * avg[0])
+                                           : a.density_floor;
+  const double pf = a.relative_floor > 0.0 ? fmax(a.pressure_floor, a.relative_floor * avg[3])
+                                           : a.pressure_floor;
+  double b[4];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    double sum = 0.0;
+#pragma unroll
+    for (int m = 1; m < M; ++m)
+      sum += fabs(lim[v * M + m]) * a.check_bound[m];
+    b[v] = sum;
+  }
+  const double rho_lo = avg[0] - b[0] - 1e-12 * (avg[0] + b[0]);
+  if (!(rho_lo >= rf))
+    return false;
+  const double mx = fabs(avg[1]) + b[1], my = fabs(avg[2]) + b[2];
+  const double energy_lo = avg[3] - b[3];
+  const double p_lo = (a.gamma - 1.0) * (energy_lo - 0.5 * (mx * mx + my * my) / rho_lo) -
+                      1e-12 * (a.gamma - 1.0) * (fabs(avg[3]) + b[3] + 0.5 * (mx * mx + my * my) / rho_lo);
+  return p_lo >= pf;
+}
+
 // The positivity limiter on every element the sensor did not flag (flags[e]
 // == 0), in place: the always-on positivity of the non-reference forms (the
 // reference limits positivity in troubled cells only,
-// cpp/src/limiting/euler_modal_limiter.cpp:81-96).
+// cpp/src/limiting/euler_modal_limiter.cpp:81-96).  Elements that provably
+// need no scaling (positivity_clear) are skipped.
 template <int M> __global__ void positivity_rest(const LimitArgs a) {
   for (std::int64_t e = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < a.ne;
        e += static_cast<std::int64_t>(gridDim.x) * blockDim.x) {
@@ -330,6 +368,8 @@ template <int M> __global__ void positivity_rest(const LimitArgs a) {
 #pragma unroll
     for (int i = 0; i < 4 * M; ++i)
       lim[i] = a.state[i * a.ne + e];
+    if (a.check_bound && positivity_clear<M>(a, lim))
+      continue;
     positivity_limit<M>(a, lim, e);
 #pragma unroll
     for (int i = 0; i < 4 * M; ++i)
@@ -636,6 +676,13 @@ void launch_sense_f64(int M, const SenseArgs &a, cudaStream_t s) {
   case 10: sense_f64<10><<<blocks, 256, 0, s>>>(a); break;
   default: throw std::invalid_argument("sensor: unsupported mode count");
   }
+}
+
+std::vector<double> positivity_check_bound(const std::vector<double> &check_basis, int M) {
+  std::vector<double> bound(M, 0.0);
+  for (std::size_t i = 0; i < check_basis.size(); ++i)
+    bound[i % M] = std::max(bound[i % M], std::fabs(check_basis[i]));
+  return bound;
 }
 
 void launch_dt_from_speed(std::int64_t cases, unsigned long long *speed, double cfl,

@@ -1112,13 +1112,13 @@ template <int P, int R, int TILE, int MINB> void tile_opt_in() {
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(tile_smem<P, TILE>())),
         "tile kernel shared memory");
-  check(cudaFuncSetAttribute(euler_tri_tile_mixed<P, R, TILE, MINB, true>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(tile_smem<P, TILE>())),
-        "tile kernel shared memory");
   if (device < 64)
     opted_in[device] = true;
 }
+
+// The second pass: one warp per CTA and no register cap, so a short rough
+// list spreads over many SMs (its elements read their neighbours from L2).
+constexpr int kRoughTile = 32;
 
 // The FP32 pass over all tiles, then (with a rough list) the pass over the
 // elements it left, sized for the worst case: its CTAs beyond the list's
@@ -1133,8 +1133,9 @@ template <int P, int R, int TILE, int MINB> void stage_tile(const StageArgs &a, 
   euler_tri_tile_mixed<P, R, TILE, MINB, false>
       <<<static_cast<unsigned>(blocks), TILE, tile_smem<P, TILE>(), s>>>(a);
   if (a.rough)
-    euler_tri_tile_mixed<P, R, TILE, MINB, true>
-        <<<static_cast<unsigned>((a.mesh.ne + TILE - 1) / TILE), TILE, tile_smem<P, TILE>(), s>>>(a);
+    euler_tri_tile_mixed<P, R, kRoughTile, 1, true>
+        <<<static_cast<unsigned>((a.mesh.ne + kRoughTile - 1) / kRoughTile), kRoughTile,
+           tile_smem<P, kRoughTile>(), s>>>(a);
 }
 
 // Launch shapes of the tile kernel (elements per CTA, register budget):

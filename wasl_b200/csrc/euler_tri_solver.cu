@@ -156,6 +156,7 @@ public:
       d_normal_x_.upload(stencil_.normal_x, stream_);
       d_normal_y_.upload(stencil_.normal_y, stream_);
       d_check_.upload(stencil_.check_basis, stream_);
+      d_check_bound_.upload(positivity_check_bound(stencil_.check_basis, M_), stream_);
       d_limited_.resize(static_cast<std::size_t>(ne_) * 4 * M_);
       d_troubled_.resize(ne_);
     }
@@ -557,6 +558,7 @@ private:
     l.positivity_all = cfg_.positivity_all ? 1 : 0;
     l.flags = flags;
     l.relative_floor = mixed_ ? kMixedRelativeFloor : 0.0;
+    l.check_bound = d_check_bound_.get();
     l.ne = ne_;
     l.state = state;
     l.troubled = d_troubled_.get();
@@ -607,6 +609,7 @@ private:
   TuneResult tuning_;
   DeviceArray<std::int32_t> d_tile_nbr_, d_tile_aux_, d_rough_;
   DeviceArray<float> d_mlp_; // learned indicator weights (empty: the reference sensor)
+  DeviceArray<double> d_check_bound_;
   DeviceArray<unsigned long long> d_mlp_stats_;
   double mlp_lo_ = 0.1, mlp_hi_ = 0.9;
   DeviceArray<std::uint8_t> d_tile_code_;

@@ -1,7 +1,9 @@
 // Launch interface of the CUDA kernels (host side; no device code here).
 #pragma once
 
+#include <cmath>
 #include <cstdint>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -151,7 +153,13 @@ struct LimitArgs {
   // e] (first error only) instead of in the error word.
   int *case_status = nullptr;
   const std::int32_t *element_case = nullptr;
+  // [M] largest |basis value| of each mode over the check points: lets the
+  // always-on pass skip elements whose bounds clear the floors (null: none).
+  const double *check_bound = nullptr;
 };
+
+// check_bound[m] = max over points |check_basis[point][m]| (host).
+std::vector<double> positivity_check_bound(const std::vector<double> &check_basis, int M);
 
 // The mixed form's positivity check-point floors relative to the mean: FP32
 // resolves a point state to ~6e-8 of the mean, so point densities and
