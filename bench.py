@@ -130,6 +130,35 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------------
+# ranks (one process per GPU under torchrun; replicas, weak scaling)
+# ---------------------------------------------------------------------------------
+
+def init_ranks(world, local_rank, backend="nccl", timeout_s=120):
+    """The process group for world > 1 (None for one rank)."""
+    if world <= 1:
+        return None
+    import datetime
+    import torch
+    import torch.distributed as dist
+    kw = {"timeout": datetime.timedelta(seconds=timeout_s)}
+    if backend == "nccl":
+        kw["device_id"] = torch.device("cuda", local_rank)
+    dist.init_process_group(backend, **kw)
+    return dist
+
+
+def reduce_over_ranks(dist, value, op="max", device="cuda"):
+    """value reduced over all ranks (max, min or sum); value itself for one rank."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op={"max": dist.ReduceOp.MAX, "min": dist.ReduceOp.MIN,
+                           "sum": dist.ReduceOp.SUM}[op])
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------------
 
@@ -255,12 +284,7 @@ def ours(args, rank, world, local_rank):
     import torch
     import wasl_b200
     torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local_rank))
+    dist = init_ranks(world, local_rank)
     form = args.form
     if form == "chosen":
         form = "mixed" if wasl_b200.form_available("mixed") else "plain"
@@ -274,17 +298,12 @@ def ours(args, rank, world, local_rank):
     sampler.start()
     total_ms, stage_ms, stage_kernels, launches = time_device_steps(g, args, torch, flush, stream)
     clocks = sampler.stop()
-    if dist:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = reduce_over_ranks(dist, total_ms, "max")
     dofs = g.state_size
     value = world * 3.0 * dofs * args.steps / (total_ms * 1e-3)
     e2e_value, e2e_steps, h2d, d2h = time_e2e(g, args, torch, stream)
     if dist:
-        t = torch.tensor([e2e_value], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MIN)
-        e2e_value = float(t.item()) * world
+        e2e_value = reduce_over_ranks(dist, e2e_value, "min") * world
     peaks, peak_kind = measured_peaks()
     per_launch_bytes = BYTES_PER_DOF * dofs + BYTES_PER_ELEMENT * g.elements
     kernel_s = stage_ms * 1e-3 / max(stage_kernels, 1)
@@ -451,12 +470,7 @@ def batched(args, rank, world, local_rank):
     import wasl_b200
     from wasl_b200 import cases
     torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local_rank))
+    dist = init_ranks(world, local_rank, timeout_s=600)
     cfl = 0.1
     t0 = time.perf_counter()
     specs = cases.batched_riemann_cases(args.cases, seed=4 + rank)
@@ -479,11 +493,7 @@ def batched(args, rank, world, local_rank):
     end.record(stream)
     torch.cuda.synchronize()
     clocks = sampler.stop()
-    ms = start.elapsed_time(end)
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = reduce_over_ranks(dist, start.elapsed_time(end), "max")
     value = world * 3.0 * b.dof * args.steps / (ms * 1e-3)
     per_step, graph, _ = b.launches()
     # e2e through the C-ABI with host buffers: every case's state in from
