@@ -158,8 +158,13 @@ int wasl_gpu_run(wasl_gpu *handle, double cfl, double start_time, double end_tim
                  uint64_t max_steps, uint64_t *steps, double *time);
 
 /* Device-resident fast path: `steps` steps with the CFL step computed on the
- * device each step, no host synchronization (capturable in a CUDA graph). */
+ * device each step, enqueued on the handle's stream without host
+ * synchronization; a device error (non-physical average, positivity floor)
+ * is raised by wasl_gpu_sync or the next call that waits for the device. */
 int wasl_gpu_advance(wasl_gpu *handle, double cfl, int64_t steps);
+
+/* Waits for the handle's stream and reports a pending device error. */
+int wasl_gpu_sync(wasl_gpu *handle);
 
 /* The mixed form's kernel in use: 0 face-centric kernels, 1 + s the fused
  * tile kernel in launch shape s (0: 128 elements per CTA at <= 128 registers

@@ -202,3 +202,18 @@ def test_rough_pass_conserves_with_the_limiter(p):
         assert g.flags().sum() > 0
     assert abs(m1 - m0) <= 1e-13 * abs(m0)
     assert abs(e1 - e0) <= 1e-13 * abs(e0)
+
+
+@pytest.mark.parametrize("precision", ["plain", "mixed"])
+def test_advance_enqueues_and_sync_reports_errors(precision):
+    """wasl_gpu_advance only enqueues; a device error from those steps (here a
+    negative cell-average density made on the host) is reported by sync."""
+    arrays = meshgen.jittered_box(8, jitter=0.15, seed=2)
+    with wasl_b200.Solver(*arrays, polynomial_order=2, precision=precision) as g:
+        state = seeded_state(g.elements, 2, 3, amplitude=0.01).reshape(4, g.modes, g.elements)
+        state[0, 0, 5] = -0.5
+        g.set_state(state.ravel())
+        g.advance(0.15, 1, sync=False)
+        with pytest.raises(wasl_b200.WaslError, match="not physical") as err:
+            g.sync()
+        assert err.value.status == -4

@@ -96,6 +96,7 @@ SIGNATURES = {
     "wasl_gpu_run": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_uint64,
                                C.POINTER(C.c_uint64), _d]),
     "wasl_gpu_advance": (C.c_int, [C.c_void_p, C.c_double, C.c_int64]),
+    "wasl_gpu_sync": (C.c_int, [C.c_void_p]),
     "wasl_gpu_state_device": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "wasl_gpu_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "wasl_gpu_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), _d, C.c_int,
@@ -315,8 +316,15 @@ class Solver:
                                            C.byref(steps), C.byref(time)))
         return steps.value, time.value
 
-    def advance(self, cfl: float, steps: int):
+    def advance(self, cfl: float, steps: int, sync: bool = True):
+        """Device-resident steps; with sync=False returns once they are
+        enqueued (device errors then surface at sync())."""
         self._check(self._lib.wasl_gpu_advance(self._h, cfl, steps))
+        if sync:
+            self.sync()
+
+    def sync(self):
+        self._check(self._lib.wasl_gpu_sync(self._h))
 
     def flags(self) -> np.ndarray:
         f = np.empty(3 * self.elements, dtype=np.uint8)

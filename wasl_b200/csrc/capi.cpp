@@ -283,6 +283,10 @@ int wasl_gpu_advance(wasl_gpu *h, double cfl, int64_t steps) {
   });
 }
 
+int wasl_gpu_sync(wasl_gpu *h) {
+  return guarded(h, [&] { h->solver->sync(); });
+}
+
 int wasl_gpu_state_device(wasl_gpu *h, double **p) {
   return guarded(h, [&] {
     need(p != nullptr, "null pointer");

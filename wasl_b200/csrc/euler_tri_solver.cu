@@ -307,8 +307,10 @@ public:
       speed_ready_ = fused_speed_ && kernel_ >= 1;
       fused_speed_ = false;
     }
-    check_error();
+    cuda_check(cudaGetLastError(), "advance");
   }
+
+  void sync() override { check_error(); }
 
   int indicator_features() const override {
     return limiting_ ? mlp_features_for_modes(M_) : 0;

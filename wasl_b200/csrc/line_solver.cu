@@ -217,8 +217,10 @@ public:
         enqueue_step(d_dt_.get(), 0.0);
       }
     }
-    check_error();
+    cuda_check(cudaGetLastError(), "advance");
   }
+
+  void sync() override { check_error(); }
 
   void flags(std::uint8_t *out) override {
     cuda_check(cudaMemcpyAsync(out, d_flags_.get(), 3 * ne_, cudaMemcpyDeviceToHost, stream_),

@@ -155,7 +155,7 @@ public:
     const double dt = stable_dt(cfl);
     for (std::int64_t n = 0; n < steps; ++n)
       enqueue_step(dt);
-    cuda_check(cudaStreamSynchronize(stream_), "advance");
+    cuda_check(cudaGetLastError(), "advance");
   }
 
   void flags(std::uint8_t *out) override {

@@ -92,7 +92,13 @@ public:
   virtual double stable_dt(double cfl) = 0;
   virtual void step(double dt) = 0;
   virtual void limit() = 0; // the stage limiter applied to the current state
+  // Enqueues `steps` device-resident steps; returns without waiting for
+  // them (device errors stay in the error word until sync()).
   virtual void advance(double cfl, std::int64_t steps) = 0;
+  // Waits for the handle's stream and raises a pending device error.
+  virtual void sync() {
+    cuda_check(cudaStreamSynchronize(stream_), "sync");
+  }
   virtual void flags(std::uint8_t *out) = 0;
   virtual void mass_energy(double &mass, double &energy) = 0;
   virtual double *state_device() = 0;
