@@ -37,7 +37,7 @@ def milder(problem):
 
 @pytest.mark.parametrize("limiting", [False, True])
 @pytest.mark.parametrize("use_graph", [True, False])
-@pytest.mark.parametrize("shape", [0, 3])
+@pytest.mark.parametrize("shape", [0, 3, 4, 6])
 def test_batch_matches_single_case_solver(limiting, use_graph, shape):
     """Bit-identical states per case, or, if a case fails alone (a positivity
     floor), the same failure from the batch."""

@@ -12,8 +12,11 @@ from wasl_b200 import cases, meshgen
 
 pytestmark = pytest.mark.gpu
 
-# mixed_kernel: 1 face-centric kernels, 2 + s the fused tile kernel in shape s.
+# mixed_kernel: 1 face-centric kernels, 2 + s the fused tile kernel in shape s
+# (s = 0..3 the tile kernel, 4..7 the shared-face tile kernel).
 KERNELS = [1, 2, 3, 4, 5]
+TILE_SHAPES = 8
+SHARED_KERNELS = [6, 7, 8, 9]
 
 
 def pair(arrays, p, **kw):
@@ -55,7 +58,7 @@ def test_one_step_close_to_plain(p):
 
 
 @pytest.mark.parametrize("p,rule,kernel", [(p, r, k) for p in (1, 2, 3) for r in (0, p)
-                                           for k in (1, 2)] + [(2, 2, k) for k in (3, 4, 5)])
+                                           for k in (1, 2, 8)] + [(2, 2, k) for k in (3, 4, 5)])
 def test_mass_and_energy_conserved(p, rule, kernel):
     """Periodic faces paired, interior faces evaluated by both sides with the
     same instructions: totals conserved to FP64 round-off."""
@@ -131,6 +134,32 @@ def test_tile_kernel_matches_face_centric(p, kernel, boundary):
     assert np.max(np.abs(out[kernel] - out[1])) <= 1e-6 * change
 
 
+@pytest.mark.parametrize("p", [1, 2, 3])
+@pytest.mark.parametrize("limiting", [False, True])
+@pytest.mark.parametrize("boundary", ["periodic", "transmissive"])
+def test_shared_face_kernel_is_bit_identical(p, limiting, boundary):
+    """The shared-face tile kernel evaluates a face inside a tile once instead
+    of once per element, with the same arithmetic: every launch shape gives
+    the tile kernel's states bit for bit, with and without the limiter (whose
+    rough pass takes the elements next to jumps of the means)."""
+    arrays = meshgen.jittered_box(20, jitter=0.15, seed=50 + p)
+    c = seeded_state(2 * 20 * 20, p, 70 + p, amplitude=0.02)
+    out = {}
+    for k in [2] + SHARED_KERNELS:
+        with wasl_b200.Solver(*arrays, polynomial_order=p, precision="mixed", mixed_kernel=k,
+                              boundary=boundary, limiting=limiting,
+                              positivity_all=limiting) as g:
+            g.set_state(c)
+            for _ in range(4):
+                g.step(g.stable_dt(0.1))
+            out[k] = (g.get_state(), g.flags())
+            assert g.tuning()[0] == k - 1
+    assert np.max(np.abs(out[2][0] - c)) > 0
+    for k in SHARED_KERNELS:
+        assert np.array_equal(out[k][0], out[2][0]), f"kernel {k}"
+        assert np.array_equal(out[k][1], out[2][1]), f"kernel {k}"
+
+
 def test_uniform_flow_tile_transmissive():
     arrays = meshgen.jittered_box(12, jitter=0.15, seed=5)
     with wasl_b200.Solver(*arrays, polynomial_order=2, precision="mixed", mixed_kernel=2,
@@ -154,8 +183,8 @@ def test_autotuner_times_every_variant():
         cases.project_initial(g, vortex.conserved)
         g.step(g.stable_dt(0.15))
         choice, ms = g.tuning()
-    assert len(ms) == 5 and all(t > 0 for t in ms)
-    assert 0 <= choice < 5 and ms[choice] == min(ms)
+    assert len(ms) == 1 + TILE_SHAPES and all(t > 0 for t in ms)
+    assert 0 <= choice < 1 + TILE_SHAPES and ms[choice] == min(ms)
     with wasl_b200.Solver(*arrays, polynomial_order=2, precision="mixed") as g:
         cases.project_initial(g, vortex.conserved)
         g.step(g.stable_dt(0.15))

@@ -60,8 +60,8 @@ private:
     DeviceArray<std::uint8_t> tile_code, flags;
     DeviceArray<float> basis32;
     DeviceArray<unsigned char> face_table, face_table64;
-    std::array<DeviceArray<TileWork>, 4> work;
-    std::array<std::int64_t, 4> work_count{};
+    std::array<DeviceArray<TileWork>, kTileShapeCount> work;
+    std::array<std::int64_t, kTileShapeCount> work_count{};
   };
 
   void check_case(std::int64_t c) const;

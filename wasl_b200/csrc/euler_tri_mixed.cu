@@ -22,6 +22,7 @@
 //   * the residual scaling and the Shu-Osher combination are FP64.
 // The plain kernels (euler_tri_f64.cu) remain the bit-consistent drop-in.
 #include <stdexcept>
+#include <type_traits>
 
 #include "euler_device.cuh"
 #include "kernels.hpp"
@@ -640,6 +641,99 @@ __device__ __noinline__ void face_fp64(double gamma, const double *own, std::int
   }
 }
 
+// The end of a tile kernel's stage for element e (thread t of the tile):
+// residual scaling by 1/det J, the Shu-Osher combination in FP64
+// (cpp/include/wasl/time/ssp_rk3.hpp:44-60), and, when asked for, the next
+// step's CFL speed and the modal-decay sensor on the result.
+template <int P, int TILE>
+__device__ __forceinline__ void tile_finish(const StageArgs &a, std::int64_t e, int t, int case_id,
+                                            const double (*sstate)[TILE], const double (&r0)[4],
+                                            const float (&racc)[4][TriShape<P>::M - 1]) {
+  constexpr int M = TriShape<P>::M;
+  const std::int64_t ne = a.mesh.ne;
+  const double gamma = a.gamma;
+  const double *__restrict__ geo = a.mesh.geo;
+  const double inv = geo[4 * ne + e];
+  const double dt = a.case_dt ? a.case_dt[case_id] : (a.dt ? *a.dt : a.dt_value);
+  double rho[M], avg[4];
+#pragma unroll
+  for (int v = 0; v < 4; ++v)
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const std::int64_t idx = (static_cast<std::int64_t>(v) * M + m) * ne + e;
+      const double cur = sstate[v * M + m][t];
+      const double rr = (m == 0 ? r0[v] : static_cast<double>(racc[v][m > 0 ? m - 1 : 0])) * inv;
+      double o;
+      if (a.stage == 0)
+        o = cur + dt * rr;
+      else if (a.stage == 1)
+        o = 0.75 * a.u0[idx] + 0.25 * (cur + dt * rr);
+      else
+        o = (1.0 / 3.0) * a.u0[idx] + (2.0 / 3.0) * (cur + dt * rr);
+      a.out[idx] = o;
+      if (v == 0)
+        rho[m] = o;
+      if (m == 0)
+        avg[v] = o;
+    }
+
+  if (a.speed_max) {
+    // The next step's CFL speed from this stage's cell averages.
+    const double scale = 1.0 / sqrt(2.0);
+    const double sa[4] = {__dmul_rn(scale, avg[0]), __dmul_rn(scale, avg[1]),
+                          __dmul_rn(scale, avg[2]), __dmul_rn(scale, avg[3])};
+    bool physical = true;
+    const double speed = cfl_speed(gamma, sa, 2, physical);
+    unsigned long long best = 0;
+    if (physical)
+      best = __double_as_longlong(speed);
+    else
+      raise_error(a.error, kNonPhysicalAverage, e);
+    // Warp max over whichever lanes are still active (past the tile's end,
+    // or handed to the rough pass, lanes have returned): the 64-bit max of
+    // positive FP64 bits as the max of the high words, then of the low words
+    // among the lanes holding it; one atomic per warp and case.
+    const unsigned mask = __activemask();
+    const int lane = threadIdx.x & 31;
+    // (No lane's match set is the whole mask unless all lanes share the case,
+    // so the branch is uniform across the warp.)
+    if (__match_any_sync(mask, case_id) == mask) {
+      const unsigned hi = __reduce_max_sync(mask, static_cast<unsigned>(best >> 32));
+      const unsigned lo = __reduce_max_sync(
+          mask, static_cast<unsigned>(best >> 32) == hi ? static_cast<unsigned>(best) : 0u);
+      if (lane == __ffs(mask) - 1)
+        atomicMax(a.speed_max + case_id, (static_cast<unsigned long long>(hi) << 32) | lo);
+    } else {
+      // Lanes of one warp from different cases (the rough pass of a batch).
+      atomicMax(a.speed_max + case_id, best);
+    }
+  }
+
+  if (a.sense) {
+    double total = 0.0, high = 0.0;
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      total += rho[m] * rho[m];
+      if (m >= a.highest_degree_begin)
+        high += rho[m] * rho[m];
+    }
+    const bool troubled = !(total == 0.0 || high / total <= a.threshold);
+    a.flags[e] = troubled ? 1 : 0;
+    const unsigned active_mask = __activemask();
+    const unsigned ballot = __ballot_sync(active_mask, troubled);
+    if (ballot) {
+      const int lane = threadIdx.x & 31;
+      const int leader = __ffs(ballot) - 1;
+      int base = 0;
+      if (lane == leader)
+        base = atomicAdd(a.troubled_count, __popc(ballot));
+      base = __shfl_sync(active_mask, base, leader);
+      if (troubled)
+        a.troubled[base + __popc(ballot & ((1u << lane) - 1u))] = static_cast<std::int32_t>(e);
+    }
+  }
+}
+
 // The fused mixed stage on a tile of TILE consecutive elements per CTA.
 // The tile's state is staged in shared memory (FP64 means, FP32 high modes)
 // with asynchronous copies; each thread then computes its element's volume
@@ -935,85 +1029,449 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_mixed(const StageAr
     }
   }
 
-  const double inv = geo[4 * ne + e];
-  const double dt = a.case_dt ? a.case_dt[case_id] : (a.dt ? *a.dt : a.dt_value);
-  double rho[M], avg[4];
+  tile_finish<P, TILE>(a, e, t, case_id, sstate, r0, racc);
+}
+
+// Dynamic shared memory of the shared-face tile kernel, in this order:
+//   state  double [4 M][TILE]    the tile's FP64 state rows (as the tile kernel)
+//   prim   double [4][TILE]      u, v, p, E + p of each element's cell average
+//   flux   float  [4 QF][3 TILE] face records: the FP32 HLLC perturbation at
+//                                each edge point (column = record)
+//   items  uint16 [3 TILE]       faces to evaluate, element * 4 + slot
+//   rec    int16  [3][TILE]      each slot's record; <= -2: -(2 + k' TILE + j),
+//                                the record of slot k' of tile element j;
+//                                -1: none (a rough element's unneeded face)
+template <int P, int TILE> struct SharedFaceSmem {
+  static constexpr int M = TriShape<P>::M, QF = TriShape<P>::QF;
+  static constexpr std::size_t state = 0;
+  static constexpr std::size_t prim = state + sizeof(double) * 4 * M * TILE;
+  static constexpr std::size_t flux = prim + sizeof(double) * 4 * TILE;
+  static constexpr std::size_t items = flux + sizeof(float) * 4 * QF * 3 * TILE;
+  static constexpr std::size_t rec = items + sizeof(std::uint16_t) * 3 * TILE;
+  static constexpr std::size_t bytes = rec + sizeof(std::int16_t) * 3 * TILE;
+};
+
+// The fused mixed stage with the faces inside a tile evaluated once.
+//
+// The arithmetic is that of euler_tri_tile_mixed<..., ROUGH = false> and the
+// output is the same, bit for bit; what changes is who evaluates a face.  In
+// that kernel every element evaluates its three faces, so a face between two
+// elements evaluates its HLLC flux twice.  Here a face whose two elements are
+// both in the tile (and not joined across the period) is evaluated once, for
+// its left element; every other face is evaluated for the tile's element on
+// it (a face between two tiles is still evaluated by both, identically).
+// The faces to evaluate are collected in a list that all threads of the CTA
+// share out evenly, each writing an FP32 record per face (the HLLC
+// perturbation at the edge points) in shared memory; then each thread lifts
+// its element's three records onto its modes, in slot order, and sums the
+// records' weighted values (in the tile kernel's order) for mode 0, adding
+// the FP64 mean terms itself.  The left mean state of a face is taken from
+// shared memory when its element is in the tile.
+// With a rough list (a.rough), the elements with a face across a jump of the
+// cell means are appended to it and left to the second pass, as in the tile
+// kernel; their faces are evaluated only where an element that stays needs
+// them.
+template <int P, int R, int TILE, int MINB>
+__global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_shared(const StageArgs a) {
+  using S = TriShape<P>;
+  using L = SharedFaceSmem<P, TILE>;
+  constexpr int M = S::M, QV = MixedVolume<P, R>::QV, QF = S::QF, H = M - 1;
+  constexpr double phi0 = 0.70710678118654752440;
+  static_assert(3 * TILE < 16384, "record indices are 16-bit");
+  __shared__ FaceTable<P, float> table;
+  __shared__ int item_count;
+  extern __shared__ __align__(16) unsigned char smem[];
+  double(*sstate)[TILE] = reinterpret_cast<double(*)[TILE]>(smem + L::state);
+  double(*prim)[TILE] = reinterpret_cast<double(*)[TILE]>(smem + L::prim);
+  float(*rflux)[3 * TILE] = reinterpret_cast<float(*)[3 * TILE]>(smem + L::flux);
+  std::uint16_t *items = reinterpret_cast<std::uint16_t *>(smem + L::items);
+  std::int16_t(*rec)[TILE] = reinterpret_cast<std::int16_t(*)[TILE]>(smem + L::rec);
+
+  const int t = threadIdx.x;
+  const std::int64_t ne = a.mesh.ne;
+  std::int64_t first = 0, count = 0;
+  int case_id = 0;
+  if (a.work) {
+    const TileWork w = a.work[blockIdx.x];
+    first = w.first;
+    count = w.count;
+    case_id = w.case_id;
+  } else {
+    first = static_cast<std::int64_t>(blockIdx.x) * TILE;
+    count = a.mesh.ne - first < TILE ? a.mesh.ne - first : TILE;
+  }
+  const bool active = t < count;
+  const std::int64_t e = first + t;
+  const double *__restrict__ in = a.in;
+  const double gamma = a.gamma;
+
+  // Stage the tile's state and the face tables (as the tile kernel).
+  if (active) {
+    const unsigned base = static_cast<unsigned>(__cvta_generic_to_shared(&sstate[0][t]));
+#pragma unroll
+    for (int r = 0; r < 4 * M; ++r)
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(base + r * TILE * 8),
+                   "l"(in + r * ne + e)
+                   : "memory");
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  {
+    const float *src = static_cast<const float *>(a.face_table);
+    float *dst = reinterpret_cast<float *>(&table);
+    for (int i = t; i < static_cast<int>(sizeof(table) / sizeof(float)); i += TILE)
+      dst[i] = src[i];
+  }
+  if (t == 0)
+    item_count = 0;
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncthreads();
+
+  // Each element: its mean's primitive values, the rough test, and its
+  // slots' records (an item to evaluate, or the left element's record).
+  bool rough = false;
+  if (active) {
+    double mean[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+      mean[v] = sstate[v * M][t] * phi0;
+    const MeanState own = mean_state(gamma, mean);
+    prim[0][t] = own.u;
+    prim[1][t] = own.v;
+    prim[2][t] = own.p;
+    prim[3][t] = own.h;
+    if (a.rough) {
+#pragma unroll 1
+      for (int k = 0; k < 3; ++k) {
+        const std::int32_t nb = a.tile.nbr[k * ne + e];
+        if (nb < 0)
+          continue;
+        const std::int64_t local = nb - first;
+        double n0, n3;
+        if (local >= 0 && local < count) {
+          n0 = sstate[0][local] * phi0;
+          n3 = sstate[3 * M][local] * phi0;
+        } else {
+          n0 = __ldg(in + nb) * phi0;
+          n3 = __ldg(in + static_cast<std::int64_t>(3) * M * ne + nb) * phi0;
+        }
+        rough = rough || mean_jump(n0, mean[0], n3, mean[3]);
+      }
+    }
+#pragma unroll 1
+    for (int k = 0; k < 3; ++k) {
+      const std::int64_t slot = k * ne + e;
+      const unsigned code = a.tile.code[slot];
+      const std::int32_t nb = a.tile.nbr[slot];
+      const std::int64_t local = nb - first;
+      const bool shared = nb >= 0 && local >= 0 && local < count && !(code & 0xC0u);
+      int r = -1;
+      if (shared && !(code & 1u)) {
+        // The left element's slot for this face.
+        for (int k2 = 0; k2 < 3; ++k2) {
+          const std::int64_t s2 = k2 * ne + nb;
+          const unsigned c2 = a.tile.code[s2];
+          if (a.tile.nbr[s2] == e && (c2 & 1u) && !(c2 & 0xC0u))
+            r = -(2 + k2 * TILE + static_cast<int>(local));
+        }
+      }
+      if (r == -1 && (shared || !rough)) {
+        // A jump face is evaluated by neither element (both are rough); a
+        // rough element's other faces only when the element across stays.
+        bool jump_face = false;
+        if (rough && nb >= 0) {
+          double n0, n3;
+          if (local >= 0 && local < count) {
+            n0 = sstate[0][local] * phi0;
+            n3 = sstate[3 * M][local] * phi0;
+          } else {
+            n0 = __ldg(in + nb) * phi0;
+            n3 = __ldg(in + static_cast<std::int64_t>(3) * M * ne + nb) * phi0;
+          }
+          jump_face = mean_jump(n0, mean[0], n3, mean[3]);
+        }
+        if (!jump_face) {
+          r = atomicAdd(&item_count, 1);
+          items[r] = static_cast<std::uint16_t>(t * 4 + k);
+        }
+      }
+      rec[k][t] = static_cast<std::int16_t>(r);
+    }
+  }
+  __syncthreads();
+
+  // Evaluate the listed faces, shared out over all threads: whole faces in
+  // full rounds of TILE, then the remaining faces split into one unit per
+  // edge point, so no thread is left with a whole extra face while the
+  // others wait at the barrier.
+  {
+    const float gamma32 = static_cast<float>(gamma), g1 = static_cast<float>(gamma - 1.0);
+    const int n = item_count;
+    // Points [q0, q0 + NQ) of face item i (NQ = QF or 1).
+    auto evaluate = [&](int i, int q0, auto whole) {
+      constexpr int NQ = decltype(whole)::value ? QF : 1;
+      const int te = items[i] >> 2, k = items[i] & 3;
+      const std::int64_t ee = first + te, slot = k * ne + ee;
+      const unsigned code = a.tile.code[slot];
+      const std::int32_t nb = a.tile.nbr[slot];
+      const bool self_left = code & 1u;
+      const int le = (code >> 1) & 3u, re = (code >> 3) & 3u, flip = (code >> 5) & 1u;
+      const double nx = a.mesh.slot_geo[(3 * k) * ne + ee];
+      const double ny = a.mesh.slot_geo[(3 * k + 1) * ne + ee];
+      const float *lb = &table.lb[le][0][0];
+      const float *rb = &table.rb[(le * 3 + re) * 2 + flip][0][0];
+      const float *own_basis = self_left ? lb : rb;
+      const float *other_basis = self_left ? rb : lb;
+      if (code & 0xC0u) {
+        const float *periodic =
+            a.boundary.basis32 + static_cast<std::int64_t>(a.tile.aux[slot]) * QF * M;
+        if (code & 0x40u)
+          own_basis = periodic;
+        else
+          other_basis = periodic;
+      }
+      double mean[4];
+      float ch[4][H];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        mean[v] = sstate[v * M][te] * phi0;
+#pragma unroll
+        for (int m = 0; m < H; ++m)
+          ch[v][m] = static_cast<float>(sstate[v * M + m + 1][te]);
+      }
+      double nmean[4] = {0.0, 0.0, 0.0, 0.0};
+      float nh[4][H];
+      const bool boundary = nb < 0;
+      const std::int64_t local = nb - first;
+      const bool near = !boundary && local >= 0 && local < count;
+      if (near) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          nmean[v] = sstate[v * M][local] * phi0;
+#pragma unroll
+          for (int m = 0; m < H; ++m)
+            nh[v][m] = static_cast<float>(sstate[v * M + m + 1][local]);
+        }
+      } else if (!boundary) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          const double *row = in + static_cast<std::int64_t>(v) * M * ne + nb;
+          nmean[v] = __ldg(row) * phi0;
+#pragma unroll
+          for (int m = 0; m < H; ++m)
+            nh[v][m] = static_cast<float>(__ldg(row + (m + 1) * ne));
+        }
+      }
+      // The face's left mean state: the reference of the perturbation form.
+      MeanState ml;
+      const bool own_left = self_left || boundary;
+      const int li = own_left ? te : static_cast<int>(local);
+      if (own_left || near) {
+        ml.rho = own_left ? mean[0] : nmean[0];
+        ml.mx = own_left ? mean[1] : nmean[1];
+        ml.my = own_left ? mean[2] : nmean[2];
+        ml.e = own_left ? mean[3] : nmean[3];
+        ml.u = prim[0][li];
+        ml.v = prim[1][li];
+        ml.p = prim[2][li];
+        ml.h = prim[3][li];
+      } else {
+        ml = mean_state(gamma, nmean);
+      }
+      const Ref32 ref = ref32(ml);
+      float jump[4];
+#pragma unroll
+      for (int v = 0; v < 4; ++v)
+        jump[v] = boundary ? 0.0f
+                           : static_cast<float>(self_left ? nmean[v] - mean[v] : mean[v] - nmean[v]);
+      const float nxf = static_cast<float>(nx), nyf = static_cast<float>(ny);
+#pragma unroll
+      for (int j = 0; j < NQ; ++j) {
+        const int q = q0 + j;
+        float to[4], tn[4], dl[4], dr[4], fl[4];
+        high_trace<P>(ch, own_basis + q * M, to);
+        if (boundary) {
+#pragma unroll
+          for (int v = 0; v < 4; ++v)
+            dl[v] = dr[v] = to[v];
+        } else {
+          high_trace<P>(nh, other_basis + q * M, tn);
+#pragma unroll
+          for (int v = 0; v < 4; ++v) {
+            dl[v] = self_left ? to[v] : tn[v];
+            dr[v] = jump[v] + (self_left ? tn[v] : to[v]);
+          }
+        }
+        hllc_perturbed(ref, dl, dr, g1, gamma32, nxf, nyf, fl);
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+          rflux[q * 4 + v][i] = fl[v];
+      }
+    };
+    const int whole = n / TILE * TILE;
+#pragma unroll 1
+    for (int i = t; i < whole; i += TILE)
+      evaluate(i, 0, std::true_type{});
+#pragma unroll 1
+    for (int u = t; u < (n - whole) * QF; u += TILE)
+      evaluate(whole + u / QF, u % QF, std::false_type{});
+  }
+  __syncthreads();
+  if (!active)
+    return;
+  if (rough) {
+    a.rough[atomicAdd(a.rough_count, 1)] = static_cast<std::int32_t>(e);
+    return;
+  }
+
+  double mean[4];
+  float ch[4][H];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    mean[v] = sstate[v * M][t] * phi0;
+#pragma unroll
+    for (int m = 0; m < H; ++m)
+      ch[v][m] = static_cast<float>(sstate[v * M + m + 1][t]);
+  }
+  MeanState own;
+  own.rho = mean[0];
+  own.mx = mean[1];
+  own.my = mean[2];
+  own.e = mean[3];
+  own.u = prim[0][t];
+  own.v = prim[1][t];
+  own.p = prim[2][t];
+  own.h = prim[3][t];
+
+  const MixedVolume<P, R> &T = c_mix<P, R>;
+  const float g1 = static_cast<float>(gamma - 1.0);
+  const double *__restrict__ geo = a.mesh.geo;
+  const Ref32 bb = ref32(own);
+
+  // Volume term of the high modes (as the tile kernel, fully unrolled).
+  float racc[4][H];
 #pragma unroll
   for (int v = 0; v < 4; ++v)
 #pragma unroll
-    for (int m = 0; m < M; ++m) {
-      const std::int64_t idx = (static_cast<std::int64_t>(v) * M + m) * ne + e;
-      const double cur = sstate[v * M + m][t];
-      const double rr = (m == 0 ? r0[v] : static_cast<double>(racc[v][m > 0 ? m - 1 : 0])) * inv;
-      double o;
-      if (a.stage == 0)
-        o = cur + dt * rr;
-      else if (a.stage == 1)
-        o = 0.75 * a.u0[idx] + 0.25 * (cur + dt * rr);
-      else
-        o = (1.0 / 3.0) * a.u0[idx] + (2.0 / 3.0) * (cur + dt * rr);
-      a.out[idx] = o;
-      if (v == 0)
-        rho[m] = o;
-      if (m == 0)
-        avg[v] = o;
-    }
-
-  if (a.speed_max) {
-    // The next step's CFL speed from this stage's cell averages.
-    const double scale = 1.0 / sqrt(2.0);
-    const double sa[4] = {__dmul_rn(scale, avg[0]), __dmul_rn(scale, avg[1]),
-                          __dmul_rn(scale, avg[2]), __dmul_rn(scale, avg[3])};
-    bool physical = true;
-    const double speed = cfl_speed(gamma, sa, 2, physical);
-    unsigned long long best = 0;
-    if (physical)
-      best = __double_as_longlong(speed);
-    else
-      raise_error(a.error, kNonPhysicalAverage, e);
-    // Warp max over whichever lanes are still active (past the tile's end,
-    // or handed to the rough pass, lanes have returned): the 64-bit max of
-    // positive FP64 bits as the max of the high words, then of the low words
-    // among the lanes holding it; one atomic per warp and case.
-    const unsigned mask = __activemask();
-    const int lane = threadIdx.x & 31;
-    // (No lane's match set is the whole mask unless all lanes share the case,
-    // so the branch is uniform across the warp.)
-    if (__match_any_sync(mask, case_id) == mask) {
-      const unsigned hi = __reduce_max_sync(mask, static_cast<unsigned>(best >> 32));
-      const unsigned lo = __reduce_max_sync(
-          mask, static_cast<unsigned>(best >> 32) == hi ? static_cast<unsigned>(best) : 0u);
-      if (lane == __ffs(mask) - 1)
-        atomicMax(a.speed_max + case_id, (static_cast<unsigned long long>(hi) << 32) | lo);
-    } else {
-      // Lanes of one warp from different cases (the rough pass of a batch).
-      atomicMax(a.speed_max + case_id, best);
-    }
-  }
-
-  if (a.sense) {
-    double total = 0.0, high = 0.0;
+    for (int m = 0; m < H; ++m)
+      racc[v][m] = 0.0f;
+  {
+    const float fax = static_cast<float>(geo[e]), fay = static_cast<float>(geo[ne + e]);
+    const float fbx = static_cast<float>(geo[2 * ne + e]), fby = static_cast<float>(geo[3 * ne + e]);
 #pragma unroll
-    for (int m = 0; m < M; ++m) {
-      total += rho[m] * rho[m];
-      if (m >= a.highest_degree_begin)
-        high += rho[m] * rho[m];
-    }
-    const bool troubled = !(total == 0.0 || high / total <= a.threshold);
-    a.flags[e] = troubled ? 1 : 0;
-    const unsigned active_mask = __activemask();
-    const unsigned ballot = __ballot_sync(active_mask, troubled);
-    if (ballot) {
-      const int lane = threadIdx.x & 31;
-      const int leader = __ffs(ballot) - 1;
-      int base = 0;
-      if (lane == leader)
-        base = atomicAdd(a.troubled_count, __popc(ballot));
-      base = __shfl_sync(active_mask, base, leader);
-      if (troubled)
-        a.troubled[base + __popc(ballot & ((1u << lane) - 1u))] = static_cast<std::int32_t>(e);
+    for (int q = 0; q < QV; ++q) {
+      float d[4];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        float s = 0.0f;
+#pragma unroll
+        for (int m = 0; m < H; ++m)
+          s = fmaf(ch[v][m], T.phi[q][m], s);
+        d[v] = s;
+      }
+      const float inv = __frcp_rn(fmaxf(bb.rho + d[0], kVacuumFraction * bb.rho));
+      const float du = (d[1] - bb.u * d[0]) * inv;
+      const float dv = (d[2] - bb.v * d[0]) * inv;
+      const float uu = bb.u + du, vv = bb.v + dv;
+      const float dmu = bb.mx * du + d[1] * uu + bb.my * dv + d[2] * vv;
+      const float dp = g1 * (d[3] - 0.5f * dmu);
+      const float dep = d[3] + dp;
+      const float fx[4] = {d[1], bb.mx * du + d[1] * uu + dp, bb.my * du + d[2] * uu,
+                           bb.h * du + dep * uu};
+      const float fy[4] = {d[2], bb.mx * dv + d[1] * vv, bb.my * dv + d[2] * vv + dp,
+                           bb.h * dv + dep * vv};
+      const float w = T.w[q];
+      const float wby = w * fby, wbx = w * fbx, wax = w * fax, way = w * fay;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const float gxi = wby * fx[v] - wbx * fy[v];
+        const float geta = wax * fy[v] - way * fx[v];
+#pragma unroll
+        for (int m = 0; m < H; ++m)
+          racc[v][m] = fmaf(T.dxi[q][m], gxi, fmaf(T.deta[q][m], geta, racc[v][m]));
+      }
     }
   }
+
+  // Lift the three faces' records, in the element's slot order.
+  double r0[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 1
+  for (int k = 0; k < 3; ++k) {
+    const std::int64_t slot = k * ne + e;
+    const unsigned code = a.tile.code[slot];
+    const std::int32_t nb = a.tile.nbr[slot];
+    const bool self_left = code & 1u;
+    const int le = (code >> 1) & 3u, re = (code >> 3) & 3u, flip = (code >> 5) & 1u;
+    const double nx = a.mesh.slot_geo[(3 * k) * ne + e];
+    const double ny = a.mesh.slot_geo[(3 * k + 1) * ne + e];
+    const double scale = a.mesh.slot_geo[(3 * k + 2) * ne + e];
+    const float *lb = &table.lb[le][0][0];
+    const float *rb = &table.rb[(le * 3 + re) * 2 + flip][0][0];
+    const float *own_basis = self_left ? lb : rb;
+    if (code & 0x40u)
+      own_basis = a.boundary.basis32 + static_cast<std::int64_t>(a.tile.aux[slot]) * QF * M;
+    int r = rec[k][t];
+    if (r < 0) {
+      const int j = -r - 2;
+      r = rec[j / TILE][j % TILE];
+    }
+    const bool boundary = nb < 0;
+    MeanState ml;
+    if (self_left) {
+      ml = own;
+    } else {
+      const std::int64_t local = nb - first;
+      if (local >= 0 && local < count) {
+        ml.rho = sstate[0][local] * phi0;
+        ml.mx = sstate[M][local] * phi0;
+        ml.my = sstate[2 * M][local] * phi0;
+        ml.e = sstate[3 * M][local] * phi0;
+        ml.u = prim[0][local];
+        ml.v = prim[1][local];
+        ml.p = prim[2][local];
+        ml.h = prim[3][local];
+      } else {
+        double nmean[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+          nmean[v] = __ldg(in + static_cast<std::int64_t>(v) * M * ne + nb) * phi0;
+        ml = mean_state(gamma, nmean);
+      }
+    }
+    double fln[4];
+    mean_normal_flux(ml, nx, ny, fln);
+    float shift[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    if (!boundary && !self_left) {
+      double frn[4];
+      mean_normal_flux(own, nx, ny, frn);
+#pragma unroll
+      for (int v = 0; v < 4; ++v)
+        shift[v] = static_cast<float>(fln[v] - frn[v]);
+    }
+    const float fscale = static_cast<float>(scale);
+    const double sgn = self_left ? -1.0 : 1.0;
+    float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int q = 0; q < QF; ++q) {
+      const float w = table.ew[le][q];
+      const float wsc = (self_left ? -w : w) * fscale;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const float fl = rflux[q * 4 + v][r];
+        acc[v] = fmaf(w, fl, acc[v]);
+        const float value = wsc * (self_left ? fl : fl + shift[v]);
+#pragma unroll
+        for (int m = 0; m < H; ++m)
+          racc[v][m] = fmaf(value, own_basis[q * M + m + 1], racc[v][m]);
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const double mode0 = fln[v] * c_edge_wsum<P>[le] + static_cast<double>(acc[v]);
+      r0[v] += sgn * scale * phi0 * mode0;
+    }
+  }
+
+  tile_finish<P, TILE>(a, e, t, case_id, sstate, r0, racc);
 }
 
 // Per-case CFL speed over a tile work list: the largest cell-average wave
@@ -1099,21 +1557,33 @@ template <int P, int TILE> constexpr std::size_t tile_smem() {
 }
 
 // Static (face table) plus dynamic shared memory above the default 48 KiB
-// needs the opt-in attribute, set once per device (and before any capture).
-template <int P, int R, int TILE, int MINB> void tile_opt_in() {
-  if (tile_smem<P, TILE>() + sizeof(FaceTable<P, float>) <= 48 * 1024)
+// needs the opt-in attribute, set once per device and kernel (and before any
+// capture).
+template <typename Kernel>
+void smem_opt_in(Kernel kernel, std::size_t dynamic, std::size_t fixed, bool (&opted_in)[64]) {
+  if (dynamic + fixed <= 48 * 1024)
     return;
-  static bool opted_in[64] = {};
   int device = 0;
   check(cudaGetDevice(&device), "cudaGetDevice");
   if (device < 64 && opted_in[device])
     return;
-  check(cudaFuncSetAttribute(euler_tri_tile_mixed<P, R, TILE, MINB, false>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(tile_smem<P, TILE>())),
+  check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(dynamic)),
         "tile kernel shared memory");
   if (device < 64)
     opted_in[device] = true;
+}
+
+template <int P, int R, int TILE, int MINB> void tile_opt_in() {
+  static bool opted_in[64] = {};
+  smem_opt_in(euler_tri_tile_mixed<P, R, TILE, MINB, false>, tile_smem<P, TILE>(),
+              sizeof(FaceTable<P, float>), opted_in);
+}
+
+template <int P, int R, int TILE, int MINB> void shared_opt_in() {
+  static bool opted_in[64] = {};
+  smem_opt_in(euler_tri_tile_shared<P, R, TILE, MINB>, SharedFaceSmem<P, TILE>::bytes,
+              sizeof(FaceTable<P, float>) + sizeof(int), opted_in);
 }
 
 // The second pass: one warp per CTA and no register cap, so a short rough
@@ -1122,27 +1592,44 @@ constexpr int kRoughTile = 32;
 
 // The FP32 pass over all tiles, then (with a rough list) the pass over the
 // elements it left, sized for the worst case: its CTAs beyond the list's
-// length return at once.
-template <int P, int R, int TILE, int MINB> void stage_tile(const StageArgs &a, cudaStream_t s) {
-  tile_opt_in<P, R, TILE, MINB>();
+// length return at once.  SHARED picks the shared-face tile kernel for the
+// FP32 pass.
+template <int P, int R, int TILE, int MINB, bool SHARED = false>
+void stage_tile(const StageArgs &a, cudaStream_t s) {
+  if constexpr (SHARED)
+    shared_opt_in<P, R, TILE, MINB>();
+  else
+    tile_opt_in<P, R, TILE, MINB>();
   const std::int64_t blocks = a.work ? a.work_count : (a.mesh.ne + TILE - 1) / TILE;
   if (blocks <= 0)
     return;
   if (a.rough)
     check(cudaMemsetAsync(a.rough_count, 0, sizeof(std::int32_t), s), "rough count");
-  euler_tri_tile_mixed<P, R, TILE, MINB, false>
-      <<<static_cast<unsigned>(blocks), TILE, tile_smem<P, TILE>(), s>>>(a);
+  if constexpr (SHARED)
+    euler_tri_tile_shared<P, R, TILE, MINB>
+        <<<static_cast<unsigned>(blocks), TILE, SharedFaceSmem<P, TILE>::bytes, s>>>(a);
+  else
+    euler_tri_tile_mixed<P, R, TILE, MINB, false>
+        <<<static_cast<unsigned>(blocks), TILE, tile_smem<P, TILE>(), s>>>(a);
   if (a.rough)
     euler_tri_tile_mixed<P, R, kRoughTile, 1, true>
         <<<static_cast<unsigned>((a.mesh.ne + kRoughTile - 1) / kRoughTile), kRoughTile,
            tile_smem<P, kRoughTile>(), s>>>(a);
 }
 
-// Launch shapes of the tile kernel (elements per CTA, register budget):
+// Launch shapes of the tile kernels (elements per CTA, register budget):
 //   0: 128 elements, <= 128 registers (4 CTAs / 16 warps per SM)
 //   1: 128 elements, no register cap
 //   2: 256 elements, <= 128 registers (2 CTAs per SM)
 //   3:  64 elements, <= 128 registers (8 CTAs per SM)
+// and of the shared-face tile kernel:
+//   4:  64 elements, sized for 7 CTAs per SM (14 warps)
+//   5:  96 elements, sized for 5 CTAs per SM (15 warps)
+//   6: 128 elements, sized for 4 CTAs per SM (16 warps)
+//   7: 128 elements, sized for 3 CTAs per SM
+constexpr int kTileShapes = kTileShapeCount;
+constexpr int kTileElements[kTileShapes] = {128, 128, 256, 64, 64, 96, 128, 128};
+
 template <int P, int R> struct StageTile {
   static void run(int shape, const StageArgs &a, cudaStream_t s) {
     switch (shape) {
@@ -1150,6 +1637,10 @@ template <int P, int R> struct StageTile {
     case 1: stage_tile<P, R, 128, 1>(a, s); break;
     case 2: stage_tile<P, R, 256, 2>(a, s); break;
     case 3: stage_tile<P, R, 64, 8>(a, s); break;
+    case 4: stage_tile<P, R, 64, 7, true>(a, s); break;
+    case 5: stage_tile<P, R, 96, 5, true>(a, s); break;
+    case 6: stage_tile<P, R, 128, 4, true>(a, s); break;
+    case 7: stage_tile<P, R, 128, 3, true>(a, s); break;
     default: throw std::invalid_argument("tile kernel: unknown launch shape");
     }
   }
@@ -1161,6 +1652,10 @@ template <int P, int R> struct PrepareTile {
     tile_opt_in<P, R, 128, 1>();
     tile_opt_in<P, R, 256, 2>();
     tile_opt_in<P, R, 64, 8>();
+    shared_opt_in<P, R, 64, 7>();
+    shared_opt_in<P, R, 96, 5>();
+    shared_opt_in<P, R, 128, 4>();
+    shared_opt_in<P, R, 128, 3>();
   }
 };
 
@@ -1212,11 +1707,10 @@ void upload_euler_tri_tables_mixed(int p, int rule) {
   dispatch_mixed<UploadMixed>(p, rule);
 }
 
-int euler_tri_tile_shapes() { return 4; }
+int euler_tri_tile_shapes() { return kTileShapes; }
 
 int euler_tri_tile_elements(int shape) {
-  static const int elements[4] = {128, 128, 256, 64};
-  return shape >= 0 && shape < 4 ? elements[shape] : 0;
+  return shape >= 0 && shape < kTileShapes ? kTileElements[shape] : 0;
 }
 
 void prepare_euler_tri_stage_tile(int p, int rule) { dispatch_mixed<PrepareTile>(p, rule); }

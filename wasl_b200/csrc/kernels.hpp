@@ -264,6 +264,9 @@ void launch_euler_tri_stage_mixed(int p, int rule, const StageArgs &a, cudaStrea
 void launch_batch_speed(const double *state, std::int64_t ne, int M, double gamma,
                         const TileWork *work, std::int64_t work_count, unsigned long long *speed,
                         unsigned long long *error, int *status, cudaStream_t stream);
+// Number of launch shapes of the tile kernels (euler_tri_tile_shapes()
+// returns it; per-shape host arrays are sized by it).
+constexpr int kTileShapeCount = 8;
 int euler_tri_tile_shapes();
 int euler_tri_tile_elements(int shape);
 void launch_euler_tri_stage_tile(int p, int rule, int shape, const StageArgs &a,
