@@ -11,6 +11,9 @@ from wasl_b200 import cases, meshgen
 
 pytestmark = pytest.mark.gpu
 
+# Launch shapes of the tile kernels (see wasl_gpu_tuning).
+TILE_SHAPES = 8
+
 
 def small_cases(seed, count=5):
     out = []
@@ -97,7 +100,7 @@ def test_batch_autotunes_each_order_and_conserves():
         b.advance(0.15, 10)
         for p in set(s[3] for s in specs):
             choice, ms = b.tuning(p)
-            assert len(ms) == 4 and ms[choice] == min(ms)
+            assert len(ms) == TILE_SHAPES and ms[choice] == min(ms)
         for c, s in enumerate(specs):
             ne, nm = b.case_size(c)
             state = b.get_state(c).reshape(4, nm, ne)
