@@ -197,7 +197,10 @@ def time_device_steps(g, args, torch, flush, stream):
     g.sync()  # device errors of the timed steps
     stage_ms, stage_kernels, launches = g.profile_end()
     total_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
-    return total_ms, stage_ms, stage_kernels, launches
+    # Mean stage-kernel ms of RK stages 0, 1, 2 (stage 0 reads u^n after the
+    # L2 flush; stages 1 and 2 also read u^n for the Shu-Osher combination).
+    by_stage = [round(ms / args.steps, 5) for ms in g.profile_stages()]
+    return total_ms, stage_ms, stage_kernels, launches, by_stage
 
 
 def time_e2e(g, args, torch, stream):
@@ -297,7 +300,8 @@ def ours(args, rank, world, local_rank):
         dist.barrier()
     torch.cuda.synchronize()
     sampler.start()
-    total_ms, stage_ms, stage_kernels, launches = time_device_steps(g, args, torch, flush, stream)
+    total_ms, stage_ms, stage_kernels, launches, by_stage = time_device_steps(g, args, torch, flush,
+                                                                              stream)
     clocks = sampler.stop()
     total_ms = reduce_over_ranks(dist, total_ms, "max")
     dofs = g.state_size
@@ -336,6 +340,7 @@ def ours(args, rank, world, local_rank):
                      "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                      "peak_source": f"{peak_kind} hbm_gbs",
                      "kernel": "euler_tri_stage", "kernel_ms": kernel_s * 1e3,
+                     "kernel_ms_by_rk_stage": by_stage,
                      "bytes_per_launch": per_launch_bytes},
         "gpu_launches": launches,
         "clocks": clocks,
@@ -344,7 +349,7 @@ def ours(args, rank, world, local_rank):
         line["accuracy"] = accuracy(args, form, local_rank)
     if rank == 0 and form != "plain":
         gp, _ = build_solver(args, "plain", local_rank)
-        p_ms, _, _, _ = time_device_steps(gp, args, torch, flush, stream_of(gp, torch))
+        p_ms, _, _, _, _ = time_device_steps(gp, args, torch, flush, stream_of(gp, torch))
         line["plain_fp64"] = {"value": 3.0 * gp.state_size * args.steps / (p_ms * 1e-3),
                               "ms_per_step": p_ms / args.steps}
         line["chosen_vs_plain"] = value / world / line["plain_fp64"]["value"]
@@ -365,7 +370,8 @@ def kernel_description(tuning):
              "tile 128 el/CTA, uncapped regs", "tile 256 el/CTA, <=128 regs",
              "tile 64 el/CTA, <=128 regs", "shared-face tile 64 el/CTA, 7 CTAs/SM",
              "shared-face tile 96 el/CTA, 5 CTAs/SM", "shared-face tile 128 el/CTA, 4 CTAs/SM",
-             "shared-face tile 128 el/CTA, 3 CTAs/SM"]
+             "shared-face tile 128 el/CTA, 3 CTAs/SM",
+             "shared-face tile 128 el/CTA, 3 CTAs/SM, u^n staged"]
     if choice < 0:
         return {"name": "single stage kernel"}
     out = {"name": names[choice] if choice < len(names) else str(choice)}

@@ -139,6 +139,7 @@ SIGNATURES = {
     "wasl_mlp_set_weights": (C.c_int, [C.c_void_p, _f, C.c_int64]),
     "wasl_gpu_profile_begin": (C.c_int, [C.c_void_p]),
     "wasl_gpu_profile_end": (C.c_int, [C.c_void_p, _d, _i64, _i64]),
+    "wasl_gpu_profile_stages": (C.c_int, [C.c_void_p, _d]),
     "wasl_gpu_write_checkpoint": (C.c_int, [C.c_void_p, C.c_char_p, C.c_double, C.c_uint64,
                                             C.c_char_p]),
     "wasl_gpu_read_checkpoint": (C.c_int, [C.c_void_p, C.c_char_p, _d,
@@ -398,6 +399,12 @@ class Solver:
         ms, k, n = C.c_double(), C.c_int64(), C.c_int64()
         self._check(self._lib.wasl_gpu_profile_end(self._h, C.byref(ms), C.byref(k), C.byref(n)))
         return ms.value, k.value, n.value
+
+    def profile_stages(self):
+        """The last profile_end's stage-kernel ms split by RK stage (0, 1, 2)."""
+        out = np.zeros(3)
+        self._check(self._lib.wasl_gpu_profile_stages(self._h, _ptr(out)))
+        return out.tolist()
 
     # ---- restart files ----------------------------------------------------------
     def write_checkpoint(self, path, time, step, prepared_mesh=""):

@@ -355,6 +355,14 @@ int wasl_gpu_profile_begin(wasl_gpu *h) {
   return guarded(h, [&] { h->solver->profile_begin(); });
 }
 
+int wasl_gpu_profile_stages(const wasl_gpu *h, double *stage_ms) {
+  return guarded(const_cast<wasl_gpu *>(h), [&] {
+    need(stage_ms != nullptr, "profile stages: null output");
+    for (int k = 0; k < 3; ++k)
+      stage_ms[k] = h->solver->profile_stage_ms()[k];
+  });
+}
+
 int wasl_gpu_profile_end(wasl_gpu *h, double *stage_ms, int64_t *stage_kernels,
                          int64_t *launches) {
   return guarded(h, [&] {

@@ -30,10 +30,12 @@ void Solver::stage_end() {
 void Solver::profile_end(double &stage_ms, std::int64_t &stage_kernels, std::int64_t &launches) {
   cuda_check(cudaStreamSynchronize(stream_), "profile");
   stage_ms = 0.0;
+  stage_split_[0] = stage_split_[1] = stage_split_[2] = 0.0;
   for (std::size_t k = 0; k + 1 < events_used_; k += 2) {
     float ms = 0.0f;
     cuda_check(cudaEventElapsedTime(&ms, events_[k], events_[k + 1]), "elapsed");
     stage_ms += ms;
+    stage_split_[(k / 2) % 3] += ms; // stage kernels come in SSP-RK3 triples
   }
   stage_kernels = static_cast<std::int64_t>(events_used_ / 2);
   launches = launches_;

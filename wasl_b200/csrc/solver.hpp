@@ -144,6 +144,8 @@ public:
   // is launched on.
   void profile_begin();
   void profile_end(double &stage_ms, std::int64_t &stage_kernels, std::int64_t &launches);
+  // The last profile_end's stage-kernel time split by RK stage (0, 1, 2).
+  const double *profile_stage_ms() const { return stage_split_; }
 
 protected:
   void count_launches(std::int64_t n) { launches_ += n; }
@@ -157,6 +159,7 @@ private:
   std::int64_t launches_ = 0;
   std::vector<cudaEvent_t> events_;
   std::size_t events_used_ = 0;
+  double stage_split_[3] = {0.0, 0.0, 0.0};
 };
 
 std::unique_ptr<Solver> make_solver(const wasl_gpu_config &config, std::int64_t node_count,
