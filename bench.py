@@ -371,7 +371,8 @@ def kernel_description(tuning):
              "tile 64 el/CTA, <=128 regs", "shared-face tile 64 el/CTA, 7 CTAs/SM",
              "shared-face tile 96 el/CTA, 5 CTAs/SM", "shared-face tile 128 el/CTA, 4 CTAs/SM",
              "shared-face tile 128 el/CTA, 3 CTAs/SM",
-             "shared-face tile 128 el/CTA, 3 CTAs/SM, u^n staged"]
+             "shared-face tile 128 el/CTA, 3 CTAs/SM, u^n staged",
+             "shared-face tile 128 el/CTA, 4 CTAs/SM, L2 prefetch"]
     if choice < 0:
         return {"name": "single stage kernel"}
     out = {"name": names[choice] if choice < len(names) else str(choice)}

@@ -12,7 +12,7 @@ from wasl_b200 import cases, meshgen
 pytestmark = pytest.mark.gpu
 
 # Launch shapes of the tile kernels (see wasl_gpu_tuning).
-TILE_SHAPES = 9
+TILE_SHAPES = 10
 
 
 def small_cases(seed, count=5):

@@ -1078,7 +1078,11 @@ template <int P, int TILE, bool U0 = false> struct SharedFaceSmem {
 // U0: in stages 1 and 2 the tile's u^n rows are copied into shared memory
 // asynchronously at the start, so the combination at the end does not wait
 // on global loads.
-template <int P, int R, int TILE, int MINB, bool U0>
+// PF: each element's geometry, slot and (stages 1 and 2) u^n rows are
+// prefetched into L2 at the start, so the later loads that depend on one
+// another (slot codes, then neighbours' slots; normals; geometry) do not
+// each wait on DRAM after an L2 flush.
+template <int P, int R, int TILE, int MINB, bool U0, bool PF = false>
 __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_shared(const StageArgs a) {
   using S = TriShape<P>;
   using L = SharedFaceSmem<P, TILE, U0>;
@@ -1113,6 +1117,25 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_shared(const StageA
   const double *__restrict__ in = a.in;
   const double gamma = a.gamma;
 
+  if constexpr (PF) {
+    if (active) {
+#pragma unroll
+      for (int r = 0; r < 5; ++r)
+        asm volatile("prefetch.global.L2 [%0];\n" ::"l"(a.mesh.geo + r * ne + e));
+#pragma unroll
+      for (int r = 0; r < 9; ++r)
+        asm volatile("prefetch.global.L2 [%0];\n" ::"l"(a.mesh.slot_geo + r * ne + e));
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        asm volatile("prefetch.global.L2 [%0];\n" ::"l"(a.tile.nbr + k * ne + e));
+        asm volatile("prefetch.global.L2 [%0];\n" ::"l"(a.tile.code + k * ne + e));
+      }
+      if (a.stage > 0)
+#pragma unroll
+        for (int r = 0; r < 4 * M; ++r)
+          asm volatile("prefetch.global.L2 [%0];\n" ::"l"(a.u0 + r * ne + e));
+    }
+  }
   // Stage the tile's state and the face tables (as the tile kernel).
   if (active) {
     const unsigned base = static_cast<unsigned>(__cvta_generic_to_shared(&sstate[0][t]));
@@ -1606,9 +1629,9 @@ template <int P, int R, int TILE, int MINB> void tile_opt_in() {
               sizeof(FaceTable<P, float>), opted_in);
 }
 
-template <int P, int R, int TILE, int MINB, bool U0> void shared_opt_in() {
+template <int P, int R, int TILE, int MINB, bool U0, bool PF = false> void shared_opt_in() {
   static bool opted_in[64] = {};
-  smem_opt_in(euler_tri_tile_shared<P, R, TILE, MINB, U0>, SharedFaceSmem<P, TILE, U0>::bytes,
+  smem_opt_in(euler_tri_tile_shared<P, R, TILE, MINB, U0, PF>, SharedFaceSmem<P, TILE, U0>::bytes,
               sizeof(FaceTable<P, float>) + sizeof(int), opted_in);
 }
 
@@ -1620,10 +1643,11 @@ constexpr int kRoughTile = 32;
 // elements it left, sized for the worst case: its CTAs beyond the list's
 // length return at once.  SHARED picks the shared-face tile kernel for the
 // FP32 pass (U0: the variant that stages u^n in shared memory).
-template <int P, int R, int TILE, int MINB, bool SHARED = false, bool U0 = false>
+template <int P, int R, int TILE, int MINB, bool SHARED = false, bool U0 = false,
+          bool PF = false>
 void stage_tile(const StageArgs &a, cudaStream_t s) {
   if constexpr (SHARED)
-    shared_opt_in<P, R, TILE, MINB, U0>();
+    shared_opt_in<P, R, TILE, MINB, U0, PF>();
   else
     tile_opt_in<P, R, TILE, MINB>();
   const std::int64_t blocks = a.work ? a.work_count : (a.mesh.ne + TILE - 1) / TILE;
@@ -1632,7 +1656,7 @@ void stage_tile(const StageArgs &a, cudaStream_t s) {
   if (a.rough)
     check(cudaMemsetAsync(a.rough_count, 0, sizeof(std::int32_t), s), "rough count");
   if constexpr (SHARED)
-    euler_tri_tile_shared<P, R, TILE, MINB, U0>
+    euler_tri_tile_shared<P, R, TILE, MINB, U0, PF>
         <<<static_cast<unsigned>(blocks), TILE, SharedFaceSmem<P, TILE, U0>::bytes, s>>>(a);
   else
     euler_tri_tile_mixed<P, R, TILE, MINB, false>
@@ -1654,8 +1678,9 @@ void stage_tile(const StageArgs &a, cudaStream_t s) {
 //   6: 128 elements, sized for 4 CTAs per SM (16 warps)
 //   7: 128 elements, sized for 3 CTAs per SM
 //   8: 128 elements, sized for 3 CTAs per SM, u^n staged in shared memory
+//   9: 128 elements, sized for 4 CTAs per SM, per-element rows prefetched to L2
 constexpr int kTileShapes = kTileShapeCount;
-constexpr int kTileElements[kTileShapes] = {128, 128, 256, 64, 64, 96, 128, 128, 128};
+constexpr int kTileElements[kTileShapes] = {128, 128, 256, 64, 64, 96, 128, 128, 128, 128};
 
 template <int P, int R> struct StageTile {
   static void run(int shape, const StageArgs &a, cudaStream_t s) {
@@ -1669,6 +1694,7 @@ template <int P, int R> struct StageTile {
     case 6: stage_tile<P, R, 128, 4, true>(a, s); break;
     case 7: stage_tile<P, R, 128, 3, true>(a, s); break;
     case 8: stage_tile<P, R, 128, 3, true, true>(a, s); break;
+    case 9: stage_tile<P, R, 128, 4, true, false, true>(a, s); break;
     default: throw std::invalid_argument("tile kernel: unknown launch shape");
     }
   }
@@ -1685,6 +1711,7 @@ template <int P, int R> struct PrepareTile {
     shared_opt_in<P, R, 128, 4, false>();
     shared_opt_in<P, R, 128, 3, false>();
     shared_opt_in<P, R, 128, 3, true>();
+    shared_opt_in<P, R, 128, 4, false, true>();
   }
 };
 
