@@ -371,7 +371,7 @@ def kernel_description(tuning):
              "tile 64 el/CTA, <=128 regs", "shared-face tile 64 el/CTA, 7 CTAs/SM",
              "shared-face tile 96 el/CTA, 5 CTAs/SM", "shared-face tile 128 el/CTA, 4 CTAs/SM",
              "shared-face tile 128 el/CTA, 3 CTAs/SM",
-             "shared-face tile 128 el/CTA, 3 CTAs/SM, u^n staged",
+             "shared-face tile 128 el/CTA, 4 CTAs/SM, L2 + u^n L1 prefetch",
              "shared-face tile 128 el/CTA, 4 CTAs/SM, L2 prefetch"]
     if choice < 0:
         return {"name": "single stage kernel"}

@@ -171,8 +171,9 @@ int wasl_gpu_sync(wasl_gpu *handle);
  * a thread; 1: 128, no register cap; 2: 256 at <= 128; 3: 64 at <= 128;
  * 4-7: the shared-face tile kernel, which evaluates a face between two
  * elements of one tile once: 4: 64 elements per CTA sized for 7 CTAs per SM;
- * 5: 96 for 5; 6: 128 for 4; 7: 128 for 3; 8: 128 for 3 with u^n staged in
- * shared memory; 9: 128 for 4 with each element's rows prefetched to L2);
+ * 5: 96 for 5; 6: 128 for 4; 7: 128 for 3; 8: 128 for 4 with each
+ * element's rows prefetched to L2 and u^n to L1; 9: 128 for 4 with the rows
+ * prefetched to L2);
  * -1 for forms with a single kernel or before the first step.  When the
  * choice was autotuned (mixed_kernel 0: every variant timed on the solver's
  * own state before its first step, the fastest kept for the process per

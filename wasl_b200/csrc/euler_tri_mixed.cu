@@ -648,8 +648,7 @@ __device__ __noinline__ void face_fp64(double gamma, const double *own, std::int
 template <int P, int TILE>
 __device__ __forceinline__ void tile_finish(const StageArgs &a, std::int64_t e, int t, int case_id,
                                             const double (*sstate)[TILE], const double (&r0)[4],
-                                            const float (&racc)[4][TriShape<P>::M - 1],
-                                            const double (*su0)[TILE] = nullptr) {
+                                            const float (&racc)[4][TriShape<P>::M - 1]) {
   constexpr int M = TriShape<P>::M;
   const std::int64_t ne = a.mesh.ne;
   const double gamma = a.gamma;
@@ -668,9 +667,9 @@ __device__ __forceinline__ void tile_finish(const StageArgs &a, std::int64_t e, 
       if (a.stage == 0)
         o = cur + dt * rr;
       else if (a.stage == 1)
-        o = 0.75 * (su0 ? su0[v * M + m][t] : a.u0[idx]) + 0.25 * (cur + dt * rr);
+        o = 0.75 * a.u0[idx] + 0.25 * (cur + dt * rr);
       else
-        o = (1.0 / 3.0) * (su0 ? su0[v * M + m][t] : a.u0[idx]) + (2.0 / 3.0) * (cur + dt * rr);
+        o = (1.0 / 3.0) * a.u0[idx] + (2.0 / 3.0) * (cur + dt * rr);
       a.out[idx] = o;
       if (v == 0)
         rho[m] = o;
@@ -1042,17 +1041,14 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_mixed(const StageAr
 //   rec    int16  [3][TILE]      each slot's record; <= -2: -(2 + k' TILE + j),
 //                                the record of slot k' of tile element j;
 //                                -1: none (a rough element's unneeded face)
-//   u0     double [4 M][TILE]    (U0 only) u^n of the tile for the Shu-Osher
-//                                combination of stages 1 and 2
-template <int P, int TILE, bool U0 = false> struct SharedFaceSmem {
+template <int P, int TILE> struct SharedFaceSmem {
   static constexpr int M = TriShape<P>::M, QF = TriShape<P>::QF;
   static constexpr std::size_t state = 0;
   static constexpr std::size_t prim = state + sizeof(double) * 4 * M * TILE;
   static constexpr std::size_t flux = prim + sizeof(double) * 4 * TILE;
   static constexpr std::size_t items = flux + sizeof(float) * 4 * QF * 3 * TILE;
   static constexpr std::size_t rec = items + sizeof(std::uint16_t) * 3 * TILE;
-  static constexpr std::size_t u0 = (rec + sizeof(std::int16_t) * 3 * TILE + 15) / 16 * 16;
-  static constexpr std::size_t bytes = U0 ? u0 + sizeof(double) * 4 * M * TILE : u0;
+  static constexpr std::size_t bytes = rec + sizeof(std::int16_t) * 3 * TILE;
 };
 
 // The fused mixed stage with the faces inside a tile evaluated once.
@@ -1075,17 +1071,15 @@ template <int P, int TILE, bool U0 = false> struct SharedFaceSmem {
 // cell means are appended to it and left to the second pass, as in the tile
 // kernel; their faces are evaluated only where an element that stays needs
 // them.
-// U0: in stages 1 and 2 the tile's u^n rows are copied into shared memory
-// asynchronously at the start, so the combination at the end does not wait
-// on global loads.
-// PF: each element's geometry, slot and (stages 1 and 2) u^n rows are
+// PF >= 1: each element's geometry, slot and (stages 1 and 2) u^n rows are
 // prefetched into L2 at the start, so the later loads that depend on one
 // another (slot codes, then neighbours' slots; normals; geometry) do not
-// each wait on DRAM after an L2 flush.
-template <int P, int R, int TILE, int MINB, bool U0, bool PF = false>
+// each wait on DRAM after an L2 flush.  PF = 2 also prefetches the u^n rows
+// into L1 before the lifting, for the combination at the end.
+template <int P, int R, int TILE, int MINB, int PF>
 __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_shared(const StageArgs a) {
   using S = TriShape<P>;
-  using L = SharedFaceSmem<P, TILE, U0>;
+  using L = SharedFaceSmem<P, TILE>;
   constexpr int M = S::M, QV = MixedVolume<P, R>::QV, QF = S::QF, H = M - 1;
   constexpr double phi0 = 0.70710678118654752440;
   static_assert(3 * TILE < 16384, "record indices are 16-bit");
@@ -1097,7 +1091,6 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_shared(const StageA
   float(*rflux)[3 * TILE] = reinterpret_cast<float(*)[3 * TILE]>(smem + L::flux);
   std::uint16_t *items = reinterpret_cast<std::uint16_t *>(smem + L::items);
   std::int16_t(*rec)[TILE] = reinterpret_cast<std::int16_t(*)[TILE]>(smem + L::rec);
-  double(*su0)[TILE] = U0 ? reinterpret_cast<double(*)[TILE]>(smem + L::u0) : nullptr;
 
   const int t = threadIdx.x;
   const std::int64_t ne = a.mesh.ne;
@@ -1117,7 +1110,7 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_shared(const StageA
   const double *__restrict__ in = a.in;
   const double gamma = a.gamma;
 
-  if constexpr (PF) {
+  if constexpr (PF >= 1) {
     if (active) {
 #pragma unroll
       for (int r = 0; r < 5; ++r)
@@ -1146,17 +1139,6 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_shared(const StageA
                    : "memory");
   }
   asm volatile("cp.async.commit_group;\n" ::: "memory");
-  if constexpr (U0) {
-    if (active && a.stage > 0) {
-      const unsigned base = static_cast<unsigned>(__cvta_generic_to_shared(&su0[0][t]));
-#pragma unroll
-      for (int r = 0; r < 4 * M; ++r)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(base + r * TILE * 8),
-                     "l"(a.u0 + r * ne + e)
-                     : "memory");
-    }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-  }
   {
     const float *src = static_cast<const float *>(a.face_table);
     float *dst = reinterpret_cast<float *>(&table);
@@ -1165,10 +1147,7 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_shared(const StageA
   }
   if (t == 0)
     item_count = 0;
-  if constexpr (U0)
-    asm volatile("cp.async.wait_group 1;\n" ::: "memory"); // the state, not u^n
-  else
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
 
   // Each element: its mean's primitive values, the rough test, and its
@@ -1364,8 +1343,6 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_shared(const StageA
   if (!active)
     return;
   if (rough) {
-    if constexpr (U0)
-      asm volatile("cp.async.wait_all;\n" ::: "memory");
     a.rough[atomicAdd(a.rough_count, 1)] = static_cast<std::int32_t>(e);
     return;
   }
@@ -1437,6 +1414,13 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_shared(const StageA
           racc[v][m] = fmaf(T.dxi[q][m], gxi, fmaf(T.deta[q][m], geta, racc[v][m]));
       }
     }
+  }
+
+  if constexpr (PF >= 2) {
+    if (a.stage > 0)
+#pragma unroll
+      for (int r = 0; r < 4 * M; ++r)
+        asm volatile("prefetch.global.L1 [%0];\n" ::"l"(a.u0 + r * ne + e));
   }
 
   // Lift the three faces' records, in the element's slot order.
@@ -1518,9 +1502,7 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_shared(const StageA
     }
   }
 
-  if constexpr (U0)
-    asm volatile("cp.async.wait_all;\n" ::: "memory"); // this thread's u^n column
-  tile_finish<P, TILE>(a, e, t, case_id, sstate, r0, racc, su0);
+  tile_finish<P, TILE>(a, e, t, case_id, sstate, r0, racc);
 }
 
 // Per-case CFL speed over a tile work list: the largest cell-average wave
@@ -1629,9 +1611,9 @@ template <int P, int R, int TILE, int MINB> void tile_opt_in() {
               sizeof(FaceTable<P, float>), opted_in);
 }
 
-template <int P, int R, int TILE, int MINB, bool U0, bool PF = false> void shared_opt_in() {
+template <int P, int R, int TILE, int MINB, int PF> void shared_opt_in() {
   static bool opted_in[64] = {};
-  smem_opt_in(euler_tri_tile_shared<P, R, TILE, MINB, U0, PF>, SharedFaceSmem<P, TILE, U0>::bytes,
+  smem_opt_in(euler_tri_tile_shared<P, R, TILE, MINB, PF>, SharedFaceSmem<P, TILE>::bytes,
               sizeof(FaceTable<P, float>) + sizeof(int), opted_in);
 }
 
@@ -1642,12 +1624,11 @@ constexpr int kRoughTile = 32;
 // The FP32 pass over all tiles, then (with a rough list) the pass over the
 // elements it left, sized for the worst case: its CTAs beyond the list's
 // length return at once.  SHARED picks the shared-face tile kernel for the
-// FP32 pass (U0: the variant that stages u^n in shared memory).
-template <int P, int R, int TILE, int MINB, bool SHARED = false, bool U0 = false,
-          bool PF = false>
+// FP32 pass (PF: its prefetch mode).
+template <int P, int R, int TILE, int MINB, bool SHARED = false, int PF = 0>
 void stage_tile(const StageArgs &a, cudaStream_t s) {
   if constexpr (SHARED)
-    shared_opt_in<P, R, TILE, MINB, U0, PF>();
+    shared_opt_in<P, R, TILE, MINB, PF>();
   else
     tile_opt_in<P, R, TILE, MINB>();
   const std::int64_t blocks = a.work ? a.work_count : (a.mesh.ne + TILE - 1) / TILE;
@@ -1656,8 +1637,8 @@ void stage_tile(const StageArgs &a, cudaStream_t s) {
   if (a.rough)
     check(cudaMemsetAsync(a.rough_count, 0, sizeof(std::int32_t), s), "rough count");
   if constexpr (SHARED)
-    euler_tri_tile_shared<P, R, TILE, MINB, U0, PF>
-        <<<static_cast<unsigned>(blocks), TILE, SharedFaceSmem<P, TILE, U0>::bytes, s>>>(a);
+    euler_tri_tile_shared<P, R, TILE, MINB, PF>
+        <<<static_cast<unsigned>(blocks), TILE, SharedFaceSmem<P, TILE>::bytes, s>>>(a);
   else
     euler_tri_tile_mixed<P, R, TILE, MINB, false>
         <<<static_cast<unsigned>(blocks), TILE, tile_smem<P, TILE>(), s>>>(a);
@@ -1677,7 +1658,7 @@ void stage_tile(const StageArgs &a, cudaStream_t s) {
 //   5:  96 elements, sized for 5 CTAs per SM (15 warps)
 //   6: 128 elements, sized for 4 CTAs per SM (16 warps)
 //   7: 128 elements, sized for 3 CTAs per SM
-//   8: 128 elements, sized for 3 CTAs per SM, u^n staged in shared memory
+//   8: 128 elements, sized for 4 CTAs per SM, rows prefetched to L2 and u^n to L1
 //   9: 128 elements, sized for 4 CTAs per SM, per-element rows prefetched to L2
 constexpr int kTileShapes = kTileShapeCount;
 constexpr int kTileElements[kTileShapes] = {128, 128, 256, 64, 64, 96, 128, 128, 128, 128};
@@ -1693,8 +1674,8 @@ template <int P, int R> struct StageTile {
     case 5: stage_tile<P, R, 96, 5, true>(a, s); break;
     case 6: stage_tile<P, R, 128, 4, true>(a, s); break;
     case 7: stage_tile<P, R, 128, 3, true>(a, s); break;
-    case 8: stage_tile<P, R, 128, 3, true, true>(a, s); break;
-    case 9: stage_tile<P, R, 128, 4, true, false, true>(a, s); break;
+    case 8: stage_tile<P, R, 128, 4, true, 2>(a, s); break;
+    case 9: stage_tile<P, R, 128, 4, true, 1>(a, s); break;
     default: throw std::invalid_argument("tile kernel: unknown launch shape");
     }
   }
@@ -1706,12 +1687,12 @@ template <int P, int R> struct PrepareTile {
     tile_opt_in<P, R, 128, 1>();
     tile_opt_in<P, R, 256, 2>();
     tile_opt_in<P, R, 64, 8>();
-    shared_opt_in<P, R, 64, 7, false>();
-    shared_opt_in<P, R, 96, 5, false>();
-    shared_opt_in<P, R, 128, 4, false>();
-    shared_opt_in<P, R, 128, 3, false>();
-    shared_opt_in<P, R, 128, 3, true>();
-    shared_opt_in<P, R, 128, 4, false, true>();
+    shared_opt_in<P, R, 64, 7, 0>();
+    shared_opt_in<P, R, 96, 5, 0>();
+    shared_opt_in<P, R, 128, 4, 0>();
+    shared_opt_in<P, R, 128, 3, 0>();
+    shared_opt_in<P, R, 128, 4, 2>();
+    shared_opt_in<P, R, 128, 4, 1>();
   }
 };
 
