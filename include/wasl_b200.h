@@ -80,7 +80,7 @@ typedef struct {
                                 rule, p..p+2; 0 = p+2, the reference residual's rule */
   int mixed_kernel;          /* mixed form: 0 autotuned; 1 face-centric kernels (face pass
                                 + element pass); 2 + s the fused tile kernel in launch
-                                shape s (0..9, see wasl_gpu_tuning) */
+                                shape s (0..7, see wasl_gpu_tuning) */
   int positivity_all;        /* with limiting: 1 applies the positivity limiter to every
                                 element, not only troubled ones (not the reference's
                                 behaviour, cpp/src/limiting/euler_modal_limiter.cpp:81-96) */
@@ -171,9 +171,7 @@ int wasl_gpu_sync(wasl_gpu *handle);
  * a thread; 1: 128, no register cap; 2: 256 at <= 128; 3: 64 at <= 128;
  * 4-7: the shared-face tile kernel, which evaluates a face between two
  * elements of one tile once: 4: 64 elements per CTA sized for 7 CTAs per SM;
- * 5: 96 for 5; 6: 128 for 4; 7: 128 for 3; 8: 128 for 4 with each
- * element's rows prefetched to L2 and u^n to L1; 9: 128 for 4 with the rows
- * prefetched to L2);
+ * 5: 96 for 5; 6: 128 for 4; 7: 128 for 3);
  * -1 for forms with a single kernel or before the first step.  When the
  * choice was autotuned (mixed_kernel 0: every variant timed on the solver's
  * own state before its first step, the fastest kept for the process per

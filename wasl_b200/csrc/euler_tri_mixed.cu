@@ -1071,12 +1071,12 @@ template <int P, int TILE> struct SharedFaceSmem {
 // cell means are appended to it and left to the second pass, as in the tile
 // kernel; their faces are evaluated only where an element that stays needs
 // them.
-// PF >= 1: each element's geometry, slot and (stages 1 and 2) u^n rows are
-// prefetched into L2 at the start, so the later loads that depend on one
-// another (slot codes, then neighbours' slots; normals; geometry) do not
-// each wait on DRAM after an L2 flush.  PF = 2 also prefetches the u^n rows
-// into L1 before the lifting, for the combination at the end.
-template <int P, int R, int TILE, int MINB, int PF>
+// Each element's geometry, slot and (stages 1 and 2) u^n rows are prefetched
+// into L2 at the start, so the later loads that depend on one another (slot
+// codes, then neighbours' slots; normals; geometry) do not each wait on DRAM
+// when the state and mesh are not in L2 (1.5% faster per step in the
+// vortex benchmark, which flushes L2 between steps).
+template <int P, int R, int TILE, int MINB>
 __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_shared(const StageArgs a) {
   using S = TriShape<P>;
   using L = SharedFaceSmem<P, TILE>;
@@ -1110,23 +1110,22 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_shared(const StageA
   const double *__restrict__ in = a.in;
   const double gamma = a.gamma;
 
-  if constexpr (PF >= 1) {
-    if (active) {
+  if (active) {
 #pragma unroll
-      for (int r = 0; r < 5; ++r)
-        asm volatile("prefetch.global.L2 [%0];\n" ::"l"(a.mesh.geo + r * ne + e));
+    for (int r = 0; r < 5; ++r)
+      asm volatile("prefetch.global.L2 [%0];\n" ::"l"(a.mesh.geo + r * ne + e));
 #pragma unroll
-      for (int r = 0; r < 9; ++r)
-        asm volatile("prefetch.global.L2 [%0];\n" ::"l"(a.mesh.slot_geo + r * ne + e));
+    for (int r = 0; r < 9; ++r)
+      asm volatile("prefetch.global.L2 [%0];\n" ::"l"(a.mesh.slot_geo + r * ne + e));
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        asm volatile("prefetch.global.L2 [%0];\n" ::"l"(a.tile.nbr + k * ne + e));
-        asm volatile("prefetch.global.L2 [%0];\n" ::"l"(a.tile.code + k * ne + e));
-      }
-      if (a.stage > 0)
+    for (int k = 0; k < 3; ++k) {
+      asm volatile("prefetch.global.L2 [%0];\n" ::"l"(a.tile.nbr + k * ne + e));
+      asm volatile("prefetch.global.L2 [%0];\n" ::"l"(a.tile.code + k * ne + e));
+    }
+    if (a.stage > 0) {
 #pragma unroll
-        for (int r = 0; r < 4 * M; ++r)
-          asm volatile("prefetch.global.L2 [%0];\n" ::"l"(a.u0 + r * ne + e));
+      for (int r = 0; r < 4 * M; ++r)
+        asm volatile("prefetch.global.L2 [%0];\n" ::"l"(a.u0 + r * ne + e));
     }
   }
   // Stage the tile's state and the face tables (as the tile kernel).
@@ -1416,13 +1415,6 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_shared(const StageA
     }
   }
 
-  if constexpr (PF >= 2) {
-    if (a.stage > 0)
-#pragma unroll
-      for (int r = 0; r < 4 * M; ++r)
-        asm volatile("prefetch.global.L1 [%0];\n" ::"l"(a.u0 + r * ne + e));
-  }
-
   // Lift the three faces' records, in the element's slot order.
   double r0[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll 1
@@ -1611,9 +1603,9 @@ template <int P, int R, int TILE, int MINB> void tile_opt_in() {
               sizeof(FaceTable<P, float>), opted_in);
 }
 
-template <int P, int R, int TILE, int MINB, int PF> void shared_opt_in() {
+template <int P, int R, int TILE, int MINB> void shared_opt_in() {
   static bool opted_in[64] = {};
-  smem_opt_in(euler_tri_tile_shared<P, R, TILE, MINB, PF>, SharedFaceSmem<P, TILE>::bytes,
+  smem_opt_in(euler_tri_tile_shared<P, R, TILE, MINB>, SharedFaceSmem<P, TILE>::bytes,
               sizeof(FaceTable<P, float>) + sizeof(int), opted_in);
 }
 
@@ -1624,11 +1616,11 @@ constexpr int kRoughTile = 32;
 // The FP32 pass over all tiles, then (with a rough list) the pass over the
 // elements it left, sized for the worst case: its CTAs beyond the list's
 // length return at once.  SHARED picks the shared-face tile kernel for the
-// FP32 pass (PF: its prefetch mode).
-template <int P, int R, int TILE, int MINB, bool SHARED = false, int PF = 0>
+// FP32 pass.
+template <int P, int R, int TILE, int MINB, bool SHARED = false>
 void stage_tile(const StageArgs &a, cudaStream_t s) {
   if constexpr (SHARED)
-    shared_opt_in<P, R, TILE, MINB, PF>();
+    shared_opt_in<P, R, TILE, MINB>();
   else
     tile_opt_in<P, R, TILE, MINB>();
   const std::int64_t blocks = a.work ? a.work_count : (a.mesh.ne + TILE - 1) / TILE;
@@ -1637,7 +1629,7 @@ void stage_tile(const StageArgs &a, cudaStream_t s) {
   if (a.rough)
     check(cudaMemsetAsync(a.rough_count, 0, sizeof(std::int32_t), s), "rough count");
   if constexpr (SHARED)
-    euler_tri_tile_shared<P, R, TILE, MINB, PF>
+    euler_tri_tile_shared<P, R, TILE, MINB>
         <<<static_cast<unsigned>(blocks), TILE, SharedFaceSmem<P, TILE>::bytes, s>>>(a);
   else
     euler_tri_tile_mixed<P, R, TILE, MINB, false>
@@ -1658,10 +1650,8 @@ void stage_tile(const StageArgs &a, cudaStream_t s) {
 //   5:  96 elements, sized for 5 CTAs per SM (15 warps)
 //   6: 128 elements, sized for 4 CTAs per SM (16 warps)
 //   7: 128 elements, sized for 3 CTAs per SM
-//   8: 128 elements, sized for 4 CTAs per SM, rows prefetched to L2 and u^n to L1
-//   9: 128 elements, sized for 4 CTAs per SM, per-element rows prefetched to L2
 constexpr int kTileShapes = kTileShapeCount;
-constexpr int kTileElements[kTileShapes] = {128, 128, 256, 64, 64, 96, 128, 128, 128, 128};
+constexpr int kTileElements[kTileShapes] = {128, 128, 256, 64, 64, 96, 128, 128};
 
 template <int P, int R> struct StageTile {
   static void run(int shape, const StageArgs &a, cudaStream_t s) {
@@ -1674,8 +1664,6 @@ template <int P, int R> struct StageTile {
     case 5: stage_tile<P, R, 96, 5, true>(a, s); break;
     case 6: stage_tile<P, R, 128, 4, true>(a, s); break;
     case 7: stage_tile<P, R, 128, 3, true>(a, s); break;
-    case 8: stage_tile<P, R, 128, 4, true, 2>(a, s); break;
-    case 9: stage_tile<P, R, 128, 4, true, 1>(a, s); break;
     default: throw std::invalid_argument("tile kernel: unknown launch shape");
     }
   }
@@ -1687,12 +1675,10 @@ template <int P, int R> struct PrepareTile {
     tile_opt_in<P, R, 128, 1>();
     tile_opt_in<P, R, 256, 2>();
     tile_opt_in<P, R, 64, 8>();
-    shared_opt_in<P, R, 64, 7, 0>();
-    shared_opt_in<P, R, 96, 5, 0>();
-    shared_opt_in<P, R, 128, 4, 0>();
-    shared_opt_in<P, R, 128, 3, 0>();
-    shared_opt_in<P, R, 128, 4, 2>();
-    shared_opt_in<P, R, 128, 4, 1>();
+    shared_opt_in<P, R, 64, 7>();
+    shared_opt_in<P, R, 96, 5>();
+    shared_opt_in<P, R, 128, 4>();
+    shared_opt_in<P, R, 128, 3>();
   }
 };
 
