@@ -55,12 +55,16 @@ def parse():
                     help="mixed form's volume rule order (default p; the reference uses p+2)")
     ap.add_argument("--kernel", type=int, default=0,
                     help="mixed form's kernel: 0 autotuned, 1 face-centric, 2+s tile shape s")
-    ap.add_argument("--workload", choices=["vortex", "batched", "quadrant", "shock-vortex"],
+    ap.add_argument("--workload", choices=["vortex", "batched", "quadrant", "shock-vortex",
+                                           "line-euler", "line-scalar", "tri-scalar"],
                     default="vortex",
                     help="vortex: the 256x256 isentropic vortex (default); batched: independent"
                          " two-state Riemann cases of uneven size and order in one batch;"
                          " quadrant: four-quadrant Riemann, 1024x1024 quads, P3, limiter;"
-                         " shock-vortex: 2048x1024 quads, P3, learned indicator")
+                         " shock-vortex: 2048x1024 quads, P3, learned indicator;"
+                         " line-euler / line-scalar / tri-scalar: the plain FP64 1D Euler"
+                         " (4M cells), 1D scalar (16M cells) and 2D scalar (1024x1024 quads)"
+                         " paths at P2")
     ap.add_argument("--cases", type=int, default=512, help="batched workload: number of cases")
     ap.add_argument("--quads", type=int, default=1024,
                     help="quadrant / shock-vortex workloads: quads per unit side")
@@ -690,6 +694,54 @@ def limited(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------------
+# plain FP64 1D Euler, 1D scalar and 2D scalar paths (meshes larger than L2)
+# ---------------------------------------------------------------------------------
+
+OTHER_PATHS = {
+    # workload: (dimensions, equation, cells or quads per side, cell means)
+    "line-euler": (1, "euler", 1 << 22, (1.0, 0.2, 0.0, 2.5)),
+    "line-scalar": (1, "scalar", 1 << 24, (1.0,)),
+    "tri-scalar": (2, "scalar", 1024, (1.0,)),
+}
+
+
+def other_path(args, rank, world, local_rank):
+    """A smooth random P2 state (mode 0 from the cell means, higher modes
+    1e-3 N(0,1), seed 1) on a periodic jittered mesh; device-resident steps
+    at CFL 0.1 timed with events on the handle's stream."""
+    import torch
+    import wasl_b200
+    from wasl_b200 import meshgen
+    torch.cuda.set_device(local_rank)
+    dims, equation, n, means = OTHER_PATHS[args.workload]
+    arrays = (meshgen.jittered_line(n, jitter=0.2, seed=1) if dims == 1
+              else meshgen.jittered_box(n, jitter=0.15, seed=1))
+    g = wasl_b200.Solver(*arrays, dimensions=dims, equation=equation, polynomial_order=2,
+                         velocity=(1.0, 0.5) if equation == "scalar" else (0.0, 0.0),
+                         device=local_rank)
+    rng = np.random.Generator(np.random.PCG64(1))
+    c = 1e-3 * rng.standard_normal((g.variables, g.modes, g.elements))
+    for v, mean in enumerate(means[:g.variables]):
+        c[v, 0] = np.sqrt(2.0) * mean
+    g.set_state(c.ravel())
+    for _ in range(args.warmup):
+        g.step(g.stable_dt(0.1))
+    steps = max(1, min(args.steps, 50))
+    ms, launches = timed_steps(g, torch, steps, 0.1)
+    line = {"metric": METRIC, "value": 3.0 * g.state_size * steps / (ms * 1e-3), "unit": UNIT,
+            "n_gpus": 1, "steps": steps, "warmup": args.warmup, "ms_per_step": ms / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded jittered mesh, smooth random state)",
+            "config": {"workload": f"{args.workload}: {g.elements} elements, P2, periodic,"
+                                   " CFL 0.1, plain FP64",
+                       "elements": g.elements, "dof": g.state_size,
+                       "l2": f"inputs larger than L2 (state {8 * g.state_size / 1e6:.0f} MB)"},
+            "gpu_launches": launches}
+    g.close()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -702,6 +754,9 @@ def main():
     elif args.workload in ("quadrant", "shock-vortex"):
         if rank == 0:
             limited(args, rank, world, local_rank)
+    elif args.workload in OTHER_PATHS:
+        if rank == 0:
+            other_path(args, rank, world, local_rank)
     else:
         ours(args, rank, world, local_rank)
 
