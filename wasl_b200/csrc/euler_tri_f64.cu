@@ -692,6 +692,12 @@ void launch_dt_from_speed(std::int64_t cases, unsigned long long *speed, double 
       cases, speed, cfl, length, p, length_all, p_all, dt, elapsed, status);
 }
 
+void launch_cfl_speed(const CflArgs &a, cudaStream_t s) {
+  check(cudaMemsetAsync(a.result, 0, sizeof(unsigned long long), s), "cfl reset");
+  const unsigned blocks = static_cast<unsigned>(std::min<std::int64_t>((a.ne + 255) / 256, 148 * 4));
+  cfl_max<<<blocks, 256, 0, s>>>(a);
+}
+
 void launch_cfl(const CflArgs &a, cudaStream_t s) {
   check(cudaMemsetAsync(a.result, 0, 8 * sizeof(unsigned long long), s), "cfl reset");
   const unsigned blocks = static_cast<unsigned>(std::min<std::int64_t>((a.ne + 255) / 256, 148 * 4));

@@ -285,24 +285,26 @@ public:
     check_error();
   }
 
-  // Device-resident steps.  With the tile kernel and no limiter, the last
-  // stage of each step also reduces the next step's CFL speed, so a step
-  // after the first needs one small kernel for dt instead of the three CFL
-  // kernels and their pass over the state.
+  // Device-resident steps: dt from the largest cell-average wave speed
+  // (cfl_max, then dt_from_speed, which also zeroes the speed word).  With
+  // the tile kernel and no limiter, the last stage of each step also reduces
+  // the next step's CFL speed, so a step after the first needs only the
+  // small dt kernel and no pass over the state.
   void advance(double cfl, std::int64_t steps) override {
     for (std::int64_t n = 0; n < steps; ++n) {
-      if (speed_ready_) {
-        launch_dt_from_speed(1, d_speed_.get(), cfl, nullptr, nullptr, length_, p_, d_dt_.get(),
-                             nullptr, nullptr, stream_);
+      if (!speed_ready_) {
+        // The speed alone: the device dt needs no arg-max (that serves the
+        // host's bit-consistent stable_dt).
+        CflArgs c = cfl_args(cfl);
+        c.result = d_speed_.get();
+        c.dt = nullptr;
+        launch_cfl_speed(c, stream_);
         count_launches(1);
-      } else {
-        launch_cfl(cfl_args(cfl), stream_);
-        count_launches(3);
       }
+      launch_dt_from_speed(1, d_speed_.get(), cfl, nullptr, nullptr, length_, p_, d_dt_.get(),
+                           nullptr, nullptr, stream_);
+      count_launches(1);
       fused_speed_ = mixed_ && !limiting_;
-      if (fused_speed_ && !speed_ready_)
-        cuda_check(cudaMemsetAsync(d_speed_.get(), 0, sizeof(unsigned long long), stream_),
-                   "speed reset");
       enqueue_step(d_dt_.get(), 0.0);
       speed_ready_ = fused_speed_ && kernel_ >= 1;
       fused_speed_ = false;

@@ -277,6 +277,10 @@ void prepare_euler_tri_stage_tile(int p, int rule);
 void launch_limit_f64(int M, int NB, const LimitArgs &a, cudaStream_t stream);
 void launch_sense_f64(int M, const SenseArgs &a, cudaStream_t stream);
 void launch_cfl(const CflArgs &a, cudaStream_t stream);
+// The largest cell-average wave speed alone (a.result[0], zeroed first; no
+// arg-max and no dt): for device-resident steps, whose dt comes from it by
+// launch_dt_from_speed with the same arithmetic as launch_cfl's dt.
+void launch_cfl_speed(const CflArgs &a, cudaStream_t stream);
 // dt[c] = cfl length[c] / (speed (2 p[c] + 1)) from reduced speeds (0 where
 // the speed is 0 or status[c] is non-zero), added to elapsed[c] when elapsed
 // is not null; then the speed words are zeroed.  length/p are per-case
