@@ -137,6 +137,14 @@ int wasl_gpu_evaluate(wasl_gpu *handle, int rule_order, double *values, int64_t 
  * (the device finds the fastest cell, the host evaluates its speed). */
 int wasl_gpu_stable_dt(wasl_gpu *handle, double cfl, double *dt);
 
+/* The two factors of that time step, dt = cfl * length / (speed * (2p + 1)):
+ * the largest cell-average wave speed (hypot(u, v) + c, evaluated as
+ * wasl_gpu_stable_dt evaluates it) and the smallest element length (the
+ * smallest altitude, cpp/src/time/cfl_timestep.cpp:22-30, 70-84).  A run
+ * partitioned over ranks reduces speed by max and length by min and forms the
+ * dt of one solver over the whole mesh (2D Euler only). */
+int wasl_gpu_cfl_parts(wasl_gpu *handle, double *speed, double *length);
+
 /* One SSP-RK3 step with the stage limiter (when enabled). */
 int wasl_gpu_step(wasl_gpu *handle, double dt);
 

@@ -246,3 +246,17 @@ def test_advance_enqueues_and_sync_reports_errors(precision):
         with pytest.raises(wasl_b200.WaslError, match="not physical") as err:
             g.sync()
         assert err.value.status == -4
+
+
+def test_profile_splits_stage_time_by_rk_stage():
+    """profile_stages: the stage-kernel time of the last profile split over
+    the three SSP-RK3 stages adds up to the total."""
+    arrays = cases.vortex_mesh(16, seed=2)
+    with wasl_b200.Solver(*arrays, polynomial_order=2, precision="mixed", mixed_kernel=8) as g:
+        cases.project_initial(g, cases.IsentropicVortex().conserved)
+        g.profile_begin()
+        g.advance(0.15, 3)
+        ms, kernels, launches = g.profile_end()
+        split = g.profile_stages()
+    assert kernels == 9 and launches >= kernels and all(t > 0 for t in split)
+    assert abs(sum(split) - ms) <= 1e-9 * ms

@@ -1,0 +1,171 @@
+"""Partition, ghost region and halo exchange (wasl_b200.halo), on the CPU.
+
+The reference checks its distributed path by splitting a mesh over ranks in
+one process and requiring the serial result for every owned element
+(cpp/tests/communication/halo_exchange_test.cpp:1-12); the same check runs
+here on the oracle's full SSP-RK3 step, with and without the limiter, and the
+torch.distributed transport is exercised by two gloo ranks."""
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from golden.make_golden import seeded_state
+from wasl_b200 import halo, meshgen
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GAMMA = 1.4
+
+
+def test_partition_is_the_reference_block_rule():
+    owners = halo.element_owners(10, 3)
+    assert owners.tolist() == [0, 0, 0, 0, 1, 1, 1, 2, 2, 2]
+    for ne, ranks in [(7, 7), (1000, 3), (131072, 8)]:
+        o = halo.element_owners(ne, ranks)
+        assert np.all(np.diff(o) >= 0) and set(o.tolist()) == set(range(ranks))
+        assert np.array_equal(o, (np.arange(ne) * ranks // ne))
+    with pytest.raises(ValueError):
+        halo.element_owners(10, 0)
+
+
+def test_face_neighbors_are_symmetric():
+    tags, xy, tris = meshgen.jittered_box(9, jitter=0.15, seed=1, ny=7)
+    nbr = halo.face_neighbors(tris)
+    assert (nbr < 0).sum() == 2 * (9 + 7)  # boundary edges of a 9 x 7 box
+    for e, row in enumerate(nbr):
+        for n in row[row >= 0]:
+            assert e in nbr[n]
+
+
+def test_first_ghost_layer_is_the_reference_ghost_set():
+    """Depth 1: every off-rank element that shares a face with an owned one
+    (rank_ghost_elements); deeper layers grow one face step at a time."""
+    tags, xy, tris = meshgen.jittered_box(10, jitter=0.15, seed=2)
+    nbr = halo.face_neighbors(tris)
+    owners = halo.element_owners(len(tris), 3)
+    for rank in range(3):
+        owned = owners == rank
+        expect = sorted({int(n) for e in np.nonzero(owned)[0] for n in nbr[e]
+                         if n >= 0 and owners[n] != rank})
+        layers = halo.ghost_layers(nbr, owned, 3)
+        assert layers[0].tolist() == expect
+        reach = owned.copy()
+        for layer in layers:
+            assert not np.any(reach[layer])
+            assert all(np.any(reach[nbr[g][nbr[g] >= 0]]) for g in layer)
+            reach[layer] = True
+
+
+def test_schedule_is_symmetric_and_sorted():
+    tags, xy, tris = meshgen.jittered_box(12, jitter=0.15, seed=3)
+    ranks, depth = 4, 3
+    meshes = [halo.local_mesh(tags, xy, tris, r, ranks, depth) for r in range(ranks)]
+    schedules = [halo.build_halo_schedule(meshes, ranks, len(tris), r) for r in range(ranks)]
+    for r, s in enumerate(schedules):
+        assert [p for p, _ in s.sends] == sorted(p for p, _ in s.sends)
+        for peer, send in s.sends:
+            assert np.all(np.diff(send) > 0)
+            recv = dict(schedules[peer].recvs)[r]
+            assert np.array_equal(send, recv)
+        ghosts = meshes[r].elements[~meshes[r].owned]
+        assert np.array_equal(np.sort(np.concatenate([g for _, g in s.recvs])), ghosts)
+
+
+@pytest.mark.parametrize("p", [1, 2])
+@pytest.mark.parametrize("limiting", [False, True])
+@pytest.mark.parametrize("ranks", [2, 3])
+def test_split_reproduces_the_serial_step(oracle, p, limiting, ranks):
+    """Each rank steps its owned elements and ghost layers with the oracle's
+    SSP-RK3 step (transmissive boundaries), one in-process exchange per step:
+    every owned element equals the serial run bit for bit."""
+    tags, xy, tris = meshgen.jittered_box(14, jitter=0.15, seed=20 + p)
+    ne = len(tris)
+    serial = oracle.tri_mesh(tags, xy, tris)
+    c = seeded_state(ne, p, 5 + p, amplitude=0.02 if limiting else 0.005)
+    M = (p + 1) * (p + 2) // 2
+    depth = halo.halo_depth(limiting)
+    meshes = [halo.local_mesh(tags, xy, tris, r, ranks, depth) for r in range(ranks)]
+    schedules = [halo.build_halo_schedule(meshes, ranks, ne, r) for r in range(ranks)]
+    locals_ = [oracle.tri_mesh(*m.arrays) for m in meshes]
+    stencils = [lm.stencil(p) if limiting else None for lm in locals_]
+    st_serial = serial.stencil(p) if limiting else None
+    states = [np.ascontiguousarray(c.reshape(4 * M, ne)[:, m.elements]) for m in meshes]
+    flagged = 0
+    for _ in range(4):
+        dt = serial.cfl(GAMMA, c, p, 0.1)
+        flags = serial.euler_step(GAMMA, p, dt, c, boundary="transmissive", stencil=st_serial,
+                                  return_flags=True)
+        flagged += int(flags.sum())
+        for r, m in enumerate(meshes):
+            u = states[r].ravel()
+            lf = locals_[r].euler_step(GAMMA, p, dt, u, boundary="transmissive",
+                                       stencil=stencils[r], return_flags=True)
+            states[r] = u.reshape(4 * M, -1)
+            assert np.array_equal(lf[:, m.owned], flags[:, m.elements[m.owned]])
+        halo.exchange_in_process(states, meshes, schedules)
+        full = c.reshape(4 * M, ne)
+        for r, m in enumerate(meshes):
+            assert np.array_equal(states[r], full[:, m.elements]), f"rank {r}"
+    assert flagged > 0 or not limiting
+
+
+def free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+class _Parts:
+    """Stands in for a solver's cfl_parts on one rank."""
+
+    def __init__(self, speed, length):
+        self.parts = (speed, length)
+
+    def cfl_parts(self):
+        return self.parts
+
+
+def rank_main(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, ROOT)
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from wasl_b200 import halo, meshgen
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=30))
+    tags, xy, tris = meshgen.jittered_box(10, jitter=0.15, seed=4)
+    ne, rows = len(tris), 6
+    meshes = [halo.local_mesh(tags, xy, tris, r, world, 3) for r in range(world)]
+    sched = halo.build_halo_schedule(meshes, world, ne, rank)
+    m = meshes[rank]
+    coded = np.arange(rows)[:, None] * 1e6 + m.elements[None, :].astype(np.float64)
+    state = torch.tensor(np.where(m.owned[None, :], coded, np.nan))
+    halo.HaloExchange(m, sched, rows).exchange(state)
+    ok = bool(np.array_equal(state.numpy(), coded))
+    dt = halo.global_dt(_Parts([2.0, 3.0][rank], [0.5, 0.25][rank]), 0.1, 2)
+    dist.barrier()
+    dist.destroy_process_group()
+    out.put((rank, ok, dt))
+
+
+def test_two_gloo_ranks_exchange_ghost_rows():
+    """Every ghost column holds its owner's values after one exchange, and
+    the reduced time step uses the largest speed and the smallest length."""
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = free_port()
+    procs = [ctx.Process(target=rank_main, args=(r, 2, port, out)) for r in range(2)]
+    for proc in procs:
+        proc.start()
+    results = {r: (ok, dt) for r, ok, dt in (out.get(timeout=120) for _ in procs)}
+    for proc in procs:
+        proc.join(timeout=60)
+        assert proc.exitcode == 0
+    assert results[0][0] and results[1][0]
+    assert results[0][1] == results[1][1] == halo.dt_from_parts(0.1, 3.0, 0.25, 2)

@@ -140,6 +140,7 @@ SIGNATURES = {
     "wasl_gpu_profile_begin": (C.c_int, [C.c_void_p]),
     "wasl_gpu_profile_end": (C.c_int, [C.c_void_p, _d, _i64, _i64]),
     "wasl_gpu_profile_stages": (C.c_int, [C.c_void_p, _d]),
+    "wasl_gpu_cfl_parts": (C.c_int, [C.c_void_p, _d, _d]),
     "wasl_gpu_write_checkpoint": (C.c_int, [C.c_void_p, C.c_char_p, C.c_double, C.c_uint64,
                                             C.c_char_p]),
     "wasl_gpu_read_checkpoint": (C.c_int, [C.c_void_p, C.c_char_p, _d,
@@ -303,6 +304,14 @@ class Solver:
         dt = C.c_double()
         self._check(self._lib.wasl_gpu_stable_dt(self._h, cfl, C.byref(dt)))
         return dt.value
+
+    def cfl_parts(self):
+        """(largest cell-average wave speed, smallest element length): the
+        factors of stable_dt = cfl length / (speed (2p + 1)), for reductions
+        over the ranks of a partitioned run (2D Euler)."""
+        speed, length = C.c_double(), C.c_double()
+        self._check(self._lib.wasl_gpu_cfl_parts(self._h, C.byref(speed), C.byref(length)))
+        return speed.value, length.value
 
     def step(self, dt: float):
         self._check(self._lib.wasl_gpu_step(self._h, dt))

@@ -225,6 +225,13 @@ int wasl_gpu_stable_dt(wasl_gpu *h, double cfl, double *dt) {
   });
 }
 
+int wasl_gpu_cfl_parts(wasl_gpu *h, double *speed, double *length) {
+  return guarded(h, [&] {
+    need(speed != nullptr && length != nullptr, "null output");
+    h->solver->cfl_parts(*speed, *length);
+  });
+}
+
 int wasl_gpu_step(wasl_gpu *h, double dt) {
   return guarded(h, [&] {
     need(std::isfinite(dt), "step: time step is not finite");

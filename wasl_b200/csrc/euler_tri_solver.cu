@@ -242,7 +242,15 @@ public:
   }
 
   double stable_dt(double cfl) override {
-    launch_cfl(cfl_args(cfl), stream_);
+    double speed = 0.0, length = 0.0;
+    cfl_parts(speed, length);
+    return speed > 0.0 ? cfl * length / (speed * (2 * p_ + 1)) : 0.0;
+  }
+
+  void cfl_parts(double &speed, double &length) override {
+    CflArgs c = cfl_args(1.0);
+    c.dt = nullptr; // the host forms dt
+    launch_cfl(c, stream_);
     count_launches(3);
     cuda_check(cudaMemcpyAsync(scratch_.words, d_cfl_.get(), 8 * sizeof(unsigned long long),
                                cudaMemcpyDeviceToHost, stream_),
@@ -255,8 +263,8 @@ public:
     double mode0[4];
     for (int v = 0; v < 4; ++v)
       mode0[v] = bits_to_double(scratch_.words[2 + v]);
-    const double speed = host_cell_speed(cfg_.heat_capacity_ratio, mode0, 2);
-    return speed > 0.0 ? cfl * length_ / (speed * (2 * p_ + 1)) : 0.0;
+    speed = host_cell_speed(cfg_.heat_capacity_ratio, mode0, 2);
+    length = length_;
   }
 
   void step(double dt) override {

@@ -90,6 +90,15 @@ public:
   virtual void set_state(const double *host) = 0;
   virtual void get_state(double *host) = 0;
   virtual double stable_dt(double cfl) = 0;
+  // The two factors of stable_dt = cfl length / (speed (2p + 1)): the
+  // largest cell-average wave speed (evaluated as stable_dt evaluates it)
+  // and the smallest element length.  A partitioned run reduces them over
+  // ranks (max, min) and forms the same dt as one solver over the whole mesh.
+  virtual void cfl_parts(double &speed, double &length) {
+    (void)speed;
+    (void)length;
+    throw SolverError(WASL_ERR_ARGUMENT, "cfl parts: only for 2D Euler");
+  }
   virtual void step(double dt) = 0;
   virtual void limit() = 0; // the stage limiter applied to the current state
   // Enqueues `steps` device-resident steps; returns without waiting for
