@@ -56,3 +56,23 @@ def test_two_handles_reproduce_one(precision, limiting):
         serial.close()
         for g in parts:
             g.close()
+
+
+def test_device_state_view_shares_the_handle_memory():
+    """halo.device_state sees the handle's state in place: what it reads is
+    get_state, and what the exchange writes through it the next step uses."""
+    import torch
+    tags, xy, tris = meshgen.jittered_box(6, jitter=0.15, seed=3)
+    with wasl_b200.Solver(tags, xy, tris, polynomial_order=2, boundary="transmissive") as g:
+        c = seeded_state(g.elements, 2, 4, amplitude=0.005)
+        g.set_state(c)
+        g.sync()
+        view = halo.device_state(g)
+        assert view.shape == (4 * g.modes, g.elements)
+        assert np.array_equal(view.cpu().numpy().ravel(), c)
+        cols = torch.tensor([0, 5, 9], device="cuda")
+        view.index_copy_(1, cols, view.index_select(1, cols) * 1.0 + 0.25)
+        torch.cuda.current_stream().synchronize()
+        expect = c.reshape(4 * g.modes, -1).copy()
+        expect[:, [0, 5, 9]] += 0.25
+        assert np.array_equal(g.get_state().reshape(4 * g.modes, -1), expect)

@@ -213,6 +213,39 @@ class HaloExchange:
             state.index_copy_(1, idx, buf)
 
 
+class _DeviceRows:
+    """A [rows][columns] float64 array in device memory, by its pointer."""
+
+    def __init__(self, pointer: int, rows: int, columns: int):
+        self.__cuda_array_interface__ = {"shape": (rows, columns), "typestr": "<f8",
+                                         "data": (pointer, False), "version": 3,
+                                         "strides": None}
+
+
+def device_state(solver):
+    """The handle's device state U[variable][mode][element] as a
+    [4 M][elements] torch tensor sharing its memory (no copy).  The handle's
+    stream must have finished (solver.sync()) before it is read, and writes
+    through it must have finished before the handle's next step."""
+    import torch
+    rows = solver.variables * solver.modes
+    return torch.as_tensor(_DeviceRows(solver.state_device_pointer(), rows, solver.elements),
+                           device="cuda")
+
+
+def step_partitioned(solver, exchange: HaloExchange, cfl: float, polynomial_order: int,
+                     group=None) -> float:
+    """One step of a rank of a partitioned run on its GPU: the whole-mesh dt
+    from the reduced CFL parts, the step, then the ghost exchange."""
+    import torch
+    dt = global_dt(solver, cfl, polynomial_order, group=group, device="cuda")
+    solver.step(dt)
+    solver.sync()
+    exchange.exchange(device_state(solver))
+    torch.cuda.current_stream().synchronize()
+    return dt
+
+
 def dt_from_parts(cfl: float, speed: float, length: float, polynomial_order: int) -> float:
     """cfl length / (speed (2p + 1)), in the order the solver evaluates it
     (cpp/src/time/cfl_timestep.cpp:70-84); 0 for a state at rest."""
