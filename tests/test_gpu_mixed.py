@@ -260,3 +260,22 @@ def test_profile_splits_stage_time_by_rk_stage():
         split = g.profile_stages()
     assert kernels == 9 and launches >= kernels and all(t > 0 for t in split)
     assert abs(sum(split) - ms) <= 1e-9 * ms
+
+
+@pytest.mark.parametrize("form,p", [("plain", 1), ("plain", 2), ("mixed", 2)])
+def test_vortex_convergence_rate(form, p):
+    """Isentropic vortex on 16, 32 and 64 quads per side to t = 0.5: the L1
+    density error falls at a rate of at least p + 0.6 between the two finest
+    meshes (the reference's vortex check,
+    cpp/tests/dg/euler_triangle_residual_test.cpp:214-233)."""
+    vortex = cases.IsentropicVortex()
+    errors = []
+    for n in (16, 32, 64):
+        with wasl_b200.Solver(*cases.vortex_mesh(n, seed=7), polynomial_order=p, precision=form,
+                              volume_rule_order=p if form == "mixed" else 0) as g:
+            cases.project_initial(g, vortex.conserved)
+            steps, t = g.run(0.15, 0.0, 0.5)
+            errors.append(cases.l1_density_error(g, lambda x, y: vortex.conserved(x, y, t)))
+    rate = np.log(errors[1] / errors[2]) / np.log(2.0)
+    assert errors[0] > errors[1] > errors[2]
+    assert rate >= p + 0.6, (errors, rate)
