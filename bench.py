@@ -607,7 +607,8 @@ def limited(args, rank, world, local_rank):
     four-quadrant data the plain path (positivity only in troubled cells, as
     the reference limits) produces a non-physical cell average after about
     60 steps, and the mixed form (positivity on every element) after about
-    300."""
+    300; the reference's algorithm on the CPU breaks down on the same data
+    too."""
     import torch
     import wasl_b200
     args.steps = min(args.steps, LIMITED_STEPS)
