@@ -34,6 +34,8 @@ def build(reference_root: str | None = None) -> None:
     root = reference_root or "/root/reference"
     if os.path.isdir(os.path.join(root, "cpp", "src")):
         subprocess.check_call(["make", "-s", "-j8", "-C", HERE, "ref", f"REF={root}"])
+        if os.path.exists(os.path.join(os.path.dirname(HERE), "wasl_b200", "libwasl_b200.so")):
+            subprocess.check_call(["make", "-s", "-C", HERE, "gpu-case", f"REF={root}"])
 
 
 def _p(a, t=_d):

@@ -20,6 +20,8 @@
 #include <vector>
 
 #include "wasl/boundaries/line_boundary_conditions.hpp"
+#include "wasl/case/euler_case.hpp"
+#include "wasl/mesh/prepared/prepare_mesh.hpp"
 #include "wasl/boundaries/line_euler_exterior.hpp"
 #include "wasl/boundaries/periodic_triangle_trace.hpp"
 #include "wasl/dg/euler/line_residual.hpp"
@@ -483,6 +485,58 @@ void wr_scalar_line_step(void *handle, int left_kind, double left_value, int rig
   wasl::SspRk3Workspace workspace;
   wasl::ssp_rk3_step(mesh, wasl::ScalarAdvection{a}, p, dt, exterior, state, workspace);
   std::memcpy(c, state.data(), state.size() * sizeof(double));
+}
+
+// ---- whole cases through the reference's own run loop ------------------------
+
+int wr_write_prepared_tri_mesh(void *handle, const char *path) {
+  return guarded([&] {
+    wasl::write_prepared_mesh(path, wasl::prepare_mesh(static_cast<TriHandle *>(handle)->mesh));
+  });
+}
+
+// The reference's run_euler_case (periodic boundaries) from flat arguments;
+// regions are 10 doubles each: shape (0 default, 1 interval, 2 circle),
+// lower, upper, centre x, centre y, radius, density, velocity x, velocity y,
+// pressure.
+int wr_run_euler_case(const char *prepared_mesh, const char *output_directory, int limiting,
+                      double sensor_threshold, double density_floor, double pressure_floor,
+                      int dimensions, int p, double gamma, double cfl, double start_time,
+                      double end_time, std::uint64_t max_steps, std::uint64_t history_interval,
+                      std::uint64_t visualization_interval, std::uint64_t checkpoint_interval,
+                      std::uint64_t keep_checkpoints, const double *regions,
+                      std::int64_t region_count, std::uint64_t *steps, double *time) {
+  return guarded([&] {
+    wasl::EulerCase c;
+    c.files = {prepared_mesh, output_directory, ""};
+    c.run = {start_time,           end_time,          max_steps,       history_interval,
+             visualization_interval, checkpoint_interval, keep_checkpoints};
+    c.limiting = limiting != 0;
+    c.sensor_threshold = sensor_threshold;
+    c.density_floor = density_floor;
+    c.pressure_floor = pressure_floor;
+    c.dimensions = dimensions;
+    c.polynomial_order = p;
+    c.heat_capacity_ratio = gamma;
+    c.cfl = cfl;
+    for (std::int64_t i = 0; i < region_count; ++i) {
+      const double *r = regions + 10 * i;
+      wasl::EulerRegion region;
+      region.shape = r[0] == 1.0   ? wasl::EulerRegion::Shape::interval
+                     : r[0] == 2.0 ? wasl::EulerRegion::Shape::circle
+                                   : wasl::EulerRegion::Shape::default_region;
+      region.lower = r[1];
+      region.upper = r[2];
+      region.center_x = r[3];
+      region.center_y = r[4];
+      region.radius = r[5];
+      region.value = {r[6], r[7], r[8], r[9]};
+      c.initial_regions.push_back(region);
+    }
+    const auto summary = wasl::run_euler_case(c);
+    *steps = summary.step;
+    *time = summary.time;
+  });
 }
 
 } // extern "C"

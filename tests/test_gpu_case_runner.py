@@ -1,0 +1,115 @@
+"""The reference's own run loop (run_serial_case: CFL stepping, history, VTU
+snapshots, checkpoint rotation) with the GPU-backed case model
+(wasl_b200/integration/serial_case_model.cpp) writes the same run directory,
+byte for byte, as the reference's run_euler_case with its CPU model.
+
+Both runs go through oracle/_ref: libwaslref.so is the reference's code (with
+the binary stand-in for its HDF5 files) and libwasl_case_gpu.so the adapter
+linked against it and libwasl_b200.so."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+import pyoracle
+from wasl_b200 import meshgen
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GPU_CASE = os.path.join(ROOT, "oracle", "_ref", "libwasl_case_gpu.so")
+_d, _u64 = C.POINTER(C.c_double), C.POINTER(C.c_uint64)
+
+# A uniform state with a denser, slower disc (shape 2 = circle): the
+# reference case regression's kind of initial data.
+REGIONS = np.array([[0, 0, 0, 0, 0, 0, 1.0, 0.4, -0.3, 1.0],
+                    [2, 0, 0, 0.5, 0.5, 0.22, 1.6, 0.1, 0.2, 1.8]], dtype=np.float64)
+
+
+def reference_library():
+    if not pyoracle.Reference.available():
+        pytest.skip("reference checker oracle/_ref not built")
+    lib = pyoracle.Reference().lib
+    lib.wr_write_prepared_tri_mesh.argtypes = [C.c_void_p, C.c_char_p]
+    lib.wr_run_euler_case.argtypes = [
+        C.c_char_p, C.c_char_p, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
+        C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64,
+        C.c_uint64, C.c_uint64, _d, C.c_int64, _u64, _d]
+    return lib
+
+
+def prepared_box(lib, path):
+    tags, xy, tris = meshgen.irregular_box(6)
+    handle = lib.wr_tri_mesh_new(len(tags), tags.ctypes.data_as(C.POINTER(C.c_int64)),
+                                 xy.ctypes.data_as(_d), len(tris),
+                                 tris.ctypes.data_as(C.POINTER(C.c_int64)))
+    assert handle, lib.wr_last_error()
+    try:
+        assert lib.wr_write_prepared_tri_mesh(handle, str(path).encode()) == 0, lib.wr_last_error()
+    finally:
+        lib.wr_tri_mesh_free(handle)
+
+
+def case_arguments(p, limiting):
+    # limiting, sensor threshold, floors, dimensions, p, gamma, cfl, t0, t1,
+    # max steps, history / visualization / checkpoint intervals, kept checkpoints
+    return (int(limiting), 1e-4, 1e-10, 1e-10, 2, p, 1.4, 0.2, 0.0, 0.03, 10000, 1, 4, 4, 2)
+
+
+def run_reference(lib, mesh, out, p, limiting):
+    steps, time = C.c_uint64(), C.c_double()
+    rc = lib.wr_run_euler_case(str(mesh).encode(), str(out).encode(), *case_arguments(p, limiting),
+                               REGIONS.ctypes.data_as(_d), len(REGIONS), C.byref(steps),
+                               C.byref(time))
+    assert rc == 0, lib.wr_last_error()
+    return steps.value, time.value
+
+
+def tree(directory):
+    out = {}
+    for name in sorted(os.listdir(directory)):
+        with open(os.path.join(directory, name), "rb") as f:
+            out[name] = f.read()
+    return out
+
+
+def test_reference_case_run_writes_its_run_directory(tmp_path):
+    """The checker side on the CPU: the reference's run_euler_case from flat
+    arguments runs to t = 0.03 and writes history, snapshots and checkpoints."""
+    lib = reference_library()
+    mesh = tmp_path / "box.mesh"
+    prepared_box(lib, mesh)
+    steps, time = run_reference(lib, mesh, tmp_path / "cpu", 2, True)
+    assert steps > 4 and time == 0.03
+    names = os.listdir(tmp_path / "cpu")
+    assert "history.csv" in names and "solution.pvd" in names
+    assert sum(n.startswith("checkpoint") for n in names) == 2
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("p,limiting", [(1, False), (2, True), (3, True)])
+def test_reference_run_loop_drives_the_gpu_model(tmp_path, p, limiting):
+    lib = reference_library()
+    if not os.path.exists(GPU_CASE):
+        pytest.skip("oracle/_ref/libwasl_case_gpu.so not built")
+    gpu = C.CDLL(GPU_CASE)
+    gpu.wasl_run_euler_case_gpu.argtypes = [
+        C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, C.c_double, C.c_double, C.c_double,
+        C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64,
+        C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, _d, C.c_size_t, C.c_int, _u64, _d,
+        C.c_char_p, C.c_size_t]
+    mesh = tmp_path / "box.mesh"
+    prepared_box(lib, mesh)
+    cpu = run_reference(lib, mesh, tmp_path / "cpu", p, limiting)
+    steps, time = C.c_uint64(), C.c_double()
+    err = C.create_string_buffer(512)
+    args = case_arguments(p, limiting)
+    rc = gpu.wasl_run_euler_case_gpu(str(mesh).encode(), str(tmp_path / "gpu").encode(), None,
+                                     *args[:2], args[2], args[3], *args[4:],
+                                     REGIONS.ctypes.data_as(_d), len(REGIONS), 0,
+                                     C.byref(steps), C.byref(time), err, len(err))
+    assert rc == 0, err.value.decode()
+    assert (steps.value, time.value) == cpu
+    a, b = tree(tmp_path / "cpu"), tree(tmp_path / "gpu")
+    assert list(a) == list(b)
+    for name in a:
+        assert a[name] == b[name], name

@@ -1,0 +1,185 @@
+// GpuEulerTriangleModel and run_euler_case_gpu (see serial_case_model.hpp).
+#include "serial_case_model.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <exception>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "case/euler_drivers.hpp"
+#include "wasl/basis/mode_count.hpp"
+#include "wasl/case/case_validation.hpp"
+#include "wasl/case/initial_state.hpp"
+#include "wasl/equations/euler/euler.hpp"
+#include "wasl/mesh/prepared/mesh_from_prepared.hpp"
+
+namespace wasl_b200 {
+
+GpuEulerTriangleModel::GpuEulerTriangleModel(const wasl::EulerCase &config,
+                                             const wasl::CaseMesh &mesh, int precision)
+    : config_(config), triangles_(wasl::triangle_mesh_from_prepared(mesh.prepared)) {
+  // The handle takes the mesh as node tags, coordinates and element nodes, in
+  // the triangles' own element and node order (it normalizes them as the
+  // reference does, so faces come out in the reference's order).
+  std::map<std::int64_t, std::pair<double, double>> nodes;
+  std::vector<std::int64_t> element_nodes;
+  element_nodes.reserve(3 * triangles_.elements.size());
+  for (const auto &el : triangles_.elements) {
+    const std::int64_t tags[3] = {el.node0, el.node1, el.node2};
+    const double xy[3][2] = {{el.x0, el.y0}, {el.x1, el.y1}, {el.x2, el.y2}};
+    for (int k = 0; k < 3; ++k) {
+      nodes.emplace(tags[k], std::make_pair(xy[k][0], xy[k][1]));
+      element_nodes.push_back(tags[k]);
+    }
+  }
+  std::vector<std::int64_t> node_tags;
+  std::vector<double> coordinates;
+  for (const auto &[tag, xy] : nodes) {
+    node_tags.push_back(tag);
+    coordinates.push_back(xy.first);
+    coordinates.push_back(xy.second);
+  }
+
+  wasl_gpu_config cfg;
+  wasl_gpu_config_default(&cfg);
+  cfg.dimensions = 2;
+  cfg.equation = WASL_EULER;
+  cfg.polynomial_order = config.polynomial_order;
+  cfg.heat_capacity_ratio = config.heat_capacity_ratio;
+  cfg.limiting = config.limiting ? 1 : 0;
+  cfg.sensor_threshold = config.sensor_threshold;
+  cfg.density_floor = config.density_floor;
+  cfg.pressure_floor = config.pressure_floor;
+  cfg.precision = precision;
+  char error[512] = {0};
+  if (wasl_gpu_create(&cfg, static_cast<std::int64_t>(node_tags.size()), node_tags.data(),
+                      coordinates.data(), static_cast<std::int64_t>(triangles_.elements.size()),
+                      element_nodes.data(), &gpu_, error, sizeof error) != 0)
+    throw std::runtime_error(error);
+
+  const wasl::Euler equation{config.heat_capacity_ratio};
+  const double cfl = config.cfl;
+  model_.variable_count = wasl::Euler::variable_count;
+  model_.mode_count = wasl::triangle_mode_count(config.polynomial_order);
+  // Layouts, mass and cell averages are host work on the state of record:
+  // the reference's own operations.
+  wasl::add_euler_state_operations(model_, triangles_);
+  const auto size = [](const wasl::SerialCaseModel::State &s) {
+    return static_cast<std::int64_t>(s.size());
+  };
+  model_.initial_state = [this, equation, size] {
+    auto state = wasl::initial_coefficients(triangles_, config_, equation);
+    check(wasl_gpu_set_state(gpu_, state.data(), size(state)));
+    check(wasl_gpu_limit(gpu_)); // the reference limits the projected state
+    check(wasl_gpu_get_state(gpu_, state.data(), size(state)));
+    return state;
+  };
+  model_.stable_time_step = [this, cfl, size](const wasl::SerialCaseModel::State &state) {
+    double dt = 0.0;
+    check(wasl_gpu_set_state(gpu_, state.data(), size(state)));
+    check(wasl_gpu_stable_dt(gpu_, cfl, &dt));
+    return dt;
+  };
+  model_.advance = [this, size](double dt, wasl::SerialCaseModel::State &state,
+                                wasl::SspRk3Workspace &) {
+    check(wasl_gpu_set_state(gpu_, state.data(), size(state)));
+    check(wasl_gpu_step(gpu_, dt));
+    check(wasl_gpu_get_state(gpu_, state.data(), size(state)));
+  };
+}
+
+GpuEulerTriangleModel::~GpuEulerTriangleModel() { wasl_gpu_destroy(gpu_); }
+
+void GpuEulerTriangleModel::check(int status) const {
+  if (status != 0)
+    throw std::runtime_error(wasl_gpu_last_error(gpu_));
+}
+
+wasl::SimulationSummary run_euler_case_gpu(const wasl::EulerCase &config, int precision) {
+  wasl::validate_euler_case(config);
+  if (config.dimensions != 2)
+    throw std::invalid_argument("run_euler_case_gpu: a triangle mesh (dimensions 2) is needed");
+  if (!config.boundaries.empty() &&
+      !std::all_of(config.boundaries.begin(), config.boundaries.end(), [](const auto &b) {
+        return b.condition.kind == wasl::BoundaryKind::periodic;
+      }))
+    throw std::runtime_error("simulation: 2D Euler boundaries must be periodic");
+  const auto mesh = wasl::load_case_mesh(config.files.prepared_mesh, config.dimensions);
+  const GpuEulerTriangleModel gpu(config, mesh, precision);
+  return wasl::run_serial_case(config.files, config.run, mesh, gpu.model());
+}
+
+wasl::EulerCase euler_case_from_arguments(const char *prepared_mesh, const char *output_directory,
+                                          const char *restart, int limiting,
+                                          double sensor_threshold, double density_floor,
+                                          double pressure_floor, int dimensions,
+                                          int polynomial_order, double heat_capacity_ratio,
+                                          double cfl, double start_time, double end_time,
+                                          std::uint64_t max_steps, std::uint64_t history_interval,
+                                          std::uint64_t visualization_interval,
+                                          std::uint64_t checkpoint_interval,
+                                          std::uint64_t keep_checkpoints, const double *regions,
+                                          std::size_t region_count) {
+  wasl::EulerCase c;
+  c.files = {prepared_mesh, output_directory, restart ? restart : ""};
+  c.run = {start_time,           end_time,           max_steps,       history_interval,
+           visualization_interval, checkpoint_interval, keep_checkpoints};
+  c.limiting = limiting != 0;
+  c.sensor_threshold = sensor_threshold;
+  c.density_floor = density_floor;
+  c.pressure_floor = pressure_floor;
+  c.dimensions = dimensions;
+  c.polynomial_order = polynomial_order;
+  c.heat_capacity_ratio = heat_capacity_ratio;
+  c.cfl = cfl;
+  for (std::size_t i = 0; i < region_count; ++i) {
+    const double *r = regions + 10 * i;
+    wasl::EulerRegion region;
+    const int shape = static_cast<int>(r[0]);
+    region.shape = shape == 1   ? wasl::EulerRegion::Shape::interval
+                   : shape == 2 ? wasl::EulerRegion::Shape::circle
+                                : wasl::EulerRegion::Shape::default_region;
+    region.lower = r[1];
+    region.upper = r[2];
+    region.center_x = r[3];
+    region.center_y = r[4];
+    region.radius = r[5];
+    region.value = {r[6], r[7], r[8], r[9]};
+    c.initial_regions.push_back(region);
+  }
+  return c;
+}
+
+} // namespace wasl_b200
+
+extern "C" int wasl_run_euler_case_gpu(
+    const char *prepared_mesh, const char *output_directory, const char *restart, int limiting,
+    double sensor_threshold, double density_floor, double pressure_floor, int dimensions,
+    int polynomial_order, double heat_capacity_ratio, double cfl, double start_time,
+    double end_time, std::uint64_t max_steps, std::uint64_t history_interval,
+    std::uint64_t visualization_interval, std::uint64_t checkpoint_interval,
+    std::uint64_t keep_checkpoints, const double *regions, std::size_t region_count,
+    int precision, std::uint64_t *steps, double *time, char *error, std::size_t error_length) {
+  try {
+    const auto config = wasl_b200::euler_case_from_arguments(
+        prepared_mesh, output_directory, restart, limiting, sensor_threshold, density_floor,
+        pressure_floor, dimensions, polynomial_order, heat_capacity_ratio, cfl, start_time,
+        end_time, max_steps, history_interval, visualization_interval, checkpoint_interval,
+        keep_checkpoints, regions, region_count);
+    const auto summary = wasl_b200::run_euler_case_gpu(config, precision);
+    if (steps)
+      *steps = summary.step;
+    if (time)
+      *time = summary.time;
+    return 0;
+  } catch (const std::exception &e) {
+    if (error && error_length) {
+      std::strncpy(error, e.what(), error_length - 1);
+      error[error_length - 1] = '\0';
+    }
+    return -2;
+  }
+}
