@@ -495,6 +495,12 @@ int wr_write_prepared_tri_mesh(void *handle, const char *path) {
   });
 }
 
+int wr_write_prepared_line_mesh(void *handle, const char *path) {
+  return guarded([&] {
+    wasl::write_prepared_mesh(path, wasl::prepare_mesh(static_cast<LineHandle *>(handle)->mesh));
+  });
+}
+
 // The reference's run_euler_case (periodic boundaries) from flat arguments;
 // regions are 10 doubles each: shape (0 default, 1 interval, 2 circle),
 // lower, upper, centre x, centre y, radius, density, velocity x, velocity y,

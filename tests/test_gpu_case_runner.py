@@ -19,10 +19,12 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GPU_CASE = os.path.join(ROOT, "oracle", "_ref", "libwasl_case_gpu.so")
 _d, _u64 = C.POINTER(C.c_double), C.POINTER(C.c_uint64)
 
-# A uniform state with a denser, slower disc (shape 2 = circle): the
-# reference case regression's kind of initial data.
-REGIONS = np.array([[0, 0, 0, 0, 0, 0, 1.0, 0.4, -0.3, 1.0],
-                    [2, 0, 0, 0.5, 0.5, 0.22, 1.6, 0.1, 0.2, 1.8]], dtype=np.float64)
+# A uniform state with a denser, slower disc (shape 2 = circle) or interval
+# (shape 1): the reference case regression's kind of initial data.
+REGIONS = {2: np.array([[0, 0, 0, 0, 0, 0, 1.0, 0.4, -0.3, 1.0],
+                        [2, 0, 0, 0.5, 0.5, 0.22, 1.6, 0.1, 0.2, 1.8]], dtype=np.float64),
+           1: np.array([[0, 0, 0, 0, 0, 0, 1.0, 0.4, 0.0, 1.0],
+                        [1, 0.3, 0.6, 0, 0, 0, 0.3, 0.0, 0.0, 0.2]], dtype=np.float64)}
 
 
 def reference_library():
@@ -30,6 +32,7 @@ def reference_library():
         pytest.skip("reference checker oracle/_ref not built")
     lib = pyoracle.Reference().lib
     lib.wr_write_prepared_tri_mesh.argtypes = [C.c_void_p, C.c_char_p]
+    lib.wr_write_prepared_line_mesh.argtypes = [C.c_void_p, C.c_char_p]
     lib.wr_run_euler_case.argtypes = [
         C.c_char_p, C.c_char_p, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
         C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64,
@@ -37,29 +40,37 @@ def reference_library():
     return lib
 
 
-def prepared_box(lib, path):
-    tags, xy, tris = meshgen.irregular_box(6)
-    handle = lib.wr_tri_mesh_new(len(tags), tags.ctypes.data_as(C.POINTER(C.c_int64)),
-                                 xy.ctypes.data_as(_d), len(tris),
-                                 tris.ctypes.data_as(C.POINTER(C.c_int64)))
+def prepared_mesh(lib, path, dims):
+    """The reference's own test meshes (a perturbed box or line), prepared."""
+    i64 = C.POINTER(C.c_int64)
+    if dims == 2:
+        tags, xy, cells = meshgen.irregular_box(6)
+        new, write, free = lib.wr_tri_mesh_new, lib.wr_write_prepared_tri_mesh, lib.wr_tri_mesh_free
+    else:
+        tags, xy, cells = meshgen.irregular_line(16)
+        new, write = lib.wr_line_mesh_new, lib.wr_write_prepared_line_mesh
+        free = lib.wr_line_mesh_free
+    handle = new(len(tags), tags.ctypes.data_as(i64), xy.ctypes.data_as(_d), len(cells),
+                 cells.ctypes.data_as(i64))
     assert handle, lib.wr_last_error()
     try:
-        assert lib.wr_write_prepared_tri_mesh(handle, str(path).encode()) == 0, lib.wr_last_error()
+        assert write(handle, str(path).encode()) == 0, lib.wr_last_error()
     finally:
-        lib.wr_tri_mesh_free(handle)
+        free(handle)
 
 
-def case_arguments(p, limiting):
+def case_arguments(p, limiting, dims=2):
     # limiting, sensor threshold, floors, dimensions, p, gamma, cfl, t0, t1,
     # max steps, history / visualization / checkpoint intervals, kept checkpoints
-    return (int(limiting), 1e-4, 1e-10, 1e-10, 2, p, 1.4, 0.2, 0.0, 0.03, 10000, 1, 4, 4, 2)
+    return (int(limiting), 1e-4, 1e-10, 1e-10, dims, p, 1.4, 0.2, 0.0, 0.03, 10000, 1, 4, 4, 2)
 
 
-def run_reference(lib, mesh, out, p, limiting):
+def run_reference(lib, mesh, out, p, limiting, dims=2):
     steps, time = C.c_uint64(), C.c_double()
-    rc = lib.wr_run_euler_case(str(mesh).encode(), str(out).encode(), *case_arguments(p, limiting),
-                               REGIONS.ctypes.data_as(_d), len(REGIONS), C.byref(steps),
-                               C.byref(time))
+    regions = REGIONS[dims]
+    rc = lib.wr_run_euler_case(str(mesh).encode(), str(out).encode(),
+                               *case_arguments(p, limiting, dims), regions.ctypes.data_as(_d),
+                               len(regions), C.byref(steps), C.byref(time))
     assert rc == 0, lib.wr_last_error()
     return steps.value, time.value
 
@@ -77,7 +88,7 @@ def test_reference_case_run_writes_its_run_directory(tmp_path):
     arguments runs to t = 0.03 and writes history, snapshots and checkpoints."""
     lib = reference_library()
     mesh = tmp_path / "box.mesh"
-    prepared_box(lib, mesh)
+    prepared_mesh(lib, mesh, 2)
     steps, time = run_reference(lib, mesh, tmp_path / "cpu", 2, True)
     assert steps > 4 and time == 0.03
     names = os.listdir(tmp_path / "cpu")
@@ -86,8 +97,9 @@ def test_reference_case_run_writes_its_run_directory(tmp_path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("p,limiting", [(1, False), (2, True), (3, True)])
-def test_reference_run_loop_drives_the_gpu_model(tmp_path, p, limiting):
+@pytest.mark.parametrize("dims,p,limiting", [(2, 1, False), (2, 2, True), (2, 3, True),
+                                             (1, 2, True), (1, 1, False)])
+def test_reference_run_loop_drives_the_gpu_model(tmp_path, dims, p, limiting):
     lib = reference_library()
     if not os.path.exists(GPU_CASE):
         pytest.skip("oracle/_ref/libwasl_case_gpu.so not built")
@@ -97,15 +109,15 @@ def test_reference_run_loop_drives_the_gpu_model(tmp_path, p, limiting):
         C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64,
         C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, _d, C.c_size_t, C.c_int, _u64, _d,
         C.c_char_p, C.c_size_t]
-    mesh = tmp_path / "box.mesh"
-    prepared_box(lib, mesh)
-    cpu = run_reference(lib, mesh, tmp_path / "cpu", p, limiting)
+    mesh = tmp_path / "case.mesh"
+    prepared_mesh(lib, mesh, dims)
+    cpu = run_reference(lib, mesh, tmp_path / "cpu", p, limiting, dims)
     steps, time = C.c_uint64(), C.c_double()
     err = C.create_string_buffer(512)
-    args = case_arguments(p, limiting)
+    regions = REGIONS[dims]
     rc = gpu.wasl_run_euler_case_gpu(str(mesh).encode(), str(tmp_path / "gpu").encode(), None,
-                                     *args[:2], args[2], args[3], *args[4:],
-                                     REGIONS.ctypes.data_as(_d), len(REGIONS), 0,
+                                     *case_arguments(p, limiting, dims),
+                                     regions.ctypes.data_as(_d), len(regions), 0,
                                      C.byref(steps), C.byref(time), err, len(err))
     assert rc == 0, err.value.decode()
     assert (steps.value, time.value) == cpu

@@ -1,4 +1,4 @@
-// GpuEulerTriangleModel and run_euler_case_gpu (see serial_case_model.hpp).
+// GpuEulerModel and run_euler_case_gpu (see serial_case_model.hpp).
 #include "serial_case_model.hpp"
 
 #include <algorithm>
@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "case/euler_drivers.hpp"
+#include "case/line_boundary_resolution.hpp"
 #include "wasl/basis/mode_count.hpp"
 #include "wasl/case/case_validation.hpp"
 #include "wasl/case/initial_state.hpp"
@@ -18,21 +19,47 @@
 
 namespace wasl_b200 {
 
-GpuEulerTriangleModel::GpuEulerTriangleModel(const wasl::EulerCase &config,
-                                             const wasl::CaseMesh &mesh, int precision)
-    : config_(config), triangles_(wasl::triangle_mesh_from_prepared(mesh.prepared)) {
+GpuEulerModel::GpuEulerModel(const wasl::EulerCase &config, const wasl::CaseMesh &mesh,
+                             int precision)
+    : config_(config) {
   // The handle takes the mesh as node tags, coordinates and element nodes, in
-  // the triangles' own element and node order (it normalizes them as the
+  // the mesh's own element and node order (it normalizes them as the
   // reference does, so faces come out in the reference's order).
+  wasl_gpu_config cfg;
+  wasl_gpu_config_default(&cfg);
+  cfg.dimensions = config.dimensions;
   std::map<std::int64_t, std::pair<double, double>> nodes;
   std::vector<std::int64_t> element_nodes;
-  element_nodes.reserve(3 * triangles_.elements.size());
-  for (const auto &el : triangles_.elements) {
-    const std::int64_t tags[3] = {el.node0, el.node1, el.node2};
-    const double xy[3][2] = {{el.x0, el.y0}, {el.x1, el.y1}, {el.x2, el.y2}};
-    for (int k = 0; k < 3; ++k) {
-      nodes.emplace(tags[k], std::make_pair(xy[k][0], xy[k][1]));
-      element_nodes.push_back(tags[k]);
+  std::size_t elements = 0;
+  if (config.dimensions == 1) {
+    line_ = wasl::line_mesh_from_prepared(mesh.prepared);
+    elements = line_.elements.size();
+    for (const auto &el : line_.elements) {
+      nodes.emplace(el.left_node, std::make_pair(el.x_left, 0.0));
+      nodes.emplace(el.right_node, std::make_pair(el.x_right, 0.0));
+      element_nodes.push_back(el.left_node);
+      element_nodes.push_back(el.right_node);
+    }
+    // Periodic or outflow ends, resolved from the named boundaries as the
+    // reference resolves them (inflow is rejected for Euler).
+    const auto ends = wasl::resolve_line_boundaries(mesh.prepared, line_, config.boundaries);
+    const auto kind = [](const wasl::BoundaryCondition &b) {
+      if (b.kind == wasl::BoundaryKind::inflow)
+        throw std::runtime_error("simulation: Euler inflow boundaries are not supported");
+      return b.kind == wasl::BoundaryKind::periodic ? WASL_PERIODIC : WASL_OUTFLOW;
+    };
+    cfg.boundary_left = kind(ends.left);
+    cfg.boundary_right = kind(ends.right);
+  } else {
+    triangles_ = wasl::triangle_mesh_from_prepared(mesh.prepared);
+    elements = triangles_.elements.size();
+    for (const auto &el : triangles_.elements) {
+      const std::int64_t tags[3] = {el.node0, el.node1, el.node2};
+      const double xy[3][2] = {{el.x0, el.y0}, {el.x1, el.y1}, {el.x2, el.y2}};
+      for (int k = 0; k < 3; ++k) {
+        nodes.emplace(tags[k], std::make_pair(xy[k][0], xy[k][1]));
+        element_nodes.push_back(tags[k]);
+      }
     }
   }
   std::vector<std::int64_t> node_tags;
@@ -40,12 +67,10 @@ GpuEulerTriangleModel::GpuEulerTriangleModel(const wasl::EulerCase &config,
   for (const auto &[tag, xy] : nodes) {
     node_tags.push_back(tag);
     coordinates.push_back(xy.first);
-    coordinates.push_back(xy.second);
+    if (config.dimensions == 2)
+      coordinates.push_back(xy.second);
   }
 
-  wasl_gpu_config cfg;
-  wasl_gpu_config_default(&cfg);
-  cfg.dimensions = 2;
   cfg.equation = WASL_EULER;
   cfg.polynomial_order = config.polynomial_order;
   cfg.heat_capacity_ratio = config.heat_capacity_ratio;
@@ -56,22 +81,28 @@ GpuEulerTriangleModel::GpuEulerTriangleModel(const wasl::EulerCase &config,
   cfg.precision = precision;
   char error[512] = {0};
   if (wasl_gpu_create(&cfg, static_cast<std::int64_t>(node_tags.size()), node_tags.data(),
-                      coordinates.data(), static_cast<std::int64_t>(triangles_.elements.size()),
+                      coordinates.data(), static_cast<std::int64_t>(elements),
                       element_nodes.data(), &gpu_, error, sizeof error) != 0)
     throw std::runtime_error(error);
 
   const wasl::Euler equation{config.heat_capacity_ratio};
   const double cfl = config.cfl;
   model_.variable_count = wasl::Euler::variable_count;
-  model_.mode_count = wasl::triangle_mode_count(config.polynomial_order);
+  model_.mode_count = config.dimensions == 1 ? wasl::line_mode_count(config.polynomial_order)
+                                             : wasl::triangle_mode_count(config.polynomial_order);
   // Layouts, mass and cell averages are host work on the state of record:
   // the reference's own operations.
-  wasl::add_euler_state_operations(model_, triangles_);
+  if (config.dimensions == 1)
+    wasl::add_euler_state_operations(model_, line_);
+  else
+    wasl::add_euler_state_operations(model_, triangles_);
   const auto size = [](const wasl::SerialCaseModel::State &s) {
     return static_cast<std::int64_t>(s.size());
   };
   model_.initial_state = [this, equation, size] {
-    auto state = wasl::initial_coefficients(triangles_, config_, equation);
+    auto state = config_.dimensions == 1
+                     ? wasl::initial_coefficients(line_, config_, equation)
+                     : wasl::initial_coefficients(triangles_, config_, equation);
     check(wasl_gpu_set_state(gpu_, state.data(), size(state)));
     check(wasl_gpu_limit(gpu_)); // the reference limits the projected state
     check(wasl_gpu_get_state(gpu_, state.data(), size(state)));
@@ -91,24 +122,19 @@ GpuEulerTriangleModel::GpuEulerTriangleModel(const wasl::EulerCase &config,
   };
 }
 
-GpuEulerTriangleModel::~GpuEulerTriangleModel() { wasl_gpu_destroy(gpu_); }
+GpuEulerModel::~GpuEulerModel() { wasl_gpu_destroy(gpu_); }
 
-void GpuEulerTriangleModel::check(int status) const {
+void GpuEulerModel::check(int status) const {
   if (status != 0)
     throw std::runtime_error(wasl_gpu_last_error(gpu_));
 }
 
 wasl::SimulationSummary run_euler_case_gpu(const wasl::EulerCase &config, int precision) {
   wasl::validate_euler_case(config);
-  if (config.dimensions != 2)
-    throw std::invalid_argument("run_euler_case_gpu: a triangle mesh (dimensions 2) is needed");
-  if (!config.boundaries.empty() &&
-      !std::all_of(config.boundaries.begin(), config.boundaries.end(), [](const auto &b) {
-        return b.condition.kind == wasl::BoundaryKind::periodic;
-      }))
+  if (config.dimensions == 2 && !wasl::all_periodic(config.boundaries))
     throw std::runtime_error("simulation: 2D Euler boundaries must be periodic");
   const auto mesh = wasl::load_case_mesh(config.files.prepared_mesh, config.dimensions);
-  const GpuEulerTriangleModel gpu(config, mesh, precision);
+  const GpuEulerModel gpu(config, mesh, precision);
   return wasl::run_serial_case(config.files, config.run, mesh, gpu.model());
 }
 

@@ -4,12 +4,12 @@
 // (cpp/src/case/serial_case_runner.cpp:107-149), which owns time, restart,
 // history, snapshots and checkpoint rotation, and calls a SerialCaseModel
 // (cpp/include/wasl/case/serial_case_runner.hpp:22-34) for the numerics.
-// GpuEulerTriangleModel is that model with its numerics on the GPU through the
-// C-ABI (include/wasl_b200.h): the host vector stays the state of record, and
-// each stable_time_step / advance copies it in and out.  run_euler_case_gpu is
-// run_euler_case (cpp/src/case/euler_case.cpp:7-11, the 2D branch
-// cpp/src/case/euler_triangle.cpp:15-50) with this model: same validation,
-// files and outputs.  This file builds against the reference's headers and
+// GpuEulerModel is that model with its numerics on the GPU through the C-ABI
+// (include/wasl_b200.h), on a line or triangle mesh: the host vector stays the
+// state of record, and each stable_time_step / advance copies it in and out.
+// run_euler_case_gpu is run_euler_case (cpp/src/case/euler_case.cpp:7-11, with
+// cpp/src/case/euler_line.cpp:14-47 and cpp/src/case/euler_triangle.cpp:15-50)
+// with this model: same validation, boundaries, files and outputs.  This file builds against the reference's headers and
 // library; it is the piece a maintainer adds to the reference's tree.
 #pragma once
 
@@ -20,18 +20,19 @@
 #include "wasl/case/euler_case.hpp"
 #include "wasl/case/serial_case_runner.hpp"
 #include "wasl/case/simulation_summary.hpp"
+#include "wasl/mesh/line/line_mesh.hpp"
 #include "wasl/mesh/triangle/triangle_mesh.hpp"
 #include "wasl_b200.h"
 
 namespace wasl_b200 {
 
-class GpuEulerTriangleModel {
+class GpuEulerModel {
 public:
   // precision: enum wasl_precision (WASL_PLAIN_FP64 is the bit-consistent drop-in).
-  GpuEulerTriangleModel(const wasl::EulerCase &config, const wasl::CaseMesh &mesh, int precision);
-  ~GpuEulerTriangleModel();
-  GpuEulerTriangleModel(const GpuEulerTriangleModel &) = delete;
-  GpuEulerTriangleModel &operator=(const GpuEulerTriangleModel &) = delete;
+  GpuEulerModel(const wasl::EulerCase &config, const wasl::CaseMesh &mesh, int precision);
+  ~GpuEulerModel();
+  GpuEulerModel(const GpuEulerModel &) = delete;
+  GpuEulerModel &operator=(const GpuEulerModel &) = delete;
 
   const wasl::SerialCaseModel &model() const { return model_; }
 
@@ -40,14 +41,15 @@ private:
 
   wasl_gpu *gpu_ = nullptr;
   wasl::EulerCase config_;
-  wasl::TriangleMesh triangles_;
+  wasl::LineMesh line_;          // dimensions 1
+  wasl::TriangleMesh triangles_; // dimensions 2
   wasl::SerialCaseModel model_;
 };
 
 wasl::SimulationSummary run_euler_case_gpu(const wasl::EulerCase &config, int precision);
 
 // The bridge's flat run_euler_case arguments (crates/wasl-bridge/include/bridge.hpp:24-32)
-// for a periodic case: each region is 10 doubles (shape 0 default, 1 interval,
+// for a periodic case (empty boundary list): each region is 10 doubles (shape 0 default, 1 interval,
 // 2 circle; lower, upper, centre x, centre y, radius; density, velocity x,
 // velocity y, pressure).
 wasl::EulerCase euler_case_from_arguments(const char *prepared_mesh, const char *output_directory,
