@@ -21,6 +21,7 @@
 
 #include "wasl/boundaries/line_boundary_conditions.hpp"
 #include "wasl/case/euler_case.hpp"
+#include "wasl/case/scalar_advection_case.hpp"
 #include "wasl/mesh/prepared/prepare_mesh.hpp"
 #include "wasl/boundaries/line_euler_exterior.hpp"
 #include "wasl/boundaries/periodic_triangle_trace.hpp"
@@ -540,6 +541,43 @@ int wr_run_euler_case(const char *prepared_mesh, const char *output_directory, i
       c.initial_regions.push_back(region);
     }
     const auto summary = wasl::run_euler_case(c);
+    *steps = summary.step;
+    *time = summary.time;
+  });
+}
+
+// The reference's run_scalar_advection_case (serial, periodic) from flat
+// arguments: intervals 3 doubles each (lower, upper, value), circles 4
+// (centre x, centre y, radius, value).
+int wr_run_scalar_advection_case(const char *prepared_mesh, const char *output_directory,
+                                 int dimensions, int p, double vx, double vy, double cfl,
+                                 double start_time, double end_time, std::uint64_t max_steps,
+                                 std::uint64_t history_interval,
+                                 std::uint64_t visualization_interval,
+                                 std::uint64_t checkpoint_interval, std::uint64_t keep_checkpoints,
+                                 double initial_default, int initial_sine, double sine_amplitude,
+                                 const double *intervals, std::int64_t interval_count,
+                                 const double *circles, std::int64_t circle_count,
+                                 std::uint64_t *steps, double *time) {
+  return guarded([&] {
+    wasl::ScalarAdvectionCase c;
+    c.files = {prepared_mesh, output_directory, ""};
+    c.run = {start_time,           end_time,          max_steps,       history_interval,
+             visualization_interval, checkpoint_interval, keep_checkpoints};
+    c.dimensions = dimensions;
+    c.polynomial_order = p;
+    c.wavespeed = vx;
+    c.velocity_y = vy;
+    c.cfl = cfl;
+    c.initial_default = initial_default;
+    c.initial_sine = initial_sine != 0;
+    c.initial_sine_amplitude = sine_amplitude;
+    for (std::int64_t i = 0; i < interval_count; ++i)
+      c.initial_intervals.push_back({intervals[3 * i], intervals[3 * i + 1], intervals[3 * i + 2]});
+    for (std::int64_t i = 0; i < circle_count; ++i)
+      c.initial_circles.push_back(
+          {circles[4 * i], circles[4 * i + 1], circles[4 * i + 2], circles[4 * i + 3]});
+    const auto summary = wasl::run_scalar_advection_case(c);
     *steps = summary.step;
     *time = summary.time;
   });

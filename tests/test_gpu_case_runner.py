@@ -33,6 +33,10 @@ def reference_library():
     lib = pyoracle.Reference().lib
     lib.wr_write_prepared_tri_mesh.argtypes = [C.c_void_p, C.c_char_p]
     lib.wr_write_prepared_line_mesh.argtypes = [C.c_void_p, C.c_char_p]
+    lib.wr_run_scalar_advection_case.argtypes = [
+        C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+        C.c_double, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64,
+        C.c_double, C.c_int, C.c_double, _d, C.c_int64, _d, C.c_int64, _u64, _d]
     lib.wr_run_euler_case.argtypes = [
         C.c_char_p, C.c_char_p, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
         C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64,
@@ -121,6 +125,57 @@ def test_reference_run_loop_drives_the_gpu_model(tmp_path, dims, p, limiting):
                                      C.byref(steps), C.byref(time), err, len(err))
     assert rc == 0, err.value.decode()
     assert (steps.value, time.value) == cpu
+    a, b = tree(tmp_path / "cpu"), tree(tmp_path / "gpu")
+    assert list(a) == list(b)
+    for name in a:
+        assert a[name] == b[name], name
+
+
+# Scalar advection as the reference's case regression sets it up: a default
+# value, an interval (lower, upper, value) and a circle (centre, radius,
+# value); on lines also the sine start.
+INTERVALS = np.array([[0.2, 0.55, 1.0]])
+CIRCLES = np.array([[0.5, 0.4, 0.25, 2.0]])
+
+
+def scalar_arguments(dims, p):
+    # dimensions, p, velocity x, velocity y, cfl, t0, t1, max steps, history /
+    # visualization / checkpoint intervals, kept checkpoints, default value,
+    # sine start, sine amplitude
+    return (dims, p, 0.7, -0.4 if dims == 2 else 0.0, 0.3, 0.0, 0.2, 10000, 3, 4, 5, 2, 0.25,
+            int(dims == 1 and p == 2), 1.5)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims,p", [(1, 2), (1, 3), (2, 1), (2, 2)])
+def test_reference_run_loop_drives_the_gpu_scalar_model(tmp_path, dims, p):
+    lib = reference_library()
+    if not os.path.exists(GPU_CASE):
+        pytest.skip("oracle/_ref/libwasl_case_gpu.so not built")
+    gpu = C.CDLL(GPU_CASE)
+    gpu.wasl_run_scalar_advection_case_gpu.argtypes = [
+        C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.c_double, C.c_double,
+        C.c_double, C.c_double, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64,
+        C.c_uint64, C.c_double, C.c_int, C.c_double, _d, C.c_size_t, _d, C.c_size_t, _u64, _d,
+        C.c_char_p, C.c_size_t]
+    mesh = tmp_path / "case.mesh"
+    prepared_mesh(lib, mesh, dims)
+    args = scalar_arguments(dims, p)
+    regions = (INTERVALS.ctypes.data_as(_d), len(INTERVALS), CIRCLES.ctypes.data_as(_d),
+               len(CIRCLES))
+    cpu_steps, cpu_time = C.c_uint64(), C.c_double()
+    rc = lib.wr_run_scalar_advection_case(str(mesh).encode(), str(tmp_path / "cpu").encode(),
+                                          *args, *regions, C.byref(cpu_steps),
+                                          C.byref(cpu_time))
+    assert rc == 0, lib.wr_last_error()
+    steps, time = C.c_uint64(), C.c_double()
+    err = C.create_string_buffer(512)
+    rc = gpu.wasl_run_scalar_advection_case_gpu(str(mesh).encode(),
+                                                str(tmp_path / "gpu").encode(), None, *args,
+                                                *regions, C.byref(steps), C.byref(time), err,
+                                                len(err))
+    assert rc == 0, err.value.decode()
+    assert (steps.value, time.value) == (cpu_steps.value, cpu_time.value)
     a, b = tree(tmp_path / "cpu"), tree(tmp_path / "gpu")
     assert list(a) == list(b)
     for name in a:

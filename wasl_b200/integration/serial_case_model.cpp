@@ -11,6 +11,7 @@
 
 #include "case/euler_drivers.hpp"
 #include "case/line_boundary_resolution.hpp"
+#include "case/scalar_advection_drivers.hpp"
 #include "wasl/basis/mode_count.hpp"
 #include "wasl/case/case_validation.hpp"
 #include "wasl/case/initial_state.hpp"
@@ -138,6 +139,107 @@ wasl::SimulationSummary run_euler_case_gpu(const wasl::EulerCase &config, int pr
   return wasl::run_serial_case(config.files, config.run, mesh, gpu.model());
 }
 
+GpuScalarAdvectionModel::GpuScalarAdvectionModel(const wasl::ScalarAdvectionCase &config,
+                                                 const wasl::CaseMesh &mesh)
+    : config_(config) {
+  wasl_gpu_config cfg;
+  wasl_gpu_config_default(&cfg);
+  cfg.dimensions = config.dimensions;
+  cfg.equation = WASL_SCALAR_ADVECTION;
+  cfg.polynomial_order = config.polynomial_order;
+  cfg.velocity_x = config.wavespeed;
+  cfg.velocity_y = config.velocity_y;
+  std::map<std::int64_t, std::pair<double, double>> nodes;
+  std::vector<std::int64_t> element_nodes;
+  std::size_t elements = 0;
+  if (config.dimensions == 1) {
+    line_ = wasl::line_mesh_from_prepared(mesh.prepared);
+    elements = line_.elements.size();
+    for (const auto &el : line_.elements) {
+      nodes.emplace(el.left_node, std::make_pair(el.x_left, 0.0));
+      nodes.emplace(el.right_node, std::make_pair(el.x_right, 0.0));
+      element_nodes.push_back(el.left_node);
+      element_nodes.push_back(el.right_node);
+    }
+    const auto ends = wasl::resolve_line_boundaries(mesh.prepared, line_, config.boundaries);
+    const auto kind = [](const wasl::BoundaryCondition &b) {
+      return b.kind == wasl::BoundaryKind::periodic  ? WASL_PERIODIC
+             : b.kind == wasl::BoundaryKind::inflow ? WASL_INFLOW
+                                                    : WASL_OUTFLOW;
+    };
+    cfg.boundary_left = kind(ends.left);
+    cfg.boundary_right = kind(ends.right);
+    cfg.inflow_left = ends.left.value;
+    cfg.inflow_right = ends.right.value;
+  } else {
+    triangles_ = wasl::triangle_mesh_from_prepared(mesh.prepared);
+    elements = triangles_.elements.size();
+    for (const auto &el : triangles_.elements) {
+      const std::int64_t tags[3] = {el.node0, el.node1, el.node2};
+      const double xy[3][2] = {{el.x0, el.y0}, {el.x1, el.y1}, {el.x2, el.y2}};
+      for (int k = 0; k < 3; ++k) {
+        nodes.emplace(tags[k], std::make_pair(xy[k][0], xy[k][1]));
+        element_nodes.push_back(tags[k]);
+      }
+    }
+  }
+  std::vector<std::int64_t> node_tags;
+  std::vector<double> coordinates;
+  for (const auto &[tag, xy] : nodes) {
+    node_tags.push_back(tag);
+    coordinates.push_back(xy.first);
+    if (config.dimensions == 2)
+      coordinates.push_back(xy.second);
+  }
+  char error[512] = {0};
+  if (wasl_gpu_create(&cfg, static_cast<std::int64_t>(node_tags.size()), node_tags.data(),
+                      coordinates.data(), static_cast<std::int64_t>(elements),
+                      element_nodes.data(), &gpu_, error, sizeof error) != 0)
+    throw std::runtime_error(error);
+  check(wasl_gpu_stable_dt(gpu_, config.cfl, &step_)); // independent of the state
+
+  model_.variable_count = 1;
+  model_.mode_count = config.dimensions == 1 ? wasl::line_mode_count(config.polynomial_order)
+                                             : wasl::triangle_mode_count(config.polynomial_order);
+  if (config.dimensions == 1)
+    wasl::add_scalar_state_operations(model_, line_);
+  else
+    wasl::add_scalar_state_operations(model_, triangles_);
+  model_.initial_state = [this] {
+    return config_.dimensions == 1 ? wasl::initial_coefficients(line_, config_)
+                                   : wasl::initial_coefficients(triangles_, config_);
+  };
+  model_.stable_time_step = [this](const wasl::SerialCaseModel::State &) { return step_; };
+  model_.advance = [this](double dt, wasl::SerialCaseModel::State &state,
+                          wasl::SspRk3Workspace &) {
+    // The handle holds U[mode][element], the reference's checkpoint layout.
+    auto persisted = model_.to_checkpoint(state);
+    const auto n = static_cast<std::int64_t>(persisted.size());
+    check(wasl_gpu_set_state(gpu_, persisted.data(), n));
+    check(wasl_gpu_step(gpu_, dt));
+    check(wasl_gpu_get_state(gpu_, persisted.data(), n));
+    state = model_.from_checkpoint(persisted);
+  };
+}
+
+GpuScalarAdvectionModel::~GpuScalarAdvectionModel() { wasl_gpu_destroy(gpu_); }
+
+void GpuScalarAdvectionModel::check(int status) const {
+  if (status != 0)
+    throw std::runtime_error(wasl_gpu_last_error(gpu_));
+}
+
+wasl::SimulationSummary run_scalar_advection_case_gpu(const wasl::ScalarAdvectionCase &config) {
+  wasl::validate_scalar_advection_case(config);
+  if (config.mpi)
+    throw std::runtime_error("run_scalar_advection_case_gpu: MPI runs are not on the GPU path");
+  if (config.dimensions == 2 && !wasl::all_periodic(config.boundaries))
+    throw std::runtime_error("simulation: 2D scalar-advection boundaries must be periodic");
+  const auto mesh = wasl::load_case_mesh(config.files.prepared_mesh, config.dimensions);
+  const GpuScalarAdvectionModel gpu(config, mesh);
+  return wasl::run_serial_case(config.files, config.run, mesh, gpu.model());
+}
+
 wasl::EulerCase euler_case_from_arguments(const char *prepared_mesh, const char *output_directory,
                                           const char *restart, int limiting,
                                           double sensor_threshold, double density_floor,
@@ -196,6 +298,48 @@ extern "C" int wasl_run_euler_case_gpu(
         end_time, max_steps, history_interval, visualization_interval, checkpoint_interval,
         keep_checkpoints, regions, region_count);
     const auto summary = wasl_b200::run_euler_case_gpu(config, precision);
+    if (steps)
+      *steps = summary.step;
+    if (time)
+      *time = summary.time;
+    return 0;
+  } catch (const std::exception &e) {
+    if (error && error_length) {
+      std::strncpy(error, e.what(), error_length - 1);
+      error[error_length - 1] = '\0';
+    }
+    return -2;
+  }
+}
+
+extern "C" int wasl_run_scalar_advection_case_gpu(
+    const char *prepared_mesh, const char *output_directory, const char *restart,
+    int dimensions, int polynomial_order, double velocity_x, double velocity_y, double cfl,
+    double start_time, double end_time, std::uint64_t max_steps, std::uint64_t history_interval,
+    std::uint64_t visualization_interval, std::uint64_t checkpoint_interval,
+    std::uint64_t keep_checkpoints, double initial_default, int initial_sine,
+    double initial_sine_amplitude, const double *intervals, std::size_t interval_count,
+    const double *circles, std::size_t circle_count, std::uint64_t *steps, double *time,
+    char *error, std::size_t error_length) {
+  try {
+    wasl::ScalarAdvectionCase c;
+    c.files = {prepared_mesh, output_directory, restart ? restart : ""};
+    c.run = {start_time,           end_time,           max_steps,       history_interval,
+             visualization_interval, checkpoint_interval, keep_checkpoints};
+    c.dimensions = dimensions;
+    c.polynomial_order = polynomial_order;
+    c.wavespeed = velocity_x;
+    c.velocity_y = velocity_y;
+    c.cfl = cfl;
+    c.initial_default = initial_default;
+    c.initial_sine = initial_sine != 0;
+    c.initial_sine_amplitude = initial_sine_amplitude;
+    for (std::size_t i = 0; i < interval_count; ++i)
+      c.initial_intervals.push_back({intervals[3 * i], intervals[3 * i + 1], intervals[3 * i + 2]});
+    for (std::size_t i = 0; i < circle_count; ++i)
+      c.initial_circles.push_back(
+          {circles[4 * i], circles[4 * i + 1], circles[4 * i + 2], circles[4 * i + 3]});
+    const auto summary = wasl_b200::run_scalar_advection_case_gpu(c);
     if (steps)
       *steps = summary.step;
     if (time)
