@@ -180,3 +180,30 @@ def test_reference_run_loop_drives_the_gpu_scalar_model(tmp_path, dims, p):
     assert list(a) == list(b)
     for name in a:
         assert a[name] == b[name], name
+
+
+def test_case_twins_report_no_device_as_a_status(tmp_path):
+    """Without a usable GPU the case twins return a status and a message, as
+    the handle's entry points do, instead of failing the process."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    lib = reference_library()
+    if not os.path.exists(GPU_CASE):
+        pytest.skip("oracle/_ref/libwasl_case_gpu.so not built")
+    gpu = C.CDLL(GPU_CASE)
+    mesh = tmp_path / "case.mesh"
+    prepared_mesh(lib, mesh, 2)
+    err = C.create_string_buffer(512)
+    steps, time = C.c_uint64(), C.c_double()
+    regions = REGIONS[2]
+    gpu.wasl_run_euler_case_gpu.argtypes = [
+        C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, C.c_double, C.c_double, C.c_double,
+        C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64,
+        C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, _d, C.c_size_t, C.c_int, _u64, _d,
+        C.c_char_p, C.c_size_t]
+    rc = gpu.wasl_run_euler_case_gpu(str(mesh).encode(), str(tmp_path / "gpu").encode(), None,
+                                     *case_arguments(2, True), regions.ctypes.data_as(_d),
+                                     len(regions), 0, C.byref(steps), C.byref(time), err,
+                                     len(err))
+    assert rc == -2 and err.value
