@@ -374,7 +374,9 @@ def kernel_description(tuning):
              "tile 128 el/CTA, uncapped regs", "tile 256 el/CTA, <=128 regs",
              "tile 64 el/CTA, <=128 regs", "shared-face tile 64 el/CTA, 7 CTAs/SM",
              "shared-face tile 96 el/CTA, 5 CTAs/SM", "shared-face tile 128 el/CTA, 4 CTAs/SM",
-             "shared-face tile 128 el/CTA, 3 CTAs/SM"]
+             "shared-face tile 128 el/CTA, 3 CTAs/SM", "patch 128 el/CTA, <=128 regs",
+             "patch 128 el/CTA, 5 CTAs/SM", "patch 64 el/CTA, 8 CTAs/SM",
+             "patch 64 el/CTA, 10 CTAs/SM"]
     if choice < 0:
         return {"name": "single stage kernel"}
     out = {"name": names[choice] if choice < len(names) else str(choice)}

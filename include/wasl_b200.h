@@ -80,10 +80,17 @@ typedef struct {
                                 rule, p..p+2; 0 = p+2, the reference residual's rule */
   int mixed_kernel;          /* mixed form: 0 autotuned; 1 face-centric kernels (face pass
                                 + element pass); 2 + s the fused tile kernel in launch
-                                shape s (0..7, see wasl_gpu_tuning) */
+                                shape s (0..11, see wasl_gpu_tuning) */
   int positivity_all;        /* with limiting: 1 applies the positivity limiter to every
                                 element, not only troubled ones (not the reference's
                                 behaviour, cpp/src/limiting/euler_modal_limiter.cpp:81-96) */
+  int element_order;         /* 2D Euler mixed form: 0 stores the elements along a Morton
+                                curve of their centroids (tiles of consecutive elements
+                                are compact), 1 in the caller's order.  Either way every
+                                face and element computes the same bits, and every call
+                                that takes or returns per-element data uses the caller's
+                                order; only wasl_gpu_state_device exposes the storage
+                                order (wasl_gpu_element_order) */
 } wasl_gpu_config;
 
 /* Fill the reference's defaults (crates/wasl-bridge/src/config.rs:87-104). */
@@ -179,13 +186,22 @@ int wasl_gpu_sync(wasl_gpu *handle);
  * a thread; 1: 128, no register cap; 2: 256 at <= 128; 3: 64 at <= 128;
  * 4-7: the shared-face tile kernel, which evaluates a face between two
  * elements of one tile once: 4: 64 elements per CTA sized for 7 CTAs per SM;
- * 5: 96 for 5; 6: 128 for 4; 7: 128 for 3);
+ * 5: 96 for 5; 6: 128 for 4; 7: 128 for 3; 8-11: the patch kernel, which
+ * evaluates each element's traces once and each face inside a patch once,
+ * without the limiter only: 8: 128 elements per CTA at <= 128 registers;
+ * 9: 128 sized for 5 CTAs per SM; 10: 64 for 8; 11: 64 for 10);
  * -1 for forms with a single kernel or before the first step.  When the
  * choice was autotuned (mixed_kernel 0: every variant timed on the solver's
  * own state before its first step, the fastest kept for the process per
  * polynomial order, rule order and mesh size class), `ms` receives up to
  * `capacity` per-variant stage times and `count` their number. */
 int wasl_gpu_tuning(const wasl_gpu *handle, int *choice, double *ms, int capacity, int *count);
+
+/* The storage order of the device state (wasl_gpu_state_device): order[i] is
+ * the caller's element stored at column i (count = element count).  The
+ * identity except for the 2D Euler mixed form with element_order 0.  No
+ * counterpart in the reference (its state lives in host vectors). */
+int wasl_gpu_element_order(const wasl_gpu *handle, int64_t *order, int64_t count);
 
 /* Device pointer of the state U[variable][mode][element] and the handle's
  * CUDA stream (cudaStream_t), for callers that keep data on the device. */
@@ -360,13 +376,15 @@ int wasl_batch_stream(wasl_batch *handle, void **stream);
  * U[variable][mode][element] in device memory, `length` the mesh's smallest
  * altitude (or length in 1D), `dt` one double of device memory that receives
  * cfl * length / (max |u|+c over cell averages * (2p+1)), or 0 when that speed
- * is 0; `stream` a cudaStream_t (NULL: the default stream).  The reduction's
- * scratch is a fixed 128 KiB array that every GPU loading the library holds
- * until exit: element_count above 33,554,432 is rejected.  Every call shares
- * that array, so calls whose kernels overlap on one GPU race.  The first call
- * on a device looks up the array's address with that device current; make it
- * before any stream capture.  The call synchronizes `stream` to return a
- * status: WASL_ERR_NONPHYSICAL for a non-physical cell average, with the
+ * is 0: the value wasl_gpu_stable_dt gives for the same state, bit for bit;
+ * `stream` a cudaStream_t (NULL: the default stream).  The reduction's
+ * scratch is a fixed 9.6 KiB array that every GPU loading the library holds
+ * until exit; element_count above 2,147,483,647 is rejected.  Every call
+ * shares that array, so calls whose kernels overlap on one GPU race.  The
+ * first call on a device looks up the array's address with that device
+ * current.  Every call copies the result through the host and synchronizes
+ * `stream`, so it cannot be called while that stream is being captured.  It
+ * returns WASL_ERR_NONPHYSICAL for a non-physical cell average, with the
  * message in `error`. */
 int wasl_cfl_dt_static(const double *state, int64_t element_count, int mode_count, int dimensions,
                        int polynomial_order, double gamma, double cfl, double length, double *dt,

@@ -29,10 +29,11 @@ _u8 = C.POINTER(C.c_uint8)
 
 
 def build(reference_root: str | None = None) -> None:
-    """Compile liboracle.so, and the reference checker when its sources exist."""
+    """Compile liboracle.so, and the reference checker when the reference
+    checkout is given (argument or REF environment variable) and present."""
     subprocess.check_call(["make", "-s", "-C", HERE, "all"])
-    root = reference_root or "/root/reference"
-    if os.path.isdir(os.path.join(root, "cpp", "src")):
+    root = reference_root or os.environ.get("REF")
+    if root and os.path.isdir(os.path.join(root, "cpp", "src")):
         subprocess.check_call(["make", "-s", "-j8", "-C", HERE, "ref", f"REF={root}"])
         if os.path.exists(os.path.join(os.path.dirname(HERE), "wasl_b200", "libwasl_b200.so")):
             subprocess.check_call(["make", "-s", "-C", HERE, "gpu-case", f"REF={root}"])
@@ -525,6 +526,8 @@ class Reference:
         L.wr_euler_line_cfl.argtypes = [vp, C.c_double, _d, C.c_int, C.c_double, _d]
         L.wr_euler_tri_step.argtypes = [vp, _i32, _d, vp, C.c_double, C.c_double, C.c_double,
                                         C.c_double, C.c_int, C.c_double, _d]
+        L.wr_euler_tri_step_ex.argtypes = [vp, C.c_int, _i32, _d, vp, C.c_double, C.c_double,
+                                           C.c_double, C.c_double, C.c_int, C.c_double, _d, _u8]
         L.wr_euler_line_step.argtypes = [vp, C.c_int, C.c_int, vp, C.c_double, C.c_double,
                                          C.c_double, C.c_double, C.c_int, C.c_double, _d]
         L.wr_scalar_line_step.argtypes = [vp, C.c_int, C.c_double, C.c_int, C.c_double,
@@ -618,6 +621,23 @@ class RefTriMesh:
                                         density_floor, pressure_floor, gamma, p, dt, _p(c))
         if rc != 0:
             raise ValueError(self.r.err())
+
+
+    def euler_step_ex(self, gamma, p, dt, c, boundary="periodic", donors=None, basis=None,
+                      stencil=None, threshold=1e-3, density_floor=1e-10, pressure_floor=1e-10):
+        """One SSP-RK3 step in place with the periodic (donors, basis) or the
+        transmissive exterior; returns the per-stage troubled-cell flags
+        [3][ne] when a stencil is given."""
+        kind = {"periodic": 0, "transmissive": 3}[boundary]
+        flags = np.zeros((3, self.ne), np.uint8)
+        st = stencil.h if stencil is not None else None
+        d = _p(donors, _i32) if donors is not None else None
+        b = _p(basis) if basis is not None else None
+        rc = self.lib.wr_euler_tri_step_ex(self.h, kind, d, b, st, threshold, density_floor,
+                                           pressure_floor, gamma, p, dt, _p(c), _p(flags, _u8))
+        if rc != 0:
+            raise ValueError(self.r.err())
+        return flags
 
 
 class RefLineMesh:

@@ -15,6 +15,7 @@
 #include <exception>
 #include <filesystem>
 #include <fstream>
+#include <sstream>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -34,6 +35,7 @@
 #include "wasl/io/prepared_mesh_file.hpp"
 #include "wasl/limiting/euler_limiter_stencil.hpp"
 #include "wasl/limiting/euler_modal_limiter.hpp"
+#include "wasl/limiting/troubled_cell/modal_decay.hpp"
 #include "wasl/mesh/line/build_line_mesh.hpp"
 #include "wasl/mesh/msh/msh_document.hpp"
 #include "wasl/mesh/triangle/build_triangle_mesh.hpp"
@@ -447,6 +449,86 @@ int wr_euler_tri_step(void *handle, const std::int32_t *donors, const double *ba
   });
 }
 
+// wr_euler_tri_step with a choice of exterior and the troubled-cell flag set
+// of each stage.  boundary_kind 0: the periodic exterior from donors/basis;
+// 3: the owner's own trace at every boundary edge point (the harness's 2D
+// transmissive boundary; the reference's 2D cases are periodic only), built
+// with the reference's edge rules, basis and evaluate_euler_state, so it is
+// the left trace the residual itself evaluates.  flags [3][ne] (may be null):
+// per stage, the sensor verdict the limiter reaches on each element, from the
+// reference's modal_energy on the stage state it receives
+// (cpp/src/limiting/euler_modal_limiter.cpp:18-24).
+int wr_euler_tri_step_ex(void *handle, int boundary_kind, const std::int32_t *donors,
+                         const double *basis, void *stencil, double threshold, double rf,
+                         double pf, double gamma, int p, double dt, double *c,
+                         std::uint8_t *flags) {
+  return guarded([&] {
+    const auto &mesh = static_cast<TriHandle *>(handle)->mesh;
+    const std::size_t M = wasl::triangle_mode_count(p), Q = p + 1, F = mesh.faces.size();
+    const std::size_t ne = mesh.num_elements();
+    const wasl::ModalLayout layout{M, ne};
+    wasl::PeriodicTriangleTrace trace;
+    if (boundary_kind == 0) {
+      trace.elements.assign(donors, donors + F * Q);
+      trace.basis.assign(basis, basis + F * Q * M);
+      trace.point_count = static_cast<int>(Q);
+    } else if (boundary_kind != 3) {
+      throw std::invalid_argument("boundary kind must be 0 (periodic) or 3 (transmissive)");
+    }
+    const auto edge_rules = wasl::triangle_edge_rules(p);
+    std::vector<double> edge_basis(M);
+    const wasl::Euler equation{gamma};
+    const wasl::ResidualFunction residual = [&](std::vector<double> &stage,
+                                                std::vector<double> &rhs) {
+      std::vector<double> exterior;
+      if (boundary_kind == 0) {
+        exterior = wasl::periodic_triangle_euler_exterior(trace, stage, ne, M, F);
+      } else {
+        exterior.assign(4 * F * Q, 0.0);
+        for (std::size_t f = 0; f < F; ++f) {
+          const auto &face = mesh.faces[f];
+          if (!face.is_boundary())
+            continue;
+          const auto &rule = edge_rules[static_cast<std::size_t>(face.left_local_edge)];
+          for (std::size_t q = 0; q < Q; ++q) {
+            wasl::dubiner_basis(rule.xi[q], rule.eta[q], p, edge_basis.data());
+            const wasl::EulerConserved s = wasl::evaluate_euler_state(
+                layout, stage.data(), static_cast<std::size_t>(face.left_element),
+                edge_basis.data());
+            for (int v = 0; v < 4; ++v)
+              exterior[(static_cast<std::size_t>(v) * F + f) * Q + q] = wasl::euler_component(s, v);
+          }
+        }
+      }
+      wasl::euler_triangle_residual(mesh, equation, wasl::hllc_flux, p, stage.data(),
+                                    exterior.data(), rhs.data());
+    };
+    int stage_index = 0;
+    const wasl::StateFunction limit = [&](std::vector<double> &state) {
+      if (!stencil)
+        return;
+      const auto &st = static_cast<StencilHandle *>(stencil)->stencil;
+      if (flags) {
+        std::uint8_t *out = flags + static_cast<std::size_t>(stage_index) * ne;
+        for (std::size_t e = 0; e < ne; ++e) {
+          const auto energy = wasl::modal_energy(state.data() + layout.index(0, 0, e), ne,
+                                                 st.mode_count, st.highest_degree_begin);
+          out[e] = st.polynomial_order > 0 &&
+                           !(energy.total == 0.0 || energy.highest_degree / energy.total <= threshold)
+                       ? 1
+                       : 0;
+        }
+      }
+      ++stage_index;
+      wasl::limit_euler_modal(st, equation, threshold, rf, pf, state);
+    };
+    std::vector<double> state(c, c + 4 * M * ne);
+    wasl::SspRk3Workspace workspace;
+    wasl::ssp_rk3_step(dt, residual, limit, state, workspace);
+    std::memcpy(c, state.data(), state.size() * sizeof(double));
+  });
+}
+
 int wr_euler_line_step(void *handle, int left_kind, int right_kind, void *stencil,
                        double threshold, double rf, double pf, double gamma, int p, double dt,
                        double *c) {
@@ -502,20 +584,57 @@ int wr_write_prepared_line_mesh(void *handle, const char *path) {
   });
 }
 
-// The reference's run_euler_case (periodic boundaries) from flat arguments;
-// regions are 10 doubles each: shape (0 default, 1 interval, 2 circle),
-// lower, upper, centre x, centre y, radius, density, velocity x, velocity y,
-// pressure.
-int wr_run_euler_case(const char *prepared_mesh, const char *output_directory, int limiting,
-                      double sensor_threshold, double density_floor, double pressure_floor,
-                      int dimensions, int p, double gamma, double cfl, double start_time,
-                      double end_time, std::uint64_t max_steps, std::uint64_t history_interval,
+// ---- the bridge's coarse functions from C arguments ----------------------------
+//
+// crates/wasl-bridge/src/bridge.cpp:79-216 with rust::Str -> const char *,
+// rust::Slice<T> -> (pointer, length) and the returned rust::String written to
+// `summary`; its argument checks and messages are restated here, since the
+// bridge itself needs the Rust toolchain's cxx headers.  The returned status
+// is 0, or -1 with the message in wr_last_error().
+
+void write_text(const std::string &text, char *out, std::size_t length) {
+  if (out && length) {
+    std::strncpy(out, text.c_str(), length - 1);
+    out[length - 1] = '\0';
+  }
+}
+
+std::string bridge_summary(const wasl::SimulationSummary &summary) {
+  std::ostringstream message;
+  message.precision(17);
+  message << "step=" << summary.step << " time=" << summary.time
+          << " checkpoint=" << summary.checkpoint.string();
+  return message.str();
+}
+
+std::vector<wasl::NamedBoundary> bridge_boundaries(const char *const *names,
+                                                   const std::uint8_t *kinds,
+                                                   const double *values, std::size_t count) {
+  std::vector<wasl::NamedBoundary> boundaries;
+  for (std::size_t i = 0; i < count; ++i) {
+    if (kinds[i] > static_cast<std::uint8_t>(wasl::BoundaryKind::outflow))
+      throw std::runtime_error("boundaries: invalid boundary kind");
+    boundaries.push_back({names[i], {static_cast<wasl::BoundaryKind>(kinds[i]), values[i]}});
+  }
+  return boundaries;
+}
+
+int wr_run_euler_case(const char *mesh_path, const char *output_path, const char *restart_path,
+                      int limiting, double sensor_threshold, double density_floor,
+                      double pressure_floor, int dimensions, int polynomial_order,
+                      double heat_capacity_ratio, double cfl, double start_time, double end_time,
+                      std::uint64_t max_steps, std::uint64_t history_interval,
                       std::uint64_t visualization_interval, std::uint64_t checkpoint_interval,
                       std::uint64_t keep_checkpoints, const double *regions,
-                      std::int64_t region_count, std::uint64_t *steps, double *time) {
+                      std::size_t regions_length, const char *const *boundary_names,
+                      const std::uint8_t *boundary_kinds, const double *boundary_values,
+                      std::size_t boundary_count, char *summary, std::size_t summary_length) {
   return guarded([&] {
+    constexpr std::size_t width = 10;
+    if (regions_length % width != 0)
+      throw std::runtime_error("initial.regions: invalid Euler region data");
     wasl::EulerCase c;
-    c.files = {prepared_mesh, output_directory, ""};
+    c.files = {mesh_path, output_path, restart_path ? restart_path : ""};
     c.run = {start_time,           end_time,          max_steps,       history_interval,
              visualization_interval, checkpoint_interval, keep_checkpoints};
     c.limiting = limiting != 0;
@@ -523,15 +642,16 @@ int wr_run_euler_case(const char *prepared_mesh, const char *output_directory, i
     c.density_floor = density_floor;
     c.pressure_floor = pressure_floor;
     c.dimensions = dimensions;
-    c.polynomial_order = p;
-    c.heat_capacity_ratio = gamma;
+    c.polynomial_order = polynomial_order;
+    c.heat_capacity_ratio = heat_capacity_ratio;
     c.cfl = cfl;
-    for (std::int64_t i = 0; i < region_count; ++i) {
-      const double *r = regions + 10 * i;
+    for (std::size_t i = 0; i < regions_length; i += width) {
+      const double *r = regions + i;
+      const int shape = static_cast<int>(r[0]);
+      if (shape < 0 || shape > 2)
+        throw std::runtime_error("initial.regions: invalid Euler region shape");
       wasl::EulerRegion region;
-      region.shape = r[0] == 1.0   ? wasl::EulerRegion::Shape::interval
-                     : r[0] == 2.0 ? wasl::EulerRegion::Shape::circle
-                                   : wasl::EulerRegion::Shape::default_region;
+      region.shape = static_cast<wasl::EulerRegion::Shape>(shape);
       region.lower = r[1];
       region.upper = r[2];
       region.center_x = r[3];
@@ -540,47 +660,93 @@ int wr_run_euler_case(const char *prepared_mesh, const char *output_directory, i
       region.value = {r[6], r[7], r[8], r[9]};
       c.initial_regions.push_back(region);
     }
-    const auto summary = wasl::run_euler_case(c);
-    *steps = summary.step;
-    *time = summary.time;
+    c.boundaries = bridge_boundaries(boundary_names, boundary_kinds, boundary_values,
+                                     boundary_count);
+    write_text(bridge_summary(wasl::run_euler_case(c)), summary, summary_length);
   });
 }
 
-// The reference's run_scalar_advection_case (serial, periodic) from flat
-// arguments: intervals 3 doubles each (lower, upper, value), circles 4
-// (centre x, centre y, radius, value).
-int wr_run_scalar_advection_case(const char *prepared_mesh, const char *output_directory,
-                                 int dimensions, int p, double vx, double vy, double cfl,
-                                 double start_time, double end_time, std::uint64_t max_steps,
-                                 std::uint64_t history_interval,
-                                 std::uint64_t visualization_interval,
-                                 std::uint64_t checkpoint_interval, std::uint64_t keep_checkpoints,
-                                 double initial_default, int initial_sine, double sine_amplitude,
-                                 const double *intervals, std::int64_t interval_count,
-                                 const double *circles, std::int64_t circle_count,
-                                 std::uint64_t *steps, double *time) {
+int wr_run_scalar_advection_case(
+    const char *mesh_path, const char *output_path, const char *restart_path, int mpi,
+    int dimensions, int polynomial_order, double velocity_x, double velocity_y, double cfl,
+    double start_time, double end_time, std::uint64_t max_steps, std::uint64_t history_interval,
+    std::uint64_t visualization_interval, std::uint64_t checkpoint_interval,
+    std::uint64_t keep_checkpoints, double initial_default, int initial_sine,
+    double initial_sine_amplitude, const double *intervals, std::size_t intervals_length,
+    const double *circles, std::size_t circles_length, const char *const *boundary_names,
+    const std::uint8_t *boundary_kinds, const double *boundary_values,
+    std::size_t boundary_count, char *summary, std::size_t summary_length) {
   return guarded([&] {
+    if (intervals_length % 3 != 0)
+      throw std::runtime_error("initial.regions: invalid interval data");
+    if (circles_length % 4 != 0)
+      throw std::runtime_error("initial.regions: invalid circle data");
     wasl::ScalarAdvectionCase c;
-    c.files = {prepared_mesh, output_directory, ""};
+    c.files = {mesh_path, output_path, restart_path ? restart_path : ""};
     c.run = {start_time,           end_time,          max_steps,       history_interval,
              visualization_interval, checkpoint_interval, keep_checkpoints};
+    c.mpi = mpi != 0;
     c.dimensions = dimensions;
-    c.polynomial_order = p;
-    c.wavespeed = vx;
-    c.velocity_y = vy;
+    c.polynomial_order = polynomial_order;
+    c.wavespeed = velocity_x;
+    c.velocity_y = velocity_y;
     c.cfl = cfl;
     c.initial_default = initial_default;
     c.initial_sine = initial_sine != 0;
-    c.initial_sine_amplitude = sine_amplitude;
-    for (std::int64_t i = 0; i < interval_count; ++i)
-      c.initial_intervals.push_back({intervals[3 * i], intervals[3 * i + 1], intervals[3 * i + 2]});
-    for (std::int64_t i = 0; i < circle_count; ++i)
-      c.initial_circles.push_back(
-          {circles[4 * i], circles[4 * i + 1], circles[4 * i + 2], circles[4 * i + 3]});
-    const auto summary = wasl::run_scalar_advection_case(c);
-    *steps = summary.step;
-    *time = summary.time;
+    c.initial_sine_amplitude = initial_sine_amplitude;
+    for (std::size_t i = 0; i < intervals_length; i += 3)
+      c.initial_intervals.push_back({intervals[i], intervals[i + 1], intervals[i + 2]});
+    for (std::size_t i = 0; i < circles_length; i += 4)
+      c.initial_circles.push_back({circles[i], circles[i + 1], circles[i + 2], circles[i + 3]});
+    c.boundaries = bridge_boundaries(boundary_names, boundary_kinds, boundary_values,
+                                     boundary_count);
+    write_text(bridge_summary(wasl::run_scalar_advection_case(c)), summary, summary_length);
   });
+}
+
+int wr_inspect_checkpoint(const char *checkpoint_path, char *summary, std::size_t summary_length) {
+  return guarded([&] {
+    const auto checkpoint = wasl::read_checkpoint(checkpoint_path);
+    std::ostringstream out;
+    out.precision(17);
+    out << "step=" << checkpoint.step << " time=" << checkpoint.time
+        << " variables=" << checkpoint.variable_count << " modes=" << checkpoint.mode_count
+        << " elements=" << checkpoint.element_count;
+    write_text(out.str(), summary, summary_length);
+  });
+}
+
+// A line mesh whose two end nodes carry the physical names "left" and
+// "right" (point entities 1 and 2), so cases can name their end boundaries.
+void *wr_line_mesh_named_new(std::int64_t node_count, const std::int64_t *tags, const double *x,
+                             std::int64_t element_count, const std::int64_t *element_nodes) {
+  auto *handle = new LineHandle;
+  const int rc = guarded([&] {
+    std::int64_t lo = 0, hi = 0;
+    for (std::int64_t i = 1; i < node_count; ++i) {
+      lo = x[i] < x[lo] ? i : lo;
+      hi = x[i] > x[hi] ? i : hi;
+    }
+    wasl::MshDocument document;
+    document.physical_names = {{0, 1, "left"}, {0, 2, "right"}};
+    document.point_entities.push_back({1, x[lo], 0.0, 0.0, {1}});
+    document.point_entities.push_back({2, x[hi], 0.0, 0.0, {2}});
+    document.curve_entities.push_back({1, 0, 0, 0, 1, 0, 0, {}, {1, 2}});
+    for (std::int64_t i = 0; i < node_count; ++i) {
+      const int dim = i == lo || i == hi ? 0 : 1;
+      const int entity = i == lo ? 1 : (i == hi ? 2 : 1);
+      document.nodes.push_back({tags[i], dim, entity, x[i], 0.0, 0.0});
+    }
+    for (std::int64_t e = 0; e < element_count; ++e)
+      document.elements.push_back({e + 1, 1, 1, wasl::msh_line_element,
+                                   {element_nodes[2 * e], element_nodes[2 * e + 1]}});
+    handle->mesh = wasl::build_line_mesh(document);
+  });
+  if (rc != 0) {
+    delete handle;
+    return nullptr;
+  }
+  return handle;
 }
 
 } // extern "C"

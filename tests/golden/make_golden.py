@@ -1,9 +1,10 @@
 """Regenerate the committed golden fixtures from the reference.
 
-Run in a container that has the reference sources (REF, default
-/root/reference) and the reference checker built (``make -C oracle ref``):
+Run where the reference sources are present and the reference checker is
+built, naming the reference checkout in REF:
 
-    python tests/golden/make_golden.py
+    make -C oracle ref REF=<reference checkout>
+    REF=<reference checkout> python tests/golden/make_golden.py
 
 * case_regression.json -- the reference's stored case-regression metrics,
   parsed from cpp/tests/runtime/case_regression_reference.txt (29 runs: step,
@@ -29,7 +30,7 @@ import pyoracle  # noqa: E402
 from golden_cases import GAMMA  # noqa: E402
 from wasl_b200 import meshgen  # noqa: E402
 
-REF = os.environ.get("REF", "/root/reference")
+REF = os.environ.get("REF", "")
 
 
 def seeded_state(ne, p, seed, amplitude=0.05):
@@ -46,6 +47,8 @@ def seeded_state(ne, p, seed, amplitude=0.05):
 
 
 def main():
+    if not os.path.isdir(os.path.join(REF, "cpp", "tests")):
+        sys.exit("set REF to the reference checkout")
     rows = {}
     with open(os.path.join(REF, "cpp/tests/runtime/case_regression_reference.txt")) as f:
         for line in f:

@@ -13,10 +13,12 @@ from wasl_b200 import cases, meshgen
 pytestmark = pytest.mark.gpu
 
 # mixed_kernel: 1 face-centric kernels, 2 + s the fused tile kernel in shape s
-# (s = 0..3 the tile kernel, 4..7 the shared-face tile kernel).
+# (s = 0..3 the tile kernel, 4..7 the shared-face tile kernel, 8..11 the patch
+# kernel).
 KERNELS = [1, 2, 3, 4, 5]
-TILE_SHAPES = 8
+TILE_SHAPES = 12
 SHARED_KERNELS = [6, 7, 8, 9]
+PATCH_KERNELS = [10, 11, 12, 13]
 
 
 def pair(arrays, p, **kw):
@@ -58,7 +60,8 @@ def test_one_step_close_to_plain(p):
 
 
 @pytest.mark.parametrize("p,rule,kernel", [(p, r, k) for p in (1, 2, 3) for r in (0, p)
-                                           for k in (1, 2, 8)] + [(2, 2, k) for k in (3, 4, 5)])
+                                           for k in (1, 2, 8, 10)] +
+                         [(2, 2, k) for k in (3, 4, 5, 12)])
 def test_mass_and_energy_conserved(p, rule, kernel):
     """Periodic faces paired, interior faces evaluated by both sides with the
     same instructions: totals conserved to FP64 round-off."""
@@ -279,3 +282,62 @@ def test_vortex_convergence_rate(form, p):
     rate = np.log(errors[1] / errors[2]) / np.log(2.0)
     assert errors[0] > errors[1] > errors[2]
     assert rate >= p + 0.6, (errors, rate)
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+@pytest.mark.parametrize("boundary", ["periodic", "transmissive"])
+def test_patch_kernel_matches_face_centric(p, boundary):
+    """The patch kernel (traces once per element, faces once per patch) is
+    the face-centric form's arithmetic up to FP32 rounding order: after three
+    steps the states differ by at most 1e-6 of the change the steps made; all
+    its launch shapes agree bit for bit (a face computes the same bits whether
+    it lies inside a patch or between two)."""
+    arrays = meshgen.jittered_box(20, jitter=0.15, seed=80 + p)
+    c = seeded_state(2 * 20 * 20, p, 90 + p, amplitude=0.02)
+    out = {}
+    for k in [1] + PATCH_KERNELS:
+        with wasl_b200.Solver(*arrays, polynomial_order=p, precision="mixed", mixed_kernel=k,
+                              boundary=boundary) as g:
+            g.set_state(c)
+            for _ in range(3):
+                g.step(g.stable_dt(0.15))
+            out[k] = g.get_state()
+            assert g.tuning()[0] == k - 1
+    change = np.max(np.abs(out[1] - c))
+    assert np.max(np.abs(out[10] - out[1])) <= 1e-6 * change
+    for k in PATCH_KERNELS[1:]:
+        assert np.array_equal(out[k], out[10]), f"kernel {k}"
+
+
+def test_patch_kernel_needs_the_limiter_off():
+    arrays = meshgen.jittered_box(6, jitter=0.1, seed=2)
+    with pytest.raises(wasl_b200.WaslError, match="patch kernel"):
+        wasl_b200.Solver(*arrays, polynomial_order=2, precision="mixed", limiting=True,
+                         mixed_kernel=PATCH_KERNELS[0])
+
+
+@pytest.mark.parametrize("kernel,limiting", [(1, False), (2, False), (8, False), (10, False),
+                                             (2, True), (8, True)])
+def test_storage_order_is_a_relabelling(kernel, limiting):
+    """The mixed form stores its elements along a Morton curve (element_order
+    "curve", the default): a relabelling only, so the states, flag sets and
+    time steps match storage in the caller's order bit for bit."""
+    arrays = meshgen.jittered_box(20, jitter=0.15, seed=12)
+    c = seeded_state(2 * 20 * 20, 2, 13, amplitude=0.02)
+    out = {}
+    for order in ("caller", "curve"):
+        with wasl_b200.Solver(*arrays, polynomial_order=2, precision="mixed", mixed_kernel=kernel,
+                              limiting=limiting, positivity_all=limiting,
+                              element_order=order) as g:
+            stored = g.element_order()
+            assert sorted(stored) == list(range(g.elements))
+            assert (order == "caller") == np.array_equal(stored, np.arange(g.elements))
+            g.set_state(c)
+            dts = []
+            for _ in range(3):
+                dts.append(g.stable_dt(0.1))
+                g.step(dts[-1])
+            out[order] = (g.get_state(), g.flags(), dts, g.mass_energy())
+    a, b = out["caller"], out["curve"]
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[2] == b[2]
+    assert np.allclose(a[3], b[3], rtol=1e-14, atol=0.0)

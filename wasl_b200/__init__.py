@@ -51,7 +51,7 @@ class Config(C.Structure):
         ("sensor_threshold", C.c_double), ("density_floor", C.c_double),
         ("pressure_floor", C.c_double), ("precision", C.c_int), ("device", C.c_int),
         ("volume_rule_order", C.c_int), ("mixed_kernel", C.c_int),
-        ("positivity_all", C.c_int),
+        ("positivity_all", C.c_int), ("element_order", C.c_int),
     ]
 
 
@@ -98,6 +98,7 @@ SIGNATURES = {
     "wasl_gpu_advance": (C.c_int, [C.c_void_p, C.c_double, C.c_int64]),
     "wasl_gpu_sync": (C.c_int, [C.c_void_p]),
     "wasl_gpu_state_device": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "wasl_gpu_element_order": (C.c_int, [C.c_void_p, _i64, C.c_int64]),
     "wasl_gpu_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "wasl_gpu_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), _d, C.c_int,
                                   C.POINTER(C.c_int)]),
@@ -193,7 +194,7 @@ class Solver:
                  boundary="periodic", boundary_right=None, inflow=(0.0, 0.0), limiting=False,
                  sensor_threshold=1e-3, density_floor=1e-10, pressure_floor=1e-10,
                  precision="plain", device=0, volume_rule_order=0, mixed_kernel=0,
-                 positivity_all=False):
+                 positivity_all=False, element_order="curve"):
         lib = library()
         cfg = default_config()
         cfg.dimensions = dimensions
@@ -213,6 +214,7 @@ class Solver:
         cfg.volume_rule_order = volume_rule_order
         cfg.mixed_kernel = mixed_kernel
         cfg.positivity_all = 1 if positivity_all else 0
+        cfg.element_order = {"curve": 0, "caller": 1}[element_order]
         self.config = cfg
         tags = np.ascontiguousarray(node_tags, dtype=np.int64)
         coords = np.ascontiguousarray(node_coordinates, dtype=np.float64)
@@ -347,6 +349,12 @@ class Solver:
         return m.value, e.value
 
     # ---- device interop -------------------------------------------------------
+    def element_order(self) -> np.ndarray:
+        """order[i]: the caller's element stored at column i of the device state."""
+        out = np.empty(self.elements, dtype=np.int64)
+        self._check(self._lib.wasl_gpu_element_order(self._h, _ptr(out, _i64), out.size))
+        return out
+
     def state_device_pointer(self) -> int:
         p = C.c_void_p()
         self._check(self._lib.wasl_gpu_state_device(self._h, C.byref(p)))

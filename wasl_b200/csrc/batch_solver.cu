@@ -67,6 +67,8 @@ BatchSolver::BatchSolver(const wasl_batch_config &cfg, std::int64_t case_count, 
     throw SolverError(WASL_ERR_ARGUMENT, "batch: boundaries must be periodic or transmissive");
   if (cfg.tile_shape < 0 || cfg.tile_shape > euler_tri_tile_shapes())
     throw SolverError(WASL_ERR_ARGUMENT, "batch: unknown tile shape");
+  if (cfg.tile_shape > 0 && euler_tri_tile_is_patch(cfg.tile_shape - 1))
+    throw SolverError(WASL_ERR_ARGUMENT, "batch: the patch kernel's shapes are for single cases");
   for (std::int64_t c = 0; c < case_count; ++c)
     if (!euler_tri_mixed_supported(orders[c], 0))
       throw SolverError(WASL_ERR_ARGUMENT, "batch: polynomial order must be 1..3 (case " +
@@ -395,7 +397,10 @@ void BatchSolver::tune() {
     const std::string key = "batch_tile/p" + std::to_string(g.p) + "/rule" +
                             std::to_string(g.rule) + "/bnd" + std::to_string(cfg_.boundary) +
                             "/size" + std::to_string(size_class(g.ne));
-    g.tuning = autotune(key, euler_tri_tile_shapes(), [&](int shape) {
+    int shapes = 0; // the tile kernels' shapes (the patch kernel's come after them)
+    while (shapes < euler_tri_tile_shapes() && !euler_tri_tile_is_patch(shapes))
+      ++shapes;
+    g.tuning = autotune(key, shapes, [&](int shape) {
       g.shape = shape;
       StageArgs a = stage_args(g, 0);
       a.sense = 0;

@@ -301,6 +301,14 @@ int wasl_gpu_state_device(wasl_gpu *h, double **p) {
   });
 }
 
+int wasl_gpu_element_order(const wasl_gpu *h, int64_t *order, int64_t count) {
+  return guarded(const_cast<wasl_gpu *>(h), [&] {
+    need(order != nullptr, "null pointer");
+    need(count == h->solver->elements(), "element order: count must be the element count");
+    h->solver->element_order(order);
+  });
+}
+
 int wasl_gpu_stream(wasl_gpu *h, void **s) {
   return guarded(h, [&] {
     need(s != nullptr, "null pointer");

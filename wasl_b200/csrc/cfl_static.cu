@@ -6,8 +6,17 @@
 // latency-critical loop that cannot accept cudaMalloc's implicit device-wide
 // synchronization.  wasl_cfl_dt_static serves them: the caller passes the
 // state and receives dt in device memory it already owns, and the reduction's
-// per-block partials live in g_cfl_scratch below, a fixed array that every
-// GPU loading this library holds until the process exits.
+// scratch (one (speed, element) pair per block of the fixed reduction grid,
+// the block counter, the winner's record and the error word) lives in
+// g_cfl_scratch below, a fixed 9.6 KiB array that every GPU loading this
+// library holds until the process exits.
+//
+// The rule is the solver handle's, step for step: the one-pass reduction
+// kernel of the handles (launch_cfl) finds the largest cell-average wave
+// speed and the smallest element reaching it, and the host re-evaluates that
+// element's speed with the C library's functions (host_cell_speed) and forms
+// dt = cfl length / (speed (2p + 1)).  So the dt is the one
+// wasl_gpu_stable_dt returns for the same state, bit for bit.
 //
 // Limits and sharing:
 //   * at most kMaxElements elements per call (larger inputs are rejected);
@@ -15,98 +24,37 @@
 //     overlap on that GPU (different streams, or different host threads)
 //     race and may return each other's results;
 //   * the first call on each device looks up the array's device address
-//     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture.
+//     (cudaGetSymbolAddress) with that device current;
+//   * every call copies the winner back to the host and synchronizes the
+//     stream, so no call can be made while that stream is being captured.
 #include <array>
 #include <atomic>
-#include <climits>
-#include <cstdio>
+#include <cstdint>
 #include <cstring>
 #include <string>
 
 #include <cuda_runtime.h>
 
 #include "../../include/wasl_b200.h"
-#include "euler_device.cuh"
+#include "kernels.hpp"
+#include "solver.hpp"
 
 namespace wasl_b200 {
 namespace {
 
-constexpr int kBlock = 256;
-constexpr int kPerThread = 8;                            // elements per thread
-constexpr int kMaxBlocks = 16384;                        // partials held
-constexpr long long kSpan = static_cast<long long>(kBlock) * kPerThread;
-constexpr long long kMaxElements = kSpan * kMaxBlocks;   // 33,554,432 elements
-
-struct CflScratch {
-  double speed[kMaxBlocks];   // largest |u|+c of each block's element range
-  unsigned long long error;   // first non-physical element, code in the top byte
-};
+// Element indices of the library's meshes are 32-bit.
+constexpr long long kMaxElements = 2147483647LL;
+// The reduction's words (kCflResultWords) and, after them, the error word.
+constexpr std::size_t kScratchWords = kCflResultWords + 1;
 
 } // namespace
 
-// 16384 x 8 B + 8 B = 128 KiB per device.
-static __device__ __align__(256) CflScratch g_cfl_scratch;
+static __device__ __align__(256) unsigned long long g_cfl_scratch[kScratchWords];
 
 namespace {
 
-__global__ void __launch_bounds__(kBlock)
-    cfl_static_partial(const double *__restrict__ state, long long ne, int M, int dimensions,
-                       double gamma, CflScratch *scratch) {
-  __shared__ double block_best[kBlock / 32];
-  const double scale = 1.0 / sqrt(2.0);
-  const long long plane = static_cast<long long>(M) * ne;
-  const long long begin = static_cast<long long>(blockIdx.x) * kSpan;
-  double best = 0.0;
-  for (int k = 0; k < kPerThread; ++k) {
-    const long long e = begin + static_cast<long long>(k) * kBlock + threadIdx.x;
-    if (e >= ne)
-      break;
-    const double s[4] = {scale * state[e], scale * state[plane + e], scale * state[2 * plane + e],
-                         scale * state[3 * plane + e]};
-    const Prim<double> v = primitive(gamma, s);
-    if (!(s[0] > 0.0 && v.p > 0.0)) {
-      raise_error(&scratch->error, kNonPhysicalAverage, e);
-      continue;
-    }
-    const double velocity = dimensions == 1 ? fabs(v.vx) : hypot(v.vx, v.vy);
-    best = smax(best, velocity + sound_speed(gamma, v));
-  }
-  for (int off = 16; off > 0; off >>= 1)
-    best = smax(best, __shfl_down_sync(0xffffffffu, best, off));
-  if ((threadIdx.x & 31) == 0)
-    block_best[threadIdx.x >> 5] = best;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double b = block_best[0];
-    for (int w = 1; w < kBlock / 32; ++w)
-      b = smax(b, block_best[w]);
-    scratch->speed[blockIdx.x] = b;
-  }
-}
-
-__global__ void __launch_bounds__(kBlock)
-    cfl_static_final(const CflScratch *scratch, int blocks, double cfl, double length, int p,
-                     double *dt) {
-  __shared__ double block_best[kBlock / 32];
-  double best = 0.0;
-  for (int b = threadIdx.x; b < blocks; b += kBlock)
-    best = smax(best, scratch->speed[b]);
-  for (int off = 16; off > 0; off >>= 1)
-    best = smax(best, __shfl_down_sync(0xffffffffu, best, off));
-  if ((threadIdx.x & 31) == 0)
-    block_best[threadIdx.x >> 5] = best;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double speed = block_best[0];
-    for (int w = 1; w < kBlock / 32; ++w)
-      speed = smax(speed, block_best[w]);
-    *dt = speed > 0.0 ? cfl * length / (speed * (2 * p + 1)) : 0.0;
-  }
-}
-
 // Device address of g_cfl_scratch, looked up once per device.
-std::array<std::atomic<CflScratch *>, 64> scratch_of_device{};
+std::array<std::atomic<unsigned long long *>, 64> scratch_of_device{};
 
 int fail(char *error, size_t length, int status, const std::string &message) {
   if (error && length) {
@@ -128,39 +76,53 @@ extern "C" int wasl_cfl_dt_static(const double *state, int64_t element_count, in
     return fail(error, error_length, WASL_ERR_ARGUMENT, "cfl: null state or dt pointer");
   if (element_count < 1 || element_count > kMaxElements)
     return fail(error, error_length, WASL_ERR_ARGUMENT,
-                "cfl: element count " + std::to_string(element_count) +
-                    " outside 1.." + std::to_string(kMaxElements) +
-                    " (the static scratch holds " + std::to_string(kMaxBlocks) +
-                    " block partials)");
+                "cfl: element count " + std::to_string(element_count) + " outside 1.." +
+                    std::to_string(kMaxElements) + " (32-bit element indices)");
   if (mode_count < 1 || (dimensions != 1 && dimensions != 2) || polynomial_order < 0)
     return fail(error, error_length, WASL_ERR_ARGUMENT, "cfl: invalid modes or dimensions");
   int device = 0;
   cudaError_t rc = cudaGetDevice(&device);
   if (rc != cudaSuccess || device < 0 || device >= static_cast<int>(scratch_of_device.size()))
     return fail(error, error_length, WASL_ERR_CUDA, "cfl: no usable CUDA device");
-  CflScratch *scratch = scratch_of_device[device].load();
+  unsigned long long *scratch = scratch_of_device[device].load();
   if (!scratch) {
     void *address = nullptr;
     rc = cudaGetSymbolAddress(&address, g_cfl_scratch);
     if (rc != cudaSuccess)
       return fail(error, error_length, WASL_ERR_CUDA,
                   std::string("cfl: scratch address: ") + cudaGetErrorString(rc));
-    scratch = static_cast<CflScratch *>(address);
+    scratch = static_cast<unsigned long long *>(address);
     scratch_of_device[device].store(scratch);
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  // The error word must start at zero; the partials are fully overwritten.
-  rc = cudaMemsetAsync(&scratch->error, 0, sizeof(unsigned long long), s);
-  const int blocks = static_cast<int>((element_count + kSpan - 1) / kSpan);
+  CflArgs a;
+  a.ne = element_count;
+  a.M = mode_count;
+  a.dimensions = dimensions;
+  a.state = state;
+  a.gamma = gamma;
+  a.cfl = cfl;
+  a.length = length;
+  a.p = polynomial_order;
+  a.result = scratch;
+  a.dt = nullptr; // the host forms dt, as the handles do
+  a.error = scratch + kCflResultWords;
+  // The error word must start at zero; launch_cfl clears its own counters
+  // and the pairs are fully overwritten.
+  rc = cudaMemsetAsync(a.error, 0, sizeof(unsigned long long), s);
   if (rc == cudaSuccess) {
-    cfl_static_partial<<<blocks, kBlock, 0, s>>>(state, element_count, mode_count, dimensions,
-                                                 gamma, scratch);
-    cfl_static_final<<<1, kBlock, 0, s>>>(scratch, blocks, cfl, length, polynomial_order, dt);
+    try {
+      launch_cfl(a, s);
+    } catch (const std::exception &e) {
+      return fail(error, error_length, WASL_ERR_CUDA, std::string("cfl: ") + e.what());
+    }
     rc = cudaGetLastError();
   }
-  unsigned long long word = 0;
+  unsigned long long words[8] = {}, word = 0;
   if (rc == cudaSuccess)
-    rc = cudaMemcpyAsync(&word, &scratch->error, sizeof(word), cudaMemcpyDeviceToHost, s);
+    rc = cudaMemcpyAsync(words, scratch, sizeof(words), cudaMemcpyDeviceToHost, s);
+  if (rc == cudaSuccess)
+    rc = cudaMemcpyAsync(&word, a.error, sizeof(word), cudaMemcpyDeviceToHost, s);
   if (rc == cudaSuccess)
     rc = cudaStreamSynchronize(s);
   if (rc != cudaSuccess)
@@ -169,5 +131,15 @@ extern "C" int wasl_cfl_dt_static(const double *state, int64_t element_count, in
     return fail(error, error_length, WASL_ERR_NONPHYSICAL,
                 "simulation: Euler cell average is not physical (element " +
                     std::to_string(word & 0xffffffffffffffULL) + ")");
+  double mode0[4];
+  for (int v = 0; v < 4; ++v)
+    mode0[v] = bits_to_double(words[2 + v]);
+  const double speed = host_cell_speed(gamma, mode0, dimensions);
+  const double value = speed > 0.0 ? cfl * length / (speed * (2 * polynomial_order + 1)) : 0.0;
+  rc = cudaMemcpyAsync(dt, &value, sizeof(value), cudaMemcpyHostToDevice, s);
+  if (rc == cudaSuccess)
+    rc = cudaStreamSynchronize(s);
+  if (rc != cudaSuccess)
+    return fail(error, error_length, WASL_ERR_CUDA, std::string("cfl: ") + cudaGetErrorString(rc));
   return WASL_OK;
 }

@@ -12,6 +12,7 @@
 //     rhs -= value * basis (left) / += (right) (triangle_residual.hpp:59-102)
 //   * rhs *= 1/det(J), then the Shu-Osher combination (time/ssp_rk3.hpp:44-60).
 // One thread owns one element, so no atomics touch the residual.
+#include <climits>
 #include <cstdio>
 #include <stdexcept>
 #include <string>
@@ -550,28 +551,93 @@ __global__ void cfl_max(const CflArgs a) {
   }
 }
 
-// The smallest element index reaching the maximum, as ~index under atomicMax.
-__global__ void cfl_argmax(const CflArgs a) {
-  const unsigned long long target = a.result[0];
+// The larger of two (speed bits, element) pairs; on equal speeds the smaller
+// element, as the reference's first strict maximum in element order.
+__device__ __forceinline__ void better_pair(unsigned long long &best, long long &arg,
+                                            unsigned long long other, long long other_arg) {
+  if (other > best || (other == best && other_arg < arg)) {
+    best = other;
+    arg = other_arg;
+  }
+}
+
+// Block-wide pair reduction; thread 0 returns the block's pair.
+__device__ __forceinline__ void block_pair(unsigned long long &best, long long &arg) {
+  __shared__ unsigned long long speeds[32];
+  __shared__ long long args[32];
+  for (int off = 16; off > 0; off >>= 1)
+    better_pair(best, arg, __shfl_down_sync(0xffffffffu, best, off),
+                __shfl_down_sync(0xffffffffu, arg, off));
+  if ((threadIdx.x & 31) == 0) {
+    speeds[threadIdx.x >> 5] = best;
+    args[threadIdx.x >> 5] = arg;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const bool live = threadIdx.x < (blockDim.x >> 5);
+    best = live ? speeds[threadIdx.x] : 0ULL;
+    arg = live ? args[threadIdx.x] : LLONG_MAX;
+    for (int off = 16; off > 0; off >>= 1)
+      better_pair(best, arg, __shfl_down_sync(0xffffffffu, best, off),
+                  __shfl_down_sync(0xffffffffu, arg, off));
+  }
+  __syncthreads();
+}
+
+// The whole CFL reduction in one pass over the cell averages: each block
+// reduces its elements to (largest speed, smallest element reaching it) and
+// stores the pair; the last block to finish reduces the pairs, records the
+// winner's mode-0 coefficients and forms dt (cfl_timestep.cpp:70-84), then
+// re-arms the block counter.
+__global__ void __launch_bounds__(256) cfl_reduce(const CflArgs a) {
+  unsigned long long best = 0;
+  long long arg = LLONG_MAX;
   for (std::int64_t e = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; e < a.ne;
        e += static_cast<std::int64_t>(gridDim.x) * blockDim.x) {
     bool physical = true;
     const double speed = cell_speed(a, e, physical);
-    if (physical && static_cast<unsigned long long>(__double_as_longlong(speed)) == target)
-      atomicMax(a.result + 1, ~static_cast<unsigned long long>(e));
+    if (!physical) {
+      raise_error(a.error, kNonPhysicalAverage, e);
+      continue;
+    }
+    // The tie key is the caller's element index (high word); the storage
+    // column rides in the low word.
+    const long long key = a.order ? a.order[e] : e;
+    better_pair(best, arg, static_cast<unsigned long long>(__double_as_longlong(speed)),
+                (key << 32) | e);
   }
-}
-
-__global__ void cfl_finish(const CflArgs a) {
-  const double speed = __longlong_as_double(static_cast<long long>(a.result[0]));
-  const std::int64_t e = a.result[1] ? static_cast<std::int64_t>(~a.result[1]) : 0;
-  const std::int64_t plane = static_cast<std::int64_t>(a.M) * a.ne;
-  for (int v = 0; v < 4; ++v)
-    a.result[2 + v] = static_cast<unsigned long long>(__double_as_longlong(a.state[v * plane + e]));
-  const double dt = speed > 0.0 ? a.cfl * a.length / (speed * (2 * a.p + 1)) : 0.0;
-  a.result[6] = static_cast<unsigned long long>(__double_as_longlong(dt));
-  if (a.dt)
-    *a.dt = dt;
+  block_pair(best, arg);
+  __shared__ bool last;
+  unsigned long long *pairs = a.result + 16;
+  if (threadIdx.x == 0) {
+    pairs[2 * blockIdx.x] = best;
+    pairs[2 * blockIdx.x + 1] = static_cast<unsigned long long>(arg);
+    __threadfence();
+    last = atomicAdd(a.result + 8, 1ULL) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last)
+    return;
+  __threadfence();
+  best = 0;
+  arg = LLONG_MAX;
+  for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+    better_pair(best, arg, __ldcg(pairs + 2 * b), static_cast<long long>(__ldcg(pairs + 2 * b + 1)));
+  block_pair(best, arg);
+  if (threadIdx.x == 0) {
+    const std::int64_t e = arg == LLONG_MAX ? 0 : (arg & 0xffffffffLL);
+    const double speed = __longlong_as_double(static_cast<long long>(best));
+    const std::int64_t plane = static_cast<std::int64_t>(a.M) * a.ne;
+    a.result[0] = best;
+    a.result[1] = ~static_cast<unsigned long long>(arg == LLONG_MAX ? 0 : arg >> 32);
+    for (int v = 0; v < 4; ++v)
+      a.result[2 + v] = static_cast<unsigned long long>(__double_as_longlong(a.state[v * plane + e]));
+    const double dt = speed > 0.0 ? a.cfl * a.length / (speed * (2 * a.p + 1)) : 0.0;
+    a.result[6] = static_cast<unsigned long long>(__double_as_longlong(dt));
+    if (a.dt)
+      *a.dt = dt;
+    a.result[8] = 0;
+  }
 }
 
 // dt from a reduced speed word per case (the finish step of the CFL kernels),
@@ -699,11 +765,10 @@ void launch_cfl_speed(const CflArgs &a, cudaStream_t s) {
 }
 
 void launch_cfl(const CflArgs &a, cudaStream_t s) {
-  check(cudaMemsetAsync(a.result, 0, 8 * sizeof(unsigned long long), s), "cfl reset");
-  const unsigned blocks = static_cast<unsigned>(std::min<std::int64_t>((a.ne + 255) / 256, 148 * 4));
-  cfl_max<<<blocks, 256, 0, s>>>(a);
-  cfl_argmax<<<blocks, 256, 0, s>>>(a);
-  cfl_finish<<<1, 1, 0, s>>>(a);
+  check(cudaMemsetAsync(a.result, 0, 16 * sizeof(unsigned long long), s), "cfl reset");
+  const unsigned blocks =
+      static_cast<unsigned>(std::min<std::int64_t>((a.ne + 255) / 256, kCflBlocks));
+  cfl_reduce<<<blocks, 256, 0, s>>>(a);
 }
 
 } // namespace wasl_b200

@@ -1497,6 +1497,512 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_shared(const StageA
   tile_finish<P, TILE>(a, e, t, case_id, sstate, r0, racc);
 }
 
+// ---- patch kernel ------------------------------------------------------------
+//
+// The mixed stage over a patch of TILE consecutive elements per CTA, each
+// face evaluated once per patch, with every element's traces computed once.
+// On a mesh whose element order keeps neighbours close (the solvers order
+// elements along a space-filling curve), most faces lie inside a patch.
+//
+//   A. Each thread loads its element's state: the FP64 mean and its primitive
+//      values, and the high modes in FP32 (shared memory), and evaluates the
+//      high-mode traces at the Gauss points of its three local edges
+//      (c_patch: that edge's points in its own order).  It lists the faces
+//      it evaluates: a face inside the patch by its left element, a face to an
+//      element outside the patch (or on a transmissive boundary) by this
+//      element, so such a face is evaluated by both patches, identically.
+//   B. All threads share out the listed faces (whole faces in full rounds,
+//      the rest one edge point per thread): the HLLC flux perturbation around
+//      the face's left mean, from the two traces (an outside neighbour's from
+//      its coefficients in global memory, with the same instructions its own
+//      patch uses), written over the evaluating element's trace in its own
+//      point order.
+//   C. Each thread computes its element's volume term (as the tile kernel),
+//      lifts the flux records of its three edges (from its own record or from
+//      its left neighbour's inside the patch) in the face's point order, and
+//      forms mode 0 from the left mean's FP64 normal flux and the FP32
+//      record sum, in the same order on both sides of the face; then the FP64
+//      Shu-Osher combination.
+//
+// Both elements of a face apply the same mode-0 value bit for bit, so mass,
+// momentum and energy are conserved to FP64 round-off, as in the tile kernel.
+template <int P> struct PatchEdge {
+  static constexpr int M = TriShape<P>::M, QF = TriShape<P>::QF, H = M - 1;
+  float phi[3][QF][H]; // modes 1..M-1 at local edge j's points, in its order
+  float w[3][QF];      // reference edge weights
+};
+template <int P> __constant__ PatchEdge<P> c_patch;
+
+// Dynamic shared memory of the patch kernel, in this order:
+//   mean  double [4][TILE]        cell means
+//   prim  double [4][TILE]        u, v, p, E + p of each mean
+//   hi    float  [4 H][TILE]      high modes, FP32
+//   edge  float  [3 QF 4][TILE]   per (local edge, point, variable): the
+//                                 element's trace, then the face's flux
+//                                 perturbation (own point order)
+//   items uint16 [3 TILE]         faces to evaluate: element * 4 + edge
+template <int P, int TILE> struct PatchSmem {
+  static constexpr int M = TriShape<P>::M, QF = TriShape<P>::QF, H = M - 1;
+  static constexpr std::size_t mean = 0;
+  static constexpr std::size_t prim = mean + sizeof(double) * 4 * TILE;
+  static constexpr std::size_t hi = prim + sizeof(double) * 4 * TILE;
+  static constexpr std::size_t edge = hi + sizeof(float) * 4 * H * TILE;
+  static constexpr std::size_t items = edge + sizeof(float) * 3 * QF * 4 * TILE;
+  static constexpr std::size_t bytes = items + sizeof(std::uint16_t) * 3 * TILE;
+};
+
+template <int P, int TILE>
+__device__ __forceinline__ MeanState patch_mean(const double (*smean)[TILE],
+                                                const double (*sprim)[TILE], int i) {
+  MeanState m;
+  m.rho = smean[0][i];
+  m.mx = smean[1][i];
+  m.my = smean[2][i];
+  m.e = smean[3][i];
+  m.u = sprim[0][i];
+  m.v = sprim[1][i];
+  m.p = sprim[2][i];
+  m.h = sprim[3][i];
+  return m;
+}
+
+// The trace of element nb's high modes (FP64 in global memory) at point q of
+// its local edge j: the instructions of phase A, so both patches agree.
+template <int P>
+__device__ __forceinline__ void patch_outside_trace(const double *__restrict__ in, std::int64_t ne,
+                                                    std::int64_t nb, const float *phi, float *out) {
+  constexpr int M = TriShape<P>::M, H = M - 1;
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    float s = 0.0f;
+#pragma unroll
+    for (int m = 0; m < H; ++m)
+      s = fmaf(static_cast<float>(__ldg(in + (static_cast<std::int64_t>(v) * M + m + 1) * ne + nb)),
+               phi[m], s);
+    out[v] = s;
+  }
+}
+
+// The end of the patch kernel's stage for element e: residual scaling, the
+// FP64 Shu-Osher combination (cpp/include/wasl/time/ssp_rk3.hpp:44-60) and the
+// optional next-step CFL speed and sensor (as tile_finish, with the stage
+// input read from global memory).
+template <int P>
+__device__ __forceinline__ void patch_finish(const StageArgs &a, std::int64_t e, int case_id,
+                                             const double (&r0)[4],
+                                             const float (&racc)[4][TriShape<P>::M - 1]) {
+  constexpr int M = TriShape<P>::M;
+  const std::int64_t ne = a.mesh.ne;
+  const double inv = a.mesh.geo[4 * ne + e];
+  const double dt = a.case_dt ? a.case_dt[case_id] : (a.dt ? *a.dt : a.dt_value);
+  double rho[M], avg[4];
+#pragma unroll
+  for (int v = 0; v < 4; ++v)
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const std::int64_t idx = (static_cast<std::int64_t>(v) * M + m) * ne + e;
+      const double cur = a.in[idx];
+      const double rr = (m == 0 ? r0[v] : static_cast<double>(racc[v][m > 0 ? m - 1 : 0])) * inv;
+      double o;
+      if (a.stage == 0)
+        o = cur + dt * rr;
+      else if (a.stage == 1)
+        o = 0.75 * a.u0[idx] + 0.25 * (cur + dt * rr);
+      else
+        o = (1.0 / 3.0) * a.u0[idx] + (2.0 / 3.0) * (cur + dt * rr);
+      a.out[idx] = o;
+      if (v == 0)
+        rho[m] = o;
+      if (m == 0)
+        avg[v] = o;
+    }
+  if (a.speed_max) {
+    const double scale = 1.0 / sqrt(2.0);
+    const double sa[4] = {__dmul_rn(scale, avg[0]), __dmul_rn(scale, avg[1]),
+                          __dmul_rn(scale, avg[2]), __dmul_rn(scale, avg[3])};
+    bool physical = true;
+    const double speed = cfl_speed(a.gamma, sa, 2, physical);
+    unsigned long long best = 0;
+    if (physical)
+      best = __double_as_longlong(speed);
+    else
+      raise_error(a.error, kNonPhysicalAverage, e);
+    const unsigned mask = __activemask();
+    const int lane = threadIdx.x & 31;
+    if (__match_any_sync(mask, case_id) == mask) {
+      const unsigned hi = __reduce_max_sync(mask, static_cast<unsigned>(best >> 32));
+      const unsigned lo = __reduce_max_sync(
+          mask, static_cast<unsigned>(best >> 32) == hi ? static_cast<unsigned>(best) : 0u);
+      if (lane == __ffs(mask) - 1)
+        atomicMax(a.speed_max + case_id, (static_cast<unsigned long long>(hi) << 32) | lo);
+    } else {
+      atomicMax(a.speed_max + case_id, best);
+    }
+  }
+  if (a.sense) {
+    double total = 0.0, high = 0.0;
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      total += rho[m] * rho[m];
+      if (m >= a.highest_degree_begin)
+        high += rho[m] * rho[m];
+    }
+    const bool troubled = !(total == 0.0 || high / total <= a.threshold);
+    a.flags[e] = troubled ? 1 : 0;
+    const unsigned active_mask = __activemask();
+    const unsigned ballot = __ballot_sync(active_mask, troubled);
+    if (ballot) {
+      const int lane = threadIdx.x & 31;
+      const int leader = __ffs(ballot) - 1;
+      int base = 0;
+      if (lane == leader)
+        base = atomicAdd(a.troubled_count, __popc(ballot));
+      base = __shfl_sync(active_mask, base, leader);
+      if (troubled)
+        a.troubled[base + __popc(ballot & ((1u << lane) - 1u))] = static_cast<std::int32_t>(e);
+    }
+  }
+}
+
+template <int P, int R, int TILE, int MINB>
+__global__ void __launch_bounds__(TILE, MINB) euler_tri_patch(const StageArgs a) {
+  using S = TriShape<P>;
+  using L = PatchSmem<P, TILE>;
+  constexpr int M = S::M, QV = MixedVolume<P, R>::QV, QF = S::QF, H = M - 1;
+  constexpr double phi0 = 0.70710678118654752440;
+  static_assert(4 * TILE < 65536, "face items are 16-bit");
+  __shared__ PatchEdge<P> table; // for the few runtime-indexed reads
+  __shared__ int item_count;
+  extern __shared__ __align__(16) unsigned char smem[];
+  double(*smean)[TILE] = reinterpret_cast<double(*)[TILE]>(smem + L::mean);
+  double(*sprim)[TILE] = reinterpret_cast<double(*)[TILE]>(smem + L::prim);
+  float(*shi)[TILE] = reinterpret_cast<float(*)[TILE]>(smem + L::hi);
+  float(*sedge)[TILE] = reinterpret_cast<float(*)[TILE]>(smem + L::edge);
+  std::uint16_t *items = reinterpret_cast<std::uint16_t *>(smem + L::items);
+
+  const int t = threadIdx.x;
+  const std::int64_t ne = a.mesh.ne;
+  std::int64_t first = 0, count = 0;
+  int case_id = 0;
+  if (a.work) {
+    const TileWork w = a.work[blockIdx.x];
+    first = w.first;
+    count = w.count;
+    case_id = w.case_id;
+  } else {
+    first = static_cast<std::int64_t>(blockIdx.x) * TILE;
+    count = ne - first < TILE ? ne - first : TILE;
+  }
+  const bool active = t < count;
+  const std::int64_t e = first + t;
+  const double *__restrict__ in = a.in;
+  const double gamma = a.gamma;
+  const PatchEdges pe = a.patch;
+
+  {
+    const float *src = reinterpret_cast<const float *>(&c_patch<P>);
+    float *dst = reinterpret_cast<float *>(&table);
+    for (int i = t; i < static_cast<int>(sizeof(table) / sizeof(float)); i += TILE)
+      dst[i] = src[i];
+  }
+  if (t == 0)
+    item_count = 0;
+  if (active && a.stage > 0) {
+#pragma unroll
+    for (int r = 0; r < 4 * M; ++r)
+      asm volatile("prefetch.global.L2 [%0];\n" ::"l"(a.u0 + r * ne + e));
+  }
+
+  // A. State, traces, and the faces this element evaluates.
+  bool evaluates[3] = {false, false, false};
+  if (active) {
+    double mean[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const double *row = in + static_cast<std::int64_t>(v) * M * ne + e;
+      mean[v] = row[0] * phi0;
+      float h[H];
+#pragma unroll
+      for (int m = 0; m < H; ++m) {
+        h[m] = static_cast<float>(row[(m + 1) * ne]);
+        shi[v * H + m][t] = h[m];
+      }
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int q = 0; q < QF; ++q) {
+          float s = 0.0f;
+#pragma unroll
+          for (int m = 0; m < H; ++m)
+            s = fmaf(h[m], c_patch<P>.phi[j][q][m], s);
+          sedge[(j * QF + q) * 4 + v][t] = s;
+        }
+    }
+    const MeanState own = mean_state(gamma, mean);
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+      smean[v][t] = mean[v];
+    sprim[0][t] = own.u;
+    sprim[1][t] = own.v;
+    sprim[2][t] = own.p;
+    sprim[3][t] = own.h;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const std::int32_t nb = pe.nbr[j * ne + e];
+      const std::int64_t local = nb - first;
+      const bool inside = nb >= 0 && local >= 0 && local < count;
+      evaluates[j] = !inside || (pe.info[j * ne + e] & 1u);
+    }
+  }
+  __syncthreads(); // item_count and the tables are set
+  {
+    const int lane = t & 31;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const unsigned ballot = __ballot_sync(0xffffffffu, evaluates[j]);
+      int base = 0;
+      if (lane == 0 && ballot)
+        base = atomicAdd(&item_count, __popc(ballot));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (evaluates[j])
+        items[base + __popc(ballot & ((1u << lane) - 1u))] = static_cast<std::uint16_t>(t * 4 + j);
+    }
+  }
+  __syncthreads();
+
+  // B. The listed faces, shared out over all threads.
+  {
+    const float gamma32 = static_cast<float>(gamma), g1 = static_cast<float>(gamma - 1.0);
+    const int n = item_count;
+    auto evaluate = [&](int i, int q0, auto whole) {
+      constexpr int NQ = decltype(whole)::value ? QF : 1;
+      const int te = items[i] >> 2, j = items[i] & 3;
+      const std::int64_t ee = first + te;
+      const std::int32_t nb = pe.nbr[j * ne + ee];
+      const unsigned info = pe.info[j * ne + ee];
+      const bool self_left = info & 1u, rev = info & 8u;
+      const int jn = (info >> 1) & 3u;
+      const double nx = pe.geo[(3 * j) * ne + ee], ny = pe.geo[(3 * j + 1) * ne + ee];
+      const bool boundary = nb < 0;
+      const std::int64_t local = nb - first;
+      const bool near = !boundary && local >= 0 && local < count;
+      double mean[4], nmean[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int v = 0; v < 4; ++v)
+        mean[v] = smean[v][te];
+      if (near) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+          nmean[v] = smean[v][local];
+      } else if (!boundary) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+          nmean[v] = __ldg(in + static_cast<std::int64_t>(v) * M * ne + nb) * phi0;
+      }
+      // The face's left mean state: the reference of the perturbation form.
+      MeanState ml;
+      if (self_left || boundary)
+        ml = patch_mean<P, TILE>(smean, sprim, te);
+      else if (near)
+        ml = patch_mean<P, TILE>(smean, sprim, static_cast<int>(local));
+      else
+        ml = mean_state(gamma, nmean);
+      const Ref32 ref = ref32(ml);
+      float jump[4];
+#pragma unroll
+      for (int v = 0; v < 4; ++v)
+        jump[v] = boundary ? 0.0f
+                           : static_cast<float>(self_left ? nmean[v] - mean[v] : mean[v] - nmean[v]);
+      const float nxf = static_cast<float>(nx), nyf = static_cast<float>(ny);
+#pragma unroll
+      for (int jq = 0; jq < NQ; ++jq) {
+        const int q = q0 + jq;              // the face's point (left element's order)
+        const int qr = rev ? QF - 1 - q : q; // the right element's point
+        const int qs = self_left ? q : qr;   // this element's point
+        float to[4], tn[4], dl[4], dr[4], fl[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+          to[v] = sedge[(j * QF + qs) * 4 + v][te];
+        if (boundary) {
+#pragma unroll
+          for (int v = 0; v < 4; ++v)
+            dl[v] = dr[v] = to[v];
+        } else {
+          const int qn = self_left ? qr : q;
+          if (near) {
+#pragma unroll
+            for (int v = 0; v < 4; ++v)
+              tn[v] = sedge[(jn * QF + qn) * 4 + v][local];
+          } else {
+            patch_outside_trace<P>(in, ne, nb, table.phi[jn][qn], tn);
+          }
+#pragma unroll
+          for (int v = 0; v < 4; ++v) {
+            dl[v] = self_left ? to[v] : tn[v];
+            dr[v] = jump[v] + (self_left ? tn[v] : to[v]);
+          }
+        }
+        hllc_perturbed(ref, dl, dr, g1, gamma32, nxf, nyf, fl);
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+          sedge[(j * QF + qs) * 4 + v][te] = fl[v];
+      }
+    };
+    const int whole = n / TILE * TILE;
+#pragma unroll 1
+    for (int i = t; i < whole; i += TILE)
+      evaluate(i, 0, std::true_type{});
+#pragma unroll 1
+    for (int u = t; u < (n - whole) * QF; u += TILE)
+      evaluate(whole + u / QF, u % QF, std::false_type{});
+  }
+  __syncthreads();
+  if (!active)
+    return;
+
+  // C. Volume term, lifting, mode 0, combination.
+  const MeanState own = patch_mean<P, TILE>(smean, sprim, t);
+  const Ref32 bb = ref32(own);
+  const MixedVolume<P, R> &T = c_mix<P, R>;
+  const float g1 = static_cast<float>(gamma - 1.0);
+  float racc[4][H];
+#pragma unroll
+  for (int v = 0; v < 4; ++v)
+#pragma unroll
+    for (int m = 0; m < H; ++m)
+      racc[v][m] = 0.0f;
+  {
+    float ch[4][H];
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+#pragma unroll
+      for (int m = 0; m < H; ++m)
+        ch[v][m] = shi[v * H + m][t];
+    const double *__restrict__ geo = a.mesh.geo;
+    const float fax = static_cast<float>(geo[e]), fay = static_cast<float>(geo[ne + e]);
+    const float fbx = static_cast<float>(geo[2 * ne + e]), fby = static_cast<float>(geo[3 * ne + e]);
+#pragma unroll
+    for (int q = 0; q < QV; ++q) {
+      float d[4];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        float s = 0.0f;
+#pragma unroll
+        for (int m = 0; m < H; ++m)
+          s = fmaf(ch[v][m], T.phi[q][m], s);
+        d[v] = s;
+      }
+      const float inv = __frcp_rn(fmaxf(bb.rho + d[0], kVacuumFraction * bb.rho));
+      const float du = (d[1] - bb.u * d[0]) * inv;
+      const float dv = (d[2] - bb.v * d[0]) * inv;
+      const float uu = bb.u + du, vv = bb.v + dv;
+      const float dmu = bb.mx * du + d[1] * uu + bb.my * dv + d[2] * vv;
+      const float dp = g1 * (d[3] - 0.5f * dmu);
+      const float dep = d[3] + dp;
+      const float fx[4] = {d[1], bb.mx * du + d[1] * uu + dp, bb.my * du + d[2] * uu,
+                           bb.h * du + dep * uu};
+      const float fy[4] = {d[2], bb.mx * dv + d[1] * vv, bb.my * dv + d[2] * vv + dp,
+                           bb.h * dv + dep * vv};
+      const float w = T.w[q];
+      const float wby = w * fby, wbx = w * fbx, wax = w * fax, way = w * fay;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const float gxi = wby * fx[v] - wbx * fy[v];
+        const float geta = wax * fy[v] - way * fx[v];
+#pragma unroll
+        for (int m = 0; m < H; ++m)
+          racc[v][m] = fmaf(T.dxi[q][m], gxi, fmaf(T.deta[q][m], geta, racc[v][m]));
+      }
+    }
+  }
+
+  double r0[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const std::int32_t nb = pe.nbr[j * ne + e];
+    const unsigned info = pe.info[j * ne + e];
+    const bool self_left = info & 1u, rev = info & 8u;
+    const int jn = (info >> 1) & 3u;
+    const double nx = pe.geo[(3 * j) * ne + e], ny = pe.geo[(3 * j + 1) * ne + e];
+    const double scale = pe.geo[(3 * j + 2) * ne + e];
+    const bool boundary = nb < 0;
+    const std::int64_t local = nb - first;
+    const bool near = !boundary && local >= 0 && local < count;
+    const int jl = self_left ? j : jn; // the face's left local edge (its weights)
+    // The face's flux perturbations in the face's point order: from this
+    // element's record, or from its left neighbour's inside the patch.
+    float fq[QF][4];
+    if (near && !self_left) {
+#pragma unroll
+      for (int q = 0; q < QF; ++q)
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+          fq[q][v] = sedge[(jn * QF + q) * 4 + v][local];
+    } else {
+#pragma unroll
+      for (int q = 0; q < QF; ++q) {
+        const int qs = self_left || !rev ? q : QF - 1 - q;
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+          fq[q][v] = sedge[(j * QF + qs) * 4 + v][t];
+      }
+    }
+    MeanState ml;
+    if (self_left || boundary) {
+      ml = own;
+    } else if (near) {
+      ml = patch_mean<P, TILE>(smean, sprim, static_cast<int>(local));
+    } else {
+      double nmean[4];
+#pragma unroll
+      for (int v = 0; v < 4; ++v)
+        nmean[v] = __ldg(in + static_cast<std::int64_t>(v) * M * ne + nb) * phi0;
+      ml = mean_state(gamma, nmean);
+    }
+    double fln[4];
+    mean_normal_flux(ml, nx, ny, fln);
+    float shift[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    if (!boundary && !self_left) {
+      double frn[4];
+      mean_normal_flux(own, nx, ny, frn);
+#pragma unroll
+      for (int v = 0; v < 4; ++v)
+        shift[v] = static_cast<float>(fln[v] - frn[v]);
+    }
+    const float fscale = static_cast<float>(scale);
+    float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int q = 0; q < QF; ++q) {
+      const float w = table.w[jl][q];
+#pragma unroll
+      for (int v = 0; v < 4; ++v)
+        acc[v] = fmaf(w, fq[q][v], acc[v]);
+    }
+    const double sgn = self_left ? -1.0 : 1.0;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const double mode0 = fln[v] * c_edge_wsum<P>[jl] + static_cast<double>(acc[v]);
+      r0[v] += sgn * scale * phi0 * mode0;
+    }
+    // High modes at this element's own points qo (the face's point q).
+#pragma unroll
+    for (int qo = 0; qo < QF; ++qo) {
+      const bool flipped = !self_left && rev;
+      const float w = table.w[jl][flipped ? QF - 1 - qo : qo];
+      const float wsc = (self_left ? -w : w) * fscale;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const float f = flipped ? fq[QF - 1 - qo][v] : fq[qo][v];
+        const float value = wsc * (self_left ? f : f + shift[v]);
+#pragma unroll
+        for (int m = 0; m < H; ++m)
+          racc[v][m] = fmaf(value, c_patch<P>.phi[j][qo][m], racc[v][m]);
+      }
+    }
+  }
+  patch_finish<P>(a, e, case_id, r0, racc);
+}
+
 // Per-case CFL speed over a tile work list: the largest cell-average wave
 // speed |u| + c of each case (the CFL kernels' formula), max-reduced as FP64
 // bits into speed[case]; a non-physical average sets the error word.
@@ -1565,6 +2071,14 @@ template <int P, int R> void upload_mixed() {
     wsum[le] = sum;
   }
   check(cudaMemcpyToSymbol(c_edge_wsum<P>, wsum, sizeof(wsum)), "upload edge weight sums");
+  static PatchEdge<P> pt;
+  for (int le = 0; le < 3; ++le)
+    for (int q = 0; q < TriShape<P>::QF; ++q) {
+      for (int m = 1; m < TriShape<P>::M; ++m)
+        pt.phi[le][q][m - 1] = static_cast<float>(f.lb[le][q][m]);
+      pt.w[le][q] = static_cast<float>(f.ew[le][q]);
+    }
+  check(cudaMemcpyToSymbol(c_patch<P>, &pt, sizeof(pt)), "upload patch edge table");
 }
 
 template <int P, int R> void stage_mixed(const StageArgs &a, cudaStream_t s) {
@@ -1640,6 +2154,26 @@ void stage_tile(const StageArgs &a, cudaStream_t s) {
            tile_smem<P, kRoughTile>(), s>>>(a);
 }
 
+template <int P, int R, int TILE, int MINB> void patch_opt_in() {
+  static bool opted_in[64] = {};
+  smem_opt_in(euler_tri_patch<P, R, TILE, MINB>, PatchSmem<P, TILE>::bytes,
+              sizeof(PatchEdge<P>) + sizeof(int), opted_in);
+}
+
+// The patch kernel over all patches (no rough pass: runs without the limiter).
+template <int P, int R, int TILE, int MINB> void stage_patch(const StageArgs &a, cudaStream_t s) {
+  if (a.rough)
+    throw std::invalid_argument("patch kernel: no rough pass (runs without the limiter)");
+  if (!a.patch.nbr)
+    throw std::invalid_argument("patch kernel: the mesh has no patch edge arrays");
+  patch_opt_in<P, R, TILE, MINB>();
+  const std::int64_t blocks = a.work ? a.work_count : (a.mesh.ne + TILE - 1) / TILE;
+  if (blocks <= 0)
+    return;
+  euler_tri_patch<P, R, TILE, MINB>
+      <<<static_cast<unsigned>(blocks), TILE, PatchSmem<P, TILE>::bytes, s>>>(a);
+}
+
 // Launch shapes of the tile kernels (elements per CTA, register budget):
 //   0: 128 elements, <= 128 registers (4 CTAs / 16 warps per SM)
 //   1: 128 elements, no register cap
@@ -1650,8 +2184,15 @@ void stage_tile(const StageArgs &a, cudaStream_t s) {
 //   5:  96 elements, sized for 5 CTAs per SM (15 warps)
 //   6: 128 elements, sized for 4 CTAs per SM (16 warps)
 //   7: 128 elements, sized for 3 CTAs per SM
+// and of the patch kernel:
+//   8: 128 elements, <= 128 registers (4 CTAs per SM)
+//   9: 128 elements, sized for 5 CTAs per SM
+//  10:  64 elements, sized for 8 CTAs per SM
+//  11:  64 elements, sized for 10 CTAs per SM
 constexpr int kTileShapes = kTileShapeCount;
-constexpr int kTileElements[kTileShapes] = {128, 128, 256, 64, 64, 96, 128, 128};
+constexpr int kTileElements[kTileShapes] = {128, 128, 256, 64, 64, 96, 128, 128,
+                                            128, 128, 64, 64};
+constexpr int kFirstPatchShape = 8;
 
 template <int P, int R> struct StageTile {
   static void run(int shape, const StageArgs &a, cudaStream_t s) {
@@ -1664,6 +2205,10 @@ template <int P, int R> struct StageTile {
     case 5: stage_tile<P, R, 96, 5, true>(a, s); break;
     case 6: stage_tile<P, R, 128, 4, true>(a, s); break;
     case 7: stage_tile<P, R, 128, 3, true>(a, s); break;
+    case 8: stage_patch<P, R, 128, 4>(a, s); break;
+    case 9: stage_patch<P, R, 128, 5>(a, s); break;
+    case 10: stage_patch<P, R, 64, 8>(a, s); break;
+    case 11: stage_patch<P, R, 64, 10>(a, s); break;
     default: throw std::invalid_argument("tile kernel: unknown launch shape");
     }
   }
@@ -1679,6 +2224,10 @@ template <int P, int R> struct PrepareTile {
     shared_opt_in<P, R, 96, 5>();
     shared_opt_in<P, R, 128, 4>();
     shared_opt_in<P, R, 128, 3>();
+    patch_opt_in<P, R, 128, 4>();
+    patch_opt_in<P, R, 128, 5>();
+    patch_opt_in<P, R, 64, 8>();
+    patch_opt_in<P, R, 64, 10>();
   }
 };
 
@@ -1735,6 +2284,8 @@ int euler_tri_tile_shapes() { return kTileShapes; }
 int euler_tri_tile_elements(int shape) {
   return shape >= 0 && shape < kTileShapes ? kTileElements[shape] : 0;
 }
+
+bool euler_tri_tile_is_patch(int shape) { return shape >= kFirstPatchShape && shape < kTileShapes; }
 
 void prepare_euler_tri_stage_tile(int p, int rule) { dispatch_mixed<PrepareTile>(p, rule); }
 

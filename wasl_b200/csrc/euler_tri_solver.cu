@@ -55,6 +55,28 @@ double host_cell_speed(double gamma, const double *mode0, int dimensions) {
   return velocity + std::sqrt(gamma * p / s[0]);
 }
 
+// dst[r][i] = src[r][index[i]] over rows x ne (gather into storage order).
+__global__ void gather_columns(const double *__restrict__ src, double *__restrict__ dst, int rows,
+                               std::int64_t ne, const std::int32_t *__restrict__ index) {
+  const std::int64_t i = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= ne)
+    return;
+  const std::int64_t from = index[i];
+  for (int r = 0; r < rows; ++r)
+    dst[r * ne + i] = src[r * ne + from];
+}
+
+// dst[r][index[i]] = src[r][i] (scatter back to the caller's order).
+__global__ void scatter_columns(const double *__restrict__ src, double *__restrict__ dst, int rows,
+                                std::int64_t ne, const std::int32_t *__restrict__ index) {
+  const std::int64_t i = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= ne)
+    return;
+  const std::int64_t to = index[i];
+  for (int r = 0; r < rows; ++r)
+    dst[r * ne + to] = src[r * ne + i];
+}
+
 class EulerTriSolver final : public Solver {
 public:
   EulerTriSolver(const wasl_gpu_config &cfg, TriTopology &&topo)
@@ -72,6 +94,18 @@ public:
     ne_ = mesh_.element_count;
     const std::int64_t nf = mesh_.face_count();
     const int QF = p_ + 1;
+    // The mixed form stores its elements along a space-filling curve (a pure
+    // relabelling: every face keeps its sides and every element its slot
+    // order, so the arithmetic is unchanged); the caller's order is restored
+    // at every call that takes or returns per-element data.
+    relabel_ = cfg.precision == WASL_MIXED && cfg.element_order == 0 && ne_ > 1;
+    if (relabel_) {
+      order_ = morton_order(mesh_);
+      rank_.resize(ne_);
+      for (std::int64_t i = 0; i < ne_; ++i)
+        rank_[order_[i]] = static_cast<std::int32_t>(i);
+      d_order_.upload(order_, stream_);
+    }
 
     bool has_boundary = false;
     for (std::int64_t f = 0; f < nf; ++f)
@@ -87,7 +121,7 @@ public:
                                  QF, M_);
     boundary_count_ = t.boundary_count;
     if (boundary_count_ > 0) {
-      d_bnd_element_.upload(t.bnd_element, stream_);
+      d_bnd_element_.upload(ids(t.bnd_element), stream_);
       d_bnd_edge_.upload(t.bnd_edge, stream_);
       d_bnd_normal_.upload(t.bnd_normal, stream_);
       d_bnd_value_.resize(static_cast<std::size_t>(4) * boundary_count_);
@@ -115,23 +149,33 @@ public:
         if (cfg.limiting)
           d_rough_.resize(ne_ + 1); // rough list, then its count
         const TileSlotArrays ts = build_tile_slots(mesh_, t, boundary_, QF);
-        d_tile_nbr_.upload(ts.nbr, stream_);
-        d_tile_code_.upload(ts.code, stream_);
-        d_tile_aux_.upload(ts.aux, stream_);
+        d_tile_nbr_.upload(columns(ids(ts.nbr), 3), stream_);
+        d_tile_code_.upload(columns(ts.code, 3), stream_);
+        d_tile_aux_.upload(columns(ts.aux, 3), stream_);
+        PatchEdgeArrays pe;
+        patch_ok_ = !cfg.limiting && build_patch_edges(mesh_, t, boundary_, QF, pe);
+        if (patch_ok_) {
+          d_patch_nbr_.upload(columns(ids(pe.nbr), 3), stream_);
+          d_patch_info_.upload(columns(pe.info, 3), stream_);
+          d_patch_geo_.upload(columns(pe.geo, 9), stream_);
+        }
       }
-      d_face_left_.upload(mesh_.face_left, stream_);
-      d_face_right_.upload(face_right, stream_);
+      if (cfg.mixed_kernel >= 2 && euler_tri_tile_is_patch(cfg.mixed_kernel - 2) && !patch_ok_)
+        throw SolverError(WASL_ERR_ARGUMENT, "2D Euler mixed form: the patch kernel runs without"
+                                             " the limiter on conforming meshes only");
+      d_face_left_.upload(ids(mesh_.face_left), stream_);
+      d_face_right_.upload(ids(face_right), stream_);
       d_face_code_.upload(face_code, stream_);
       d_face_normal_.upload(face_normal, stream_);
-      d_slot_face_.upload(slot_face, stream_);
+      d_slot_face_.upload(columns(slot_face, 3), stream_);
       d_face_record_.resize(euler_tri_mixed_face_record_bytes(p_) * nf);
     }
-    d_geo_.upload(geo, stream_);
-    d_slot_nbr_.upload(slot_nbr, stream_);
-    d_slot_code_.upload(slot_code, stream_);
-    d_slot_geo_.upload(slot_geo, stream_);
+    d_geo_.upload(columns(geo, 5), stream_);
+    d_slot_nbr_.upload(columns(ids(slot_nbr), 3), stream_);
+    d_slot_code_.upload(columns(slot_code, 3), stream_);
+    d_slot_geo_.upload(columns(slot_geo, 9), stream_);
     if (!donors.empty()) {
-      d_donor_.upload(donors, stream_);
+      d_donor_.upload(ids(donors), stream_);
       d_donor_basis_.upload(donor_basis, stream_);
     }
     mixed_ = cfg.precision == WASL_MIXED;
@@ -151,10 +195,10 @@ public:
     limiting_ = cfg.limiting && p_ > 0;
     if (limiting_) {
       stencil_ = triangle_stencil(mesh_, p_, trace.donors);
-      d_neighbors_.upload(stencil_.neighbors, stream_);
-      d_transforms_.upload(stencil_.transforms, stream_);
-      d_normal_x_.upload(stencil_.normal_x, stream_);
-      d_normal_y_.upload(stencil_.normal_y, stream_);
+      d_neighbors_.upload(blocks(ids(stencil_.neighbors), 3), stream_);
+      d_transforms_.upload(blocks(stencil_.transforms, 3 * M_ * M_), stream_);
+      d_normal_x_.upload(columns(stencil_.normal_x, 1), stream_);
+      d_normal_y_.upload(columns(stencil_.normal_y, 1), stream_);
       d_check_.upload(stencil_.check_basis, stream_);
       d_check_bound_.upload(positivity_check_bound(stencil_.check_basis, M_), stream_);
       d_limited_.resize(static_cast<std::size_t>(ne_) * 4 * M_);
@@ -168,7 +212,7 @@ public:
     cuda_check(cudaMemsetAsync(d_u_.get(), 0, d_u_.size() * sizeof(double), stream_), "memset");
     d_error_.resize(1);
     d_speed_.resize(1);
-    d_cfl_.resize(8);
+    d_cfl_.resize(kCflResultWords);
     d_dt_.resize(1);
     cuda_check(cudaMemsetAsync(d_error_.get(), 0, sizeof(unsigned long long), stream_), "memset");
     length_ = minimum_altitude(mesh_);
@@ -212,17 +256,36 @@ public:
 
   void set_state(const double *host) override {
     speed_ready_ = false;
-    cuda_check(cudaMemcpyAsync(d_u_.get(), host, d_u_.size() * sizeof(double),
+    // Relabelled storage: the caller's columns go through the stage buffer.
+    double *target = relabel_ ? d_e_.get() : d_u_.get();
+    cuda_check(cudaMemcpyAsync(target, host, d_u_.size() * sizeof(double),
                                cudaMemcpyHostToDevice, stream_),
                "set_state");
+    if (relabel_) {
+      gather_columns<<<static_cast<unsigned>((ne_ + 255) / 256), 256, 0, stream_>>>(
+          d_e_.get(), d_u_.get(), 4 * M_, ne_, d_order_.get());
+      count_launches(1);
+    }
     cuda_check(cudaStreamSynchronize(stream_), "set_state");
   }
 
   void get_state(double *host) override {
-    cuda_check(cudaMemcpyAsync(host, d_u_.get(), d_u_.size() * sizeof(double),
+    const double *source = d_u_.get();
+    if (relabel_) {
+      scatter_columns<<<static_cast<unsigned>((ne_ + 255) / 256), 256, 0, stream_>>>(
+          d_u_.get(), d_e_.get(), 4 * M_, ne_, d_order_.get());
+      count_launches(1);
+      source = d_e_.get();
+    }
+    cuda_check(cudaMemcpyAsync(host, source, d_u_.size() * sizeof(double),
                                cudaMemcpyDeviceToHost, stream_),
                "get_state");
     cuda_check(cudaStreamSynchronize(stream_), "get_state");
+  }
+
+  void element_order(std::int64_t *order) const override {
+    for (std::int64_t i = 0; i < ne_; ++i)
+      order[i] = relabel_ ? order_[i] : i;
   }
 
   CflArgs cfl_args(double cfl) {
@@ -238,6 +301,7 @@ public:
     a.result = d_cfl_.get();
     a.dt = d_dt_.get();
     a.error = d_error_.get();
+    a.order = relabel_ ? d_order_.get() : nullptr;
     return a;
   }
 
@@ -251,7 +315,7 @@ public:
     CflArgs c = cfl_args(1.0);
     c.dt = nullptr; // the host forms dt
     launch_cfl(c, stream_);
-    count_launches(3);
+    count_launches(1);
     cuda_check(cudaMemcpyAsync(scratch_.words, d_cfl_.get(), 8 * sizeof(unsigned long long),
                                cudaMemcpyDeviceToHost, stream_),
                "cfl result");
@@ -352,11 +416,21 @@ public:
     DeviceArray<std::uint8_t> y(ne_);
     launch_mlp_features(d_u_.get(), ne_, M_, d_neighbors_.get(), F, cfg_.sensor_threshold,
                         stencil_.highest_degree_begin, f.get(), y.get(), stream_);
-    cuda_check(cudaMemcpyAsync(features, f.get(), sizeof(float) * f.size(), cudaMemcpyDeviceToHost,
-                               stream_),
+    std::vector<float> fs(relabel_ ? f.size() : 0);
+    std::vector<std::uint8_t> ys(relabel_ ? ne_ : 0);
+    cuda_check(cudaMemcpyAsync(relabel_ ? fs.data() : features, f.get(), sizeof(float) * f.size(),
+                               cudaMemcpyDeviceToHost, stream_),
                "features");
-    cuda_check(cudaMemcpyAsync(labels, y.get(), ne_, cudaMemcpyDeviceToHost, stream_), "labels");
+    cuda_check(cudaMemcpyAsync(relabel_ ? ys.data() : labels, y.get(), ne_,
+                               cudaMemcpyDeviceToHost, stream_),
+               "labels");
     cuda_check(cudaStreamSynchronize(stream_), "indicator data");
+    if (relabel_)
+      for (std::int64_t i = 0; i < ne_; ++i) {
+        std::copy(fs.begin() + i * F, fs.begin() + (i + 1) * F,
+                  features + static_cast<std::int64_t>(order_[i]) * F);
+        labels[order_[i]] = ys[i];
+      }
   }
 
   // The network's logits for the current state, from the inference kernel
@@ -384,10 +458,14 @@ public:
     m.troubled_count = list.get() + ne_;
     m.logits = z.get();
     launch_mlp_indicator(m, stream_);
-    cuda_check(cudaMemcpyAsync(logits, z.get(), sizeof(float) * ne_, cudaMemcpyDeviceToHost,
-                               stream_),
+    std::vector<float> zs(relabel_ ? ne_ : 0);
+    cuda_check(cudaMemcpyAsync(relabel_ ? zs.data() : logits, z.get(), sizeof(float) * ne_,
+                               cudaMemcpyDeviceToHost, stream_),
                "logits");
     cuda_check(cudaStreamSynchronize(stream_), "indicator logits");
+    if (relabel_)
+      for (std::int64_t i = 0; i < ne_; ++i)
+        logits[order_[i]] = zs[i];
   }
 
   void indicator_stats(unsigned long long *stats, bool reset) override {
@@ -410,9 +488,15 @@ public:
   }
 
   void flags(std::uint8_t *out) override {
-    cuda_check(cudaMemcpyAsync(out, d_flags_.get(), 3 * ne_, cudaMemcpyDeviceToHost, stream_),
+    std::vector<std::uint8_t> stored(relabel_ ? 3 * ne_ : 0);
+    cuda_check(cudaMemcpyAsync(relabel_ ? stored.data() : out, d_flags_.get(), 3 * ne_,
+                               cudaMemcpyDeviceToHost, stream_),
                "flags");
     cuda_check(cudaStreamSynchronize(stream_), "flags");
+    if (relabel_)
+      for (int k = 0; k < 3; ++k)
+        for (std::int64_t i = 0; i < ne_; ++i)
+          out[k * ne_ + order_[i]] = stored[k * ne_ + i];
   }
 
   void mass_energy(double &mass, double &energy) override {
@@ -426,7 +510,7 @@ public:
     cuda_check(cudaStreamSynchronize(stream_), "mass");
     mass = energy = 0.0;
     for (std::int64_t e = 0; e < ne_; ++e) {
-      const double w = std::sqrt(2.0) * mesh_.maps[e].jacobian_determinant();
+      const double w = std::sqrt(2.0) * mesh_.maps[relabel_ ? order_[e] : e].jacobian_determinant();
       mass += w * rho[e];
       energy += w * en[e];
     }
@@ -464,6 +548,9 @@ private:
     a.tile.nbr = d_tile_nbr_.get();
     a.tile.code = d_tile_code_.get();
     a.tile.aux = d_tile_aux_.get();
+    a.patch.nbr = d_patch_nbr_.get();
+    a.patch.info = d_patch_info_.get();
+    a.patch.geo = d_patch_geo_.get();
     // FP64 face islands at discontinuities (the rough pass), with the limiter.
     a.rough = limiting_ ? d_rough_.get() : nullptr;
     a.rough_count = a.rough ? d_rough_.get() + ne_ : nullptr;
@@ -541,9 +628,14 @@ private:
   // fastest, per polynomial order, rule order and mesh size class.
   void tune_mixed(StageArgs a) {
     // With the limiter (flows with discontinuities) only the tile kernel,
-    // whose second pass evaluates faces at discontinuities in FP64, competes.
+    // whose second pass evaluates faces at discontinuities in FP64, competes;
+    // the patch kernel's shapes only where its edge arrays were built.
     const int base = tile_ok_ && limiting_ ? 1 : 0;
-    const int variants = tile_ok_ ? 1 + euler_tri_tile_shapes() - base : 1;
+    int shapes = 0;
+    for (int sh = 0; sh < euler_tri_tile_shapes(); ++sh)
+      if (!euler_tri_tile_is_patch(sh) || patch_ok_)
+        shapes = sh + 1;
+    const int variants = tile_ok_ ? 1 + shapes - base : 1;
     a.stage = 0;
     a.in = d_u_.get();
     a.u0 = d_u_.get();
@@ -563,6 +655,35 @@ private:
       tuning_.ms.insert(tuning_.ms.begin(), 0.0); // face-centric: not timed
     kernel_ = tuning_.choice + base;
     tuning_.choice = kernel_;
+  }
+
+  // Per-element host arrays [count][ne] in storage order.
+  template <typename T> std::vector<T> columns(const std::vector<T> &v, int count) const {
+    if (!relabel_)
+      return v;
+    std::vector<T> out(v.size());
+    for (int r = 0; r < count; ++r)
+      for (std::int64_t i = 0; i < ne_; ++i)
+        out[r * ne_ + i] = v[r * ne_ + order_[i]];
+    return out;
+  }
+  // Per-element host arrays [ne][width] in storage order.
+  template <typename T> std::vector<T> blocks(const std::vector<T> &v, std::int64_t width) const {
+    if (!relabel_)
+      return v;
+    std::vector<T> out(v.size());
+    for (std::int64_t i = 0; i < ne_; ++i)
+      std::copy(v.begin() + order_[i] * width, v.begin() + (order_[i] + 1) * width,
+                out.begin() + i * width);
+    return out;
+  }
+  // Element indices (>= 0) relabelled; negative codes kept.
+  std::vector<std::int32_t> ids(std::vector<std::int32_t> v) const {
+    if (relabel_)
+      for (auto &x : v)
+        if (x >= 0)
+          x = rank_[x];
+    return v;
   }
 
   LimitArgs limit_args(double *state, const std::uint8_t *flags) {
@@ -614,6 +735,13 @@ private:
   bool mixed_ = false;
   bool paired_ = false;
   bool tile_ok_ = false;
+  bool relabel_ = false;  // elements stored along a space-filling curve
+  std::vector<std::int32_t> order_, rank_; // storage -> caller, caller -> storage
+  DeviceArray<std::int32_t> d_order_;
+  bool patch_ok_ = false; // the patch kernel's edge arrays exist (no limiter)
+  DeviceArray<std::int32_t> d_patch_nbr_;
+  DeviceArray<std::uint8_t> d_patch_info_;
+  DeviceArray<double> d_patch_geo_;
   bool fused_speed_ = false; // this step's last stage reduces the next CFL speed
   bool speed_ready_ = false; // d_speed_ holds the current state's CFL speed
   DeviceArray<unsigned long long> d_speed_;

@@ -75,6 +75,17 @@ struct TileSlots {
   const std::int32_t *aux = nullptr;
 };
 
+// Per-local-edge arrays of the patch kernel, [3][ne] each (geo [3][3][ne]):
+// the element across local edge j (-1 on a transmissive boundary), an info
+// byte (bit 0 this element is the face's left side, bits 1-2 the neighbour's
+// local edge, bit 3 the neighbour's points run in the opposite order), and the
+// face's normal (left to right) and scale.
+struct PatchEdges {
+  const std::int32_t *nbr = nullptr;
+  const std::uint8_t *info = nullptr;
+  const double *geo = nullptr;
+};
+
 // One entry of a tile work list: elements [first, first + count) of one case
 // (count <= the kernel's tile size), and the case whose dt applies.
 struct TileWork {
@@ -110,6 +121,7 @@ struct StageArgs {
   // Fused tile kernel: slots, and an optional work list (null: tile b covers
   // elements [b T, b T + T)) with per-case time steps (null: dt / dt_value).
   TileSlots tile;
+  PatchEdges patch;
   const TileWork *work = nullptr;
   std::int64_t work_count = 0;
   const double *case_dt = nullptr;
@@ -178,9 +190,13 @@ struct SenseArgs {
 };
 
 // Largest cell-average wave speed |u| + c (cpp/src/time/cfl_timestep.cpp:33-47).
-// result[0] = speed bits (max), result[1] = smallest element index reaching it,
-// result[2..5] = that element's mode-0 coefficients, then dt in result[6]
-// computed on the device as cfl h / (speed (2p+1)).
+// result[0] = speed bits (max), result[1] = ~(smallest element index reaching
+// it), result[2..5] = that element's mode-0 coefficients, then dt in result[6]
+// computed on the device as cfl h / (speed (2p+1)).  result[8] counts the
+// blocks that have finished and result[16..) holds each block's (speed,
+// element) pair: the buffer has kCflResultWords words.
+constexpr int kCflBlocks = 148 * 4;
+constexpr std::size_t kCflResultWords = 16 + 2 * kCflBlocks;
 struct CflArgs {
   std::int64_t ne = 0;
   int M = 1;
@@ -190,9 +206,12 @@ struct CflArgs {
   double cfl = 0.1;
   double length = 0.0; // minimum altitude (2D) or length (1D)
   int p = 0;
-  unsigned long long *result = nullptr; // 8 words, zeroed by the first kernel
+  unsigned long long *result = nullptr; // kCflResultWords words
   double *dt = nullptr;                 // device dt written by the final kernel
   unsigned long long *error = nullptr;
+  // Storage order (storage column -> caller's element), or null: ties of the
+  // largest speed go to the smallest caller's index either way.
+  const std::int32_t *order = nullptr;
 };
 
 // Reference-line tables of the 1D kernels: orthonormal Legendre modes and
@@ -266,9 +285,12 @@ void launch_batch_speed(const double *state, std::int64_t ne, int M, double gamm
                         unsigned long long *error, int *status, cudaStream_t stream);
 // Number of launch shapes of the tile kernels (euler_tri_tile_shapes()
 // returns it; per-shape host arrays are sized by it).
-constexpr int kTileShapeCount = 8;
+constexpr int kTileShapeCount = 12;
 int euler_tri_tile_shapes();
 int euler_tri_tile_elements(int shape);
+// Shapes of the patch kernel (StageArgs::patch; no rough pass, so runs
+// without the limiter only).
+bool euler_tri_tile_is_patch(int shape);
 void launch_euler_tri_stage_tile(int p, int rule, int shape, const StageArgs &a,
                                  cudaStream_t stream);
 // Sets the tile kernels' launch attributes on the current device (call
@@ -276,6 +298,7 @@ void launch_euler_tri_stage_tile(int p, int rule, int shape, const StageArgs &a,
 void prepare_euler_tri_stage_tile(int p, int rule);
 void launch_limit_f64(int M, int NB, const LimitArgs &a, cudaStream_t stream);
 void launch_sense_f64(int M, const SenseArgs &a, cudaStream_t stream);
+// One kernel: the speed, the arg-max and dt (result[0..6], and *a.dt).
 void launch_cfl(const CflArgs &a, cudaStream_t stream);
 // The largest cell-average wave speed alone (a.result[0], zeroed first; no
 // arg-max and no dt): for device-resident steps, whose dt comes from it by

@@ -63,7 +63,7 @@ public:
       b->resize(static_cast<std::size_t>(V_) * M_ * ne_);
     cuda_check(cudaMemsetAsync(d_u_.get(), 0, d_u_.size() * sizeof(double), stream_), "memset");
     d_error_.resize(1);
-    d_cfl_.resize(8);
+    d_cfl_.resize(kCflResultWords);
     d_dt_.resize(1);
     cuda_check(cudaMemsetAsync(d_error_.get(), 0, sizeof(unsigned long long), stream_), "memset");
     length_ = minimum_length(mesh_);
@@ -165,7 +165,7 @@ public:
       return cfl * length_ / (std::fabs(cfg_.velocity_x) * (2.0 * p_ + 1.0));
     }
     launch_cfl(cfl_args(cfl), stream_);
-    count_launches(3);
+    count_launches(1);
     cuda_check(cudaMemcpyAsync(scratch_.words, d_cfl_.get(), 8 * sizeof(unsigned long long),
                                cudaMemcpyDeviceToHost, stream_),
                "cfl result");
@@ -213,7 +213,7 @@ public:
     } else {
       for (std::int64_t n = 0; n < steps; ++n) {
         launch_cfl(cfl_args(cfl), stream_);
-        count_launches(3);
+        count_launches(1);
         enqueue_step(d_dt_.get(), 0.0);
       }
     }

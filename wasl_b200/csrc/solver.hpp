@@ -111,6 +111,11 @@ public:
   virtual void flags(std::uint8_t *out) = 0;
   virtual void mass_energy(double &mass, double &energy) = 0;
   virtual double *state_device() = 0;
+  // order[i]: the caller's element stored at column i of state_device().
+  virtual void element_order(std::int64_t *order) const {
+    for (std::int64_t e = 0; e < elements(); ++e)
+      order[e] = e;
+  }
   // Quadrature of rule order r on every element: physical points and weights
   // (reference weight x |det J|), packed [element][point].
   virtual int rule_points(int rule_order) const = 0;

@@ -29,6 +29,35 @@ struct TileSlotArrays {
 };
 TileSlotArrays build_tile_slots(const TriTopology &mesh, const TriSlots &t, int boundary, int QF);
 
+// Per-element, per-local-edge arrays of the patch kernel, [3][ne] (the
+// element's local edges 0..2, not its faces in face order):
+//   nbr   the element across the edge; -1 on a transmissive boundary.  A
+//         periodic face pair is one face between the two elements (the
+//         lower-numbered face of the pair is kept: its element is the left
+//         side, with that face's normal and scale).
+//   info  bit 0: this element is the face's left side (on a boundary: set);
+//         bits 1-2: the neighbour's local edge; bit 3: the neighbour's edge
+//         points run in the opposite order (its point QF-1-q is this face's
+//         point q).
+//   geo   [3 edges][3][ne]: the face's normal (left to right) and scale.
+// The point order of every face is matched on physical coordinates (periodic
+// pairs relative to each edge's midpoint); returns false, leaving `out`
+// incomplete, where a face's points do not match (a non-conforming mesh) or a
+// periodic boundary face has no single partner.
+struct PatchEdgeArrays {
+  std::vector<std::int32_t> nbr;
+  std::vector<std::uint8_t> info;
+  std::vector<double> geo;
+};
+bool build_patch_edges(const TriTopology &mesh, const TriSlots &t, int boundary, int QF,
+                       PatchEdgeArrays &out);
+
+// An element order along a space-filling (Morton) curve of the element
+// centroids: order[i] is the element stored at position i.  Consecutive
+// positions are then close in space, so a patch of consecutive elements
+// shares most of its faces.  Ties keep the mesh order.
+std::vector<std::int32_t> morton_order(const TriTopology &mesh);
+
 // Physical points and weights (reference weight x |det J|) of the collapsed
 // rule of order r on every element, packed [element][point]; w may be null.
 void tri_quadrature(const TriTopology &mesh, int rule_order, double *x, double *y, double *w);

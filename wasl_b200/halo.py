@@ -184,15 +184,25 @@ class HaloExchange:
     it as well)."""
 
     def __init__(self, mesh: LocalMesh, schedule: HaloSchedule, rows: int, device="cpu",
-                 group=None):
+                 group=None, element_order=None):
+        """element_order: the handle's storage order (Solver.element_order()),
+        when the exchanged state is its device storage; None: the local mesh's
+        own element order."""
         import torch
         self.torch = torch
         self.group = group
         self.rows = rows
-        self.sends = [(peer, torch.as_tensor(mesh.local_index(el), device=device))
-                      for peer, el in schedule.sends]
-        self.recvs = [(peer, torch.as_tensor(mesh.local_index(el), device=device))
-                      for peer, el in schedule.recvs]
+        column = None
+        if element_order is not None:
+            column = np.empty(len(element_order), dtype=np.int64)
+            column[np.asarray(element_order)] = np.arange(len(element_order))
+
+        def index(elements):
+            local = mesh.local_index(elements)
+            return torch.as_tensor(local if column is None else column[local], device=device)
+
+        self.sends = [(peer, index(el)) for peer, el in schedule.sends]
+        self.recvs = [(peer, index(el)) for peer, el in schedule.recvs]
 
     def exchange(self, state) -> None:
         """state: [rows][local elements] float64 tensor on the rank's device."""
@@ -224,7 +234,8 @@ class _DeviceRows:
 
 def device_state(solver):
     """The handle's device state U[variable][mode][element] as a
-    [4 M][elements] torch tensor sharing its memory (no copy).  The handle's
+    [4 M][elements] torch tensor sharing its memory (no copy), its columns in
+    the handle's storage order (Solver.element_order()).  The handle's
     stream must have finished (solver.sync()) before it is read, and writes
     through it must have finished before the handle's next step."""
     import torch

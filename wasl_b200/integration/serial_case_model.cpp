@@ -2,9 +2,11 @@
 #include "serial_case_model.hpp"
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <exception>
 #include <map>
+#include <sstream>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -16,7 +18,15 @@
 #include "wasl/case/case_validation.hpp"
 #include "wasl/case/initial_state.hpp"
 #include "wasl/equations/euler/euler.hpp"
+#include "wasl/case/mpi_run_directory.hpp"
+#include "wasl/io/checkpoint_file.hpp"
+#include "wasl/io/prepared_mesh_file.hpp"
+#include "wasl/io/vtu_writer.hpp"
+#include "wasl/mesh/line/build_line_mesh.hpp"
+#include "wasl/mesh/msh/msh_reader.hpp"
 #include "wasl/mesh/prepared/mesh_from_prepared.hpp"
+#include "wasl/mesh/prepared/prepare_mesh.hpp"
+#include "wasl/mesh/triangle/build_triangle_mesh.hpp"
 
 namespace wasl_b200 {
 
@@ -109,15 +119,22 @@ GpuEulerModel::GpuEulerModel(const wasl::EulerCase &config, const wasl::CaseMesh
     check(wasl_gpu_get_state(gpu_, state.data(), size(state)));
     return state;
   };
+  // run_serial_case calls advance right after stable_time_step on the same
+  // state (cpp/src/case/serial_case_runner.cpp:127-129), so the state that
+  // stable_time_step uploaded is still on the device: advance uploads only a
+  // vector other than that one.
   model_.stable_time_step = [this, cfl, size](const wasl::SerialCaseModel::State &state) {
     double dt = 0.0;
     check(wasl_gpu_set_state(gpu_, state.data(), size(state)));
+    uploaded_ = state.data();
     check(wasl_gpu_stable_dt(gpu_, cfl, &dt));
     return dt;
   };
   model_.advance = [this, size](double dt, wasl::SerialCaseModel::State &state,
                                 wasl::SspRk3Workspace &) {
-    check(wasl_gpu_set_state(gpu_, state.data(), size(state)));
+    if (state.data() != uploaded_)
+      check(wasl_gpu_set_state(gpu_, state.data(), size(state)));
+    uploaded_ = nullptr;
     check(wasl_gpu_step(gpu_, dt));
     check(wasl_gpu_get_state(gpu_, state.data(), size(state)));
   };
@@ -231,101 +248,163 @@ void GpuScalarAdvectionModel::check(int status) const {
 
 wasl::SimulationSummary run_scalar_advection_case_gpu(const wasl::ScalarAdvectionCase &config) {
   wasl::validate_scalar_advection_case(config);
-  if (config.mpi)
-    throw std::runtime_error("run_scalar_advection_case_gpu: MPI runs are not on the GPU path");
   if (config.dimensions == 2 && !wasl::all_periodic(config.boundaries))
     throw std::runtime_error("simulation: 2D scalar-advection boundaries must be periodic");
   const auto mesh = wasl::load_case_mesh(config.files.prepared_mesh, config.dimensions);
+  // The reference's distributed line driver, in a build without MPI
+  // (cpp/src/case/scalar_advection_distributed.cpp:286-289); triangles ignore
+  // the flag (cpp/src/case/scalar_advection_case.cpp:10-15).
+  if (config.dimensions == 1 && config.mpi)
+    throw std::runtime_error("simulation: bridge was built without MPI support");
   const GpuScalarAdvectionModel gpu(config, mesh);
   return wasl::run_serial_case(config.files, config.run, mesh, gpu.model());
 }
 
-wasl::EulerCase euler_case_from_arguments(const char *prepared_mesh, const char *output_directory,
-                                          const char *restart, int limiting,
-                                          double sensor_threshold, double density_floor,
-                                          double pressure_floor, int dimensions,
-                                          int polynomial_order, double heat_capacity_ratio,
-                                          double cfl, double start_time, double end_time,
-                                          std::uint64_t max_steps, std::uint64_t history_interval,
-                                          std::uint64_t visualization_interval,
-                                          std::uint64_t checkpoint_interval,
-                                          std::uint64_t keep_checkpoints, const double *regions,
-                                          std::size_t region_count) {
-  wasl::EulerCase c;
-  c.files = {prepared_mesh, output_directory, restart ? restart : ""};
-  c.run = {start_time,           end_time,           max_steps,       history_interval,
-           visualization_interval, checkpoint_interval, keep_checkpoints};
-  c.limiting = limiting != 0;
-  c.sensor_threshold = sensor_threshold;
-  c.density_floor = density_floor;
-  c.pressure_floor = pressure_floor;
-  c.dimensions = dimensions;
-  c.polynomial_order = polynomial_order;
-  c.heat_capacity_ratio = heat_capacity_ratio;
-  c.cfl = cfl;
-  for (std::size_t i = 0; i < region_count; ++i) {
-    const double *r = regions + 10 * i;
-    wasl::EulerRegion region;
-    const int shape = static_cast<int>(r[0]);
-    region.shape = shape == 1   ? wasl::EulerRegion::Shape::interval
-                   : shape == 2 ? wasl::EulerRegion::Shape::circle
-                                : wasl::EulerRegion::Shape::default_region;
-    region.lower = r[1];
-    region.upper = r[2];
-    region.center_x = r[3];
-    region.center_y = r[4];
-    region.radius = r[5];
-    region.value = {r[6], r[7], r[8], r[9]};
-    c.initial_regions.push_back(region);
+namespace {
+
+void write_text(const std::string &text, char *out, std::size_t length) {
+  if (out && length) {
+    std::strncpy(out, text.c_str(), length - 1);
+    out[length - 1] = '\0';
   }
-  return c;
 }
 
-} // namespace wasl_b200
+// The bridge's summary string (crates/wasl-bridge/src/bridge.cpp:39-45).
+std::string summary_message(const wasl::SimulationSummary &summary) {
+  std::ostringstream message;
+  message.precision(17);
+  message << "step=" << summary.step << " time=" << summary.time
+          << " checkpoint=" << summary.checkpoint.string();
+  return message.str();
+}
 
-extern "C" int wasl_run_euler_case_gpu(
-    const char *prepared_mesh, const char *output_directory, const char *restart, int limiting,
-    double sensor_threshold, double density_floor, double pressure_floor, int dimensions,
-    int polynomial_order, double heat_capacity_ratio, double cfl, double start_time,
-    double end_time, std::uint64_t max_steps, std::uint64_t history_interval,
-    std::uint64_t visualization_interval, std::uint64_t checkpoint_interval,
-    std::uint64_t keep_checkpoints, const double *regions, std::size_t region_count,
-    int precision, std::uint64_t *steps, double *time, char *error, std::size_t error_length) {
+// The bridge's named boundaries (bridge.cpp:48-62); one length for the three
+// parallel arrays, so only the kind needs checking.
+std::vector<wasl::NamedBoundary> named_boundaries(const char *const *names,
+                                                  const std::uint8_t *kinds,
+                                                  const double *values, std::size_t count) {
+  std::vector<wasl::NamedBoundary> boundaries;
+  if (count && (!names || !kinds || !values))
+    throw std::runtime_error("boundaries: invalid boundary data");
+  for (std::size_t i = 0; i < count; ++i) {
+    if (!names[i] || kinds[i] > static_cast<std::uint8_t>(wasl::BoundaryKind::outflow))
+      throw std::runtime_error("boundaries: invalid boundary kind");
+    boundaries.push_back({names[i], {static_cast<wasl::BoundaryKind>(kinds[i]), values[i]}});
+  }
+  return boundaries;
+}
+
+wasl::CaseFiles case_files(const char *mesh, const char *output, const char *restart) {
+  if (!mesh || !output)
+    throw std::runtime_error("files: mesh and output paths are required");
+  return {mesh, output, restart ? restart : ""};
+}
+
+template <typename Body>
+int twin(char *summary, std::size_t summary_length, char *error, std::size_t error_length,
+         Body &&body) {
   try {
-    const auto config = wasl_b200::euler_case_from_arguments(
-        prepared_mesh, output_directory, restart, limiting, sensor_threshold, density_floor,
-        pressure_floor, dimensions, polynomial_order, heat_capacity_ratio, cfl, start_time,
-        end_time, max_steps, history_interval, visualization_interval, checkpoint_interval,
-        keep_checkpoints, regions, region_count);
-    const auto summary = wasl_b200::run_euler_case_gpu(config, precision);
-    if (steps)
-      *steps = summary.step;
-    if (time)
-      *time = summary.time;
+    write_text(body(), summary, summary_length);
     return 0;
   } catch (const std::exception &e) {
-    if (error && error_length) {
-      std::strncpy(error, e.what(), error_length - 1);
-      error[error_length - 1] = '\0';
-    }
+    write_text(e.what(), error, error_length);
     return -2;
   }
 }
 
+} // namespace
+} // namespace wasl_b200
+
+extern "C" int wasl_run_euler_case_gpu_ex(
+    const char *mesh_path, const char *output_path, const char *restart_path, int limiting,
+    double sensor_threshold, double density_floor, double pressure_floor, int dimensions,
+    int polynomial_order, double heat_capacity_ratio, double cfl, double start_time,
+    double end_time, std::uint64_t max_steps, std::uint64_t history_interval,
+    std::uint64_t visualization_interval, std::uint64_t checkpoint_interval,
+    std::uint64_t keep_checkpoints, const double *regions, std::size_t regions_length,
+    const char *const *boundary_names, const std::uint8_t *boundary_kinds,
+    const double *boundary_values, std::size_t boundary_count, int precision, char *summary,
+    std::size_t summary_length, char *error, std::size_t error_length) {
+  using namespace wasl_b200;
+  return twin(summary, summary_length, error, error_length, [&] {
+    // bridge.cpp:183-216
+    constexpr std::size_t width = 10;
+    if (regions_length % width != 0 || (regions_length && !regions))
+      throw std::runtime_error("initial.regions: invalid Euler region data");
+    wasl::EulerCase c;
+    c.files = case_files(mesh_path, output_path, restart_path);
+    c.run = {start_time,           end_time,           max_steps,       history_interval,
+             visualization_interval, checkpoint_interval, keep_checkpoints};
+    c.limiting = limiting != 0;
+    c.sensor_threshold = sensor_threshold;
+    c.density_floor = density_floor;
+    c.pressure_floor = pressure_floor;
+    c.dimensions = dimensions;
+    c.polynomial_order = polynomial_order;
+    c.heat_capacity_ratio = heat_capacity_ratio;
+    c.cfl = cfl;
+    for (std::size_t i = 0; i < regions_length; i += width) {
+      const double *r = regions + i;
+      const int shape = static_cast<int>(r[0]);
+      if (shape < 0 || shape > 2)
+        throw std::runtime_error("initial.regions: invalid Euler region shape");
+      wasl::EulerRegion region;
+      region.shape = static_cast<wasl::EulerRegion::Shape>(shape);
+      region.lower = r[1];
+      region.upper = r[2];
+      region.center_x = r[3];
+      region.center_y = r[4];
+      region.radius = r[5];
+      region.value = {r[6], r[7], r[8], r[9]};
+      c.initial_regions.push_back(region);
+    }
+    c.boundaries = named_boundaries(boundary_names, boundary_kinds, boundary_values,
+                                    boundary_count);
+    return summary_message(run_euler_case_gpu(c, precision));
+  });
+}
+
+extern "C" int wasl_run_euler_case_gpu(
+    const char *mesh_path, const char *output_path, const char *restart_path, int limiting,
+    double sensor_threshold, double density_floor, double pressure_floor, int dimensions,
+    int polynomial_order, double heat_capacity_ratio, double cfl, double start_time,
+    double end_time, std::uint64_t max_steps, std::uint64_t history_interval,
+    std::uint64_t visualization_interval, std::uint64_t checkpoint_interval,
+    std::uint64_t keep_checkpoints, const double *regions, std::size_t regions_length,
+    const char *const *boundary_names, const std::uint8_t *boundary_kinds,
+    const double *boundary_values, std::size_t boundary_count, char *summary,
+    std::size_t summary_length, char *error, std::size_t error_length) {
+  return wasl_run_euler_case_gpu_ex(
+      mesh_path, output_path, restart_path, limiting, sensor_threshold, density_floor,
+      pressure_floor, dimensions, polynomial_order, heat_capacity_ratio, cfl, start_time, end_time,
+      max_steps, history_interval, visualization_interval, checkpoint_interval, keep_checkpoints,
+      regions, regions_length, boundary_names, boundary_kinds, boundary_values, boundary_count,
+      WASL_PLAIN_FP64, summary, summary_length, error, error_length);
+}
+
 extern "C" int wasl_run_scalar_advection_case_gpu(
-    const char *prepared_mesh, const char *output_directory, const char *restart,
+    const char *mesh_path, const char *output_path, const char *restart_path, int mpi,
     int dimensions, int polynomial_order, double velocity_x, double velocity_y, double cfl,
     double start_time, double end_time, std::uint64_t max_steps, std::uint64_t history_interval,
     std::uint64_t visualization_interval, std::uint64_t checkpoint_interval,
     std::uint64_t keep_checkpoints, double initial_default, int initial_sine,
-    double initial_sine_amplitude, const double *intervals, std::size_t interval_count,
-    const double *circles, std::size_t circle_count, std::uint64_t *steps, double *time,
-    char *error, std::size_t error_length) {
-  try {
+    double initial_sine_amplitude, const double *intervals, std::size_t intervals_length,
+    const double *circles, std::size_t circles_length, const char *const *boundary_names,
+    const std::uint8_t *boundary_kinds, const double *boundary_values,
+    std::size_t boundary_count, char *summary, std::size_t summary_length, char *error,
+    std::size_t error_length) {
+  using namespace wasl_b200;
+  return twin(summary, summary_length, error, error_length, [&] {
+    // bridge.cpp:141-181
+    if (intervals_length % 3 != 0 || (intervals_length && !intervals))
+      throw std::runtime_error("initial.regions: invalid interval data");
+    if (circles_length % 4 != 0 || (circles_length && !circles))
+      throw std::runtime_error("initial.regions: invalid circle data");
     wasl::ScalarAdvectionCase c;
-    c.files = {prepared_mesh, output_directory, restart ? restart : ""};
+    c.files = case_files(mesh_path, output_path, restart_path);
     c.run = {start_time,           end_time,           max_steps,       history_interval,
              visualization_interval, checkpoint_interval, keep_checkpoints};
+    c.mpi = mpi != 0;
     c.dimensions = dimensions;
     c.polynomial_order = polynomial_order;
     c.wavespeed = velocity_x;
@@ -334,22 +413,92 @@ extern "C" int wasl_run_scalar_advection_case_gpu(
     c.initial_default = initial_default;
     c.initial_sine = initial_sine != 0;
     c.initial_sine_amplitude = initial_sine_amplitude;
-    for (std::size_t i = 0; i < interval_count; ++i)
-      c.initial_intervals.push_back({intervals[3 * i], intervals[3 * i + 1], intervals[3 * i + 2]});
-    for (std::size_t i = 0; i < circle_count; ++i)
-      c.initial_circles.push_back(
-          {circles[4 * i], circles[4 * i + 1], circles[4 * i + 2], circles[4 * i + 3]});
-    const auto summary = wasl_b200::run_scalar_advection_case_gpu(c);
-    if (steps)
-      *steps = summary.step;
-    if (time)
-      *time = summary.time;
-    return 0;
-  } catch (const std::exception &e) {
-    if (error && error_length) {
-      std::strncpy(error, e.what(), error_length - 1);
-      error[error_length - 1] = '\0';
-    }
-    return -2;
-  }
+    for (std::size_t i = 0; i < intervals_length; i += 3)
+      c.initial_intervals.push_back({intervals[i], intervals[i + 1], intervals[i + 2]});
+    for (std::size_t i = 0; i < circles_length; i += 4)
+      c.initial_circles.push_back({circles[i], circles[i + 1], circles[i + 2], circles[i + 3]});
+    c.boundaries = named_boundaries(boundary_names, boundary_kinds, boundary_values,
+                                    boundary_count);
+    return summary_message(run_scalar_advection_case_gpu(c));
+  });
+}
+
+extern "C" int wasl_inspect_checkpoint(const char *checkpoint_path, char *summary,
+                                       std::size_t summary_length, char *error,
+                                       std::size_t error_length) {
+  using namespace wasl_b200;
+  return twin(summary, summary_length, error, error_length, [&] {
+    // bridge.cpp:93-101
+    const auto checkpoint = wasl::read_checkpoint(checkpoint_path ? checkpoint_path : "");
+    std::ostringstream out;
+    out.precision(17);
+    out << "step=" << checkpoint.step << " time=" << checkpoint.time
+        << " variables=" << checkpoint.variable_count << " modes=" << checkpoint.mode_count
+        << " elements=" << checkpoint.element_count;
+    return out.str();
+  });
+}
+
+extern "C" int wasl_inspect_prepared_mesh(const char *mesh_path, char *summary,
+                                          std::size_t summary_length, char *error,
+                                          std::size_t error_length) {
+  using namespace wasl_b200;
+  return twin(summary, summary_length, error, error_length, [&] {
+    // bridge.cpp:103-107
+    const auto mesh = wasl::read_prepared_mesh(mesh_path ? mesh_path : "");
+    return std::to_string(mesh.dimension) + "D mesh with " + std::to_string(mesh.element_count()) +
+           " elements";
+  });
+}
+
+extern "C" int wasl_export_checkpoint(const char *checkpoint_path, const char *mesh_path,
+                                      const char *output_path, char *summary,
+                                      std::size_t summary_length, char *error,
+                                      std::size_t error_length) {
+  using namespace wasl_b200;
+  return twin(summary, summary_length, error, error_length, [&] {
+    // bridge.cpp:109-129: cell averages c_0 / sqrt(2) of every variable to VTU.
+    const auto checkpoint = wasl::read_checkpoint(checkpoint_path ? checkpoint_path : "");
+    const auto mesh = wasl::read_prepared_mesh(mesh_path ? mesh_path : "");
+    if (checkpoint.element_count != mesh.element_count())
+      throw std::runtime_error("checkpoint export: mesh element count mismatch");
+    const double inverse_sqrt2 = 1.0 / std::sqrt(2.0);
+    const std::size_t nv = checkpoint.variable_count, ne = checkpoint.element_count;
+    std::vector<double> averages(nv * ne);
+    for (std::size_t v = 0; v < nv; ++v)
+      for (std::size_t e = 0; e < ne; ++e)
+        averages[e * nv + v] = checkpoint.coefficients[(v * checkpoint.mode_count) * ne + e] *
+                               inverse_sqrt2;
+    wasl::write_vtu(output_path ? output_path : "", mesh, averages, nv);
+    return "exported " + std::to_string(ne) + " cells";
+  });
+}
+
+extern "C" int wasl_prepare_mesh(const char *source_path, const char *output_path, char *summary,
+                                 std::size_t summary_length, char *error,
+                                 std::size_t error_length) {
+  using namespace wasl_b200;
+  return twin(summary, summary_length, error, error_length, [&] {
+    // bridge.cpp:79-91
+    const auto document = wasl::read_msh(source_path ? source_path : "");
+    const bool has_triangles = std::any_of(
+        document.elements.begin(), document.elements.end(),
+        [](const auto &element) { return element.element_type == wasl::msh_triangle_element; });
+    const auto prepared = has_triangles ? wasl::prepare_mesh(wasl::build_triangle_mesh(document))
+                                        : wasl::prepare_mesh(wasl::build_line_mesh(document));
+    wasl::write_prepared_mesh(output_path ? output_path : "", prepared);
+    return "prepared " + std::to_string(prepared.element_count()) + " elements";
+  });
+}
+
+extern "C" int wasl_prepare_mpi_run_directory(const char *root_path, const char *effective_config,
+                                              char *summary, std::size_t summary_length,
+                                              char *error, std::size_t error_length) {
+  using namespace wasl_b200;
+  return twin(summary, summary_length, error, error_length, [&] {
+    // bridge.cpp:131-133
+    return wasl::prepare_mpi_run_directory(root_path ? root_path : "",
+                                           effective_config ? effective_config : "")
+        .string();
+  });
 }

@@ -41,6 +41,7 @@ private:
   void check(int status) const;
 
   wasl_gpu *gpu_ = nullptr;
+  const double *uploaded_ = nullptr; // the host vector stable_time_step just uploaded
   wasl::EulerCase config_;
   wasl::LineMesh line_;          // dimensions 1
   wasl::TriangleMesh triangles_; // dimensions 2
@@ -79,50 +80,81 @@ private:
 // GPU model, for serial runs (the two-rank MPI driver is not on this path).
 wasl::SimulationSummary run_scalar_advection_case_gpu(const wasl::ScalarAdvectionCase &config);
 
-// The bridge's flat run_euler_case arguments (crates/wasl-bridge/include/bridge.hpp:24-32)
-// for a periodic case (empty boundary list): each region is 10 doubles (shape 0 default, 1 interval,
-// 2 circle; lower, upper, centre x, centre y, radius; density, velocity x,
-// velocity y, pressure).
-wasl::EulerCase euler_case_from_arguments(const char *prepared_mesh, const char *output_directory,
-                                          const char *restart, int limiting,
-                                          double sensor_threshold, double density_floor,
-                                          double pressure_floor, int dimensions,
-                                          int polynomial_order, double heat_capacity_ratio,
-                                          double cfl, double start_time, double end_time,
-                                          std::uint64_t max_steps, std::uint64_t history_interval,
-                                          std::uint64_t visualization_interval,
-                                          std::uint64_t checkpoint_interval,
-                                          std::uint64_t keep_checkpoints, const double *regions,
-                                          std::size_t region_count);
-
 } // namespace wasl_b200
 
+// C twins of the reference bridge's coarse functions
+// (crates/wasl-bridge/include/bridge.hpp:7-32, defined at
+// crates/wasl-bridge/src/bridge.cpp:79-216), so the Rust `ffi` block can bind
+// them directly: rust::Str becomes a NUL-terminated const char *,
+// rust::Slice<const T> a pointer and its length (element count, as
+// Slice::size()), rust::Slice<const rust::String> an array of const char *,
+// `bool` an int, and the returned rust::String is written to `summary`
+// (truncated to summary_length - 1 bytes, NUL-terminated).  Every twin returns
+// 0 on success; on failure -2 with the reference's message (the
+// std::exception text cxx would turn into Err) in `error`.  They run the
+// reference's own case code; the solver runs use the GPU-backed models above.
 extern "C" {
-// run_euler_case_gpu from flat arguments (as euler_case_from_arguments); 0 on
-// success with the summary's step count and final time, else -2 with the
-// reference's message in `error`.
-int wasl_run_euler_case_gpu(const char *prepared_mesh, const char *output_directory,
-                            const char *restart, int limiting, double sensor_threshold,
+// run_euler_case (bridge.hpp:24-32) on the plain FP64 GPU path: the drop-in.
+// regions: 10 doubles per region (shape 0 default, 1 interval, 2 circle;
+// lower, upper, centre x, centre y, radius; density, velocity x, velocity y,
+// pressure); boundary kinds 0 periodic, 1 inflow, 2 outflow.
+int wasl_run_euler_case_gpu(const char *mesh_path, const char *output_path,
+                            const char *restart_path, int limiting, double sensor_threshold,
                             double density_floor, double pressure_floor, int dimensions,
                             int polynomial_order, double heat_capacity_ratio, double cfl,
                             double start_time, double end_time, std::uint64_t max_steps,
                             std::uint64_t history_interval, std::uint64_t visualization_interval,
                             std::uint64_t checkpoint_interval, std::uint64_t keep_checkpoints,
-                            const double *regions, std::size_t region_count, int precision,
-                            std::uint64_t *steps, double *time, char *error,
+                            const double *regions, std::size_t regions_length,
+                            const char *const *boundary_names, const std::uint8_t *boundary_kinds,
+                            const double *boundary_values, std::size_t boundary_count,
+                            char *summary, std::size_t summary_length, char *error,
                             std::size_t error_length);
 
-// run_scalar_advection_case_gpu from the bridge's flat arguments
-// (crates/wasl-bridge/include/bridge.hpp:13-22) for a periodic serial case:
-// intervals are 3 doubles each (lower, upper, value), circles 4 (centre x,
-// centre y, radius, value).  Statuses as wasl_run_euler_case_gpu.
+// wasl_run_euler_case_gpu with a choice of precision form (enum
+// wasl_precision; WASL_PLAIN_FP64 gives wasl_run_euler_case_gpu).  No
+// counterpart in the bridge.
+int wasl_run_euler_case_gpu_ex(
+    const char *mesh_path, const char *output_path, const char *restart_path, int limiting,
+    double sensor_threshold, double density_floor, double pressure_floor, int dimensions,
+    int polynomial_order, double heat_capacity_ratio, double cfl, double start_time,
+    double end_time, std::uint64_t max_steps, std::uint64_t history_interval,
+    std::uint64_t visualization_interval, std::uint64_t checkpoint_interval,
+    std::uint64_t keep_checkpoints, const double *regions, std::size_t regions_length,
+    const char *const *boundary_names, const std::uint8_t *boundary_kinds,
+    const double *boundary_values, std::size_t boundary_count, int precision, char *summary,
+    std::size_t summary_length, char *error, std::size_t error_length);
+
+// run_scalar_advection_case (bridge.hpp:13-22) on the GPU: intervals 3
+// doubles each (lower, upper, value), circles 4 (centre x, centre y, radius,
+// value).  mpi on a line mesh fails as the reference's non-MPI build does
+// ("simulation: bridge was built without MPI support"); on triangles it is
+// ignored, as the reference ignores it.
 int wasl_run_scalar_advection_case_gpu(
-    const char *prepared_mesh, const char *output_directory, const char *restart,
+    const char *mesh_path, const char *output_path, const char *restart_path, int mpi,
     int dimensions, int polynomial_order, double velocity_x, double velocity_y, double cfl,
     double start_time, double end_time, std::uint64_t max_steps, std::uint64_t history_interval,
     std::uint64_t visualization_interval, std::uint64_t checkpoint_interval,
     std::uint64_t keep_checkpoints, double initial_default, int initial_sine,
-    double initial_sine_amplitude, const double *intervals, std::size_t interval_count,
-    const double *circles, std::size_t circle_count, std::uint64_t *steps, double *time,
-    char *error, std::size_t error_length);
+    double initial_sine_amplitude, const double *intervals, std::size_t intervals_length,
+    const double *circles, std::size_t circles_length, const char *const *boundary_names,
+    const std::uint8_t *boundary_kinds, const double *boundary_values,
+    std::size_t boundary_count, char *summary, std::size_t summary_length, char *error,
+    std::size_t error_length);
+
+// inspect_checkpoint, inspect_prepared_mesh, export_checkpoint, prepare_mesh
+// and prepare_mpi_run_directory (bridge.hpp:7-11): host file utilities, the
+// reference's own code behind the same C conventions.
+int wasl_inspect_checkpoint(const char *checkpoint_path, char *summary,
+                            std::size_t summary_length, char *error, std::size_t error_length);
+int wasl_inspect_prepared_mesh(const char *mesh_path, char *summary, std::size_t summary_length,
+                               char *error, std::size_t error_length);
+int wasl_export_checkpoint(const char *checkpoint_path, const char *mesh_path,
+                           const char *output_path, char *summary, std::size_t summary_length,
+                           char *error, std::size_t error_length);
+int wasl_prepare_mesh(const char *source_path, const char *output_path, char *summary,
+                      std::size_t summary_length, char *error, std::size_t error_length);
+int wasl_prepare_mpi_run_directory(const char *root_path, const char *effective_config,
+                                   char *summary, std::size_t summary_length, char *error,
+                                   std::size_t error_length);
 }
