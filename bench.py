@@ -55,10 +55,12 @@ def parse():
                     help="mixed form's volume rule order (default p; the reference uses p+2)")
     ap.add_argument("--kernel", type=int, default=0,
                     help="mixed form's kernel: 0 autotuned, 1 face-centric, 2+s tile shape s")
-    ap.add_argument("--workload", choices=["vortex", "batched", "quadrant", "shock-vortex",
-                                           "line-euler", "line-scalar", "tri-scalar"],
+    ap.add_argument("--workload", choices=["vortex", "advection-line", "batched", "quadrant",
+                                           "shock-vortex", "line-euler", "line-scalar",
+                                           "tri-scalar"],
                     default="vortex",
-                    help="vortex: the 256x256 isentropic vortex (default); batched: independent"
+                    help="vortex: the 256x256 isentropic vortex (default); advection-line: the"
+                         " 400-cell P2 advection run to t = 1 in one launch; batched: independent"
                          " two-state Riemann cases of uneven size and order in one batch;"
                          " quadrant: four-quadrant Riemann, 1024x1024 quads, P3, limiter;"
                          " shock-vortex: 2048x1024 quads, P3, learned indicator;"
@@ -393,7 +395,10 @@ def stream_of(g, torch):
 # reference arm: the reference CPU solver on the host cores
 # ---------------------------------------------------------------------------------
 
-REF_SAMPLE_N = 64  # quads per side of the per-process sample mesh
+# The reference arm's bounded sample: each host process runs the full
+# workload mesh for at most REF_STEPS timed steps after at most REF_WARMUP
+# untimed ones (a reference step on the 256x256 mesh takes ~10 s on one core).
+REF_STEPS, REF_WARMUP = 3, 1
 
 
 def _ref_worker(n, p, steps, warmup, queue, barrier):
@@ -433,9 +438,10 @@ def reference(args, rank):
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    steps, warmup = max(1, min(args.steps, REF_STEPS)), min(args.warmup, REF_WARMUP)
     queue, barrier = ctx.Queue(), ctx.Barrier(cores)
     procs = [ctx.Process(target=_ref_worker,
-                         args=(REF_SAMPLE_N, args.p, args.steps, args.warmup, queue, barrier))
+                         args=(args.n, args.p, steps, warmup, queue, barrier))
              for _ in range(cores)]
     for pr in procs:
         pr.start()
@@ -445,27 +451,138 @@ def reference(args, rank):
     elapsed = max(r[0] for r in results)
     dofs = results[0][1]
     kind = results[0][2]
-    value = cores * 3.0 * dofs * args.steps / elapsed
-    sample = (f"{cores} independent processes (one per host core), each {args.steps} SSP-RK3"
-              f" steps of the same vortex workload on a {REF_SAMPLE_N}x{REF_SAMPLE_N}-quad"
-              f" sample mesh ({2 * REF_SAMPLE_N ** 2} triangles, P{args.p});"
-              " the reference solver is single-threaded")
+    value = cores * 3.0 * dofs * steps / elapsed
+    sample = (f"{cores} independent processes (one per host core), each {steps} timed SSP-RK3"
+              f" steps (after {warmup} untimed) of the full workload mesh ({args.n}x{args.n}"
+              f" quads, {2 * args.n * args.n} triangles, P{args.p}); the reference solver is"
+              " single-threaded")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": elapsed * 1e3 / args.steps, "higher_is_better": True,
+        "n_gpus": args.gpus, "steps": steps, "warmup": warmup,
+        "ms_per_step": elapsed * 1e3 / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded jittered mesh, projected isentropic vortex)",
         "config": {"workload": f"isentropic vortex, {args.n}x{args.n} quads ->"
                                f" {2 * args.n * args.n} jittered triangles, P{args.p} Euler,"
                                f" periodic, CFL {CFL}, limiter off",
                    "form": "reference CPU (oracle/_ref)" if kind == "reference" else "oracle port",
-                   "parallelism": f"{cores} host processes"},
+                   "parallelism": f"{cores} host processes, each the full mesh",
+                   "sample": sample},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------
+# 1D advection: the whole 400-cell run in one launch
+# ---------------------------------------------------------------------------------
+
+ADVECTION_CELLS, ADVECTION_CFL = 400, 0.1
+
+
+def advection_cpu(arrays, c0):
+    """The reference's own CPU run of the same case (oracle/_ref: its
+    SSP-RK3 and run-loop arithmetic in C++, one core), else the oracle port."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    ne, M = ADVECTION_CELLS, 3
+    c = np.ascontiguousarray(c0.reshape(M, ne).T).ravel()  # solver layout [element][mode]
+    if pyoracle.Reference.available():
+        mesh = pyoracle.Reference().line_mesh(*arrays)
+        t0 = time.perf_counter()
+        steps, _ = mesh.scalar_run(1.0, 2, ADVECTION_CFL, 0.0, 1.0, c)
+        return time.perf_counter() - t0, steps, "reference"
+    om = pyoracle.Oracle().line_mesh(*arrays)
+    dt = om.advection_cfl(1.0, 2, ADVECTION_CFL)
+    t, steps = 0.0, 0
+    t0 = time.perf_counter()
+    while t < 1.0:
+        d = min(dt, 1.0 - t)
+        om.scalar_step(1.0, 2, d, c)
+        t += d
+        steps += 1
+    return time.perf_counter() - t0, steps, "port"
+
+
+def advection_line(args, local_rank, cpu=True):
+    """1D linear advection u_t + u_x = 0 on 400 jittered periodic cells, P2,
+    u0 = sin(2 pi x) + exp(-300 (x - 0.5)^2), CFL 0.1, to t = 1 (~33,000
+    steps): each timed repetition is the whole run, on the device in one
+    kernel launch (wasl_gpu_run_resident), plain FP64 and bit-identical to the
+    reference's run.  e2e adds the state's copies in and out through the
+    C-ABI; the reference's CPU run of the same case is timed beside it."""
+    import torch
+    import wasl_b200
+    from wasl_b200 import cases
+    torch.cuda.set_device(local_rank)
+    arrays = cases.advection_line_mesh(ADVECTION_CELLS)
+    pulse = cases.AdvectedPulse(1.0)
+    g = wasl_b200.Solver(*arrays, dimensions=1, equation="scalar", polynomial_order=2,
+                         velocity=(1.0, 0.0), device=local_rank)
+    cases.project_line(g, pulse.value)
+    c0 = g.get_state()
+    stream = torch.cuda.ExternalStream(g.stream_handle())
+    reps = max(1, min(args.steps, 5))
+    for _ in range(max(1, min(args.warmup, 2))):
+        g.set_state(c0)
+        steps, t = g.run_resident(ADVECTION_CFL, 0.0, 1.0)
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    ms = 0.0
+    launches = 0
+    for _ in range(reps):
+        g.set_state(c0)
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g.profile_begin()
+        start.record(stream)
+        steps, t = g.run_resident(ADVECTION_CFL, 0.0, 1.0)
+        end.record(stream)
+        torch.cuda.synchronize()
+        launches += g.profile_end()[2]
+        ms += start.elapsed_time(end)
+    # end to end: host state in, the whole run, state out
+    host = torch.empty(g.state_size, dtype=torch.float64, pin_memory=True).numpy()
+    host[:] = c0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        g.set_state(host)
+        g.run_resident(ADVECTION_CFL, 0.0, 1.0)
+        g.get_state_into(host)
+        host[:] = c0
+    e2e_s = time.perf_counter() - t0
+    clocks = sampler.stop()
+    error = cases.l1_line_error(g, lambda x: pulse.value(x, t))
+    dof_stages = 3.0 * g.state_size * steps
+    line = {"metric": METRIC, "value": dof_stages * reps / (ms * 1e-3), "unit": UNIT,
+            "n_gpus": 1, "steps": steps, "repetitions": reps, "ms_per_run": ms / reps,
+            "ms_per_step": ms / reps / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded jittered line, projected sine + Gaussian)",
+            "config": {"workload": f"1D scalar advection, {ADVECTION_CELLS} jittered periodic"
+                                   f" cells, P2, a = 1, CFL {ADVECTION_CFL}, t = 1 ({steps}"
+                                   " steps), limiter off, whole run in one kernel launch",
+                       "form": "plain-fp64", "dof": g.state_size,
+                       "l1_error_at_t1": error},
+            "e2e": {"value": dof_stages * reps / e2e_s, "unit": UNIT,
+                    "h2d_bytes_per_step": 8 * g.state_size / steps,
+                    "d2h_bytes_per_step": 8 * g.state_size / steps,
+                    "path": "C-ABI set_state / run_resident / get_state, host wall clock"},
+            "roofline": {"bound": "latency",
+                         "note": "the state (9.6 KB) lives in one SM's shared memory for the"
+                                 " whole run; the run is a chain of 3 x steps dependent stages"},
+            "gpu_launches": launches, "clocks": clocks}
+    if cpu:
+        cpu_s, cpu_steps, kind = advection_cpu(arrays, c0)
+        line["cpu_baseline"] = {"value": 3.0 * g.state_size * cpu_steps / cpu_s, "unit": UNIT,
+                                "cores": 1, "kind": kind,
+                                "sample": f"the whole run to t = 1 ({cpu_steps} steps),"
+                                          f" single-threaded, {cpu_s:.2f} s"}
+    g.close()
+    return line
 
 
 # ---------------------------------------------------------------------------------
@@ -752,6 +869,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         reference(args, rank)
+    elif args.workload == "advection-line":
+        if rank == 0:
+            print(json.dumps(advection_line(args, local_rank, cpu=not args.no_cpu)), flush=True)
     elif args.workload == "batched":
         batched(args, rank, world, local_rank)
     elif args.workload in ("quadrant", "shock-vortex"):

@@ -172,6 +172,15 @@ int wasl_gpu_mass_energy(wasl_gpu *handle, double *mass, double *energy);
 int wasl_gpu_run(wasl_gpu *handle, double cfl, double start_time, double end_time,
                  uint64_t max_steps, uint64_t *steps, double *time);
 
+/* wasl_gpu_run in one kernel launch with no host round trip per step: the
+ * same loop, dt and results bit for bit, for line meshes whose state (three
+ * buffers of variables x modes x elements doubles, at most 200 KiB) fits in
+ * one CTA's shared memory, without the limiter (the 400-cell P2 advection
+ * run, for one).  WASL_ERR_ARGUMENT otherwise.  No counterpart in the
+ * reference (its loop is the host loop wasl_gpu_run mirrors). */
+int wasl_gpu_run_resident(wasl_gpu *handle, double cfl, double start_time, double end_time,
+                          uint64_t max_steps, uint64_t *steps, double *time);
+
 /* Device-resident fast path: `steps` steps with the CFL step computed on the
  * device each step, enqueued on the handle's stream without host
  * synchronization; a device error (non-physical average, positivity floor)

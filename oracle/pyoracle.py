@@ -530,6 +530,8 @@ class Reference:
                                            C.c_double, C.c_double, C.c_int, C.c_double, _d, _u8]
         L.wr_euler_line_step.argtypes = [vp, C.c_int, C.c_int, vp, C.c_double, C.c_double,
                                          C.c_double, C.c_double, C.c_int, C.c_double, _d]
+        L.wr_scalar_line_run.argtypes = [vp, C.c_int, C.c_double, C.c_double, C.c_double,
+                                         C.c_double, C.c_uint64, _d, C.POINTER(C.c_uint64), _d]
         L.wr_scalar_line_step.argtypes = [vp, C.c_int, C.c_double, C.c_int, C.c_double,
                                           C.c_double, C.c_int, C.c_double, _d]
 
@@ -699,6 +701,15 @@ class RefLineMesh:
 
     def scalar_step(self, a, p, dt, c, lk=0, lv=0.0, rk=0, rv=0.0):
         self.lib.wr_scalar_line_step(self.h, lk, lv, rk, rv, a, p, dt, _p(c))
+
+    def scalar_run(self, a, p, cfl, start_time, end_time, c, max_steps=2**62):
+        """The reference's periodic advection run in place (c: U[element][mode]);
+        returns (steps, time)."""
+        steps, t = C.c_uint64(), np.zeros(1)
+        if self.lib.wr_scalar_line_run(self.h, p, a, cfl, start_time, end_time, max_steps,
+                                       _p(c), C.byref(steps), _p(t)) != 0:
+            raise ValueError(self.r.err())
+        return steps.value, float(t[0])
 
 
 class RefStencil:

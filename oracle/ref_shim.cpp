@@ -9,6 +9,7 @@
 // It also supplies stand-ins for the four HDF5 functions the case layer links
 // (cpp/src/io/checkpoint_file.cpp, cpp/src/io/prepared_mesh_file.cpp), in a
 // plain binary format, because HDF5 is not installed here.
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -568,6 +569,39 @@ void wr_scalar_line_step(void *handle, int left_kind, double left_value, int rig
   wasl::SspRk3Workspace workspace;
   wasl::ssp_rk3_step(mesh, wasl::ScalarAdvection{a}, p, dt, exterior, state, workspace);
   std::memcpy(c, state.data(), state.size() * sizeof(double));
+}
+
+// The serial run of a periodic 1D advection case, as
+// cpp/src/case/scalar_advection_line.cpp:11-33 composes it (CFL step fixed at
+// setup, SSP-RK3 with the reused workspace) inside the run loop's time
+// arithmetic (cpp/src/case/serial_case_runner.cpp:107-142), without the
+// files: the reference's CPU run of the 400-cell configuration, timed whole.
+// c: the solver layout U[element][mode]; returns -1 if time cannot advance.
+int wr_scalar_line_run(void *handle, int p, double a, double cfl, double start_time,
+                       double end_time, std::uint64_t max_steps, double *c,
+                       std::uint64_t *steps, double *time) {
+  return guarded([&] {
+    const auto &mesh = static_cast<LineHandle *>(handle)->mesh;
+    const wasl::ScalarAdvection equation{a};
+    const auto exterior = wasl::make_line_boundary_exterior(mesh, p, {});
+    const double cfl_step = wasl::advection_cfl_timestep(mesh, equation, p, cfl);
+    std::vector<double> state(c, c + wasl::line_mode_count(p) * mesh.num_elements());
+    wasl::SspRk3Workspace workspace;
+    double t = start_time;
+    std::uint64_t n = 0;
+    while (t < end_time && n < max_steps) {
+      const double remaining = end_time - t;
+      const double dt = std::min(cfl_step > 0.0 ? cfl_step : remaining, remaining);
+      if (dt <= 0.0 || t + dt == t)
+        throw std::runtime_error("simulation: timestep cannot advance time");
+      wasl::ssp_rk3_step(mesh, equation, p, dt, exterior, state, workspace);
+      t += dt;
+      ++n;
+    }
+    std::memcpy(c, state.data(), state.size() * sizeof(double));
+    *steps = n;
+    *time = t;
+  });
 }
 
 // ---- whole cases through the reference's own run loop ------------------------

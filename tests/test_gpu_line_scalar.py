@@ -206,6 +206,56 @@ def test_scalar_line_advected_pulse_full_run(oracle):
     assert error < 1e-3
 
 
+def test_resident_run_is_the_host_loop_bit_for_bit():
+    """The whole 400-cell advection run (P2, a = 1, CFL 0.1, to t = 1: ~33,000
+    steps) in one kernel launch gives the host loop's step count, final time
+    and state bit for bit (the host loop's run is the reference's, above)."""
+    arrays = cases.advection_line_mesh()
+    pulse = cases.AdvectedPulse(1.0)
+    out = []
+    for resident in (False, True):
+        with line(arrays, 2, equation="scalar", velocity=(1.0, 0.0)) as g:
+            cases.project_line(g, pulse.value)
+            run = g.run_resident if resident else g.run
+            steps, time = run(0.1, 0.0, 1.0, 10 ** 9)
+            out.append((steps, time, g.get_state()))
+    assert out[0][:2] == out[1][:2] and out[0][0] > 10000
+    assert same(out[0][2], out[1][2])
+
+
+@pytest.mark.parametrize("p,ends", [(1, "periodic"), (2, "periodic"), (2, "outflow")])
+def test_resident_euler_run_is_the_host_loop_bit_for_bit(p, ends):
+    """1D Euler with the CFL step taken from the state every step, on the
+    device in one launch: the host loop's steps, time and state."""
+    arrays = meshgen.jittered_line(96, jitter=0.2, seed=3)
+    rng = np.random.Generator(np.random.PCG64(8))
+    M = p + 1
+    c = 0.02 * rng.standard_normal((4, M, 96))
+    c[0, 0] = np.sqrt(2) * (1.0 + 0.2 * rng.uniform(-1, 1, 96))
+    c[1, 0] = np.sqrt(2) * 0.3
+    c[3, 0] = np.sqrt(2) * 2.5
+    out = []
+    for resident in (False, True):
+        with line(arrays, p, boundary=ends) as g:
+            g.set_state(c.ravel())
+            run = g.run_resident if resident else g.run
+            out.append((*run(0.3, 0.0, 0.05), g.get_state()))
+    assert out[0][:2] == out[1][:2] and out[0][0] > 5
+    assert same(out[0][2], out[1][2])
+
+
+def test_resident_run_limits():
+    """Runs with the limiter, or meshes whose state does not fit in one
+    CTA's shared memory, are refused with a status."""
+    with line(meshgen.jittered_line(64, jitter=0.2, seed=1), 2, limiting=True) as g:
+        with pytest.raises(wasl_b200.WaslError, match="limiter"):
+            g.run_resident(0.3, 0.0, 0.01)
+    with line(meshgen.jittered_line(20000, jitter=0.2, seed=1), 2, equation="scalar",
+              velocity=(1.0, 0.0)) as g:
+        with pytest.raises(wasl_b200.WaslError, match="shared memory"):
+            g.run_resident(0.1, 0.0, 0.01)
+
+
 def test_scalar_line_large_mesh_single_step(oracle):
     """A 2^20-cell line: parity does not depend on size."""
     arrays = meshgen.jittered_line(1 << 20, jitter=0.2, seed=1)

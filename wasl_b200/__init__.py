@@ -95,6 +95,8 @@ SIGNATURES = {
     "wasl_gpu_mass_energy": (C.c_int, [C.c_void_p, _d, _d]),
     "wasl_gpu_run": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_uint64,
                                C.POINTER(C.c_uint64), _d]),
+    "wasl_gpu_run_resident": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double,
+                                        C.c_uint64, C.POINTER(C.c_uint64), _d]),
     "wasl_gpu_advance": (C.c_int, [C.c_void_p, C.c_double, C.c_int64]),
     "wasl_gpu_sync": (C.c_int, [C.c_void_p]),
     "wasl_gpu_state_device": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
@@ -326,6 +328,13 @@ class Solver:
         steps, time = C.c_uint64(), C.c_double()
         self._check(self._lib.wasl_gpu_run(self._h, cfl, start_time, end_time, max_steps,
                                            C.byref(steps), C.byref(time)))
+        return steps.value, time.value
+
+    def run_resident(self, cfl, start_time, end_time, max_steps=2**62):
+        """run() in one kernel launch (small line meshes, no limiter)."""
+        steps, time = C.c_uint64(), C.c_double()
+        self._check(self._lib.wasl_gpu_run_resident(self._h, cfl, start_time, end_time,
+                                                    max_steps, C.byref(steps), C.byref(time)))
         return steps.value, time.value
 
     def advance(self, cfl: float, steps: int, sync: bool = True):

@@ -283,6 +283,19 @@ int wasl_gpu_run(wasl_gpu *h, double cfl, double start_time, double end_time, ui
   });
 }
 
+int wasl_gpu_run_resident(wasl_gpu *h, double cfl, double start_time, double end_time,
+                          uint64_t max_steps, uint64_t *steps, double *time) {
+  return guarded(h, [&] {
+    std::uint64_t n = 0;
+    double t = start_time;
+    h->solver->run_resident(cfl, start_time, end_time, max_steps, n, t);
+    if (steps)
+      *steps = n;
+    if (time)
+      *time = t;
+  });
+}
+
 int wasl_gpu_advance(wasl_gpu *h, double cfl, int64_t steps) {
   return guarded(h, [&] {
     need(steps >= 0, "advance: negative step count");

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cmath>
+#include <cstddef>
 #include <cstdint>
 #include <vector>
 
@@ -252,6 +253,24 @@ struct LineStageArgs {
   std::int32_t *troubled_count = nullptr;
   LineTable table;
 };
+
+// A whole serial run of a line mesh in one launch of one CTA (the state's
+// three buffers in its shared memory): see line_run_f64.  result[0] steps,
+// result[1] final time (FP64 bits), result[2] status (0 done, 1 the time step
+// cannot advance time, 2 a non-physical cell average, also in *error).
+struct LineRunArgs {
+  LineStageArgs stage; // mesh, table, ends, physics (in/out/u0/dt unused)
+  double *state = nullptr;
+  double fixed_dt = 0.0; // > 0: this step (scalar advection); 0: CFL per step
+  double cfl = 0.0, length = 0.0;
+  double start_time = 0.0, end_time = 0.0;
+  unsigned long long max_steps = 0;
+  unsigned long long *result = nullptr; // 3 words
+  unsigned long long *error = nullptr;
+};
+constexpr std::size_t kLineRunMaxBytes = 200 * 1024;
+std::size_t line_run_bytes(int variables, int p, std::int64_t ne);
+void launch_line_run_f64(int variables, int p, const LineRunArgs &r, cudaStream_t stream);
 
 bool line_order_supported(int p); // 0..6
 void fill_line_table(int p, int points, LineTable &table);

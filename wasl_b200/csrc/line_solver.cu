@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <string>
 
 #include "basis.hpp"
 #include "kernels.hpp"
@@ -222,6 +223,38 @@ public:
 
   void sync() override { check_error(); }
 
+  void run_resident(double cfl, double start_time, double end_time, std::uint64_t max_steps,
+                    std::uint64_t &steps, double &time) override {
+    if (limiting_)
+      throw SolverError(WASL_ERR_ARGUMENT, "resident run: runs without the limiter only");
+    if (line_run_bytes(V_, p_, ne_) > kLineRunMaxBytes)
+      throw SolverError(WASL_ERR_ARGUMENT,
+                        "resident run: " + std::to_string(ne_) +
+                            " elements do not fit in one CTA's shared memory");
+    LineRunArgs r;
+    r.stage = stage_args();
+    r.state = d_u_.get();
+    r.fixed_dt = V_ == 1 ? stable_dt(cfl) : 0.0;
+    r.cfl = cfl;
+    r.length = length_;
+    r.start_time = start_time;
+    r.end_time = end_time;
+    r.max_steps = max_steps;
+    r.result = d_cfl_.get();
+    r.error = d_error_.get();
+    launch_line_run_f64(V_, p_, r, stream_);
+    count_launches(1);
+    cuda_check(cudaGetLastError(), "resident run");
+    cuda_check(cudaMemcpyAsync(scratch_.words, d_cfl_.get(), 3 * sizeof(unsigned long long),
+                               cudaMemcpyDeviceToHost, stream_),
+               "resident run");
+    check_error();
+    steps = scratch_.words[0];
+    time = bits_to_double(scratch_.words[1]);
+    if (scratch_.words[2] == 1)
+      throw SolverError(WASL_ERR_RUNTIME, "simulation: timestep cannot advance time");
+  }
+
   void flags(std::uint8_t *out) override {
     cuda_check(cudaMemcpyAsync(out, d_flags_.get(), 3 * ne_, cudaMemcpyDeviceToHost, stream_),
                "flags");
@@ -273,6 +306,21 @@ private:
     a.result = d_cfl_.get();
     a.dt = d_dt_.get();
     a.error = d_error_.get();
+    return a;
+  }
+
+  // The stage arguments common to every stage (mesh, table, ends, physics).
+  LineStageArgs stage_args() const {
+    LineStageArgs a;
+    a.ne = ne_;
+    a.inv_jacobian = d_inv_jacobian_.get();
+    a.gamma = cfg_.heat_capacity_ratio;
+    a.speed = cfg_.velocity_x;
+    a.left_kind = left_kind_;
+    a.right_kind = right_kind_;
+    a.left_value = cfg_.inflow_left;
+    a.right_value = cfg_.inflow_right;
+    a.table = table_;
     return a;
   }
 

@@ -108,6 +108,13 @@ public:
   virtual void sync() {
     cuda_check(cudaStreamSynchronize(stream_), "sync");
   }
+  // The serial run loop on the device, in one launch with no host round trip
+  // per step (line meshes small enough for one CTA, without the limiter).
+  virtual void run_resident(double cfl, double start_time, double end_time,
+                            std::uint64_t max_steps, std::uint64_t &steps, double &time) {
+    (void)cfl, (void)start_time, (void)end_time, (void)max_steps, (void)steps, (void)time;
+    throw SolverError(WASL_ERR_ARGUMENT, "resident run: line meshes only");
+  }
   virtual void flags(std::uint8_t *out) = 0;
   virtual void mass_energy(double &mass, double &energy) = 0;
   virtual double *state_device() = 0;
