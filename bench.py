@@ -52,7 +52,8 @@ def parse():
     ap.add_argument("--n", type=int, default=256, help="quads per side")
     ap.add_argument("--p", type=int, default=2)
     ap.add_argument("--rule", type=int, default=None,
-                    help="mixed form's volume rule order (default p; the reference uses p+2)")
+                    help="mixed form's volume rule: -1 the symmetric degree-2p rule (default),"
+                         " p..p+2 the collapsed rule of that order (the reference uses p+2)")
     ap.add_argument("--kernel", type=int, default=0,
                     help="mixed form's kernel: 0 autotuned, 1 face-centric, 2+s tile shape s")
     ap.add_argument("--workload", choices=["vortex", "advection-line", "batched", "quadrant",
@@ -84,55 +85,68 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """SM clocks and throttle reasons of this process's GPU during the timed
+    region, polled through NVML every millisecond from a thread (the timed
+    regions are milliseconds long), with one sample when polling starts and
+    one when it stops; nvidia-smi polling where NVML is unavailable."""
 
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event reason bits (nvmlClocksEventReason*).
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4}
 
     def __init__(self, index):
-        self.index, self.proc, self.lines = index, None, []
+        self.index, self.samples, self.nvml, self.handle = index, [], None, None
+        self.smax, self.stop_flag, self.thread = None, threading.Event(), None
+
+    def _open(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+        try:
+            handle = pynvml.nvmlDeviceGetHandleByUUID(
+                uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except pynvml.NVMLError:
+            handle = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+        self.nvml, self.handle = pynvml, handle
+        self.smax = pynvml.nvmlDeviceGetMaxClockInfo(handle, pynvml.NVML_CLOCK_SM)
+
+    def _sample(self):
+        nv, h = self.nvml, self.handle
+        self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM),
+                             nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
+
+    def _poll(self):
+        while not self.stop_flag.wait(0.001):
+            try:
+                self._sample()
+            except Exception:
+                return
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "50"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            self._open()
+            self._sample()
+            self.thread = threading.Thread(target=self._poll, daemon=True)
             self.thread.start()
-        except (OSError, FileNotFoundError):
-            self.proc = None
-
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+        except Exception:
+            self.nvml = None
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
+        if self.nvml is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["NVML unavailable"],
+                    "samples": 0}
+        self.stop_flag.set()
         self.thread.join(timeout=2)
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                smax = float(f[2])
-            except ValueError:
-                continue
-            for name, flag in zip(names, f[5:9]):
-                if flag.lower().startswith("active"):
-                    reasons.add(name)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        try:
+            self._sample()
+        except Exception:
+            pass
+        reasons = sorted(name for name, bit in self.REASONS.items()
+                         if any(r & bit for _, r in self.samples))
+        sm = [c for c, _ in self.samples]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.smax,
+                "reasons": reasons, "samples": len(sm), "source": "NVML, 1 ms polling"}
 
 
 # ---------------------------------------------------------------------------------
@@ -169,9 +183,18 @@ def reduce_over_ranks(dist, value, op="max", device="cuda"):
 # ---------------------------------------------------------------------------------
 
 def rule_order(args, form):
+    """The plain path: the reference's order-(p+2) rule; the mixed form: the
+    symmetric degree-2p rule unless --rule names another."""
     if form == "plain":
         return 0
-    return args.p if args.rule is None else args.rule
+    return -1 if args.rule is None else args.rule
+
+
+def rule_description(rule, p):
+    if rule == -1:
+        return f"symmetric, degree {2 * p} ({ {1: 3, 2: 6, 3: 12}[p]} points)"
+    order = rule or p + 2
+    return f"collapsed order {order} ({(order + 1) ** 2} points)"
 
 
 def build_solver(args, form, device):
@@ -334,8 +357,7 @@ def ours(args, rank, world, local_rank):
                                f" jittered triangles, P{args.p} Euler, periodic, CFL {CFL},"
                                " limiter off",
                    "form": "plain-fp64" if form == "plain" else "mixed-precision",
-                   "volume_rule": (f"collapsed order {rule_order(args, form) or args.p + 2}"
-                                   f" ({((rule_order(args, form) or args.p + 2) + 1) ** 2} points)"),
+                   "volume_rule": rule_description(rule_order(args, form), args.p),
                    "kernel": kernel_description(g.tuning()),
                    "elements": g.elements, "dof": dofs, "parallelism": f"replicas x{world}",
                    "l2": "flushed between timed steps (256 MiB write)"},
@@ -759,7 +781,7 @@ def limited(args, rank, world, local_rank):
     for form in forms:
         g = wasl_b200.Solver(*arrays, polynomial_order=p, precision=form, limiting=True,
                              boundary="transmissive", device=local_rank,
-                             volume_rule_order=p if form == "mixed" else 0,
+                             volume_rule_order=-1 if form == "mixed" else 0,
                              positivity_all=form == "mixed")
         setup_s = time.perf_counter() - t0
         cases.project_initial(g, problem.conserved)

@@ -77,7 +77,9 @@ typedef struct {
   int precision;             /* enum wasl_precision */
   int device;                /* CUDA device ordinal */
   int volume_rule_order;     /* mixed form: order r of the collapsed (r+1)^2-point volume
-                                rule, p..p+2; 0 = p+2, the reference residual's rule */
+                                rule, p..p+2; 0 = p+2, the reference residual's rule;
+                                -1 = the fully symmetric rule of degree 2p (3, 6, 12
+                                points at P1, P2, P3) */
   int mixed_kernel;          /* mixed form: 0 autotuned; 1 face-centric kernels (face pass
                                 + element pass); 2 + s the fused tile kernel in launch
                                 shape s (0..11, see wasl_gpu_tuning) */

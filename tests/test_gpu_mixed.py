@@ -26,7 +26,7 @@ def pair(arrays, p, **kw):
             wasl_b200.Solver(*arrays, polynomial_order=p, precision="mixed", **kw))
 
 
-@pytest.mark.parametrize("p,rule", [(p, r) for p in (1, 2, 3) for r in (0, p, p + 1)])
+@pytest.mark.parametrize("p,rule", [(p, r) for p in (1, 2, 3) for r in (0, p, p + 1, -1)])
 def test_uniform_flow_stays_uniform(p, rule):
     """A constant state is preserved to FP64 round-off: the FP32 part sees dU = 0."""
     arrays = meshgen.jittered_box(16, jitter=0.15, seed=p)
@@ -61,7 +61,8 @@ def test_one_step_close_to_plain(p):
 
 @pytest.mark.parametrize("p,rule,kernel", [(p, r, k) for p in (1, 2, 3) for r in (0, p)
                                            for k in (1, 2, 8, 10)] +
-                         [(2, 2, k) for k in (3, 4, 5, 12)])
+                         [(2, 2, k) for k in (3, 4, 5, 12)] +
+                         [(p, -1, k) for p in (1, 2, 3) for k in (2, 11)])
 def test_mass_and_energy_conserved(p, rule, kernel):
     """Periodic faces paired, interior faces evaluated by both sides with the
     same instructions: totals conserved to FP64 round-off."""
@@ -77,7 +78,7 @@ def test_mass_and_energy_conserved(p, rule, kernel):
     assert abs(e1 - e0) <= 1e-13 * abs(e0)
 
 
-@pytest.mark.parametrize("p,rule", [(2, 0), (2, 2), (3, 3)])
+@pytest.mark.parametrize("p,rule", [(2, 0), (2, 2), (3, 3), (2, -1), (3, -1)])
 def test_vortex_accuracy_matches_plain(p, rule):
     """Isentropic vortex on a 64x64-quad mesh to t=0.5: the mixed form's L1
     density error is within 1.5x of the plain FP64 path's."""
@@ -265,8 +266,9 @@ def test_profile_splits_stage_time_by_rk_stage():
     assert abs(sum(split) - ms) <= 1e-9 * ms
 
 
-@pytest.mark.parametrize("form,p", [("plain", 1), ("plain", 2), ("mixed", 2)])
-def test_vortex_convergence_rate(form, p):
+@pytest.mark.parametrize("form,p,rule", [("plain", 1, 0), ("plain", 2, 0), ("mixed", 2, 2),
+                                         ("mixed", 2, -1)])
+def test_vortex_convergence_rate(form, p, rule):
     """Isentropic vortex on 16, 32 and 64 quads per side to t = 0.5: the L1
     density error falls at a rate of at least p + 0.6 between the two finest
     meshes (the reference's vortex check,
@@ -275,7 +277,7 @@ def test_vortex_convergence_rate(form, p):
     errors = []
     for n in (16, 32, 64):
         with wasl_b200.Solver(*cases.vortex_mesh(n, seed=7), polynomial_order=p, precision=form,
-                              volume_rule_order=p if form == "mixed" else 0) as g:
+                              volume_rule_order=rule) as g:
             cases.project_initial(g, vortex.conserved)
             steps, t = g.run(0.15, 0.0, 0.5)
             errors.append(cases.l1_density_error(g, lambda x, y: vortex.conserved(x, y, t)))

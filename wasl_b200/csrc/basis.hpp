@@ -203,6 +203,133 @@ inline Rule2D triangle_rule(int p) {
   return r;
 }
 
+// Fully symmetric rules on the reference triangle, exact for total degree
+// `degree` (2: 3 points, 4: 6, 6: 12): orbits of barycentric points
+// (a, a, 1-2a) and (a, b, 1-a-b) with their weights, found by Gauss-Newton
+// on the moment equations int lambda1^i lambda2^j = i! j! / (i+j+2)! (over a
+// triangle of unit area) from approximate published values (Dunavant's rules
+// of those degrees; Int. J. Numer. Meth. Eng. 21 (1985) 1129-1148), then
+// checked on every monomial up to the degree.  Weights sum to 2, the
+// reference triangle's area.
+inline Rule2D symmetric_triangle_rule(int degree) {
+  // Unknowns: per S21 orbit (a, w), per S111 orbit (a, b, w).
+  struct Start {
+    std::vector<double> s21, s111;
+  };
+  Start start;
+  if (degree == 2)
+    start = {{1.0 / 6.0, 1.0 / 3.0}, {}};
+  else if (degree == 4)
+    start = {{0.44595, 0.22338, 0.09158, 0.10995}, {}};
+  else if (degree == 6)
+    start = {{0.24929, 0.11679, 0.06309, 0.05084}, {0.31035, 0.05314, 0.08285}};
+  else
+    throw std::invalid_argument("symmetric triangle rule: degree 2, 4 or 6");
+  std::vector<double> x = start.s21;
+  x.insert(x.end(), start.s111.begin(), start.s111.end());
+  const std::size_t n21 = start.s21.size() / 2, n111 = start.s111.size() / 3;
+  // Barycentric points and weights (unit-area normalization) of the unknowns.
+  auto expand = [&](const std::vector<double> &u, std::vector<std::array<double, 3>> &pts,
+                    std::vector<double> &ws) {
+    pts.clear();
+    ws.clear();
+    for (std::size_t k = 0; k < n21; ++k) {
+      const double a = u[2 * k], w = u[2 * k + 1], b = 1.0 - 2.0 * a;
+      for (const auto &pt : {std::array<double, 3>{a, a, b}, {a, b, a}, {b, a, a}}) {
+        pts.push_back(pt);
+        ws.push_back(w);
+      }
+    }
+    for (std::size_t k = 0; k < n111; ++k) {
+      const double a = u[2 * n21 + 3 * k], b = u[2 * n21 + 3 * k + 1];
+      const double w = u[2 * n21 + 3 * k + 2], c = 1.0 - a - b;
+      for (const auto &pt : {std::array<double, 3>{a, b, c}, {a, c, b}, {b, a, c}, {b, c, a},
+                             {c, a, b}, {c, b, a}}) {
+        pts.push_back(pt);
+        ws.push_back(w);
+      }
+    }
+  };
+  auto factorial = [](int k) {
+    double f = 1.0;
+    for (int i = 2; i <= k; ++i)
+      f *= i;
+    return f;
+  };
+  // Residuals of the moment equations (unit-area triangle: integral x 2).
+  auto residual = [&](const std::vector<double> &u) {
+    std::vector<std::array<double, 3>> pts;
+    std::vector<double> ws;
+    expand(u, pts, ws);
+    std::vector<double> r;
+    for (int i = 0; i <= degree; ++i)
+      for (int j = 0; i + j <= degree; ++j) {
+        double sum = 0.0;
+        for (std::size_t q = 0; q < pts.size(); ++q)
+          sum += ws[q] * std::pow(pts[q][0], i) * std::pow(pts[q][1], j);
+        r.push_back(sum - 2.0 * factorial(i) * factorial(j) / factorial(i + j + 2));
+      }
+    return r;
+  };
+  const std::size_t nu = x.size();
+  for (int iteration = 0; iteration < 50; ++iteration) {
+    const std::vector<double> r = residual(x);
+    // Normal equations J^T J dx = -J^T r with a central-difference Jacobian.
+    std::vector<std::vector<double>> J(r.size(), std::vector<double>(nu));
+    for (std::size_t k = 0; k < nu; ++k) {
+      std::vector<double> hi = x, lo = x;
+      const double h = 1e-7;
+      hi[k] += h;
+      lo[k] -= h;
+      const auto rh = residual(hi), rl = residual(lo);
+      for (std::size_t e = 0; e < r.size(); ++e)
+        J[e][k] = (rh[e] - rl[e]) / (2.0 * h);
+    }
+    std::vector<std::vector<double>> A(nu, std::vector<double>(nu + 1, 0.0));
+    for (std::size_t a = 0; a < nu; ++a) {
+      for (std::size_t b = 0; b < nu; ++b)
+        for (std::size_t e = 0; e < r.size(); ++e)
+          A[a][b] += J[e][a] * J[e][b];
+      for (std::size_t e = 0; e < r.size(); ++e)
+        A[a][nu] -= J[e][a] * r[e];
+    }
+    for (std::size_t c = 0; c < nu; ++c) { // Gaussian elimination, partial pivoting
+      std::size_t best = c;
+      for (std::size_t k = c + 1; k < nu; ++k)
+        if (std::fabs(A[k][c]) > std::fabs(A[best][c]))
+          best = k;
+      std::swap(A[c], A[best]);
+      for (std::size_t k = 0; k < nu; ++k)
+        if (k != c) {
+          const double f = A[k][c] / A[c][c];
+          for (std::size_t m = c; m <= nu; ++m)
+            A[k][m] -= f * A[c][m];
+        }
+    }
+    double step = 0.0;
+    for (std::size_t k = 0; k < nu; ++k) {
+      x[k] += A[k][nu] / A[k][k];
+      step = std::max(step, std::fabs(A[k][nu] / A[k][k]));
+    }
+    if (step < 1e-15)
+      break;
+  }
+  for (const double e : residual(x))
+    if (std::fabs(e) > 1e-13)
+      throw std::runtime_error("symmetric triangle rule: moment equations not solved");
+  std::vector<std::array<double, 3>> pts;
+  std::vector<double> ws;
+  expand(x, pts, ws);
+  Rule2D r;
+  for (std::size_t q = 0; q < pts.size(); ++q) {
+    // Reference triangle (-1,-1), (1,-1), (-1,1): x = -l0 + l1 - l2, etc.
+    r.xi.push_back(-1.0 + 2.0 * pts[q][1]);
+    r.eta.push_back(-1.0 + 2.0 * pts[q][2]);
+    r.w.push_back(2.0 * ws[q]);
+  }
+  return r;
+}
+
 // p+1 Gauss points on each reference edge (0: v0->v1, 1: v1->v2, 2: v2->v0),
 // packed [edge][point]; weights scaled by the reference edge length.
 inline Rule2D triangle_edges(int p) {

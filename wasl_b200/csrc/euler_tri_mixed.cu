@@ -32,8 +32,19 @@ namespace wasl_b200 {
 
 // FP32 volume tables for modes 1..M-1 on the collapsed rule of order R
 // ((R+1)^2 points, exact to degree 2R; the reference residual uses R = p+2).
+// Volume rule R: the collapsed rule of order R ((R+1)^2 points, exact to
+// degree 2R), or, for R = 0, the fully symmetric rule of degree 2P (3, 6 and
+// 12 points at P1, P2, P3: the collapsed order-P rule's exactness with fewer
+// points).
+template <int P, int R> struct VolumeRuleSize {
+  static constexpr int value = (R + 1) * (R + 1);
+};
+template <int P> struct VolumeRuleSize<P, 0> {
+  static constexpr int value = P == 1 ? 3 : (P == 2 ? 6 : 12);
+};
+
 template <int P, int R> struct MixedVolume {
-  static constexpr int M = TriShape<P>::M, QV = (R + 1) * (R + 1), H = M - 1;
+  static constexpr int M = TriShape<P>::M, QV = VolumeRuleSize<P, R>::value, H = M - 1;
   float phi[QV][H > 0 ? H : 1];
   float dxi[QV][H > 0 ? H : 1];
   float deta[QV][H > 0 ? H : 1];
@@ -143,11 +154,26 @@ struct Side32 {
 // the mean (and the pressure to zero), which changes nothing elsewhere.
 constexpr float kVacuumFraction = 1e-6f;
 
+// The reciprocal of the perturbation formulas: correctly rounded (the tile
+// kernels, whose launch shapes agree bit for bit), or the one-instruction
+// approximation of the SFU, within one unit in the last place (FAST: the
+// patch kernel; FP32 carries only perturbations there).
+template <bool FAST> __device__ __forceinline__ float perturbation_rcp(float x) {
+  if constexpr (FAST) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+  } else {
+    return __frcp_rn(x);
+  }
+}
+
+template <bool FAST = false>
 __device__ __forceinline__ Side32 perturbed_side(const Ref32 &b, const float *d, float g1,
                                                  float gamma, float nx, float ny) {
   Side32 s;
   s.rho = fmaxf(b.rho + d[0], kVacuumFraction * b.rho);
-  s.inv = __frcp_rn(s.rho);
+  s.inv = perturbation_rcp<FAST>(s.rho);
   const float du = (d[1] - b.u * d[0]) * s.inv;
   const float dv = (d[2] - b.v * d[0]) * s.inv;
   s.u = b.u + du;
@@ -171,11 +197,12 @@ __device__ __forceinline__ Side32 perturbed_side(const Ref32 &b, const float *d,
 // the star-state jumps are rewritten so that no O(1) terms cancel:
 //   S* - u_L = (dp - rho_R (S_R - u_R) du_n) / D,
 //   rho* - rho_K = rho_K (S* - u_K) / (S_K - S*).
+template <bool FAST = false>
 __device__ __forceinline__ void hllc_perturbed(const Ref32 &b, const float *dl, const float *dr,
                                                float g1, float gamma, float nx, float ny,
                                                float *f) {
-  const Side32 L = perturbed_side(b, dl, g1, gamma, nx, ny);
-  const Side32 R = perturbed_side(b, dr, g1, gamma, nx, ny);
+  const Side32 L = perturbed_side<FAST>(b, dl, g1, gamma, nx, ny);
+  const Side32 R = perturbed_side<FAST>(b, dr, g1, gamma, nx, ny);
   const float sl = fminf(L.un - L.c, R.un - R.c);
   const float sr = fmaxf(L.un + L.c, R.un + R.c);
   // The star states are evaluated unconditionally and the supersonic cases
@@ -1551,6 +1578,19 @@ template <int P, int TILE> struct PatchSmem {
   static constexpr std::size_t bytes = items + sizeof(std::uint16_t) * 3 * TILE;
 };
 
+// Asks the TMA engine to bring the 16-byte-aligned interior of [begin,
+// begin + bytes) into L2 (one instruction per row; no data returns to the
+// SM).  Only addresses inside the range are named.
+__device__ __forceinline__ void prefetch_row_l2(const void *begin, std::size_t bytes) {
+  const std::uintptr_t a = reinterpret_cast<std::uintptr_t>(begin);
+  const std::uintptr_t lo = (a + 15) & ~static_cast<std::uintptr_t>(15);
+  const std::uintptr_t hi = (a + bytes) & ~static_cast<std::uintptr_t>(15);
+  if (hi > lo)
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(lo),
+                 "r"(static_cast<unsigned>(hi - lo))
+                 : "memory");
+}
+
 template <int P, int TILE>
 __device__ __forceinline__ MeanState patch_mean(const double (*smean)[TILE],
                                                 const double (*sprim)[TILE], int i) {
@@ -1707,15 +1747,39 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_patch(const StageArgs a)
   }
   if (t == 0)
     item_count = 0;
-  if (active && a.stage > 0) {
-#pragma unroll
-    for (int r = 0; r < 4 * M; ++r)
-      asm volatile("prefetch.global.L2 [%0];\n" ::"l"(a.u0 + r * ne + e));
+  // The patch's rows of mesh data (read in every phase) and, in stages 2-3,
+  // of u^n (read at the end) into L2, one bulk prefetch per row.
+  {
+    constexpr int kMeshRows = 5 + 9 + 3 + 3;
+    const int rows = kMeshRows + (a.stage > 0 ? 4 * M : 0);
+    if (t < rows) {
+      const void *row;
+      std::size_t bytes;
+      if (t < 5) {
+        row = a.mesh.geo + t * ne + first, bytes = 8 * count;
+      } else if (t < 14) {
+        row = pe.geo + (t - 5) * ne + first, bytes = 8 * count;
+      } else if (t < 17) {
+        row = pe.nbr + (t - 14) * ne + first, bytes = 4 * count;
+      } else if (t < 20) {
+        row = pe.info + (t - 17) * ne + first, bytes = count;
+      } else {
+        row = a.u0 + (t - kMeshRows) * ne + first, bytes = 8 * count;
+      }
+      prefetch_row_l2(row, bytes);
+    }
   }
 
   // A. State, traces, and the faces this element evaluates.
   bool evaluates[3] = {false, false, false};
   if (active) {
+    std::int32_t nbrs[3];
+    unsigned infos[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      nbrs[j] = pe.nbr[j * ne + e];
+      infos[j] = pe.info[j * ne + e];
+    }
     double mean[4];
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
@@ -1748,10 +1812,9 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_patch(const StageArgs a)
     sprim[3][t] = own.h;
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-      const std::int32_t nb = pe.nbr[j * ne + e];
-      const std::int64_t local = nb - first;
-      const bool inside = nb >= 0 && local >= 0 && local < count;
-      evaluates[j] = !inside || (pe.info[j * ne + e] & 1u);
+      const std::int64_t local = nbrs[j] - first;
+      const bool inside = nbrs[j] >= 0 && local >= 0 && local < count;
+      evaluates[j] = !inside || (infos[j] & 1u);
     }
   }
   __syncthreads(); // item_count and the tables are set
@@ -1842,7 +1905,7 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_patch(const StageArgs a)
             dr[v] = jump[v] + (self_left ? tn[v] : to[v]);
           }
         }
-        hllc_perturbed(ref, dl, dr, g1, gamma32, nxf, nyf, fl);
+        hllc_perturbed<true>(ref, dl, dr, g1, gamma32, nxf, nyf, fl);
 #pragma unroll
         for (int v = 0; v < 4; ++v)
           sedge[(j * QF + qs) * 4 + v][te] = fl[v];
@@ -1892,7 +1955,7 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_patch(const StageArgs a)
           s = fmaf(ch[v][m], T.phi[q][m], s);
         d[v] = s;
       }
-      const float inv = __frcp_rn(fmaxf(bb.rho + d[0], kVacuumFraction * bb.rho));
+      const float inv = perturbation_rcp<true>(fmaxf(bb.rho + d[0], kVacuumFraction * bb.rho));
       const float du = (d[1] - bb.u * d[0]) * inv;
       const float dv = (d[2] - bb.v * d[0]) * inv;
       const float uu = bb.u + du, vv = bb.v + dv;
@@ -2048,7 +2111,9 @@ void check(cudaError_t rc, const char *what) {
 template <int P, int R> void upload_mixed() {
   static MixedVolume<P, R> t;
   constexpr int M = TriShape<P>::M, QV = MixedVolume<P, R>::QV;
-  const Rule2D rule = triangle_rule(R);
+  const Rule2D rule = R == 0 ? symmetric_triangle_rule(2 * P) : triangle_rule(R);
+  if (rule.size() != QV)
+    throw std::logic_error("mixed volume table: rule size");
   std::vector<double> gx, ge;
   for (int q = 0; q < QV; ++q) {
     const auto b = dubiner(rule.xi[q], rule.eta[q], P);
@@ -2242,6 +2307,8 @@ template <int P, int R> struct StageMixed {
 template <template <int, int> class Op, typename... A> void dispatch_mixed(int p, int rule, A &&...args) {
   if (rule == 0)
     rule = p + 2;
+  else if (rule == kSymmetricVolumeRule)
+    rule = 0; // the template's code for the symmetric rule
   switch (p * 10 + rule) {
   case 11: Op<1, 1>::run(args...); break;
   case 12: Op<1, 2>::run(args...); break;
@@ -2252,6 +2319,9 @@ template <template <int, int> class Op, typename... A> void dispatch_mixed(int p
   case 33: Op<3, 3>::run(args...); break;
   case 34: Op<3, 4>::run(args...); break;
   case 35: Op<3, 5>::run(args...); break;
+  case 10: Op<1, 0>::run(args...); break;
+  case 20: Op<2, 0>::run(args...); break;
+  case 30: Op<3, 0>::run(args...); break;
   default:
     throw std::invalid_argument("mixed form: polynomial order must be 1..3 and the volume rule"
                                 " order p..p+2");
@@ -2263,7 +2333,7 @@ template <template <int, int> class Op, typename... A> void dispatch_mixed(int p
 bool euler_tri_mixed_supported(int p, int rule) {
   if (rule == 0)
     rule = p + 2;
-  return p >= 1 && p <= 3 && rule >= p && rule <= p + 2;
+  return p >= 1 && p <= 3 && (rule == kSymmetricVolumeRule || (rule >= p && rule <= p + 2));
 }
 
 std::size_t euler_tri_mixed_face_record_bytes(int p) {
@@ -2286,6 +2356,8 @@ int euler_tri_tile_elements(int shape) {
 }
 
 bool euler_tri_tile_is_patch(int shape) { return shape >= kFirstPatchShape && shape < kTileShapes; }
+
+
 
 void prepare_euler_tri_stage_tile(int p, int rule) { dispatch_mixed<PrepareTile>(p, rule); }
 

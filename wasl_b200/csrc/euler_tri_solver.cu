@@ -86,7 +86,8 @@ public:
       throw SolverError(WASL_ERR_ARGUMENT, "2D Euler: polynomial order must be 0..3");
     if (cfg.precision == WASL_MIXED && !euler_tri_mixed_supported(p_, cfg.volume_rule_order))
       throw SolverError(WASL_ERR_ARGUMENT, "2D Euler mixed form: polynomial order must be 1..3"
-                                           " and the volume rule order p..p+2");
+                                           " and the volume rule order p..p+2 (or -1,"
+                                           " the symmetric rule)");
     if (cfg.precision != WASL_PLAIN_FP64 && cfg.precision != WASL_MIXED)
       throw SolverError(WASL_ERR_ARGUMENT, "unknown precision form");
     cuda_check(cudaSetDevice(cfg.device), "cudaSetDevice");

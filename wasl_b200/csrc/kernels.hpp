@@ -287,7 +287,10 @@ std::size_t euler_tri_face_table_bytes(int p, bool fp32);
 void fill_euler_tri_face_table(int p, bool fp32, void *host_buffer);
 void launch_euler_tri_stage_f64(int p, const StageArgs &a, cudaStream_t stream);
 // The mixed form's volume rule: the collapsed rule of order `rule` (p..p+2;
-// 0 means p+2, the reference residual's rule).
+// 0 means p+2, the reference residual's rule), or kSymmetricVolumeRule: the
+// fully symmetric rule of degree 2p (3, 6, 12 points at P1-P3), as exact as
+// the collapsed order-p rule with fewer points.
+constexpr int kSymmetricVolumeRule = -1;
 bool euler_tri_mixed_supported(int p, int rule);
 void upload_euler_tri_tables_mixed(int p, int rule);
 std::size_t euler_tri_mixed_face_record_bytes(int p);
@@ -310,6 +313,7 @@ int euler_tri_tile_elements(int shape);
 // Shapes of the patch kernel (StageArgs::patch; no rough pass, so runs
 // without the limiter only).
 bool euler_tri_tile_is_patch(int shape);
+
 void launch_euler_tri_stage_tile(int p, int rule, int shape, const StageArgs &a,
                                  cudaStream_t stream);
 // Sets the tile kernels' launch attributes on the current device (call
