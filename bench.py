@@ -400,7 +400,8 @@ def kernel_description(tuning):
              "shared-face tile 96 el/CTA, 5 CTAs/SM", "shared-face tile 128 el/CTA, 4 CTAs/SM",
              "shared-face tile 128 el/CTA, 3 CTAs/SM", "patch 128 el/CTA, <=128 regs",
              "patch 128 el/CTA, 5 CTAs/SM", "patch 64 el/CTA, 8 CTAs/SM",
-             "patch 64 el/CTA, 10 CTAs/SM"]
+             "patch 64 el/CTA, 10 CTAs/SM", "patch + tensor-core volume 128 el/CTA, <=128 regs",
+             "patch + tensor-core volume 128 el/CTA, 5 CTAs/SM"]
     if choice < 0:
         return {"name": "single stage kernel"}
     out = {"name": names[choice] if choice < len(names) else str(choice)}

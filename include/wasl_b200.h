@@ -82,7 +82,7 @@ typedef struct {
                                 points at P1, P2, P3) */
   int mixed_kernel;          /* mixed form: 0 autotuned; 1 face-centric kernels (face pass
                                 + element pass); 2 + s the fused tile kernel in launch
-                                shape s (0..11, see wasl_gpu_tuning) */
+                                shape s (0..13, see wasl_gpu_tuning) */
   int positivity_all;        /* with limiting: 1 applies the positivity limiter to every
                                 element, not only troubled ones (not the reference's
                                 behaviour, cpp/src/limiting/euler_modal_limiter.cpp:81-96) */
@@ -200,7 +200,9 @@ int wasl_gpu_sync(wasl_gpu *handle);
  * 5: 96 for 5; 6: 128 for 4; 7: 128 for 3; 8-11: the patch kernel, which
  * evaluates each element's traces once and each face inside a patch once,
  * without the limiter only: 8: 128 elements per CTA at <= 128 registers;
- * 9: 128 sized for 5 CTAs per SM; 10: 64 for 8; 11: 64 for 10);
+ * 9: 128 sized for 5 CTAs per SM; 10: 64 for 8; 11: 64 for 10; 12-13: the
+ * patch kernel with its volume contractions on the tensor cores (split-TF32
+ * mma.sync, FP32 accumulation): 12: 128 at <= 128 registers, 13: 128 for 5);
  * -1 for forms with a single kernel or before the first step.  When the
  * choice was autotuned (mixed_kernel 0: every variant timed on the solver's
  * own state before its first step, the fastest kept for the process per

@@ -14,11 +14,12 @@ pytestmark = pytest.mark.gpu
 
 # mixed_kernel: 1 face-centric kernels, 2 + s the fused tile kernel in shape s
 # (s = 0..3 the tile kernel, 4..7 the shared-face tile kernel, 8..11 the patch
-# kernel).
+# kernel, 12..13 the patch kernel with its volume term on the tensor cores).
 KERNELS = [1, 2, 3, 4, 5]
-TILE_SHAPES = 12
+TILE_SHAPES = 14
 SHARED_KERNELS = [6, 7, 8, 9]
 PATCH_KERNELS = [10, 11, 12, 13]
+MMA_KERNELS = [14, 15]
 
 
 def pair(arrays, p, **kw):
@@ -62,7 +63,7 @@ def test_one_step_close_to_plain(p):
 @pytest.mark.parametrize("p,rule,kernel", [(p, r, k) for p in (1, 2, 3) for r in (0, p)
                                            for k in (1, 2, 8, 10)] +
                          [(2, 2, k) for k in (3, 4, 5, 12)] +
-                         [(p, -1, k) for p in (1, 2, 3) for k in (2, 11)])
+                         [(p, -1, k) for p in (1, 2, 3) for k in (2, 11, 14)])
 def test_mass_and_energy_conserved(p, rule, kernel):
     """Periodic faces paired, interior faces evaluated by both sides with the
     same instructions: totals conserved to FP64 round-off."""
@@ -343,3 +344,41 @@ def test_storage_order_is_a_relabelling(kernel, limiting):
     a, b = out["caller"], out["curve"]
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[2] == b[2]
     assert np.allclose(a[3], b[3], rtol=1e-14, atol=0.0)
+
+
+@pytest.mark.parametrize("p,rule", [(1, -1), (2, -1), (3, -1), (2, 2), (3, 3)])
+@pytest.mark.parametrize("boundary", ["periodic", "transmissive"])
+def test_tensor_core_volume_matches_the_fma_pipe(p, rule, boundary):
+    """The patch kernel with its volume contractions as split-TF32 tensor-core
+    products (FP32 accumulation) against the same kernel on the FMA pipe:
+    after three steps the states differ by at most 1e-6 of the change the
+    steps made, and its two launch shapes agree bit for bit."""
+    arrays = meshgen.jittered_box(20, jitter=0.15, seed=60 + p)
+    c = seeded_state(2 * 20 * 20, p, 61 + p, amplitude=0.02)
+    out = {}
+    for k in [10] + MMA_KERNELS:
+        with wasl_b200.Solver(*arrays, polynomial_order=p, precision="mixed", mixed_kernel=k,
+                              boundary=boundary, volume_rule_order=rule) as g:
+            g.set_state(c)
+            for _ in range(3):
+                g.step(g.stable_dt(0.15))
+            out[k] = g.get_state()
+    change = np.max(np.abs(out[10] - c))
+    assert np.max(np.abs(out[14] - out[10])) <= 1e-6 * change
+    assert np.array_equal(out[15], out[14])
+
+
+@pytest.mark.parametrize("p", [2, 3])
+def test_tensor_core_volume_vortex_accuracy(p):
+    """Isentropic vortex, 64x64 quads to t = 0.5 with the tensor-core volume
+    term: L1 density error within 1.5x of the plain FP64 path's."""
+    vortex = cases.IsentropicVortex()
+    arrays = cases.vortex_mesh(64, seed=7)
+    errors = {}
+    for form, kernel in (("plain", 0), ("mixed", 14)):
+        with wasl_b200.Solver(*arrays, polynomial_order=p, precision=form, mixed_kernel=kernel,
+                              volume_rule_order=-1 if form == "mixed" else 0) as g:
+            cases.project_initial(g, vortex.conserved)
+            steps, t = g.run(0.15, 0.0, 0.5)
+            errors[form] = cases.l1_density_error(g, lambda x, y: vortex.conserved(x, y, t))
+    assert errors["mixed"] <= 1.5 * errors["plain"]

@@ -1560,6 +1560,211 @@ template <int P> struct PatchEdge {
 };
 template <int P> __constant__ PatchEdge<P> c_patch;
 
+// ---- the volume term on the tensor cores (patch kernel, MMA variant) ---------
+//
+// Per warp, for its 32 elements (two 16-row tiles), the two contractions of
+// the volume term run as TF32 tensor-core products with FP32 accumulation:
+//   evaluation  d[e][v][q] = sum_m hi[e][v][m] phi[q][m]           (16 x K1 x 8)
+//   projection  r[e][v][m] = sum_q dxi[q][m] Gxi[e][v][q] + deta[q][m] Geta[e][v][q]
+// each operand split into a TF32 high part and the TF32 remainder
+// (a b ~ ahi bhi + alo bhi + ahi blo), which keeps the products at about
+// FP32 accuracy.  The pointwise perturbation flux between the two runs on
+// the FP32 pipe in the evaluation's accumulator layout, and the projection
+// takes its operands straight from those registers: its K index runs over
+// the points in the order (2c, 2c+1) of the accumulator's columns, with the
+// projection table permuted to match.  The results go through shared memory
+// (over the element's high modes, no longer needed) to each element's thread.
+template <int P, int R> struct VolumeMmaShape {
+  static constexpr int H = TriShape<P>::M - 1, QV = MixedVolume<P, R>::QV;
+  static constexpr int KS1 = (H + 7) / 8;  // evaluation k-steps (modes)
+  static constexpr int NB = (QV + 7) / 8;  // point blocks
+  static constexpr int KS2 = 2 * NB;       // projection k-steps (direction, point block)
+  static constexpr int MB = (H + 7) / 8;   // projection mode blocks
+  static constexpr int FRAGS = KS1 * NB + KS2 * MB; // float4 per lane
+};
+
+__device__ __forceinline__ unsigned tf32_of(float x) {
+  unsigned r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+// x as a TF32 high part and the TF32 rounding of the remainder.
+__device__ __forceinline__ void tf32_split(float x, unsigned &hi, unsigned &lo) {
+  hi = tf32_of(x);
+  lo = tf32_of(x - __uint_as_float(hi));
+}
+
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const unsigned (&a)[4], unsigned b0,
+                                         unsigned b1) {
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 "
+               "{%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};\n"
+               : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+               : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// d += A B with both split: alo bhi, ahi blo, then ahi bhi.
+__device__ __forceinline__ void mma_tf32x3(float (&d)[4], const unsigned (&ahi)[4],
+                                           const unsigned (&alo)[4], const float4 &b) {
+  mma_tf32(d, alo, __float_as_uint(b.x), __float_as_uint(b.y));
+  mma_tf32(d, ahi, __float_as_uint(b.z), __float_as_uint(b.w));
+  mma_tf32(d, ahi, __float_as_uint(b.x), __float_as_uint(b.y));
+}
+
+// The B fragments of both products for every lane, split into TF32 high
+// parts (x, y) and remainders (z, w): [KS1][NB] evaluation blocks, then
+// [KS2][MB] projection blocks, 32 lanes each.  For lane (g = lane / 4,
+// c = lane % 4) a block holds B[c][g] and B[c + 4][g].
+template <int P, int R> __device__ void fill_volume_fragments(float4 *frag, int t, int threads) {
+  using V = VolumeMmaShape<P, R>;
+  const MixedVolume<P, R> &T = c_mix<P, R>;
+  for (int i = t; i < V::FRAGS * 32; i += threads) {
+    const int block = i / 32, lane = i % 32, g = lane / 4, c = lane % 4;
+    float b[2];
+    if (block < V::KS1 * V::NB) {
+      const int ks = block / V::NB, nb = block % V::NB;
+      const int q = nb * 8 + g;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int m = ks * 8 + c + 4 * h;
+        b[h] = q < V::QV && m < V::H ? T.phi[q][m] : 0.0f;
+      }
+    } else {
+      const int j = block - V::KS1 * V::NB, ks = j / V::MB, mb = j % V::MB;
+      const int dir = ks / V::NB, nb = ks % V::NB, m = mb * 8 + g;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int k = c + 4 * h;
+        const int q = nb * 8 + (k < 4 ? 2 * k : 2 * (k - 4) + 1);
+        b[h] = q < V::QV && m < V::H ? (dir == 0 ? T.dxi[q][m] : T.deta[q][m]) : 0.0f;
+      }
+    }
+    unsigned h0, l0, h1, l1;
+    tf32_split(b[0], h0, l0);
+    tf32_split(b[1], h1, l1);
+    frag[i] = make_float4(__uint_as_float(h0), __uint_as_float(h1), __uint_as_float(l0),
+                          __uint_as_float(l1));
+  }
+}
+
+// The warp's volume term: hi modes in shi[4 H][TILE] (FP32), each element's
+// FP32 mean state in sbb[8][TILE] (rho, u, v, E, E + p, rho u, rho v, p) and
+// map columns in sgeo[4][TILE]; the results replace the warp's columns of shi
+// (racc[v][m] at row v H + m).  All 32 lanes of the warp must call it.
+template <int P, int R, int TILE>
+__device__ __forceinline__ void patch_volume_mma(float (*shi)[TILE], const float (*sbb)[TILE],
+                                                 const float (*sgeo)[TILE], const float4 *frag,
+                                                 float g1, int warp_base, int lane) {
+  using V = VolumeMmaShape<P, R>;
+  constexpr int H = V::H;
+  const MixedVolume<P, R> &T = c_mix<P, R>;
+  const int g = lane >> 2, c = lane & 3;
+#pragma unroll 1
+  for (int mt = 0; mt < 2; ++mt) {
+    const int r0 = warp_base + mt * 16 + g, r1 = r0 + 8;
+    // Evaluation: d[v][nb] holds (r0, 2c), (r0, 2c + 1), (r1, 2c), (r1, 2c + 1).
+    float d[4][V::NB][4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+#pragma unroll
+      for (int nb = 0; nb < V::NB; ++nb)
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          d[v][nb][k] = 0.0f;
+#pragma unroll
+      for (int ks = 0; ks < V::KS1; ++ks) {
+        const int m0 = ks * 8 + c, m1 = m0 + 4;
+        const float x[4] = {m0 < H ? shi[v * H + m0][r0] : 0.0f, m0 < H ? shi[v * H + m0][r1] : 0.0f,
+                            m1 < H ? shi[v * H + m1][r0] : 0.0f, m1 < H ? shi[v * H + m1][r1] : 0.0f};
+        unsigned ahi[4], alo[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          tf32_split(x[k], ahi[k], alo[k]);
+#pragma unroll
+        for (int nb = 0; nb < V::NB; ++nb)
+          mma_tf32x3(d[v][nb], ahi, alo, frag[(ks * V::NB + nb) * 32 + lane]);
+      }
+    }
+    // Pointwise perturbation flux in the contravariant form, as the FP32 pass.
+    Ref32 bb[2];
+    float geo[2][4];
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      const int r = s ? r1 : r0;
+      bb[s] = {sbb[0][r], sbb[1][r], sbb[2][r], sbb[3][r],
+               sbb[4][r], sbb[5][r], sbb[6][r], sbb[7][r]};
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        geo[s][k] = sgeo[k][r];
+    }
+    __syncwarp(); // every lane has read its rows' hi modes (overwritten below)
+    // The projection's A operands: G[v][direction][nb][slot], slots in the A
+    // fragment's order (r0, 2c), (r1, 2c), (r0, 2c + 1), (r1, 2c + 1).
+    float G[4][2][V::NB][4];
+#pragma unroll
+    for (int nb = 0; nb < V::NB; ++nb)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int s = k >> 1, q = nb * 8 + 2 * c + (k & 1);
+        const Ref32 &b = bb[s];
+        const float w = q < V::QV ? T.w[q] : 0.0f;
+        const float dd[4] = {d[0][nb][k], d[1][nb][k], d[2][nb][k], d[3][nb][k]};
+        const float inv = perturbation_rcp<true>(fmaxf(b.rho + dd[0], kVacuumFraction * b.rho));
+        const float du = (dd[1] - b.u * dd[0]) * inv;
+        const float dv = (dd[2] - b.v * dd[0]) * inv;
+        const float uu = b.u + du, vv = b.v + dv;
+        const float dmu = b.mx * du + dd[1] * uu + b.my * dv + dd[2] * vv;
+        const float dp = g1 * (dd[3] - 0.5f * dmu);
+        const float dep = dd[3] + dp;
+        const float fx[4] = {dd[1], b.mx * du + dd[1] * uu + dp, b.my * du + dd[2] * uu,
+                             b.h * du + dep * uu};
+        const float fy[4] = {dd[2], b.mx * dv + dd[1] * vv, b.my * dv + dd[2] * vv + dp,
+                             b.h * dv + dep * vv};
+        const float wby = w * geo[s][3], wbx = w * geo[s][2], wax = w * geo[s][0],
+                    way = w * geo[s][1];
+        // Accumulator slot k = (row s, column 2c + (k & 1)) -> A slot (k & 1) * 2 + s.
+        const int slot = (k & 1) * 2 + s;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          G[v][0][nb][slot] = wby * fx[v] - wbx * fy[v];
+          G[v][1][nb][slot] = wax * fy[v] - way * fx[v];
+        }
+      }
+    // Projection onto the high modes; results over the hi modes of the rows.
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      unsigned ghi[2][V::NB][4], glo[2][V::NB][4];
+#pragma unroll
+      for (int dir = 0; dir < 2; ++dir)
+#pragma unroll
+        for (int nb = 0; nb < V::NB; ++nb)
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            tf32_split(G[v][dir][nb][k], ghi[dir][nb][k], glo[dir][nb][k]);
+#pragma unroll
+      for (int mb = 0; mb < V::MB; ++mb) {
+        float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int dir = 0; dir < 2; ++dir)
+#pragma unroll
+          for (int nb = 0; nb < V::NB; ++nb)
+            mma_tf32x3(acc, ghi[dir][nb], glo[dir][nb],
+                       frag[(V::KS1 * V::NB + (dir * V::NB + nb) * V::MB + mb) * 32 + lane]);
+        const int m0 = mb * 8 + 2 * c, m1 = m0 + 1;
+        if (m0 < H) {
+          shi[v * H + m0][r0] = acc[0];
+          shi[v * H + m0][r1] = acc[2];
+        }
+        if (m1 < H) {
+          shi[v * H + m1][r0] = acc[1];
+          shi[v * H + m1][r1] = acc[3];
+        }
+      }
+    }
+  }
+  __syncwarp();
+}
+
 // Dynamic shared memory of the patch kernel, in this order:
 //   mean  double [4][TILE]        cell means
 //   prim  double [4][TILE]        u, v, p, E + p of each mean
@@ -1568,13 +1773,21 @@ template <int P> __constant__ PatchEdge<P> c_patch;
 //                                 element's trace, then the face's flux
 //                                 perturbation (own point order)
 //   items uint16 [3 TILE]         faces to evaluate: element * 4 + edge
-template <int P, int TILE> struct PatchSmem {
+//   and with the volume term on the tensor cores (MMA):
+//   frag  float4 [FRAGS][32]      B fragments of its two products
+//   bb    float  [8][TILE]        each mean state in FP32 (Ref32's fields)
+//   geo   float  [4][TILE]        each element's map columns a_x, a_y, b_x, b_y
+template <int P, int R, int TILE, bool MMA> struct PatchSmem {
   static constexpr int M = TriShape<P>::M, QF = TriShape<P>::QF, H = M - 1;
   static constexpr std::size_t mean = 0;
   static constexpr std::size_t prim = mean + sizeof(double) * 4 * TILE;
   static constexpr std::size_t hi = prim + sizeof(double) * 4 * TILE;
   static constexpr std::size_t edge = hi + sizeof(float) * 4 * H * TILE;
-  static constexpr std::size_t items = edge + sizeof(float) * 3 * QF * 4 * TILE;
+  static constexpr std::size_t frag = edge + sizeof(float) * 3 * QF * 4 * TILE;
+  static constexpr std::size_t bb =
+      frag + (MMA ? sizeof(float4) * 32 * VolumeMmaShape<P, R>::FRAGS : 0);
+  static constexpr std::size_t geo = bb + (MMA ? sizeof(float) * 8 * TILE : 0);
+  static constexpr std::size_t items = geo + (MMA ? sizeof(float) * 4 * TILE : 0);
   static constexpr std::size_t bytes = items + sizeof(std::uint16_t) * 3 * TILE;
 };
 
@@ -1704,10 +1917,10 @@ __device__ __forceinline__ void patch_finish(const StageArgs &a, std::int64_t e,
   }
 }
 
-template <int P, int R, int TILE, int MINB>
+template <int P, int R, int TILE, int MINB, bool MMA>
 __global__ void __launch_bounds__(TILE, MINB) euler_tri_patch(const StageArgs a) {
   using S = TriShape<P>;
-  using L = PatchSmem<P, TILE>;
+  using L = PatchSmem<P, R, TILE, MMA>;
   constexpr int M = S::M, QV = MixedVolume<P, R>::QV, QF = S::QF, H = M - 1;
   constexpr double phi0 = 0.70710678118654752440;
   static_assert(4 * TILE < 65536, "face items are 16-bit");
@@ -1719,6 +1932,9 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_patch(const StageArgs a)
   float(*shi)[TILE] = reinterpret_cast<float(*)[TILE]>(smem + L::hi);
   float(*sedge)[TILE] = reinterpret_cast<float(*)[TILE]>(smem + L::edge);
   std::uint16_t *items = reinterpret_cast<std::uint16_t *>(smem + L::items);
+  float4 *sfrag = reinterpret_cast<float4 *>(smem + L::frag);
+  float(*sbb)[TILE] = reinterpret_cast<float(*)[TILE]>(smem + L::bb);
+  float(*sgeo)[TILE] = reinterpret_cast<float(*)[TILE]>(smem + L::geo);
 
   const int t = threadIdx.x;
   const std::int64_t ne = a.mesh.ne;
@@ -1747,6 +1963,8 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_patch(const StageArgs a)
   }
   if (t == 0)
     item_count = 0;
+  if constexpr (MMA)
+    fill_volume_fragments<P, R>(sfrag, t, TILE);
   // The patch's rows of mesh data (read in every phase) and, in stages 2-3,
   // of u^n (read at the end) into L2, one bulk prefetch per row.
   {
@@ -1810,6 +2028,16 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_patch(const StageArgs a)
     sprim[1][t] = own.v;
     sprim[2][t] = own.p;
     sprim[3][t] = own.h;
+    if constexpr (MMA) {
+      const Ref32 r = ref32(own);
+      const float f[8] = {r.rho, r.u, r.v, r.e, r.h, r.mx, r.my, r.p};
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        sbb[k][t] = f[k];
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        sgeo[k][t] = static_cast<float>(a.mesh.geo[k * ne + e]);
+    }
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
       const std::int64_t local = nbrs[j] - first;
@@ -1920,21 +2148,29 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_patch(const StageArgs a)
       evaluate(whole + u / QF, u % QF, std::false_type{});
   }
   __syncthreads();
+  const float g1 = static_cast<float>(gamma - 1.0);
+  if constexpr (MMA) // every lane of every warp, active or not
+    patch_volume_mma<P, R, TILE>(shi, sbb, sgeo, sfrag, g1, t & ~31, t & 31);
   if (!active)
     return;
 
   // C. Volume term, lifting, mode 0, combination.
   const MeanState own = patch_mean<P, TILE>(smean, sprim, t);
-  const Ref32 bb = ref32(own);
-  const MixedVolume<P, R> &T = c_mix<P, R>;
-  const float g1 = static_cast<float>(gamma - 1.0);
   float racc[4][H];
+  if constexpr (MMA) {
 #pragma unroll
-  for (int v = 0; v < 4; ++v)
+    for (int v = 0; v < 4; ++v)
 #pragma unroll
-    for (int m = 0; m < H; ++m)
-      racc[v][m] = 0.0f;
-  {
+      for (int m = 0; m < H; ++m)
+        racc[v][m] = shi[v * H + m][t];
+  } else {
+    const Ref32 bb = ref32(own);
+    const MixedVolume<P, R> &T = c_mix<P, R>;
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+#pragma unroll
+      for (int m = 0; m < H; ++m)
+        racc[v][m] = 0.0f;
     float ch[4][H];
 #pragma unroll
     for (int v = 0; v < 4; ++v)
@@ -2219,24 +2455,25 @@ void stage_tile(const StageArgs &a, cudaStream_t s) {
            tile_smem<P, kRoughTile>(), s>>>(a);
 }
 
-template <int P, int R, int TILE, int MINB> void patch_opt_in() {
+template <int P, int R, int TILE, int MINB, bool MMA> void patch_opt_in() {
   static bool opted_in[64] = {};
-  smem_opt_in(euler_tri_patch<P, R, TILE, MINB>, PatchSmem<P, TILE>::bytes,
+  smem_opt_in(euler_tri_patch<P, R, TILE, MINB, MMA>, PatchSmem<P, R, TILE, MMA>::bytes,
               sizeof(PatchEdge<P>) + sizeof(int), opted_in);
 }
 
 // The patch kernel over all patches (no rough pass: runs without the limiter).
-template <int P, int R, int TILE, int MINB> void stage_patch(const StageArgs &a, cudaStream_t s) {
+template <int P, int R, int TILE, int MINB, bool MMA = false>
+void stage_patch(const StageArgs &a, cudaStream_t s) {
   if (a.rough)
     throw std::invalid_argument("patch kernel: no rough pass (runs without the limiter)");
   if (!a.patch.nbr)
     throw std::invalid_argument("patch kernel: the mesh has no patch edge arrays");
-  patch_opt_in<P, R, TILE, MINB>();
+  patch_opt_in<P, R, TILE, MINB, MMA>();
   const std::int64_t blocks = a.work ? a.work_count : (a.mesh.ne + TILE - 1) / TILE;
   if (blocks <= 0)
     return;
-  euler_tri_patch<P, R, TILE, MINB>
-      <<<static_cast<unsigned>(blocks), TILE, PatchSmem<P, TILE>::bytes, s>>>(a);
+  euler_tri_patch<P, R, TILE, MINB, MMA>
+      <<<static_cast<unsigned>(blocks), TILE, PatchSmem<P, R, TILE, MMA>::bytes, s>>>(a);
 }
 
 // Launch shapes of the tile kernels (elements per CTA, register budget):
@@ -2254,9 +2491,12 @@ template <int P, int R, int TILE, int MINB> void stage_patch(const StageArgs &a,
 //   9: 128 elements, sized for 5 CTAs per SM
 //  10:  64 elements, sized for 8 CTAs per SM
 //  11:  64 elements, sized for 10 CTAs per SM
+// and of the patch kernel with its volume term on the tensor cores:
+//  12: 128 elements, <= 128 registers
+//  13: 128 elements, sized for 5 CTAs per SM
 constexpr int kTileShapes = kTileShapeCount;
 constexpr int kTileElements[kTileShapes] = {128, 128, 256, 64, 64, 96, 128, 128,
-                                            128, 128, 64, 64};
+                                            128, 128, 64, 64, 128, 128};
 constexpr int kFirstPatchShape = 8;
 
 template <int P, int R> struct StageTile {
@@ -2274,6 +2514,8 @@ template <int P, int R> struct StageTile {
     case 9: stage_patch<P, R, 128, 5>(a, s); break;
     case 10: stage_patch<P, R, 64, 8>(a, s); break;
     case 11: stage_patch<P, R, 64, 10>(a, s); break;
+    case 12: stage_patch<P, R, 128, 4, true>(a, s); break;
+    case 13: stage_patch<P, R, 128, 5, true>(a, s); break;
     default: throw std::invalid_argument("tile kernel: unknown launch shape");
     }
   }
@@ -2289,10 +2531,12 @@ template <int P, int R> struct PrepareTile {
     shared_opt_in<P, R, 96, 5>();
     shared_opt_in<P, R, 128, 4>();
     shared_opt_in<P, R, 128, 3>();
-    patch_opt_in<P, R, 128, 4>();
-    patch_opt_in<P, R, 128, 5>();
-    patch_opt_in<P, R, 64, 8>();
-    patch_opt_in<P, R, 64, 10>();
+    patch_opt_in<P, R, 128, 4, false>();
+    patch_opt_in<P, R, 128, 5, false>();
+    patch_opt_in<P, R, 64, 8, false>();
+    patch_opt_in<P, R, 64, 10, false>();
+    patch_opt_in<P, R, 128, 4, true>();
+    patch_opt_in<P, R, 128, 5, true>();
   }
 };
 
