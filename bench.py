@@ -72,6 +72,10 @@ def parse():
     ap.add_argument("--quads", type=int, default=1024,
                     help="quadrant / shock-vortex workloads: quads per unit side")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the other workloads the default run reports under other_workloads")
+    ap.add_argument("--extra-budget", type=float, default=900.0,
+                    help="seconds allowed for the other workloads in total")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
 
@@ -313,6 +317,50 @@ def cpu_baseline(args):
                       f" single-threaded, {elapsed:.1f} s"}
 
 
+# The other workloads of the benchmark suite, run after the headline one in
+# the default invocation (one GPU), each in its own process with its own clock
+# record: (workload, extra arguments, seconds allowed).
+EXTRA_WORKLOADS = [
+    ("advection-line", [], 120),
+    ("quadrant", ["--steps", "20", "--warmup", "3"], 420),
+    ("batched", ["--steps", "200", "--warmup", "3"], 600),
+    ("shock-vortex", ["--steps", "20", "--warmup", "3"], 600),
+]
+EXTRA_KEYS = ("value", "unit", "steps", "ms_per_step", "ms_per_run", "chosen_vs_plain", "roofline",
+              "e2e", "gpu_launches", "clocks", "cpu_baseline", "failed_cases", "simulated_time")
+
+
+def extra_workloads(args):
+    """Each other workload's JSON line (its key fields), or why it is absent."""
+    out = {}
+    budget = time.perf_counter() + args.extra_budget
+    for name, extra, limit in EXTRA_WORKLOADS:
+        left = budget - time.perf_counter()
+        if left < 30:
+            out[name] = {"skipped": f"time budget of {args.extra_budget} s used up"}
+            continue
+        cmd = [sys.executable, os.path.abspath(__file__), "--workload", name, *extra]
+        if args.no_cpu:
+            cmd.append("--no-cpu")
+        t0 = time.perf_counter()
+        try:
+            run = subprocess.run(cmd, capture_output=True, text=True, timeout=min(limit, left),
+                                 cwd=ROOT)
+        except subprocess.TimeoutExpired:
+            out[name] = {"skipped": f"timed out after {min(limit, left):.0f} s"}
+            continue
+        lines = [x for x in run.stdout.splitlines() if x.startswith("{")]
+        if run.returncode != 0 or not lines:
+            out[name] = {"failed": (run.stderr or run.stdout).strip().splitlines()[-1:]}
+            continue
+        line = json.loads(lines[-1])
+        entry = {k: line[k] for k in EXTRA_KEYS if k in line}
+        entry["workload"] = line["config"]["workload"]
+        entry["wall_s"] = round(time.perf_counter() - t0, 1)
+        out[name] = entry
+    return out
+
+
 def ours(args, rank, world, local_rank):
     import torch
     import wasl_b200
@@ -385,6 +433,8 @@ def ours(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(args)
     g.close()
+    if rank == 0 and world == 1 and not args.no_extra:
+        line["other_workloads"] = extra_workloads(args)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -793,12 +843,16 @@ def limited(args, rank, world, local_rank):
             g.step(g.stable_dt(cfl))
         if weights is not None:
             g.indicator_stats(reset=True)
+        sampler = ClockSampler(local_rank)
+        sampler.start()
         ms, launches = timed_steps(g, torch, args.steps, cfl)
+        clocks = sampler.stop()
         flags = g.flags()
         entry = {"value": 3.0 * g.state_size * args.steps / (ms * 1e-3),
                  "ms_per_step": ms / args.steps, "gpu_launches": launches,
                  "troubled_fraction_last_step": float(flags.mean()),
-                 "setup_s": round(setup_s, 1), "kernel": kernel_description(g.tuning())}
+                 "setup_s": round(setup_s, 1), "kernel": kernel_description(g.tuning()),
+                 "clocks": clocks}
         if weights is not None:
             entry["indicator"] = g.indicator_stats()
             entry["indicator_training_loss"] = train_loss
@@ -831,6 +885,7 @@ def limited(args, rank, world, local_rank):
                      "note": "whole step (CFL, stages, indicator, limiter) over algorithmic"
                              " bytes"},
         "gpu_launches": chosen["gpu_launches"],
+        "clocks": chosen["clocks"],
     }
     if "plain" in out:
         line["chosen_vs_plain"] = chosen["value"] / out["plain"]["value"]

@@ -378,102 +378,208 @@ template <int M> __global__ void positivity_rest(const LimitArgs a) {
   }
 }
 
+// The warp's minimum under smin (the reference's running std::min; the
+// minimum of a set does not depend on the order it is taken in).
+__device__ __forceinline__ double warp_min(double x) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1)
+    x = smin(x, __shfl_xor_sync(0xffffffffu, x, off));
+  return x;
+}
+
+// The stage limiter (cpp/src/limiting/euler_modal_limiter.cpp:70-98) with one
+// warp per troubled element of the compacted list: the lanes share out the
+// candidates (one output mode each), the characteristic projections (one mode
+// of one candidate each), the WENO smoothness sums and weights (one wave each),
+// the recombination, and the positivity limiter's check points, whose
+// 64-step pressure bisections then run side by side instead of one after
+// another.  Every value is still one lane's serial sum in the reference's
+// order, so the result is the reference's bit for bit.  Limited modes go to
+// scratch by list position; scatter_limited writes them back.
 template <int M, int NB>
-__global__ void __launch_bounds__(64) limit_f64(const LimitArgs a) {
+__global__ void __launch_bounds__(128) limit_f64(const LimitArgs a) {
+  constexpr int W = 4 * M;  // one element's values
+  constexpr int WARPS = 128 / 32;
+  struct Cell {
+    double target[W], cand[NB * W], tc[W], cc[NB * W], lim[W];
+    double smooth[4][NB + 1], weights[4][NB + 1], sum[4];
+    int slot[NB];
+  };
+  __shared__ Cell cells[WARPS];
+  Cell &cell = cells[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
   const int count = *a.troubled_count;
   const std::int64_t ne = a.ne;
-  const double *__restrict__ u = a.state;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+  const double *u = a.state;
+  const int warps = gridDim.x * WARPS;
+  for (int k = blockIdx.x * WARPS + (threadIdx.x >> 5); k < count; k += warps) {
     const std::int64_t e = a.troubled[k];
-    double target[4 * M], cand[NB * 4 * M];
-#pragma unroll
-    for (int i = 0; i < 4 * M; ++i)
-      target[i] = u[i * ne + e];
-    // Candidates: each neighbour mapped into this element's basis, with this
-    // element's own mean (euler_modal_limiter.cpp:43-66).
+    for (int i = lane; i < W; i += 32)
+      cell.target[i] = u[i * ne + e];
+    // Candidate slots in neighbour order (absent neighbours leave none).
     int n = 0;
+    std::int32_t nbs[NB];
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
-      const std::int32_t nb = a.neighbors[e * NB + j];
-      if (nb < 0)
-        continue;
-      const double *__restrict__ T = a.transforms + (e * NB + j) * M * M;
-      for (int v = 0; v < 4; ++v) {
-        for (int t = 0; t < M; ++t) {
-          double acc = 0.0;
-          for (int s = 0; s < M; ++s)
-            acc += T[t * M + s] * u[(static_cast<std::int64_t>(v) * M + s) * ne + nb];
-          cand[(n * 4 + v) * M + t] = acc;
-        }
-        cand[(n * 4 + v) * M] = target[v * M];
-      }
-      ++n;
+      nbs[j] = a.neighbors[e * NB + j];
+      if (lane == 0)
+        cell.slot[j] = nbs[j] >= 0 ? n : -1;
+      n += nbs[j] >= 0 ? 1 : 0;
     }
+    __syncwarp();
+    // Candidates: T_{e,j} c_nbr per variable and target mode, then this
+    // element's own mean as mode 0 (euler_modal_limiter.cpp:43-66).
+    for (int i = lane; i < NB * W; i += 32) {
+      const int j = i / W, v = (i % W) / M, t = i % M;
+      if (nbs[j] < 0)
+        continue;
+      const double *T = a.transforms + (e * NB + j) * M * M;
+      double acc = 0.0;
+      for (int q = 0; q < M; ++q)
+        acc += T[t * M + q] * u[(static_cast<std::int64_t>(v) * M + q) * ne + nbs[j]];
+      cell.cand[(cell.slot[j] * 4 + v) * M + t] = t == 0 ? cell.target[v * M] : acc;
+    }
+    __syncwarp();
     const double root2 = sqrt(2.0);
-    const double avg[4] = {target[0] / root2, target[M] / root2, target[2 * M] / root2,
-                           target[3 * M] / root2};
+    const double avg[4] = {cell.target[0] / root2, cell.target[M] / root2,
+                           cell.target[2 * M] / root2, cell.target[3 * M] / root2};
     const double nx = a.normal_x[e], ny = a.normal_y[e];
-
-    // Characteristic projection of target and candidates (euler_characteristic_weno.hpp:31-44).
-    double tc[4 * M], cc[NB * 4 * M], lim[4 * M];
-    for (int m = 0; m < M; ++m) {
-      const double d[4] = {target[m], target[M + m], target[2 * M + m], target[3 * M + m]};
+    // Characteristic projection of the target (item 0) and the candidates
+    // (euler_characteristic_weno.hpp:31-44), one mode of one item per lane.
+    for (int i = lane; i < (n + 1) * M; i += 32) {
+      const int item = i / M, m = i % M;
+      const double *src = item == 0 ? cell.target : cell.cand + (item - 1) * W;
+      const double d[4] = {src[m], src[M + m], src[2 * M + m], src[3 * M + m]};
       double w[4];
       to_characteristic(a.gamma, avg, d, nx, ny, w);
+      double *dst = item == 0 ? cell.tc : cell.cc + (item - 1) * W;
       for (int wv = 0; wv < 4; ++wv)
-        tc[wv * M + m] = w[wv];
+        dst[wv * M + m] = w[wv];
     }
-    for (int i = 0; i < n; ++i)
-      for (int m = 0; m < M; ++m) {
-        const double *src = cand + i * 4 * M;
-        const double d[4] = {src[m], src[M + m], src[2 * M + m], src[3 * M + m]};
-        double w[4];
-        to_characteristic(a.gamma, avg, d, nx, ny, w);
-        for (int wv = 0; wv < 4; ++wv)
-          cc[(i * 4 + wv) * M + m] = w[wv];
-      }
-    // Simple WENO per wave (simple_weno.hpp:21-48).
-    double lc[4 * M];
-    for (int wv = 0; wv < 4; ++wv) {
-      const double *tw = tc + wv * M;
-      double *lw = lc + wv * M;
-      if (n == 0) {
-        for (int m = 0; m < M; ++m)
-          lw[m] = tw[m];
-        continue;
-      }
-      double weights[NB + 1];
-      const double td = 1e-12 + smoothness<M>(tw);
-      weights[0] = 0.5 / (td * td);
-      double sum = weights[0];
+    __syncwarp();
+    // Simple WENO per wave (simple_weno.hpp:21-48): smoothness per item,
+    // then each wave's weights and their sum in the reference's order.
+    for (int i = lane; i < 4 * (n + 1); i += 32) {
+      const int wv = i / (n + 1), item = i % (n + 1);
+      cell.smooth[wv][item] =
+          smoothness<M>(item == 0 ? cell.tc + wv * M : cell.cc + ((item - 1) * 4 + wv) * M);
+    }
+    __syncwarp();
+    if (lane < 4 && n > 0) {
+      const int wv = lane;
+      const double td = 1e-12 + cell.smooth[wv][0];
+      cell.weights[wv][0] = 0.5 / (td * td);
+      double sum = cell.weights[wv][0];
       const double ideal = 0.5 / static_cast<double>(n);
       for (int i = 0; i < n; ++i) {
-        const double dd = 1e-12 + smoothness<M>(cc + (i * 4 + wv) * M);
-        weights[i + 1] = ideal / (dd * dd);
-        sum += weights[i + 1];
+        const double dd = 1e-12 + cell.smooth[wv][i + 1];
+        cell.weights[wv][i + 1] = ideal / (dd * dd);
+        sum += cell.weights[wv][i + 1];
       }
-      lw[0] = tw[0];
-      for (int m = 1; m < M; ++m) {
-        double value = weights[0] * tw[m];
-        for (int i = 0; i < n; ++i)
-          value += weights[i + 1] * cc[(i * 4 + wv) * M + m];
-        lw[m] = value / sum;
+      cell.sum[wv] = sum;
+    }
+    __syncwarp();
+    // Recombined characteristic modes (mode 0 kept), into lim as scratch.
+    for (int i = lane; i < W; i += 32) {
+      const int wv = i / M, m = i % M;
+      const double *tw = cell.tc + wv * M;
+      double out = tw[m];
+      if (n > 0 && m > 0) {
+        double value = cell.weights[wv][0] * tw[m];
+        for (int c = 0; c < n; ++c)
+          value += cell.weights[wv][c + 1] * cell.cc[(c * 4 + wv) * M + m];
+        out = value / cell.sum[wv];
+      }
+      cell.lim[i] = out;
+    }
+    __syncwarp();
+    // Back to conserved variables, one mode per lane; mode 0 is the target's.
+    double back[W > 32 ? (W + 31) / 32 * 4 : 4];
+    {
+      int r = 0;
+      for (int m = lane; m < M; m += 32, ++r) {
+        const double w[4] = {cell.lim[m], cell.lim[M + m], cell.lim[2 * M + m],
+                             cell.lim[3 * M + m]};
+        from_characteristic(a.gamma, avg, w, nx, ny, back + 4 * r);
       }
     }
-    for (int m = 0; m < M; ++m) {
-      const double w[4] = {lc[m], lc[M + m], lc[2 * M + m], lc[3 * M + m]};
-      double s[4];
-      from_characteristic(a.gamma, avg, w, nx, ny, s);
-      for (int v = 0; v < 4; ++v)
-        lim[v * M + m] = s[v];
+    __syncwarp();
+    {
+      int r = 0;
+      for (int m = lane; m < M; m += 32, ++r)
+        for (int v = 0; v < 4; ++v)
+          cell.lim[v * M + m] = m == 0 ? cell.target[v * M] : back[4 * r + v];
     }
-    for (int v = 0; v < 4; ++v)
-      lim[v * M] = target[v * M];
-
-    positivity_limit<M>(a, lim, e);
-    double *dst = a.limited + static_cast<std::int64_t>(k) * 4 * M;
-    for (int i = 0; i < 4 * M; ++i)
-      dst[i] = lim[i];
+    __syncwarp();
+    // Positivity (euler_positivity.hpp:63-102), one check point per lane.
+    const double inv_root2 = 1.0 / sqrt(2.0);
+    const double pavg[4] = {cell.lim[0] * inv_root2, cell.lim[M] * inv_root2,
+                            cell.lim[2 * M] * inv_root2, cell.lim[3 * M] * inv_root2};
+    if (!(pavg[0] > a.density_floor && primitive(a.gamma, pavg).p > a.pressure_floor)) {
+      if (lane == 0) {
+        if (a.case_status)
+          atomicCAS(a.case_status + a.element_case[e], 0, static_cast<int>(kBelowFloor));
+        else
+          raise_error(a.error, kBelowFloor, e);
+      }
+    } else {
+      const double rf = a.relative_floor > 0.0
+                            ? fmax(a.density_floor, a.relative_floor * pavg[0])
+                            : a.density_floor;
+      const double pf = a.relative_floor > 0.0
+                            ? fmax(a.pressure_floor, a.relative_floor * pavg[3])
+                            : a.pressure_floor;
+      double dscale = 1.0;
+      for (int pt = lane; pt < a.check_points; pt += 32) {
+        const double *b = a.check_basis + pt * M;
+        double rho = 0.0;
+        for (int m = 0; m < M; ++m)
+          rho += cell.lim[m] * b[m];
+        if (rho < rf)
+          dscale = smin(dscale, (pavg[0] - rf) / (pavg[0] - rho));
+      }
+      dscale = warp_min(dscale);
+      __syncwarp();
+      for (int i = lane; i < W; i += 32)
+        if (i % M != 0)
+          cell.lim[i] *= dscale;
+      __syncwarp();
+      double pscale = 1.0;
+      for (int pt = lane; pt < a.check_points; pt += 32) {
+        const double *b = a.check_basis + pt * M;
+        double st[4];
+        for (int v = 0; v < 4; ++v) {
+          double acc = 0.0;
+          for (int m = 0; m < M; ++m)
+            acc += cell.lim[v * M + m] * b[m];
+          st[v] = acc;
+        }
+        if (primitive(a.gamma, st).p >= pf)
+          continue;
+        double lower = 0.0, upper = 1.0;
+        for (int it = 0; it < 64; ++it) {
+          const double middle = 0.5 * (lower + upper);
+          double x[4];
+          for (int v = 0; v < 4; ++v)
+            x[v] = pavg[v] + middle * (st[v] - pavg[v]);
+          if (primitive(a.gamma, x).p >= pf)
+            lower = middle;
+          else
+            upper = middle;
+        }
+        pscale = smin(pscale, lower);
+      }
+      pscale = warp_min(pscale);
+      __syncwarp();
+      for (int i = lane; i < W; i += 32)
+        if (i % M != 0)
+          cell.lim[i] *= pscale;
+    }
+    __syncwarp();
+    double *dst = a.limited + static_cast<std::int64_t>(k) * W;
+    for (int i = lane; i < W; i += 32)
+      dst[i] = cell.lim[i];
+    __syncwarp();
   }
 }
 
@@ -704,12 +810,13 @@ void launch_euler_tri_stage_f64(int p, const StageArgs &a, cudaStream_t s) {
 }
 
 void launch_limit_f64(int M, int NB, const LimitArgs &a, cudaStream_t s) {
-  const unsigned blocks = static_cast<unsigned>(std::min<std::int64_t>((a.ne + 63) / 64, 148 * 16));
+  // Four warps (troubled elements) per block.
+  const unsigned blocks = static_cast<unsigned>(std::min<std::int64_t>((a.ne + 3) / 4, 148 * 16));
   const unsigned sblocks = static_cast<unsigned>(std::min<std::int64_t>((a.ne + 255) / 256, 148 * 8));
   const unsigned pblocks = static_cast<unsigned>(std::min<std::int64_t>((a.ne + 127) / 128, 148 * 16));
 #define WASL_LIMIT(MM, NN)                                                                     \
   if (M == MM && NB == NN) {                                                                   \
-    limit_f64<MM, NN><<<blocks, 64, 0, s>>>(a);                                                \
+    limit_f64<MM, NN><<<blocks, 128, 0, s>>>(a);                                               \
     scatter_limited<MM><<<sblocks, 256, 0, s>>>(a.state, a.ne, a.troubled, a.troubled_count,   \
                                                  a.limited);                                   \
     if (a.positivity_all)                                                                      \
