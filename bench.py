@@ -74,7 +74,7 @@ def parse():
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the other workloads the default run reports under other_workloads")
-    ap.add_argument("--extra-budget", type=float, default=900.0,
+    ap.add_argument("--extra-budget", type=float, default=480.0,
                     help="seconds allowed for the other workloads in total")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -838,7 +838,7 @@ def limited(args, rank, world, local_rank):
         cases.project_initial(g, problem.conserved)
         g.limit()
         if weights is not None:
-            g.set_indicator(weights, 0.05, 0.95)
+            g.set_indicator(weights, 0.005, 0.999)
         for _ in range(args.warmup):
             g.step(g.stable_dt(cfl))
         if weights is not None:

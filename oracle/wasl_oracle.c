@@ -1984,15 +1984,28 @@ void wo_tri_project(const wo_tri_mesh *mesh, int p, int rule_order, int nv, cons
   const int64_t ne = mesh->element_count;
   double qxi[MAXQ], qeta[MAXQ], qw[MAXQ], b[MAXM];
   const int Q = wo_tri_volume_rule(rule_order, qxi, qeta, qw);
-  memset(c, 0, sizeof(double) * (size_t)nv * (size_t)M * (size_t)ne);
-  for (int64_t e = 0; e < ne; ++e)
+  /* The basis at the rule's points is the same on every element; each
+     coefficient still sums its terms over q in order from 0.0. */
+  double *basis = (double *)malloc(sizeof(double) * (size_t)Q * (size_t)M);
+  double *acc = (double *)malloc(sizeof(double) * (size_t)nv * (size_t)M);
+  for (int q = 0; q < Q; ++q) {
+    wo_dubiner_basis(qxi[q], qeta[q], p, b);
+    memcpy(basis + (size_t)q * M, b, sizeof(double) * (size_t)M);
+  }
+  for (int64_t e = 0; e < ne; ++e) {
+    memset(acc, 0, sizeof(double) * (size_t)nv * (size_t)M);
     for (int q = 0; q < Q; ++q) {
-      wo_dubiner_basis(qxi[q], qeta[q], p, b);
       const double *val = values + (e * Q + q) * nv;
       for (int v = 0; v < nv; ++v)
         for (int m = 0; m < M; ++m)
-          c[((int64_t)v * M + m) * ne + e] += qw[q] * val[v] * b[m];
+          acc[v * M + m] += qw[q] * val[v] * basis[q * M + m];
     }
+    for (int v = 0; v < nv; ++v)
+      for (int m = 0; m < M; ++m)
+        c[((int64_t)v * M + m) * ne + e] = acc[v * M + m];
+  }
+  free(basis);
+  free(acc);
 }
 
 void wo_line_rule_points(const wo_line_mesh *mesh, int point_count, double *x) {

@@ -170,6 +170,7 @@ class PlanarRiemann:
 
     def __init__(self, seed=0, gamma=GAMMA):
         rng = np.random.Generator(np.random.PCG64(seed))
+        self.gamma = gamma
         self.angle = rng.uniform(0.0, 2.0 * math.pi)
         self.cx, self.cy = rng.uniform(0.3, 0.7, size=2)
         nx, ny = math.cos(self.angle), math.sin(self.angle)
@@ -183,6 +184,21 @@ class PlanarRiemann:
     def conserved(self, x, y, t=0.0):
         side = (x - self.cx) * math.cos(self.angle) + (y - self.cy) * math.sin(self.angle) >= 0.0
         return np.where(side[..., None], self.right, self.left)
+
+    def density(self, x, y, t):
+        """Exact density at time t > 0 (before any wave reaches the boundary):
+        the 1D Riemann solution along the interface normal, whose tangential
+        velocity only rides along."""
+        nx, ny = math.cos(self.angle), math.sin(self.angle)
+
+        def normal(state):
+            rho, mx, my, e = map(float, state)
+            u, v = mx / rho, my / rho
+            return rho, u * nx + v * ny, (self.gamma - 1.0) * (e - 0.5 * rho * (u * u + v * v))
+
+        exact = ExactRiemann(normal(self.left), normal(self.right), gamma=self.gamma)
+        s = ((x - self.cx) * nx + (y - self.cy) * ny) / t
+        return exact.sample(s)[0]
 
 
 class ShockVortex:

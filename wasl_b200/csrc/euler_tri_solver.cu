@@ -624,7 +624,7 @@ private:
     }
   }
 
-  // Times every kernel choice on a first-stage evaluation of the current
+  // Times every kernel choice on the three stages of a step of the current
   // state into scratch (u^n is read, not written; sensing off) and keeps the
   // fastest, per polynomial order, rule order and mesh size class.
   void tune_mixed(StageArgs a) {
@@ -637,21 +637,30 @@ private:
       if (!euler_tri_tile_is_patch(sh) || patch_ok_)
         shapes = sh + 1;
     const int variants = tile_ok_ ? 1 + shapes - base : 1;
-    a.stage = 0;
-    a.in = d_u_.get();
+    // Each variant runs the three stages of a step on the current state, into
+    // the stage buffers only (the last stage writes the first stage buffer
+    // instead of u^n), so the stages that also read u^n weigh in.
     a.u0 = d_u_.get();
-    a.out = d_e_.get();
     a.sense = 0;
     a.dt = nullptr;
     a.dt_value = 0.0;
+    double *ins[3] = {d_u_.get(), d_e_.get(), d_s_.get()};
+    double *outs[3] = {d_e_.get(), d_s_.get(), d_e_.get()};
     const std::string key = "euler_tri_mixed/p" + std::to_string(p_) + "/rule" +
                             std::to_string(cfg_.volume_rule_order ? cfg_.volume_rule_order : p_ + 2) +
                             "/bnd" + std::to_string(boundary_count_ > 0 ? boundary_ : -1) +
                             "/size" + std::to_string(size_class(ne_));
     tuning_ = autotune(key + (base ? "/tile-only" : ""), variants, [&](int i) {
       kernel_ = i + base;
-      launch_mixed(a);
+      for (int k = 0; k < 3; ++k) {
+        a.stage = k;
+        a.in = ins[k];
+        a.out = outs[k];
+        launch_mixed(a);
+      }
     }, stream_);
+    for (double &ms : tuning_.ms)
+      ms /= 3.0; // per stage
     if (base)
       tuning_.ms.insert(tuning_.ms.begin(), 0.0); // face-centric: not timed
     kernel_ = tuning_.choice + base;
