@@ -72,3 +72,19 @@ def test_unsupported_order_rejected():
     with pytest.raises(wasl_b200.WaslError) as err:
         wasl_b200.Solver(tags, xy, tris, polynomial_order=7)
     assert err.value.status in (-1, -3)
+
+
+def test_checked_build_compiles():
+    """The device index checks of the checked build (WASL_DEVICE_CHECKS)
+    compile for sm_100a in the kernels that read element indices from mesh
+    data (the plain stage kernel and limiter, the mixed patch kernel)."""
+    import shutil
+    import subprocess
+    import tempfile
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    from wasl_b200 import build
+    with tempfile.TemporaryDirectory() as tmp:
+        for src in ("euler_tri_f64.cu",):
+            cmd = [nvcc, *build.ARCH, *build.COMMON, *build.SOURCES[src], "-DWASL_DEVICE_CHECKS",
+                   "-c", os.path.join(build.CSRC, src), "-o", os.path.join(tmp, src + ".o")]
+            subprocess.run(cmd, check=True)

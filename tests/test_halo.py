@@ -169,3 +169,18 @@ def test_two_gloo_ranks_exchange_ghost_rows():
         assert proc.exitcode == 0
     assert results[0][0] and results[1][0]
     assert results[0][1] == results[1][1] == halo.dt_from_parts(0.1, 3.0, 0.25, 2)
+
+
+def test_partitioned_runs_refuse_periodic_handles():
+    """A rank's handle with periodic boundaries would pair its cut faces
+    across the period; the partitioned step refuses it up front."""
+    class Config:
+        boundary_left = 0  # periodic
+
+    class Handle:
+        config = Config()
+
+    with pytest.raises(ValueError, match="periodic"):
+        halo.check_partitioned_solver(Handle())
+    Handle.config.boundary_left = 3  # transmissive
+    halo.check_partitioned_solver(Handle())

@@ -24,7 +24,9 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libwasl_b200.so")
+# WASL_B200_LIBRARY selects another build of the library (the checked build,
+# libwasl_b200_checked.so, for one).
+LIB_PATH = os.environ.get("WASL_B200_LIBRARY", os.path.join(HERE, "libwasl_b200.so"))
 
 PERIODIC, INFLOW, OUTFLOW, TRANSMISSIVE = 0, 1, 2, 3
 SCALAR_ADVECTION, EULER = 0, 1

@@ -2,6 +2,13 @@
 
     python -m wasl_b200.build            # incremental
     python -m wasl_b200.build --clean
+    python -m wasl_b200.build --checked  # libwasl_b200_checked.so: device index
+                                         # checks on (WASL_DEVICE_CHECKS)
+
+The checked build records an out-of-range element index read from mesh data
+in the handle's error word instead of faulting (euler_device.cuh,
+checked_index); load it with WASL_B200_LIBRARY=<path> in place of the
+ordinary one.
 
 Kernels whose results must match the reference bit for bit are compiled with
 --fmad=false (no fused multiply-add contraction); host code with
@@ -57,8 +64,8 @@ def _newest_header() -> float:
     return max(os.path.getmtime(p) for p in paths)
 
 
-def _compile(src: str, flags: list[str]) -> str:
-    obj = os.path.join(BUILD, src + ".o")
+def _compile(src: str, flags: list[str], build_dir: str = BUILD) -> str:
+    obj = os.path.join(build_dir, src + ".o")
     path = os.path.join(CSRC, src)
     if (os.path.exists(obj) and os.path.getmtime(obj) >= os.path.getmtime(path)
             and os.path.getmtime(obj) >= _newest_header()):
@@ -69,24 +76,28 @@ def _compile(src: str, flags: list[str]) -> str:
     return obj
 
 
-def build(clean: bool = False, verbose: bool = False) -> str:
-    if clean and os.path.isdir(BUILD):
-        shutil.rmtree(BUILD)
-    os.makedirs(BUILD, exist_ok=True)
+def build(clean: bool = False, verbose: bool = False, checked: bool = False) -> str:
+    build_dir = BUILD + ("_checked" if checked else "")
+    lib = LIB.replace(".so", "_checked.so") if checked else LIB
+    extra = ["-DWASL_DEVICE_CHECKS"] if checked else []
+    if clean and os.path.isdir(build_dir):
+        shutil.rmtree(build_dir)
+    os.makedirs(build_dir, exist_ok=True)
     with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as pool:
-        futures = [pool.submit(_compile, s, f) for s, f in SOURCES.items()]
+        futures = [pool.submit(_compile, s, f + extra, build_dir) for s, f in SOURCES.items()]
         objs = [f.result() for f in futures]
-    if (not os.path.exists(LIB) or
-            max(os.path.getmtime(o) for o in objs) > os.path.getmtime(LIB)):
-        subprocess.run([NVCC, *ARCH, "-shared", "-o", LIB, *objs], check=True)
+    if (not os.path.exists(lib) or
+            max(os.path.getmtime(o) for o in objs) > os.path.getmtime(lib)):
+        subprocess.run([NVCC, *ARCH, "-shared", "-o", lib, *objs], check=True)
     if verbose:
-        print(LIB)
-    return LIB
+        print(lib)
+    return lib
 
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--clean", action="store_true")
+    ap.add_argument("--checked", action="store_true", help="device index checks on")
     args = ap.parse_args()
-    build(clean=args.clean, verbose=True)
+    build(clean=args.clean, verbose=True, checked=args.checked)
     sys.exit(0)

@@ -451,7 +451,23 @@ void BatchSolver::advance(double cfl, std::int64_t steps) {
       }
       cudaGraph_t graph = nullptr;
       cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
-      enqueue_step(cfl);
+      {
+        // Ends the capture (and drops the partial graph) if enqueuing throws,
+        // so the stream leaves capture mode and later calls still work.
+        struct CaptureGuard {
+          cudaStream_t stream;
+          bool open = true;
+          ~CaptureGuard() {
+            if (!open)
+              return;
+            cudaGraph_t partial = nullptr;
+            if (cudaStreamEndCapture(stream, &partial) == cudaSuccess && partial)
+              cudaGraphDestroy(partial);
+          }
+        } guard{stream_};
+        enqueue_step(cfl);
+        guard.open = false;
+      }
       cuda_check(cudaStreamEndCapture(stream_, &graph), "capture end");
       cuda_check(cudaGraphInstantiate(&graph_exec_, graph, 0), "graph instantiate");
       cuda_check(cudaGraphDestroy(graph), "graph destroy");

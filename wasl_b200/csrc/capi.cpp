@@ -172,6 +172,7 @@ static int64_t state_count(const wasl_gpu *h) {
 
 int wasl_gpu_set_state(wasl_gpu *h, const double *c, int64_t count) {
   return guarded(h, [&] {
+    const wasl_b200::NvtxRange range("wasl_gpu_set_state");
     need(c && count == state_count(h), "state: coefficient count does not match the layout");
     h->solver->set_state(c);
   });
@@ -179,6 +180,7 @@ int wasl_gpu_set_state(wasl_gpu *h, const double *c, int64_t count) {
 
 int wasl_gpu_get_state(wasl_gpu *h, double *c, int64_t count) {
   return guarded(h, [&] {
+    const wasl_b200::NvtxRange range("wasl_gpu_get_state");
     need(c && count == state_count(h), "state: coefficient count does not match the layout");
     h->solver->get_state(c);
   });
@@ -220,6 +222,7 @@ int wasl_gpu_evaluate(wasl_gpu *h, int rule_order, double *values, int64_t count
 
 int wasl_gpu_stable_dt(wasl_gpu *h, double cfl, double *dt) {
   return guarded(h, [&] {
+    const wasl_b200::NvtxRange range("wasl_gpu_stable_dt");
     need(dt != nullptr, "null dt");
     *dt = h->solver->stable_dt(cfl);
   });
@@ -234,13 +237,17 @@ int wasl_gpu_cfl_parts(wasl_gpu *h, double *speed, double *length) {
 
 int wasl_gpu_step(wasl_gpu *h, double dt) {
   return guarded(h, [&] {
+    const wasl_b200::NvtxRange range("wasl_gpu_step");
     need(std::isfinite(dt), "step: time step is not finite");
     h->solver->step(dt);
   });
 }
 
 int wasl_gpu_limit(wasl_gpu *h) {
-  return guarded(h, [&] { h->solver->limit(); });
+  return guarded(h, [&] {
+    const wasl_b200::NvtxRange range("wasl_gpu_limit");
+    h->solver->limit();
+  });
 }
 
 int wasl_gpu_get_flags(wasl_gpu *h, uint8_t *flags, int64_t count) {
@@ -264,6 +271,7 @@ int wasl_gpu_mass_energy(wasl_gpu *h, double *mass, double *energy) {
 int wasl_gpu_run(wasl_gpu *h, double cfl, double start_time, double end_time, uint64_t max_steps,
                  uint64_t *steps, double *time) {
   return guarded(h, [&] {
+    const wasl_b200::NvtxRange range("wasl_gpu_run");
     double t = start_time;
     uint64_t n = 0;
     while (t < end_time && n < max_steps) {
@@ -286,6 +294,7 @@ int wasl_gpu_run(wasl_gpu *h, double cfl, double start_time, double end_time, ui
 int wasl_gpu_run_resident(wasl_gpu *h, double cfl, double start_time, double end_time,
                           uint64_t max_steps, uint64_t *steps, double *time) {
   return guarded(h, [&] {
+    const wasl_b200::NvtxRange range("wasl_gpu_run_resident");
     std::uint64_t n = 0;
     double t = start_time;
     h->solver->run_resident(cfl, start_time, end_time, max_steps, n, t);
@@ -298,6 +307,7 @@ int wasl_gpu_run_resident(wasl_gpu *h, double cfl, double start_time, double end
 
 int wasl_gpu_advance(wasl_gpu *h, double cfl, int64_t steps) {
   return guarded(h, [&] {
+    const wasl_b200::NvtxRange range("wasl_gpu_advance");
     need(steps >= 0, "advance: negative step count");
     h->solver->advance(cfl, steps);
   });

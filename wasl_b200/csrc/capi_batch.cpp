@@ -158,6 +158,7 @@ int wasl_batch_limit(wasl_batch *h) {
 int wasl_batch_advance(wasl_batch *h, double cfl, int64_t steps) {
   return guarded(h, [&] {
     need(cfl > 0.0 && steps >= 0, "batch advance: cfl must be positive and steps non-negative");
+    const wasl_b200::NvtxRange range("wasl_batch_advance");
     h->solver->advance(cfl, steps);
   });
 }

@@ -130,12 +130,38 @@ __device__ __forceinline__ void hllc(T gamma, const T *l, const T *r, T nx, T ny
 }
 
 // Device error word: the first failure of a step, read by the host after the step.
-enum ErrorCode : int { kOk = 0, kNonPhysicalAverage = 1, kBelowFloor = 2, kNonFinite = 3 };
+enum ErrorCode : int {
+  kOk = 0,
+  kNonPhysicalAverage = 1,
+  kBelowFloor = 2,
+  kNonFinite = 3,
+  kIndexCheck = 4 // a device index check of the checked build failed
+};
 
 __device__ __forceinline__ void raise_error(unsigned long long *word, int code, long long element) {
   const unsigned long long value =
       (static_cast<unsigned long long>(code) << 56) | (static_cast<unsigned long long>(element) & 0xffffffffffffffULL);
   atomicCAS(word, 0ULL, value);
+}
+
+// An element index read from mesh data, checked in the checked build
+// (compiled with WASL_DEVICE_CHECKS, python -m wasl_b200.build --checked): an
+// index outside [0, n) is recorded in the error word (code kIndexCheck, with
+// the index) and replaced by 0, so the kernel neither faults nor leaves a
+// barrier its block waits at; the host raises the error when the step ends.
+// In the ordinary build this is the index itself.
+__device__ __forceinline__ long long checked_index(long long i, long long n,
+                                                   unsigned long long *word) {
+#ifdef WASL_DEVICE_CHECKS
+  if (i < 0 || i >= n) {
+    raise_error(word, kIndexCheck, i < 0 ? -i : i);
+    return 0;
+  }
+#else
+  (void)n;
+  (void)word;
+#endif
+  return i;
 }
 
 } // namespace wasl_b200

@@ -105,7 +105,9 @@ __global__ void __launch_bounds__(128) euler_tri_stage_f64(const StageArgs a) {
   // Face terms in ascending global face index.
 #pragma unroll 1
   for (int k = 0; k < 3; ++k) {
-    const std::int32_t nb = a.mesh.slot_nbr[k * ne + e];
+    const std::int32_t raw = a.mesh.slot_nbr[k * ne + e];
+    const std::int32_t nb =
+        raw >= 0 ? static_cast<std::int32_t>(checked_index(raw, ne, a.error)) : raw;
     const unsigned code = a.mesh.slot_code[k * ne + e];
     const double nx = a.mesh.slot_geo[(3 * k) * ne + e];
     const double ny = a.mesh.slot_geo[(3 * k + 1) * ne + e];
@@ -127,7 +129,8 @@ __global__ void __launch_bounds__(128) euler_tri_stage_f64(const StageArgs a) {
             rs[v] = ls[v];
         } else {
           const std::int64_t point = static_cast<std::int64_t>(-nb - 1) * QF + q;
-          eval_global<M>(in, ne, a.mesh.donor[point], a.mesh.donor_basis + point * M, rs);
+          eval_global<M>(in, ne, checked_index(a.mesh.donor[point], ne, a.error),
+                         a.mesh.donor_basis + point * M, rs);
         }
       } else {
         eval_global<M>(in, ne, nb, lb[q], ls);
@@ -422,6 +425,8 @@ __global__ void __launch_bounds__(128) limit_f64(const LimitArgs a) {
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
       nbs[j] = a.neighbors[e * NB + j];
+      if (nbs[j] >= 0)
+        nbs[j] = static_cast<std::int32_t>(checked_index(nbs[j], ne, a.error));
       if (lane == 0)
         cell.slot[j] = nbs[j] >= 0 ? n : -1;
       n += nbs[j] >= 0 ? 1 : 0;

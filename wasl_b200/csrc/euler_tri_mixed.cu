@@ -1996,6 +1996,8 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_patch(const StageArgs a)
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
       nbrs[j] = pe.nbr[j * ne + e];
+      if (nbrs[j] >= 0)
+        nbrs[j] = static_cast<std::int32_t>(checked_index(nbrs[j], ne, a.error));
       infos[j] = pe.info[j * ne + e];
     }
     double mean[4];
@@ -2069,7 +2071,9 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_patch(const StageArgs a)
       constexpr int NQ = decltype(whole)::value ? QF : 1;
       const int te = items[i] >> 2, j = items[i] & 3;
       const std::int64_t ee = first + te;
-      const std::int32_t nb = pe.nbr[j * ne + ee];
+      const std::int32_t raw = pe.nbr[j * ne + ee];
+      const std::int32_t nb =
+          raw >= 0 ? static_cast<std::int32_t>(checked_index(raw, ne, a.error)) : raw;
       const unsigned info = pe.info[j * ne + ee];
       const bool self_left = info & 1u, rev = info & 8u;
       const int jn = (info >> 1) & 3u;
@@ -2218,7 +2222,9 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_patch(const StageArgs a)
   double r0[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
-    const std::int32_t nb = pe.nbr[j * ne + e];
+    const std::int32_t raw = pe.nbr[j * ne + e];
+    const std::int32_t nb =
+        raw >= 0 ? static_cast<std::int32_t>(checked_index(raw, ne, a.error)) : raw;
     const unsigned info = pe.info[j * ne + e];
     const bool self_left = info & 1u, rev = info & 8u;
     const int jn = (info >> 1) & 3u;

@@ -40,6 +40,9 @@ void throw_device_error(unsigned long long word) {
   if (code == 1)
     throw SolverError(WASL_ERR_NONPHYSICAL, "simulation: Euler cell average is not physical"
                                             " (element " + std::to_string(element) + ")");
+  if (code == 4)
+    throw SolverError(WASL_ERR_RUNTIME, "device index check: element index " +
+                                            std::to_string(element) + " out of range");
   throw SolverError(WASL_ERR_FLOOR, "Euler positivity limiter: cell average is below a floor"
                                     " (element " + std::to_string(element) + ")");
 }

@@ -9,10 +9,21 @@
 #include <vector>
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "../../include/wasl_b200.h"
 
 namespace wasl_b200 {
+
+// An NVTX range around a C-ABI call (header-only NVTX v3: free when no
+// profiler is attached; under Nsight tools each call shows as a named range
+// over the kernels it enqueues).
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 // Failure carrying a C-ABI status code.
 struct SolverError : std::runtime_error {

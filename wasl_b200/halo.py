@@ -244,11 +244,30 @@ def device_state(solver):
                            device="cuda")
 
 
+def check_partitioned_solver(solver) -> None:
+    """A rank's handle must treat its boundary faces as transmissive: with
+    periodic boundaries it would pair the faces where its ghost region is cut
+    across the period and silently compute wrong values there.  Raises
+    ValueError for such a handle."""
+    from . import BOUNDARY_KINDS
+    if solver.config.boundary_left == BOUNDARY_KINDS["periodic"]:
+        raise ValueError("partitioned runs: periodic boundaries are not supported (a rank's"
+                         " cut faces would be paired across the period); build each rank's"
+                         " handle with boundary='transmissive'")
+
+
 def step_partitioned(solver, exchange: HaloExchange, cfl: float, polynomial_order: int,
                      group=None) -> float:
     """One step of a rank of a partitioned run on its GPU: the whole-mesh dt
-    from the reduced CFL parts, the step, then the ghost exchange."""
+    from the reduced CFL parts, the step, then the ghost exchange.
+
+    The handle checks every local element, ghosts included: a non-physical
+    cell average or a mean below a positivity floor in a ghost layer (the
+    outer layers are spoiled by the cut, by design, and overwritten by the
+    exchange) raises the error on this rank even though another rank owns the
+    element."""
     import torch
+    check_partitioned_solver(solver)
     dt = global_dt(solver, cfl, polynomial_order, group=group, device="cuda")
     solver.step(dt)
     solver.sync()
