@@ -835,6 +835,7 @@ def limited(args, rank, world, local_rank):
                              volume_rule_order=-1 if form == "mixed" else 0,
                              positivity_all=form == "mixed")
         setup_s = time.perf_counter() - t0
+        setup_ms = {k: round(v, 1) for k, v in g.setup_times().items()}
         cases.project_initial(g, problem.conserved)
         g.limit()
         if weights is not None:
@@ -851,8 +852,8 @@ def limited(args, rank, world, local_rank):
         entry = {"value": 3.0 * g.state_size * args.steps / (ms * 1e-3),
                  "ms_per_step": ms / args.steps, "gpu_launches": launches,
                  "troubled_fraction_last_step": float(flags.mean()),
-                 "setup_s": round(setup_s, 1), "kernel": kernel_description(g.tuning()),
-                 "clocks": clocks}
+                 "setup_s": round(setup_s, 1), "setup_ms_by_phase": setup_ms,
+                 "kernel": kernel_description(g.tuning()), "clocks": clocks}
         if weights is not None:
             entry["indicator"] = g.indicator_stats()
             entry["indicator_training_loss"] = train_loss

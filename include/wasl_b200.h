@@ -216,6 +216,37 @@ int wasl_gpu_tuning(const wasl_gpu *handle, int *choice, double *ms, int capacit
  * counterpart in the reference (its state lives in host vectors). */
 int wasl_gpu_element_order(const wasl_gpu *handle, int64_t *order, int64_t count);
 
+/* Setup phases timed by wasl_gpu_create (wall clock, ms), for
+ * wasl_gpu_setup_times.  The reference builds the same data in its case
+ * drivers (cpp/src/case/euler_triangle.cpp:16-25). */
+enum wasl_setup_phase {
+  WASL_SETUP_TOPOLOGY = 0, /* mesh normalisation and faces (host) */
+  WASL_SETUP_ORDER = 1,    /* element storage order (host) */
+  WASL_SETUP_PERIODIC = 2, /* periodic donor search (device) and donor basis (host) */
+  WASL_SETUP_FACES = 3,    /* face slots, tile and patch arrays, reference tables */
+  WASL_SETUP_STENCIL = 4,  /* limiter stencil: neighbours (host), transforms (device) */
+  WASL_SETUP_OTHER = 5,    /* state buffers and the remaining uploads */
+  WASL_SETUP_PHASES = 6
+};
+/* The setup phases' times: ms[phase] for phase < count (count <= 6).  Phases
+ * a solver has no work for read 0. */
+int wasl_gpu_setup_times(const wasl_gpu *handle, double *ms, int count);
+
+/* The limiter stencil's candidate transforms as the limiter reads them,
+ * [element][candidate][target mode][source mode] in the caller's order
+ * (count = elements x 3 x modes^2), built on the device at setup.  Matches
+ * the reference's CandidateTransform (cpp/include/wasl/limiting/weno/
+ * candidate_transform.hpp:18-41).  2D Euler with limiting only. */
+int wasl_gpu_stencil_transforms(wasl_gpu *handle, double *transforms, int64_t count);
+
+/* The periodic trace as the stage kernels read it: for every boundary face
+ * b (ascending face index) and edge point q, the donor element (caller's
+ * index) and the donor's basis at the image point, donors [b][q], basis
+ * [b][q][mode] (points = boundary faces x (p + 1)).  Matches the reference's
+ * periodic trace (cpp/src/boundaries/periodic_triangle_trace.cpp:40-67).
+ * Periodic triangle meshes only. */
+int wasl_gpu_periodic_trace(wasl_gpu *handle, int32_t *donors, double *basis, int64_t points);
+
 /* Device pointer of the state U[variable][mode][element] and the handle's
  * CUDA stream (cudaStream_t), for callers that keep data on the device. */
 int wasl_gpu_state_device(wasl_gpu *handle, double **device_pointer);

@@ -104,6 +104,9 @@ SIGNATURES = {
     "wasl_gpu_state_device": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "wasl_gpu_element_order": (C.c_int, [C.c_void_p, _i64, C.c_int64]),
     "wasl_gpu_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "wasl_gpu_setup_times": (C.c_int, [C.c_void_p, _d, C.c_int]),
+    "wasl_gpu_stencil_transforms": (C.c_int, [C.c_void_p, _d, C.c_int64]),
+    "wasl_gpu_periodic_trace": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), _d, C.c_int64]),
     "wasl_gpu_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), _d, C.c_int,
                                   C.POINTER(C.c_int)]),
     "wasl_batch_config_default": (None, [C.POINTER(BatchConfig)]),
@@ -375,6 +378,29 @@ class Solver:
         s = C.c_void_p()
         self._check(self._lib.wasl_gpu_stream(self._h, C.byref(s)))
         return s.value or 0
+
+    # ---- setup products -----------------------------------------------------------
+    SETUP_PHASES = ("topology", "order", "periodic", "faces", "stencil", "other")
+
+    def setup_times(self) -> dict:
+        """Wall-clock ms of each setup phase (wasl_gpu_setup_times)."""
+        ms = np.zeros(len(self.SETUP_PHASES))
+        self._check(self._lib.wasl_gpu_setup_times(self._h, _ptr(ms), len(ms)))
+        return dict(zip(self.SETUP_PHASES, ms.tolist()))
+
+    def stencil_transforms(self) -> np.ndarray:
+        """The limiter's candidate transforms [element][3][target][source]."""
+        out = np.empty((self.elements, 3, self.modes, self.modes))
+        self._check(self._lib.wasl_gpu_stencil_transforms(self._h, _ptr(out), out.size))
+        return out
+
+    def periodic_trace(self, boundary_faces: int, points: int):
+        """(donors [boundary face][point], basis [boundary face][point][mode])."""
+        donors = np.empty((boundary_faces, points), dtype=np.int32)
+        basis = np.empty((boundary_faces, points, self.modes))
+        self._check(self._lib.wasl_gpu_periodic_trace(
+            self._h, donors.ctypes.data_as(C.POINTER(C.c_int32)), _ptr(basis), donors.size))
+        return donors, basis
 
     # ---- measurement ------------------------------------------------------------
     def tuning(self):

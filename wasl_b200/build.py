@@ -55,6 +55,7 @@ SOURCES = {
     "capi_batch.cpp": [],
     "mlp.cu": [],
     "mlp_trainer.cpp": [],
+    "setup_device.cu": ["--fmad=false"],
 }
 HEADERS = [f for f in os.listdir(CSRC) if f.endswith((".hpp", ".cuh", ".h"))]
 

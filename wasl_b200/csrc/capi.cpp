@@ -33,15 +33,23 @@ std::unique_ptr<Solver> make_solver(const wasl_gpu_config &cfg, std::int64_t nod
   if (!form_supported(cfg.precision, cfg.dimensions, cfg.equation, cfg.polynomial_order))
     throw SolverError(WASL_ERR_ARGUMENT,
                       "unsupported combination of dimension, equation, order and precision");
+  SetupTimes topology;
+  topology.start();
+  std::unique_ptr<Solver> solver;
   if (cfg.dimensions == 2) {
     TriTopology topo =
         build_triangle_topology(node_count, node_tags, coordinates, element_count, element_nodes);
-    if (cfg.equation == WASL_EULER)
-      return make_euler_tri_solver(cfg, std::move(topo));
-    return make_scalar_tri_solver(cfg, std::move(topo));
+    topology.lap(WASL_SETUP_TOPOLOGY);
+    solver = cfg.equation == WASL_EULER ? make_euler_tri_solver(cfg, std::move(topo))
+                                        : make_scalar_tri_solver(cfg, std::move(topo));
+  } else {
+    LineTopology topo =
+        build_line_topology(node_count, node_tags, coordinates, element_count, element_nodes);
+    topology.lap(WASL_SETUP_TOPOLOGY);
+    solver = make_line_solver(cfg, std::move(topo));
   }
-  return make_line_solver(cfg, build_line_topology(node_count, node_tags, coordinates,
-                                                   element_count, element_nodes));
+  solver->setup_times().ms[WASL_SETUP_TOPOLOGY] = topology.ms[WASL_SETUP_TOPOLOGY];
+  return solver;
 }
 } // namespace wasl_b200
 
@@ -329,6 +337,29 @@ int wasl_gpu_element_order(const wasl_gpu *h, int64_t *order, int64_t count) {
     need(order != nullptr, "null pointer");
     need(count == h->solver->elements(), "element order: count must be the element count");
     h->solver->element_order(order);
+  });
+}
+
+int wasl_gpu_setup_times(const wasl_gpu *h, double *ms, int count) {
+  return guarded(const_cast<wasl_gpu *>(h), [&] {
+    need(ms != nullptr, "null pointer");
+    need(count >= 0 && count <= WASL_SETUP_PHASES, "setup times: count must be 0..6");
+    for (int k = 0; k < count; ++k)
+      ms[k] = h->solver->setup_times().ms[k];
+  });
+}
+
+int wasl_gpu_stencil_transforms(wasl_gpu *h, double *transforms, int64_t count) {
+  return guarded(h, [&] {
+    need(transforms != nullptr, "null pointer");
+    h->solver->stencil_transforms(transforms, count);
+  });
+}
+
+int wasl_gpu_periodic_trace(wasl_gpu *h, int32_t *donors, double *basis, int64_t points) {
+  return guarded(h, [&] {
+    need(donors != nullptr && basis != nullptr, "null pointer");
+    h->solver->periodic_trace(donors, basis, points);
   });
 }
 

@@ -15,6 +15,7 @@
 #include "kernels.hpp"
 #include "mesh.hpp"
 #include "mlp.hpp"
+#include "setup_device.hpp"
 #include "solver.hpp"
 #include "tri_setup.hpp"
 #include "tri_tables.hpp"
@@ -95,6 +96,7 @@ public:
       throw SolverError(WASL_ERR_ARGUMENT, "unknown precision form");
     cuda_check(cudaSetDevice(cfg.device), "cudaSetDevice");
     cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
+    setup_.start();
     ne_ = mesh_.element_count;
     const std::int64_t nf = mesh_.face_count();
     const int QF = p_ + 1;
@@ -110,6 +112,7 @@ public:
         rank_[order_[i]] = static_cast<std::int32_t>(i);
       d_order_.upload(order_, stream_);
     }
+    setup_.lap(WASL_SETUP_ORDER);
 
     bool has_boundary = false;
     for (std::int64_t f = 0; f < nf; ++f)
@@ -117,9 +120,16 @@ public:
     boundary_ = cfg.boundary_left;
     if (boundary_ != WASL_PERIODIC && boundary_ != WASL_TRANSMISSIVE)
       throw SolverError(WASL_ERR_RUNTIME, "simulation: 2D Euler boundaries must be periodic");
+    // The element maps on the device, for the donor search and the limiter
+    // stencil's transforms (freed when setup ends).
+    DeviceArray<double> d_maps;
+    const bool periodic_search = has_boundary && boundary_ == WASL_PERIODIC;
+    if (periodic_search || (cfg.limiting && p_ > 0))
+      upload_maps(mesh_, d_maps, stream_);
     PeriodicTrace trace;
-    if (has_boundary && boundary_ == WASL_PERIODIC)
-      trace = periodic_trace(mesh_, p_);
+    if (periodic_search)
+      trace = periodic_trace_device(mesh_, p_, d_maps.get(), stream_);
+    setup_.lap(WASL_SETUP_PERIODIC);
 
     TriSlots t = build_tri_slots(mesh_, boundary_ == WASL_PERIODIC && has_boundary ? &trace : nullptr,
                                  QF, M_);
@@ -195,12 +205,15 @@ public:
     std::vector<unsigned char> table64(euler_tri_face_table_bytes(p_, false));
     fill_euler_tri_face_table(p_, false, table64.data());
     d_face_table64_.upload(table64, stream_);
+    setup_.lap(WASL_SETUP_FACES);
 
     limiting_ = cfg.limiting && p_ > 0;
     if (limiting_) {
-      stencil_ = triangle_stencil(mesh_, p_, trace.donors);
+      stencil_ = triangle_stencil(mesh_, p_, trace.donors, /*transforms=*/false);
       d_neighbors_.upload(blocks(ids(stencil_.neighbors), 3), stream_);
-      d_transforms_.upload(blocks(stencil_.transforms, 3 * M_ * M_), stream_);
+      d_transforms_.resize(static_cast<std::size_t>(ne_) * 3 * M_ * M_);
+      stencil_transforms_device(mesh_, p_, stencil_.neighbors, order_, d_maps.get(),
+                                d_transforms_.get(), stream_);
       d_normal_x_.upload(columns(stencil_.normal_x, 1), stream_);
       d_normal_y_.upload(columns(stencil_.normal_y, 1), stream_);
       d_check_.upload(stencil_.check_basis, stream_);
@@ -208,6 +221,7 @@ public:
       d_limited_.resize(static_cast<std::size_t>(ne_) * 4 * M_);
       d_troubled_.resize(ne_);
     }
+    setup_.lap(WASL_SETUP_STENCIL);
     d_flags_.resize(3 * ne_);
     cuda_check(cudaMemsetAsync(d_flags_.get(), 0, 3 * ne_, stream_), "memset");
     d_count_.resize(4);
@@ -221,6 +235,7 @@ public:
     cuda_check(cudaMemsetAsync(d_error_.get(), 0, sizeof(unsigned long long), stream_), "memset");
     length_ = minimum_altitude(mesh_);
     cuda_check(cudaStreamSynchronize(stream_), "setup");
+    setup_.lap(WASL_SETUP_OTHER);
   }
 
   ~EulerTriSolver() override {
@@ -285,6 +300,42 @@ public:
                                cudaMemcpyDeviceToHost, stream_),
                "get_state");
     cuda_check(cudaStreamSynchronize(stream_), "get_state");
+  }
+
+  void stencil_transforms(double *out, std::int64_t count) override {
+    const std::int64_t width = 3 * static_cast<std::int64_t>(M_) * M_;
+    if (!limiting_)
+      throw SolverError(WASL_ERR_ARGUMENT, "stencil transforms: the handle has no limiter");
+    if (count != ne_ * width)
+      throw SolverError(WASL_ERR_ARGUMENT,
+                        "stencil transforms: count must be elements x 3 x modes^2");
+    std::vector<double> stored(static_cast<std::size_t>(count));
+    cuda_check(cudaMemcpyAsync(stored.data(), d_transforms_.get(), count * sizeof(double),
+                               cudaMemcpyDeviceToHost, stream_),
+               "transforms");
+    cuda_check(cudaStreamSynchronize(stream_), "transforms");
+    for (std::int64_t i = 0; i < ne_; ++i)
+      std::copy(stored.begin() + i * width, stored.begin() + (i + 1) * width,
+                out + (relabel_ ? order_[i] : i) * width);
+  }
+
+  void periodic_trace(std::int32_t *donors, double *basis, std::int64_t points) override {
+    const std::int64_t n = static_cast<std::int64_t>(d_donor_.size());
+    if (n == 0)
+      throw SolverError(WASL_ERR_ARGUMENT, "periodic trace: the mesh has no periodic faces");
+    if (points != n)
+      throw SolverError(WASL_ERR_ARGUMENT,
+                        "periodic trace: points must be boundary faces x (order + 1)");
+    cuda_check(cudaMemcpyAsync(donors, d_donor_.get(), n * sizeof(std::int32_t),
+                               cudaMemcpyDeviceToHost, stream_),
+               "donors");
+    cuda_check(cudaMemcpyAsync(basis, d_donor_basis_.get(), n * M_ * sizeof(double),
+                               cudaMemcpyDeviceToHost, stream_),
+               "donor basis");
+    cuda_check(cudaStreamSynchronize(stream_), "periodic trace");
+    if (relabel_)
+      for (std::int64_t k = 0; k < n; ++k)
+        donors[k] = order_[donors[k]];
   }
 
   void element_order(std::int64_t *order) const override {

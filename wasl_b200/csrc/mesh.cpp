@@ -1,15 +1,19 @@
 #include "mesh.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <limits>
+#include <mutex>
 #include <stdexcept>
 #include <thread>
 #include <unordered_map>
 
 #include "basis.hpp"
+#include "parallel.hpp"
 
 namespace wasl_b200 {
+
 
 // ---- affine triangle map (cpp/include/wasl/mesh/triangle/triangle_geometry.hpp) ----
 
@@ -71,17 +75,48 @@ namespace {
 
 constexpr int edge_vertices[3][2] = {{0, 1}, {1, 2}, {2, 0}};
 
-std::unordered_map<std::int64_t, std::int64_t> node_index(std::int64_t count,
-                                                          const std::int64_t *tags,
-                                                          const char *context) {
-  std::unordered_map<std::int64_t, std::int64_t> index;
-  index.reserve(static_cast<std::size_t>(count) * 2);
-  for (std::int64_t i = 0; i < count; ++i)
-    if (!index.emplace(tags[i], i).second)
-      throw std::runtime_error(std::string(context) + ": duplicate node tag " +
-                               std::to_string(tags[i]));
-  return index;
-}
+// Position of every node tag: a direct table when the tags are dense (the
+// usual 1..N numbering), a hash map otherwise.  Throws on the first
+// duplicate tag in input order.
+class NodeIndex {
+public:
+  NodeIndex(std::int64_t count, const std::int64_t *tags, const char *context) {
+    std::int64_t lo = std::numeric_limits<std::int64_t>::max(), hi = std::numeric_limits<std::int64_t>::min();
+    for (std::int64_t i = 0; i < count; ++i)
+      lo = std::min(lo, tags[i]), hi = std::max(hi, tags[i]);
+    dense_ = count > 0 && hi - lo < 4 * count + 1024;
+    if (dense_) {
+      base_ = lo;
+      table_.assign(static_cast<std::size_t>(hi - lo + 1), -1);
+    } else {
+      map_.reserve(static_cast<std::size_t>(count) * 2);
+    }
+    for (std::int64_t i = 0; i < count; ++i) {
+      const bool fresh = dense_ ? table_[tags[i] - base_] < 0 : map_.emplace(tags[i], i).second;
+      if (!fresh)
+        throw std::runtime_error(std::string(context) + ": duplicate node tag " +
+                                 std::to_string(tags[i]));
+      if (dense_)
+        table_[tags[i] - base_] = i;
+    }
+  }
+  // -1 when the tag is not a node.
+  std::int64_t find(std::int64_t tag) const {
+    if (dense_) {
+      if (tag < base_ || tag - base_ >= static_cast<std::int64_t>(table_.size()))
+        return -1;
+      return table_[tag - base_];
+    }
+    const auto it = map_.find(tag);
+    return it == map_.end() ? -1 : it->second;
+  }
+
+private:
+  bool dense_ = false;
+  std::int64_t base_ = 0;
+  std::vector<std::int64_t> table_;
+  std::unordered_map<std::int64_t, std::int64_t> map_;
+};
 
 double reference_edge_length(int edge) { return edge == 1 ? 2.0 * std::sqrt(2.0) : 2.0; }
 
@@ -94,81 +129,122 @@ TriTopology build_triangle_topology(std::int64_t node_count, const std::int64_t 
     throw std::runtime_error("triangle mesh: document contains no triangle elements");
   if (element_count > std::numeric_limits<std::int32_t>::max())
     throw std::runtime_error("triangle mesh: more elements than 32-bit indices address");
-  const auto index = node_index(node_count, node_tags, "triangle mesh");
+  const NodeIndex index(node_count, node_tags, "triangle mesh");
   TriTopology mesh;
   mesh.element_count = element_count;
   mesh.maps.resize(element_count);
   mesh.nodes.resize(3 * element_count);
-  for (std::int64_t e = 0; e < element_count; ++e) {
-    std::int64_t tag[3];
-    double x[3], y[3];
-    for (int k = 0; k < 3; ++k) {
-      tag[k] = element_nodes[3 * e + k];
-      const auto found = index.find(tag[k]);
-      if (found == index.end())
-        throw std::runtime_error("triangle mesh: element references missing node " +
-                                 std::to_string(tag[k]));
-      x[k] = node_xy[2 * found->second];
-      y[k] = node_xy[2 * found->second + 1];
+  // Node positions of every element's vertices (after reorientation), and the
+  // first failing element in element order, reported as a serial loop would.
+  std::vector<std::int64_t> position(3 * element_count);
+  std::atomic<std::int64_t> first_error{element_count};
+  std::vector<std::string> messages(element_count > 0 ? 1 : 0);
+  std::mutex message_lock;
+  parallel_for(element_count, [&](std::int64_t begin, std::int64_t end) {
+    for (std::int64_t e = begin; e < end; ++e) {
+      std::int64_t tag[3], at[3];
+      double x[3], y[3];
+      std::string error;
+      for (int k = 0; k < 3 && error.empty(); ++k) {
+        tag[k] = element_nodes[3 * e + k];
+        at[k] = index.find(tag[k]);
+        if (at[k] < 0)
+          error = "triangle mesh: element references missing node " + std::to_string(tag[k]);
+        else
+          x[k] = node_xy[2 * at[k]], y[k] = node_xy[2 * at[k] + 1];
+      }
+      if (error.empty()) {
+        const double area2 = x[0] * (y[1] - y[2]) + x[1] * (y[2] - y[0]) + x[2] * (y[0] - y[1]);
+        if (area2 == 0.0)
+          error = "triangle mesh: zero-area element " + std::to_string(e + 1);
+        else if (area2 < 0.0) {
+          std::swap(x[1], x[2]);
+          std::swap(y[1], y[2]);
+          std::swap(tag[1], tag[2]);
+          std::swap(at[1], at[2]);
+        }
+      }
+      if (!error.empty()) {
+        std::lock_guard<std::mutex> guard(message_lock);
+        if (e < first_error.load()) {
+          first_error.store(e);
+          messages[0] = error;
+        }
+        return; // later elements of this range cannot come first
+      }
+      mesh.maps[e] = TriMap{x[0], y[0], x[1], y[1], x[2], y[2]};
+      for (int k = 0; k < 3; ++k) {
+        mesh.nodes[3 * e + k] = tag[k];
+        position[3 * e + k] = at[k];
+      }
     }
-    const double area2 = x[0] * (y[1] - y[2]) + x[1] * (y[2] - y[0]) + x[2] * (y[0] - y[1]);
-    if (area2 == 0.0)
-      throw std::runtime_error("triangle mesh: zero-area element " + std::to_string(e + 1));
-    if (area2 < 0.0) {
-      std::swap(x[1], x[2]);
-      std::swap(y[1], y[2]);
-      std::swap(tag[1], tag[2]);
-    }
-    mesh.maps[e] = TriMap{x[0], y[0], x[1], y[1], x[2], y[2]};
-    for (int k = 0; k < 3; ++k)
-      mesh.nodes[3 * e + k] = tag[k];
-  }
+  });
+  if (first_error.load() < element_count)
+    throw std::runtime_error(messages[0]);
 
-  // Each element edge keyed by its sorted vertex pair; a stable sort keeps the
-  // element order inside a key, so the first entry is the first element to
-  // reach the edge.
-  struct Side {
-    std::int64_t lo, hi, v0;
-    std::int32_t element;
-    std::int32_t edge;
-  };
-  std::vector<Side> sides(3 * element_count);
+  // Edges matched through their smaller-tag endpoint: the element edges are
+  // bucketed by that node (a counting sort, which keeps element order inside
+  // a bucket), and a bucket's edges are grouped by the other endpoint.  An
+  // edge's first element (by index, then local edge) is its left side, as
+  // the reference's stable sort by (smaller tag, larger tag) makes it.
+  const std::int64_t sides = 3 * element_count;
+  std::vector<std::int64_t> low(sides), high(sides);
   for (std::int64_t e = 0; e < element_count; ++e)
     for (int k = 0; k < 3; ++k) {
-      const std::int64_t a = mesh.nodes[3 * e + edge_vertices[k][0]];
-      const std::int64_t b = mesh.nodes[3 * e + edge_vertices[k][1]];
-      sides[3 * e + k] = {std::min(a, b), std::max(a, b), a, static_cast<std::int32_t>(e), k};
+      const int a = edge_vertices[k][0], b = edge_vertices[k][1];
+      const bool a_first = mesh.nodes[3 * e + a] < mesh.nodes[3 * e + b];
+      low[3 * e + k] = position[3 * e + (a_first ? a : b)];
+      high[3 * e + k] = position[3 * e + (a_first ? b : a)];
     }
-  std::stable_sort(sides.begin(), sides.end(), [](const Side &a, const Side &b) {
-    return a.lo != b.lo ? a.lo < b.lo : a.hi < b.hi;
-  });
-
-  struct Face {
-    std::int32_t left, right, le, re;
-    std::uint8_t flip;
-  };
-  std::vector<Face> faces;
-  faces.reserve(sides.size() / 2 + 64);
-  for (std::size_t i = 0; i < sides.size();) {
-    std::size_t j = i + 1;
-    while (j < sides.size() && sides[j].lo == sides[i].lo && sides[j].hi == sides[i].hi)
-      ++j;
-    if (j - i > 2)
-      throw std::runtime_error("triangle mesh: edge " + std::to_string(sides[i].lo) + "-" +
-                               std::to_string(sides[i].hi) +
-                               " has more than two adjacent elements (non-conforming mesh)");
-    if (j - i == 2)
-      faces.push_back({sides[i].element, sides[i + 1].element, sides[i].edge, sides[i + 1].edge,
-                       static_cast<std::uint8_t>(sides[i].v0 != sides[i + 1].v0)});
-    else
-      faces.push_back({sides[i].element, -1, sides[i].edge, 0, 0});
-    i = j;
+  std::vector<std::int64_t> start(node_count + 1, 0), bucket(sides);
+  for (std::int64_t i = 0; i < sides; ++i)
+    ++start[low[i] + 1];
+  for (std::int64_t n = 0; n < node_count; ++n)
+    start[n + 1] += start[n];
+  {
+    std::vector<std::int64_t> fill(start.begin(), start.end() - 1);
+    for (std::int64_t i = 0; i < sides; ++i)
+      bucket[fill[low[i]]++] = i;
   }
-  std::sort(faces.begin(), faces.end(), [](const Face &a, const Face &b) {
-    return a.left != b.left ? a.left < b.left : a.le < b.le;
-  });
+  // Per side: the other side of its face (-1: boundary, -2: not yet grouped)
+  // and whether it is the face's left side.
+  std::vector<std::int64_t> other(sides, -2);
+  std::vector<std::uint8_t> is_left(sides, 0);
+  std::int64_t worst_low = -1, worst_high = -1; // first edge, by tags, with > 2 sides
+  for (std::int64_t n = 0; n < node_count; ++n)
+    for (std::int64_t u = start[n]; u < start[n + 1]; ++u) {
+      const std::int64_t i = bucket[u];
+      if (other[i] != -2)
+        continue;
+      std::int64_t j = -1, extra = 0;
+      for (std::int64_t w = u + 1; w < start[n + 1]; ++w) {
+        const std::int64_t c = bucket[w];
+        if (other[c] == -2 && high[c] == high[i]) {
+          if (j < 0)
+            j = c;
+          else
+            ++extra, other[c] = -1;
+        }
+      }
+      if (extra > 0) {
+        const std::int64_t lt = node_tags[low[i]], ht = node_tags[high[i]];
+        if (worst_low < 0 || lt < worst_low || (lt == worst_low && ht < worst_high))
+          worst_low = lt, worst_high = ht;
+      }
+      is_left[i] = 1;
+      other[i] = j;
+      if (j >= 0)
+        other[j] = i;
+    }
+  if (worst_low >= 0)
+    throw std::runtime_error("triangle mesh: edge " + std::to_string(worst_low) + "-" +
+                             std::to_string(worst_high) +
+                             " has more than two adjacent elements (non-conforming mesh)");
 
-  const std::size_t nf = faces.size();
+  // Faces in (left element, left local edge) order: the left sides in side order.
+  std::int64_t nf = 0;
+  for (std::int64_t i = 0; i < sides; ++i)
+    nf += is_left[i];
   mesh.face_left.resize(nf);
   mesh.face_right.resize(nf);
   mesh.face_left_edge.resize(nf);
@@ -177,17 +253,33 @@ TriTopology build_triangle_topology(std::int64_t node_count, const std::int64_t 
   mesh.face_nx.resize(nf);
   mesh.face_ny.resize(nf);
   mesh.face_scale.resize(nf);
-  for (std::size_t f = 0; f < nf; ++f) {
-    const Face &face = faces[f];
-    mesh.face_left[f] = face.left;
-    mesh.face_right[f] = face.right;
-    mesh.face_left_edge[f] = face.le;
-    mesh.face_right_edge[f] = face.re;
-    mesh.face_flip[f] = face.flip;
-    const TriMap &m = mesh.maps[face.left];
-    m.edge_normal(face.le, mesh.face_nx[f], mesh.face_ny[f]);
-    mesh.face_scale[f] = m.edge_length(face.le) / reference_edge_length(face.le);
-  }
+  std::vector<std::int64_t> face_side(nf);
+  for (std::int64_t i = 0, f = 0; i < sides; ++i)
+    if (is_left[i])
+      face_side[f++] = i;
+  parallel_for(nf, [&](std::int64_t begin, std::int64_t end) {
+    for (std::int64_t f = begin; f < end; ++f) {
+      const std::int64_t i = face_side[f], j = other[i];
+      const std::int32_t left = static_cast<std::int32_t>(i / 3), le = static_cast<std::int32_t>(i % 3);
+      mesh.face_left[f] = left;
+      mesh.face_left_edge[f] = le;
+      if (j >= 0) {
+        mesh.face_right[f] = static_cast<std::int32_t>(j / 3);
+        mesh.face_right_edge[f] = static_cast<std::int32_t>(j % 3);
+        // The two sides traverse the edge from different first vertices.
+        mesh.face_flip[f] = static_cast<std::uint8_t>(
+            mesh.nodes[3 * (i / 3) + edge_vertices[i % 3][0]] !=
+            mesh.nodes[3 * (j / 3) + edge_vertices[j % 3][0]]);
+      } else {
+        mesh.face_right[f] = -1;
+        mesh.face_right_edge[f] = 0;
+        mesh.face_flip[f] = 0;
+      }
+      const TriMap &m = mesh.maps[left];
+      m.edge_normal(le, mesh.face_nx[f], mesh.face_ny[f]);
+      mesh.face_scale[f] = m.edge_length(le) / reference_edge_length(le);
+    }
+  });
   return mesh;
 }
 
@@ -196,21 +288,21 @@ LineTopology build_line_topology(std::int64_t node_count, const std::int64_t *no
                                  const std::int64_t *element_nodes) {
   if (element_count <= 0)
     throw std::runtime_error("line mesh: document contains no line elements");
-  const auto index = node_index(node_count, node_tags, "line mesh");
+  const NodeIndex index(node_count, node_tags, "line mesh");
   struct Segment {
     std::int64_t left_node, right_node;
     double xl, xr;
   };
   std::vector<Segment> segs(element_count);
   for (std::int64_t e = 0; e < element_count; ++e) {
-    const auto a = index.find(element_nodes[2 * e]);
-    const auto b = index.find(element_nodes[2 * e + 1]);
-    if (a == index.end() || b == index.end())
+    const std::int64_t ta = element_nodes[2 * e], tb = element_nodes[2 * e + 1];
+    const std::int64_t a = index.find(ta), b = index.find(tb);
+    if (a < 0 || b < 0)
       throw std::runtime_error("line mesh: element references missing node");
-    const double xa = node_x[a->second], xb = node_x[b->second];
+    const double xa = node_x[a], xb = node_x[b];
     if (xa == xb)
       throw std::runtime_error("line mesh: zero-length element " + std::to_string(e + 1));
-    segs[e] = xa < xb ? Segment{a->first, b->first, xa, xb} : Segment{b->first, a->first, xb, xa};
+    segs[e] = xa < xb ? Segment{ta, tb, xa, xb} : Segment{tb, ta, xb, xa};
   }
   std::stable_sort(segs.begin(), segs.end(),
                    [](const Segment &a, const Segment &b) { return a.xl < b.xl; });
@@ -237,17 +329,9 @@ LineTopology build_line_topology(std::int64_t node_count, const std::int64_t *no
   return mesh;
 }
 
-namespace {
-
-struct Box {
-  double min_x = std::numeric_limits<double>::max();
-  double max_x = std::numeric_limits<double>::lowest();
-  double min_y = std::numeric_limits<double>::max();
-  double max_y = std::numeric_limits<double>::lowest();
-};
-
 Box bounding_box(const TriTopology &mesh) {
-  Box b;
+  Box b{std::numeric_limits<double>::max(), std::numeric_limits<double>::lowest(),
+        std::numeric_limits<double>::max(), std::numeric_limits<double>::lowest()};
   for (const auto &m : mesh.maps) {
     b.min_x = std::min({b.min_x, m.x0, m.x1, m.x2});
     b.max_x = std::max({b.max_x, m.x0, m.x1, m.x2});
@@ -257,124 +341,136 @@ Box bounding_box(const TriTopology &mesh) {
   return b;
 }
 
-// Uniform bucket grid over element bounding boxes, padded so that any element
-// passing the 1e-10 reference-coordinate containment test is a candidate.
-class ElementGrid {
-public:
-  explicit ElementGrid(const TriTopology &mesh) : mesh_(mesh) {
-    const Box box = bounding_box(mesh);
-    x0_ = box.min_x;
-    y0_ = box.min_y;
-    const double n = std::max(1.0, std::sqrt(static_cast<double>(mesh.element_count) / 2.0));
-    nx_ = ny_ = static_cast<int>(n);
-    dx_ = std::max((box.max_x - box.min_x) / nx_, 1e-300);
-    dy_ = std::max((box.max_y - box.min_y) / ny_, 1e-300);
-    start_.assign(static_cast<std::size_t>(nx_) * ny_ + 1, 0);
-    std::vector<std::pair<int, std::int32_t>> entries;
-    for (std::int64_t e = 0; e < mesh.element_count; ++e) {
-      int i0, i1, j0, j1;
-      cells(e, i0, i1, j0, j1);
-      for (int j = j0; j <= j1; ++j)
-        for (int i = i0; i <= i1; ++i)
-          entries.emplace_back(j * nx_ + i, static_cast<std::int32_t>(e));
-    }
-    std::stable_sort(entries.begin(), entries.end(),
-                     [](const auto &a, const auto &b) { return a.first < b.first; });
-    items_.resize(entries.size());
-    for (std::size_t k = 0; k < entries.size(); ++k) {
-      items_[k] = entries[k].second;
-      ++start_[entries[k].first + 1];
-    }
-    for (std::size_t c = 1; c < start_.size(); ++c)
-      start_[c] += start_[c - 1];
-  }
 
-  // The first element, by index, containing (x, y) within the tolerance.
-  std::int32_t find(double x, double y, double &xi, double &eta) const {
-    constexpr double tolerance = 1e-10;
-    const int i = clamp_cell(static_cast<int>(std::floor((x - x0_) / dx_)), nx_);
-    const int j = clamp_cell(static_cast<int>(std::floor((y - y0_) / dy_)), ny_);
-    const std::size_t c = static_cast<std::size_t>(j) * nx_ + i;
-    for (std::size_t k = start_[c]; k < start_[c + 1]; ++k) { // ascending element index
-      const std::int32_t e = items_[k];
-      mesh_.maps[e].to_reference(x, y, xi, eta);
-      if (xi >= -1.0 - tolerance && eta >= -1.0 - tolerance && xi + eta <= tolerance)
-        return e;
-    }
-    return -1;
-  }
-
-private:
-  static int clamp_cell(int v, int n) { return v < 0 ? 0 : (v >= n ? n - 1 : v); }
-
-  void cells(std::int64_t e, int &i0, int &i1, int &j0, int &j1) const {
-    const TriMap &m = mesh_.maps[e];
-    const double lx = std::min({m.x0, m.x1, m.x2}), hx = std::max({m.x0, m.x1, m.x2});
-    const double ly = std::min({m.y0, m.y1, m.y2}), hy = std::max({m.y0, m.y1, m.y2});
-    const double pad = 1e-6 * ((hx - lx) + (hy - ly));
-    i0 = clamp_cell(static_cast<int>(std::floor((lx - pad - x0_) / dx_)), nx_);
-    i1 = clamp_cell(static_cast<int>(std::floor((hx + pad - x0_) / dx_)), nx_);
-    j0 = clamp_cell(static_cast<int>(std::floor((ly - pad - y0_) / dy_)), ny_);
-    j1 = clamp_cell(static_cast<int>(std::floor((hy + pad - y0_) / dy_)), ny_);
-  }
-
-  const TriTopology &mesh_;
-  double x0_, y0_, dx_, dy_;
-  int nx_, ny_;
-  std::vector<std::size_t> start_;
-  std::vector<std::int32_t> items_;
-};
-
-template <typename F> void parallel_for(std::int64_t n, F &&body) {
-  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const std::int64_t workers = std::min<std::int64_t>(hw, std::max<std::int64_t>(1, n / 256));
-  if (workers <= 1) {
-    body(0, n);
-    return;
-  }
-  std::vector<std::thread> pool;
-  for (std::int64_t w = 0; w < workers; ++w)
-    pool.emplace_back([&, w] { body(n * w / workers, n * (w + 1) / workers); });
-  for (auto &t : pool)
-    t.join();
+GridShape element_grid_shape(const TriTopology &mesh) {
+  const Box box = bounding_box(mesh);
+  GridShape g;
+  g.x0 = box.min_x;
+  g.y0 = box.min_y;
+  const double n = std::max(1.0, std::sqrt(static_cast<double>(mesh.element_count) / 2.0));
+  g.nx = g.ny = static_cast<int>(n);
+  g.dx = std::max((box.max_x - box.min_x) / g.nx, 1e-300);
+  g.dy = std::max((box.max_y - box.min_y) / g.ny, 1e-300);
+  return g;
 }
 
-} // namespace
-
-PeriodicTrace periodic_trace(const TriTopology &mesh, int p) {
-  const int Q = p + 1, M = tri_modes(p);
+PeriodicImages periodic_images(const TriTopology &mesh, int p) {
+  const int Q = p + 1;
   const Rule2D edges = triangle_edges(p);
   const Box box = bounding_box(mesh);
-  const std::int64_t nf = mesh.face_count();
-  PeriodicTrace trace;
-  trace.donors.assign(nf * Q, -1);
-  trace.basis.assign(nf * Q * M, 0.0);
-  const ElementGrid grid(mesh);
-  for (std::int64_t f = 0; f < nf; ++f) {
+  PeriodicImages im;
+  im.points = Q;
+  for (std::int64_t f = 0; f < mesh.face_count(); ++f) {
     if (mesh.face_right[f] >= 0)
       continue;
+    const double nx = mesh.face_nx[f], ny = mesh.face_ny[f];
+    const bool along_x = std::fabs(nx) > 0.5 && std::fabs(ny) < 1e-10;
+    const bool along_y = std::fabs(ny) > 0.5 && std::fabs(nx) < 1e-10;
+    if (!along_x && !along_y) {
+      // Reported after the donors of the faces before it, in face order.
+      im.misaligned = true;
+      break;
+    }
     const TriMap &m = mesh.maps[mesh.face_left[f]];
     const int le = mesh.face_left_edge[f];
-    const double nx = mesh.face_nx[f], ny = mesh.face_ny[f];
     for (int q = 0; q < Q; ++q) {
       double x = 0.0, y = 0.0;
       m.to_physical(edges.xi[le * Q + q], edges.eta[le * Q + q], x, y);
-      if (std::fabs(nx) > 0.5 && std::fabs(ny) < 1e-10)
+      if (along_x)
         x += nx < 0.0 ? box.max_x - box.min_x : box.min_x - box.max_x;
-      else if (std::fabs(ny) > 0.5 && std::fabs(nx) < 1e-10)
-        y += ny < 0.0 ? box.max_y - box.min_y : box.min_y - box.max_y;
       else
-        throw std::runtime_error("simulation: 2D periodic boundaries require an axis-aligned box");
-      double xi = 0.0, eta = 0.0;
-      const std::int32_t donor = grid.find(x, y, xi, eta);
-      if (donor < 0)
-        throw std::runtime_error("simulation: periodic 2D trace has no donor element");
-      trace.donors[f * Q + q] = donor;
-      const auto b = dubiner(xi, eta, p);
-      std::copy(b.begin(), b.end(), trace.basis.begin() + (f * Q + q) * M);
+        y += ny < 0.0 ? box.max_y - box.min_y : box.min_y - box.max_y;
+      im.x.push_back(x);
+      im.y.push_back(y);
+    }
+    ++im.faces;
+  }
+  return im;
+}
+
+ImageCells image_cells(const GridShape &g, const PeriodicImages &images) {
+  const std::int64_t n = static_cast<std::int64_t>(images.x.size());
+  std::vector<std::pair<int, std::int64_t>> by_cell(n);
+  for (std::int64_t k = 0; k < n; ++k)
+    by_cell[k] = {grid_cell(g, images.x[k], images.y[k]), k};
+  std::sort(by_cell.begin(), by_cell.end());
+  ImageCells ic;
+  for (std::int64_t k = 0; k < n; ++k) {
+    if (ic.cells.empty() || ic.cells.back() != by_cell[k].first) {
+      ic.cells.push_back(by_cell[k].first);
+      ic.start.push_back(k);
+    }
+    ic.point.push_back(by_cell[k].second);
+  }
+  ic.start.push_back(n);
+  return ic;
+}
+
+PeriodicTrace periodic_trace_from_donors(const TriTopology &mesh, int p,
+                                         const PeriodicImages &images,
+                                         std::vector<std::int32_t> &&donors) {
+  const int Q = images.points, M = tri_modes(p);
+  PeriodicTrace trace;
+  trace.basis.resize(static_cast<std::size_t>(images.faces) * Q * M);
+  for (std::int64_t k = 0; k < images.faces * Q; ++k) {
+    if (donors[k] < 0)
+      throw std::runtime_error("simulation: periodic 2D trace has no donor element");
+    double xi = 0.0, eta = 0.0;
+    mesh.maps[donors[k]].to_reference(images.x[k], images.y[k], xi, eta);
+    const auto b = dubiner(xi, eta, p);
+    std::copy(b.begin(), b.end(), trace.basis.begin() + k * M);
+  }
+  if (images.misaligned)
+    throw std::runtime_error("simulation: 2D periodic boundaries require an axis-aligned box");
+  trace.donors = std::move(donors);
+  return trace;
+}
+
+PeriodicTrace periodic_trace(const TriTopology &mesh, int p) {
+  const PeriodicImages images = periodic_images(mesh, p);
+  const std::int64_t n = static_cast<std::int64_t>(images.x.size());
+  std::vector<std::int32_t> donors(n, -1);
+  if (n > 0) {
+    // Every element checks the image points in the cells its padded box
+    // covers; a point's donor is the smallest element index that contains it,
+    // which is the first candidate of its cell in ascending order.
+    const GridShape g = element_grid_shape(mesh);
+    const ImageCells ic = image_cells(g, images);
+    std::vector<std::atomic<std::int32_t>> best(n);
+    for (auto &b : best)
+      b.store(std::numeric_limits<std::int32_t>::max());
+    parallel_for(mesh.element_count, [&](std::int64_t begin, std::int64_t end) {
+      for (std::int64_t e = begin; e < end; ++e) {
+        const TriMap &m = mesh.maps[e];
+        const double v[6] = {m.x0, m.y0, m.x1, m.y1, m.x2, m.y2};
+        int i0, i1, j0, j1;
+        grid_cell_range(g, v, i0, i1, j0, j1);
+        for (int j = j0; j <= j1; ++j)
+          for (int i = i0; i <= i1; ++i) {
+            const auto it = std::lower_bound(ic.cells.begin(), ic.cells.end(), j * g.nx + i);
+            if (it == ic.cells.end() || *it != j * g.nx + i)
+              continue;
+            const std::size_t r = static_cast<std::size_t>(it - ic.cells.begin());
+            for (std::int64_t k = ic.start[r]; k < ic.start[r + 1]; ++k) {
+              const std::int64_t pt = ic.point[k];
+              double xi = 0.0, eta = 0.0;
+              grid_to_reference(v, images.x[pt], images.y[pt], xi, eta);
+              if (!grid_contains(xi, eta))
+                continue;
+              std::int32_t cur = best[pt].load();
+              while (static_cast<std::int32_t>(e) < cur &&
+                     !best[pt].compare_exchange_weak(cur, static_cast<std::int32_t>(e))) {
+              }
+            }
+          }
+      }
+    });
+    for (std::int64_t k = 0; k < n; ++k) {
+      const std::int32_t b = best[k].load();
+      donors[k] = b == std::numeric_limits<std::int32_t>::max() ? -1 : b;
     }
   }
-  return trace;
+  return periodic_trace_from_donors(mesh, p, images, std::move(donors));
 }
 
 namespace {
@@ -392,14 +488,25 @@ void add_neighbor(LimiterStencil &s, std::int64_t element, std::int32_t neighbor
   }
 }
 
-double period_shift(double gap, double period) {
-  return gap > 0.5 * period ? period : gap < -0.5 * period ? -period : 0.0;
+// Check points: volume rule of order p, then the three edge rules
+// (euler_limiter_stencil_triangle.cpp:81-93).
+void fill_check_basis(LimiterStencil &s, int p) {
+  const Rule2D rule = triangle_rule(p), edges = triangle_edges(p);
+  for (int q = 0; q < rule.size(); ++q) {
+    const auto b = dubiner(rule.xi[q], rule.eta[q], p);
+    s.check_basis.insert(s.check_basis.end(), b.begin(), b.end());
+  }
+  for (int q = 0; q < edges.size(); ++q) {
+    const auto b = dubiner(edges.xi[q], edges.eta[q], p);
+    s.check_basis.insert(s.check_basis.end(), b.begin(), b.end());
+  }
 }
 
 } // namespace
 
 LimiterStencil triangle_stencil(const TriTopology &mesh, int p,
-                                const std::vector<std::int32_t> &periodic_donors) {
+                                const std::vector<std::int32_t> &periodic_donors,
+                                bool transforms) {
   const std::int64_t ne = mesh.element_count;
   const int M = tri_modes(p), Q = p + 1;
   LimiterStencil s;
@@ -412,12 +519,14 @@ LimiterStencil triangle_stencil(const TriTopology &mesh, int p,
   std::vector<std::uint8_t> has_normal(ne, 0);
   // Each element's characteristic direction is the first face giving it a
   // neighbour, outward from it (euler_limiter_stencil_triangle.cpp:16-44).
+  std::int64_t b = 0; // boundary face ordinal
   for (std::int64_t f = 0; f < mesh.face_count(); ++f) {
     const std::int32_t left = mesh.face_left[f];
     std::int32_t right = mesh.face_right[f];
     const bool boundary = right < 0;
     if (boundary && !periodic_donors.empty())
-      right = periodic_donors[f * Q];
+      right = periodic_donors[b * Q];
+    b += boundary;
     if (right < 0)
       continue;
     add_neighbor(s, left, right);
@@ -443,6 +552,10 @@ LimiterStencil triangle_stencil(const TriTopology &mesh, int p,
   const Box box = bounding_box(mesh);
   const double width = box.max_x - box.min_x, height = box.max_y - box.min_y;
   const Rule2D rule = triangle_rule(p);
+  if (!transforms) {
+    fill_check_basis(s, p);
+    return s;
+  }
   std::vector<std::vector<double>> target_basis(rule.size());
   for (int q = 0; q < rule.size(); ++q)
     target_basis[q] = dubiner(rule.xi[q], rule.eta[q], p);
@@ -488,17 +601,7 @@ LimiterStencil triangle_stencil(const TriTopology &mesh, int p,
     }
   });
 
-  // Check points: volume rule of order p, then the three edge rules
-  // (euler_limiter_stencil_triangle.cpp:81-93).
-  const Rule2D edges = triangle_edges(p);
-  for (int q = 0; q < rule.size(); ++q) {
-    const auto b = dubiner(rule.xi[q], rule.eta[q], p);
-    s.check_basis.insert(s.check_basis.end(), b.begin(), b.end());
-  }
-  for (int q = 0; q < edges.size(); ++q) {
-    const auto b = dubiner(edges.xi[q], edges.eta[q], p);
-    s.check_basis.insert(s.check_basis.end(), b.begin(), b.end());
-  }
+  fill_check_basis(s, p);
   return s;
 }
 
@@ -596,12 +699,13 @@ TriSlots build_tri_slots(const TriTopology &mesh, const PeriodicTrace *trace, in
       t.bnd_edge.push_back(static_cast<std::uint8_t>(le));
       t.bnd_normal.push_back(mesh.face_nx[f]);
       bny.push_back(mesh.face_ny[f]);
-      if (trace)
-        for (int q = 0; q < QF; ++q) {
-          t.donors.push_back(trace->donors[f * QF + q]);
-          t.donor_basis.insert(t.donor_basis.end(), trace->basis.begin() + (f * QF + q) * M,
-                               trace->basis.begin() + (f * QF + q + 1) * M);
-        }
+      if (trace) {
+        const std::int64_t b = t.boundary_count;
+        t.donors.insert(t.donors.end(), trace->donors.begin() + b * QF,
+                        trace->donors.begin() + (b + 1) * QF);
+        t.donor_basis.insert(t.donor_basis.end(), trace->basis.begin() + b * QF * M,
+                             trace->basis.begin() + (b + 1) * QF * M);
+      }
       ++t.boundary_count;
     }
     t.face_right[f] = right;

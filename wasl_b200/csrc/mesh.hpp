@@ -13,6 +13,8 @@
 
 #include <cstdint>
 #include <string>
+
+#include "element_grid.hpp"
 #include <vector>
 
 namespace wasl_b200 {
@@ -70,13 +72,49 @@ LineTopology build_line_topology(std::int64_t node_count, const std::int64_t *no
 // point is the first element, by index, whose reference coordinates contain it
 // within 1e-10; a uniform bucket grid narrows the candidates, so the search is
 // near-linear instead of the reference's O(boundary x elements), with the same
-// answer.  donors [face][point] (-1 on interior faces), basis
-// [face][point][mode].
+// answer.  Indexed by boundary face b (the faces without a right element, in
+// ascending face index): donors [b][point], basis [b][point][mode].
 struct PeriodicTrace {
   std::vector<std::int32_t> donors;
   std::vector<double> basis;
 };
 PeriodicTrace periodic_trace(const TriTopology &mesh, int p);
+
+// The mesh's bounding box.
+struct Box {
+  double min_x, max_x, min_y, max_y;
+};
+Box bounding_box(const TriTopology &mesh);
+
+// The boundary edge points' periodic images, in boundary face order: point
+// [b][q] of boundary face b is its left element's edge point q moved by one
+// period across the box (the face's normal is axis-aligned; otherwise throws
+// the reference's "2D periodic boundaries require an axis-aligned box").
+struct PeriodicImages {
+  std::int64_t faces = 0;  // boundary faces with images (all, unless misaligned)
+  int points = 0;          // per face
+  bool misaligned = false; // a boundary face after the last one here is not axis-aligned
+  std::vector<double> x, y;
+};
+PeriodicImages periodic_images(const TriTopology &mesh, int p);
+
+// The donor search's grid over this mesh (element_grid.hpp).
+GridShape element_grid_shape(const TriTopology &mesh);
+
+// The cells holding image points, ascending, each with its points (indices
+// into PeriodicImages::x/y): point[start[r] .. start[r + 1]) lie in cells[r].
+struct ImageCells {
+  std::vector<int> cells;
+  std::vector<std::int64_t> start, point;
+};
+ImageCells image_cells(const GridShape &g, const PeriodicImages &images);
+
+// The periodic trace from each image's donor (-1: none found, which throws
+// the reference's "periodic 2D trace has no donor element"): donors as given,
+// basis evaluated in the donor's reference coordinates.
+PeriodicTrace periodic_trace_from_donors(const TriTopology &mesh, int p,
+                                         const PeriodicImages &images,
+                                         std::vector<std::int32_t> &&donors);
 
 // The face slots and boundary lists the triangle stage kernels read, built in
 // ascending global face index (the reference's flux summation order):
@@ -119,8 +157,19 @@ struct LimiterStencil {
 };
 
 // periodic_donors may be empty (open boundaries).
+// periodic_donors: PeriodicTrace::donors (empty without periodic faces).
+// Without `transforms` the candidate transforms are left empty (the device
+// builds them, setup_device.cu).
 LimiterStencil triangle_stencil(const TriTopology &mesh, int p,
-                                const std::vector<std::int32_t> &periodic_donors);
+                                const std::vector<std::int32_t> &periodic_donors,
+                                bool transforms = true);
+
+// The period a neighbour's copy is shifted by in the limiter stencil: one
+// period toward the target when their centroids lie more than half a period
+// apart (euler_limiter_stencil_triangle.cpp:51-79).
+WASL_HD double period_shift(double gap, double period) {
+  return gap > 0.5 * period ? period : gap < -0.5 * period ? -period : 0.0;
+}
 LimiterStencil line_stencil(const LineTopology &mesh, int p, bool periodic);
 
 // cpp/src/time/cfl_timestep.cpp:14-30

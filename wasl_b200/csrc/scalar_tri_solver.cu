@@ -9,6 +9,7 @@
 #include "basis.hpp"
 #include "kernels.hpp"
 #include "mesh.hpp"
+#include "setup_device.hpp"
 #include "solver.hpp"
 #include "tri_tables.hpp"
 
@@ -27,14 +28,19 @@ public:
                         "simulation: 2D scalar-advection boundaries must be periodic");
     cuda_check(cudaSetDevice(cfg.device), "cudaSetDevice");
     cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
+    setup_.start();
     ne_ = mesh_.element_count;
     const int QF = p_ + 1;
     bool has_boundary = false;
     for (std::int64_t f = 0; f < mesh_.face_count(); ++f)
       has_boundary |= mesh_.face_right[f] < 0;
     PeriodicTrace trace;
-    if (has_boundary)
-      trace = periodic_trace(mesh_, p_);
+    if (has_boundary) {
+      DeviceArray<double> d_maps;
+      upload_maps(mesh_, d_maps, stream_);
+      trace = periodic_trace_device(mesh_, p_, d_maps.get(), stream_);
+    }
+    setup_.lap(WASL_SETUP_PERIODIC);
     const TriSlots t = build_tri_slots(mesh_, has_boundary ? &trace : nullptr, QF, M_);
     d_geo_.upload(t.geo, stream_);
     d_slot_nbr_.upload(t.slot_nbr, stream_);
@@ -55,11 +61,28 @@ public:
     cuda_check(cudaMemsetAsync(d_flags_.get(), 0, 3 * ne_, stream_), "memset");
     length_ = minimum_altitude(mesh_);
     cuda_check(cudaStreamSynchronize(stream_), "setup");
+    setup_.lap(WASL_SETUP_OTHER);
   }
 
   ~ScalarTriSolver() override {
     if (stream_)
       cudaStreamDestroy(stream_);
+  }
+
+  void periodic_trace(std::int32_t *donors, double *basis, std::int64_t points) override {
+    const std::int64_t n = static_cast<std::int64_t>(d_donor_.size());
+    if (n == 0)
+      throw SolverError(WASL_ERR_ARGUMENT, "periodic trace: the mesh has no periodic faces");
+    if (points != n)
+      throw SolverError(WASL_ERR_ARGUMENT,
+                        "periodic trace: points must be boundary faces x (order + 1)");
+    cuda_check(cudaMemcpyAsync(donors, d_donor_.get(), n * sizeof(std::int32_t),
+                               cudaMemcpyDeviceToHost, stream_),
+               "donors");
+    cuda_check(cudaMemcpyAsync(basis, d_donor_basis_.get(), n * M_ * sizeof(double),
+                               cudaMemcpyDeviceToHost, stream_),
+               "donor basis");
+    cuda_check(cudaStreamSynchronize(stream_), "periodic trace");
   }
 
   std::int64_t elements() const override { return ne_; }

@@ -2,6 +2,7 @@
 // and the SSP-RK3 step orchestration.
 #pragma once
 
+#include <chrono>
 #include <cstdint>
 #include <memory>
 #include <stdexcept>
@@ -23,6 +24,19 @@ struct NvtxRange {
   ~NvtxRange() { nvtxRangePop(); }
   NvtxRange(const NvtxRange &) = delete;
   NvtxRange &operator=(const NvtxRange &) = delete;
+};
+
+// Wall-clock time of a solver's setup phases (enum wasl_setup_phase), in ms.
+struct SetupTimes {
+  double ms[WASL_SETUP_PHASES] = {};
+  std::chrono::steady_clock::time_point mark;
+  void start() { mark = std::chrono::steady_clock::now(); }
+  // Adds the time since the last mark to `phase` and moves the mark.
+  void lap(int phase) {
+    const auto now = std::chrono::steady_clock::now();
+    ms[phase] += std::chrono::duration<double, std::milli>(now - mark).count();
+    mark = now;
+  }
 };
 
 // Failure carrying a C-ABI status code.
@@ -171,6 +185,21 @@ public:
     return -1;
   }
 
+  // The limiter's candidate transforms [element][candidate][target][source]
+  // and the periodic trace (donors [boundary face][point], basis
+  // [boundary face][point][mode]) as the kernels read them, in the caller's
+  // element order (2D Euler; the trace also 2D scalar advection).
+  virtual void stencil_transforms(double *out, std::int64_t count) {
+    (void)out, (void)count;
+    throw SolverError(WASL_ERR_ARGUMENT, "stencil transforms: 2D Euler with limiting only");
+  }
+  virtual void periodic_trace(std::int32_t *donors, double *basis, std::int64_t points) {
+    (void)donors, (void)basis, (void)points;
+    throw SolverError(WASL_ERR_ARGUMENT, "periodic trace: periodic triangle meshes only");
+  }
+  const SetupTimes &setup_times() const { return setup_; }
+  SetupTimes &setup_times() { return setup_; }
+
   // Kernel accounting for measurement: every launch is counted; while
   // profiling, each stage kernel is bracketed by CUDA events on the stream it
   // is launched on.
@@ -185,6 +214,7 @@ protected:
   void stage_end();
 
   cudaStream_t stream_ = nullptr;
+  SetupTimes setup_;
 
 private:
   bool profiling_ = false;
