@@ -2,12 +2,14 @@
 #include "tri_setup.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <map>
 #include <utility>
 
 #include "../../include/wasl_b200.h"
 #include "basis.hpp"
+#include "parallel.hpp"
 
 namespace wasl_b200 {
 
@@ -99,9 +101,11 @@ namespace {
 // Whether element b's points on local edge jb run opposite to element a's on
 // edge ja (point QF-1-q of b is point q of a); points compared relative to
 // each edge's midpoint, so periodic images match too.  -1: no match.
+constexpr int kMaxEdgePoints = 8; // Gauss points per edge, order <= 7
+
 int point_order(const TriTopology &mesh, const Rule2D &edges, int QF, std::int64_t a, int ja,
                 std::int64_t b, int jb) {
-  std::vector<double> ax(QF), ay(QF), bx(QF), by(QF);
+  double ax[kMaxEdgePoints], ay[kMaxEdgePoints], bx[kMaxEdgePoints], by[kMaxEdgePoints];
   double amx = 0.0, amy = 0.0, bmx = 0.0, bmy = 0.0;
   for (int q = 0; q < QF; ++q) {
     mesh.maps[a].to_physical(edges.xi[ja * QF + q], edges.eta[ja * QF + q], ax[q], ay[q]);
@@ -149,18 +153,32 @@ bool build_patch_edges(const TriTopology &mesh, const TriSlots &t, int boundary,
     for (std::size_t b = 0; b < bface.size(); ++b)
       by_pair[{mesh.face_left[bface[b]], t.donors[b * QF]}].push_back(b);
   }
+  if (QF > kMaxEdgePoints)
+    return false;
+  // Interior faces (each writes only its two sides' slots), on all threads.
+  std::atomic<bool> matched{true};
+  parallel_for(nf, [&](std::int64_t begin, std::int64_t end) {
+    for (std::int64_t f = begin; f < end; ++f) {
+      const std::int32_t L = mesh.face_left[f], R = mesh.face_right[f];
+      if (R < 0)
+        continue;
+      const int jl = mesh.face_left_edge[f], jr = mesh.face_right_edge[f];
+      const int rev = point_order(mesh, edges, QF, L, jl, R, jr);
+      if (rev < 0) {
+        matched = false;
+        return;
+      }
+      set(L, jl, R, 1u | (jr << 1) | (rev << 3), f);
+      set(R, jr, L, (jl << 1) | (rev << 3), f);
+    }
+  });
+  if (!matched)
+    return false;
   for (std::int64_t f = 0, b = 0; f < nf; ++f) {
     const std::int32_t L = mesh.face_left[f], R = mesh.face_right[f];
     const int jl = mesh.face_left_edge[f];
-    if (R >= 0) {
-      const int jr = mesh.face_right_edge[f];
-      const int rev = point_order(mesh, edges, QF, L, jl, R, jr);
-      if (rev < 0)
-        return false;
-      set(L, jl, R, 1u | (jr << 1) | (rev << 3), f);
-      set(R, jr, L, (jl << 1) | (rev << 3), f);
+    if (R >= 0)
       continue;
-    }
     const std::size_t bi = static_cast<std::size_t>(b++);
     if (!periodic) {
       set(L, jl, -1, 1u, f);
