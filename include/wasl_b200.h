@@ -110,6 +110,40 @@ int wasl_gpu_create(const wasl_gpu_config *config, int64_t node_count, const int
                     const double *node_coordinates, int64_t element_count,
                     const int64_t *element_nodes, wasl_gpu **handle, char *error,
                     size_t error_length);
+
+/* wasl_gpu_create on one part of a partitioned periodic triangle mesh (a
+ * rank's owned elements and ghost layers): the periodic faces are given
+ * instead of found by the donor search, since the part's own boundary also
+ * holds the faces where its ghost region ends.  Per boundary face b of the
+ * part's mesh (ascending face index, the faces without a second element) and
+ * edge point q (p + 1 Gauss points): boundary_donors[b][q], the donor element
+ * (an index into the part's elements), and boundary_basis[b][q][mode], the
+ * donor's basis at the point's periodic image (wasl_mesh_periodic_trace of
+ * the whole mesh gives both); donor -1 on every point of a face takes the
+ * face's own element's trace (a cut face, whose neighbours are spoiled by
+ * design).  config->boundary_left must be WASL_PERIODIC; 2D only.  The
+ * reference distributes its meshes with MPI halos instead
+ * (cpp/src/case/scalar_advection_distributed.cpp). */
+int wasl_gpu_create_part(const wasl_gpu_config *config, int64_t node_count,
+                         const int64_t *node_tags, const double *node_coordinates,
+                         int64_t element_count, const int64_t *element_nodes,
+                         int64_t boundary_faces, const int32_t *boundary_donors,
+                         const double *boundary_basis, wasl_gpu **handle, char *error,
+                         size_t error_length);
+
+/* The periodic trace of a whole triangle mesh, without a handle (host
+ * only): for every boundary face b (ascending face index) its element and
+ * local edge (element[b], edge[b], in the normalized mesh: counter-clockwise
+ * elements), and per edge point q the donor element donors[b][q] and the
+ * donor's basis basis[b][q][mode] at the point's periodic image.  Call with
+ * element == NULL to get the boundary face count in *boundary_faces, then
+ * with arrays sized from it.  The reference's
+ * cpp/src/boundaries/periodic_triangle_trace.cpp:40-67. */
+int wasl_mesh_periodic_trace(int64_t node_count, const int64_t *node_tags,
+                             const double *node_coordinates, int64_t element_count,
+                             const int64_t *element_nodes, int polynomial_order,
+                             int64_t *boundary_faces, int32_t *element, int32_t *edge,
+                             int32_t *donors, double *basis, char *error, size_t error_length);
 void wasl_gpu_destroy(wasl_gpu *handle);
 const char *wasl_gpu_last_error(const wasl_gpu *handle);
 
@@ -246,6 +280,46 @@ int wasl_gpu_stencil_transforms(wasl_gpu *handle, double *transforms, int64_t co
  * periodic trace (cpp/src/boundaries/periodic_triangle_trace.cpp:40-67).
  * Periodic triangle meshes only. */
 int wasl_gpu_periodic_trace(wasl_gpu *handle, int32_t *donors, double *basis, int64_t points);
+
+/* ---- halo exchange of a partitioned run (one rank per GPU) ----------------
+ *
+ * A rank holds its part of the mesh (owned elements and ghost layers) on one
+ * handle; per peer rank, the halo schedule lists the owned elements the peer
+ * imports (sends) and the ghosts imported from it (receives), each ascending
+ * (cpp/include/wasl/communication/halo_schedule.hpp:17-42).  The halo packs
+ * a peer's send columns into one [rows][count] device buffer, unpacks a
+ * receive buffer into the ghost columns (rows = variables x modes), and moves
+ * the buffers over NCCL, or leaves them to the caller's transport
+ * (wasl_halo_buffers).  All work runs on the handle's stream.  Element
+ * indices are the handle's (caller's) element indices. */
+typedef struct wasl_halo wasl_halo;
+
+/* peers: count of peer ranks; peer_ranks[k]: the k-th peer's rank;
+ * send_counts[k] / recv_counts[k]: its list lengths; send_elements /
+ * recv_elements: the lists, peer after peer. */
+int wasl_halo_create(wasl_gpu *handle, int peers, const int32_t *peer_ranks,
+                     const int64_t *send_counts, const int64_t *send_elements,
+                     const int64_t *recv_counts, const int64_t *recv_elements, wasl_halo **halo,
+                     char *error, size_t error_length);
+void wasl_halo_destroy(wasl_halo *halo);
+const char *wasl_halo_last_error(const wasl_halo *halo);
+int wasl_halo_pack(wasl_halo *halo);
+int wasl_halo_unpack(wasl_halo *halo);
+/* Peer k's device buffers ([rows][count] doubles), counts and rows. */
+int wasl_halo_buffers(wasl_halo *halo, int peer, double **send, double **recv,
+                      int64_t *send_count, int64_t *recv_count, int64_t *rows);
+/* pack, one NCCL group of a send and a receive per peer (comm: an
+ * ncclComm_t of the run's ranks), unpack; returns when enqueued. */
+int wasl_halo_exchange_nccl(wasl_halo *halo, void *comm);
+/* The whole mesh's CFL step: the handle's CFL parts all-reduced (largest
+ * speed, smallest length) over comm, then stable_dt's formula (2D Euler). */
+int wasl_gpu_stable_dt_nccl(wasl_gpu *handle, void *comm, double cfl, double *dt);
+/* NCCL communicators for callers without their own: an id made on one rank
+ * and shared with the others, then one communicator per rank. */
+int wasl_nccl_unique_id(uint8_t *id /* 128 bytes */);
+int wasl_nccl_comm_create(int ranks, const uint8_t *id, int rank, int device, void **comm,
+                          char *error, size_t error_length);
+void wasl_nccl_comm_destroy(void *comm);
 
 /* Device pointer of the state U[variable][mode][element] and the handle's
  * CUDA stream (cudaStream_t), for callers that keep data on the device. */

@@ -112,6 +112,91 @@ def test_split_reproduces_the_serial_step(oracle, p, limiting, ranks):
     assert flagged > 0 or not limiting
 
 
+def dense_part_trace(oracle, om, part, p):
+    """A part's boundary (LocalMesh.part_boundary) as the oracle's per-face
+    periodic trace: owner faces (donor -1) take the face's own element and its
+    basis at its edge points; the stencil's donors keep -1 there."""
+    Q, M = p + 1, (p + 1) * (p + 2) // 2
+    donors = np.full(om.nf * Q, -1, dtype=np.int32)
+    stencil_donors = donors.copy()
+    basis = np.zeros(om.nf * Q * M)
+    faces = np.flatnonzero(om.face_right < 0)
+    part_donors, part_basis = part
+    assert len(faces) == len(part_donors)
+    xi, eta = oracle.tri_edge_rules(p)[:2]
+    for b, f in enumerate(faces):
+        rows = slice(f * Q, (f + 1) * Q)
+        if part_donors[b, 0] < 0:
+            le = om.face_left_edge[f]
+            donors[rows] = om.face_left[f]
+            for q in range(Q):
+                basis[(f * Q + q) * M:(f * Q + q + 1) * M] = oracle.dubiner(
+                    xi[le * Q + q], eta[le * Q + q], p)
+        else:
+            donors[rows] = stencil_donors[rows] = part_donors[b]
+            basis[f * Q * M:(f + 1) * Q * M] = part_basis[b].ravel()
+    return donors, basis, stencil_donors
+
+
+@pytest.mark.parametrize("p", [1, 2])
+@pytest.mark.parametrize("limiting", [False, True])
+@pytest.mark.parametrize("ranks", [2, 3])
+def test_periodic_split_reproduces_the_serial_step(oracle, p, limiting, ranks):
+    """A periodic mesh split over ranks: ghost layers across the periodic
+    seams and each part's boundary from the whole mesh's periodic trace
+    (halo.periodic_pairs, from the library's host setup); every rank steps its
+    part with the oracle's SSP-RK3 step on that boundary, one in-process
+    exchange per step, and every owned element equals the serial periodic run
+    bit for bit."""
+    tags, xy, tris = meshgen.jittered_box(12, jitter=0.15, seed=40 + p, ny=10)
+    ne = len(tris)
+    serial = oracle.tri_mesh(tags, xy, tris)
+    gd, gb = serial.periodic_trace(p)
+    st_serial = serial.stencil(p, gd) if limiting else None
+    c = seeded_state(ne, p, 9 + p, amplitude=0.02 if limiting else 0.005)
+    M = (p + 1) * (p + 2) // 2
+    pairs = halo.periodic_pairs(tags, xy, tris, p)
+    depth = halo.halo_depth(limiting)
+    meshes = [halo.local_mesh(tags, xy, tris, r, ranks, depth, pairs=pairs)
+              for r in range(ranks)]
+    schedules = [halo.build_halo_schedule(meshes, ranks, ne, r) for r in range(ranks)]
+    locals_ = [oracle.tri_mesh(*m.arrays) for m in meshes]
+    traces = [dense_part_trace(oracle, lm, m.part_boundary, p)
+              for lm, m in zip(locals_, meshes)]
+    stencils = [lm.stencil(p, t[2]) if limiting else None for lm, t in zip(locals_, traces)]
+    states = [np.ascontiguousarray(c.reshape(4 * M, ne)[:, m.elements]) for m in meshes]
+    assert any(np.any(m.part_boundary[0][:, 0] >= 0) for m in meshes)  # seams inside parts
+    for _ in range(4):
+        dt = serial.cfl(GAMMA, c, p, 0.1)
+        flags = serial.euler_step(GAMMA, p, dt, c, donors=gd, basis=gb, stencil=st_serial,
+                                  return_flags=True)
+        for r, m in enumerate(meshes):
+            u = states[r].ravel()
+            lf = locals_[r].euler_step(GAMMA, p, dt, u, donors=traces[r][0],
+                                       basis=traces[r][1], stencil=stencils[r],
+                                       return_flags=True)
+            states[r] = u.reshape(4 * M, -1)
+            assert np.array_equal(lf[:, m.owned], flags[:, m.elements[m.owned]])
+        halo.exchange_in_process(states, meshes, schedules)
+        full = c.reshape(4 * M, ne)
+        for r, m in enumerate(meshes):
+            assert np.array_equal(states[r], full[:, m.elements]), f"rank {r}"
+
+
+def test_periodic_pairs_are_the_oracle_trace(oracle):
+    tags, xy, tris = meshgen.jittered_box(9, jitter=0.15, seed=5, ny=6)
+    om = oracle.tri_mesh(tags, xy, tris)
+    for p in (0, 1, 2, 3):
+        pairs = halo.periodic_pairs(tags, xy, tris, p)
+        Q, M = p + 1, (p + 1) * (p + 2) // 2
+        donors, basis = om.periodic_trace(p)
+        faces = np.flatnonzero(om.face_right < 0)
+        assert np.array_equal(pairs.element, om.face_left[faces])
+        assert np.array_equal(pairs.edge, om.face_left_edge[faces])
+        assert np.array_equal(pairs.donors, donors.reshape(om.nf, Q)[faces])
+        assert np.array_equal(pairs.basis, basis.reshape(om.nf, Q, M)[faces])
+
+
 def free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
@@ -171,16 +256,21 @@ def test_two_gloo_ranks_exchange_ghost_rows():
     assert results[0][1] == results[1][1] == halo.dt_from_parts(0.1, 3.0, 0.25, 2)
 
 
-def test_partitioned_runs_refuse_periodic_handles():
-    """A rank's handle with periodic boundaries would pair its cut faces
-    across the period; the partitioned step refuses it up front."""
+def test_partitioned_runs_refuse_periodic_handles_without_a_part_boundary():
+    """A rank's periodic handle built by its own donor search would pair its
+    cut faces across the period; the partitioned step refuses it up front,
+    and accepts a handle built on its part's boundary."""
     class Config:
         boundary_left = 0  # periodic
 
     class Handle:
         config = Config()
+        part = False
 
     with pytest.raises(ValueError, match="periodic"):
         halo.check_partitioned_solver(Handle())
+    Handle.part = True
+    halo.check_partitioned_solver(Handle())
+    Handle.part = False
     Handle.config.boundary_left = 3  # transmissive
     halo.check_partitioned_solver(Handle())

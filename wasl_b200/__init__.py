@@ -78,7 +78,27 @@ SIGNATURES = {
     "wasl_gpu_config_default": (None, [C.POINTER(Config)]),
     "wasl_gpu_create": (C.c_int, [C.POINTER(Config), C.c_int64, _i64, _d, C.c_int64, _i64,
                                   C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
+    "wasl_gpu_create_part": (C.c_int, [C.POINTER(Config), C.c_int64, _i64, _d, C.c_int64, _i64,
+                                       C.c_int64, C.POINTER(C.c_int32), _d,
+                                       C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
+    "wasl_mesh_periodic_trace": (C.c_int, [C.c_int64, _i64, _d, C.c_int64, _i64, C.c_int, _i64,
+                                           C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                           C.POINTER(C.c_int32), _d, C.c_char_p, C.c_size_t]),
     "wasl_gpu_form_supported": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int]),
+    "wasl_halo_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int32), _i64, _i64, _i64,
+                                   _i64, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
+    "wasl_halo_destroy": (None, [C.c_void_p]),
+    "wasl_halo_last_error": (C.c_char_p, [C.c_void_p]),
+    "wasl_halo_pack": (C.c_int, [C.c_void_p]),
+    "wasl_halo_unpack": (C.c_int, [C.c_void_p]),
+    "wasl_halo_buffers": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p),
+                                    C.POINTER(C.c_void_p), _i64, _i64, _i64]),
+    "wasl_halo_exchange_nccl": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "wasl_gpu_stable_dt_nccl": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, _d]),
+    "wasl_nccl_unique_id": (C.c_int, [C.POINTER(C.c_uint8)]),
+    "wasl_nccl_comm_create": (C.c_int, [C.c_int, C.POINTER(C.c_uint8), C.c_int, C.c_int,
+                                        C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
+    "wasl_nccl_comm_destroy": (None, [C.c_void_p]),
     "wasl_gpu_destroy": (None, [C.c_void_p]),
     "wasl_gpu_last_error": (C.c_char_p, [C.c_void_p]),
     "wasl_gpu_sizes": (C.c_int, [C.c_void_p, _i64, _i64, C.POINTER(C.c_int),
@@ -193,6 +213,38 @@ def default_config() -> Config:
     return cfg
 
 
+def mesh_periodic_trace(node_tags, node_coordinates, element_nodes, polynomial_order):
+    """The periodic trace of a whole triangle mesh (wasl_mesh_periodic_trace):
+    (element [b], edge [b], donors [b][p+1], basis [b][p+1][modes]) for every
+    boundary face b in ascending face order; edges are local edge indices of
+    the counter-clockwise normalized element."""
+    lib = library()
+    tags = np.ascontiguousarray(node_tags, dtype=np.int64)
+    coords = np.ascontiguousarray(node_coordinates, dtype=np.float64)
+    elems = np.ascontiguousarray(element_nodes, dtype=np.int64)
+    err = C.create_string_buffer(1024)
+    count = C.c_int64()
+    i32 = C.POINTER(C.c_int32)
+    args = (len(tags), _ptr(tags, _i64), _ptr(coords), len(elems), _ptr(elems, _i64),
+            polynomial_order)
+    rc = lib.wasl_mesh_periodic_trace(*args, C.byref(count), None, None, None, None, err,
+                                      len(err))
+    if rc != 0:
+        raise WaslError(rc, err.value.decode())
+    b, Q = count.value, polynomial_order + 1
+    M = (polynomial_order + 1) * (polynomial_order + 2) // 2
+    element = np.empty(b, dtype=np.int32)
+    edge = np.empty(b, dtype=np.int32)
+    donors = np.empty((b, Q), dtype=np.int32)
+    basis = np.empty((b, Q, M))
+    rc = lib.wasl_mesh_periodic_trace(*args, C.byref(count), element.ctypes.data_as(i32),
+                                      edge.ctypes.data_as(i32), donors.ctypes.data_as(i32),
+                                      _ptr(basis), err, len(err))
+    if rc != 0:
+        raise WaslError(rc, err.value.decode())
+    return element, edge, donors, basis
+
+
 class Solver:
     """One mesh, one equation, one polynomial order, state resident on the GPU."""
 
@@ -201,7 +253,10 @@ class Solver:
                  boundary="periodic", boundary_right=None, inflow=(0.0, 0.0), limiting=False,
                  sensor_threshold=1e-3, density_floor=1e-10, pressure_floor=1e-10,
                  precision="plain", device=0, volume_rule_order=0, mixed_kernel=0,
-                 positivity_all=False, element_order="curve"):
+                 positivity_all=False, element_order="curve", part_boundary=None):
+        """part_boundary: (donors [b][p+1] int32, basis [b][p+1][modes]) for a
+        part of a partitioned periodic mesh (wasl_gpu_create_part;
+        halo.LocalMesh.part_boundary), None for a whole mesh."""
         lib = library()
         cfg = default_config()
         cfg.dimensions = dimensions
@@ -228,8 +283,18 @@ class Solver:
         elems = np.ascontiguousarray(element_nodes, dtype=np.int64)
         err = C.create_string_buffer(1024)
         h = C.c_void_p()
-        rc = lib.wasl_gpu_create(C.byref(cfg), len(tags), _ptr(tags, _i64), _ptr(coords),
-                                 len(elems), _ptr(elems, _i64), C.byref(h), err, len(err))
+        if part_boundary is None:
+            rc = lib.wasl_gpu_create(C.byref(cfg), len(tags), _ptr(tags, _i64), _ptr(coords),
+                                     len(elems), _ptr(elems, _i64), C.byref(h), err, len(err))
+        else:
+            donors = np.ascontiguousarray(part_boundary[0], dtype=np.int32)
+            basis = np.ascontiguousarray(part_boundary[1], dtype=np.float64)
+            rc = lib.wasl_gpu_create_part(
+                C.byref(cfg), len(tags), _ptr(tags, _i64), _ptr(coords), len(elems),
+                _ptr(elems, _i64), donors.shape[0] if donors.ndim else 0,
+                donors.ctypes.data_as(C.POINTER(C.c_int32)), _ptr(basis), C.byref(h), err,
+                len(err))
+        self.part = part_boundary is not None
         if rc != 0:
             raise WaslError(rc, err.value.decode())
         self._lib, self._h = lib, h

@@ -56,6 +56,7 @@ SOURCES = {
     "mlp.cu": [],
     "mlp_trainer.cpp": [],
     "setup_device.cu": ["--fmad=false"],
+    "halo.cu": [],
 }
 HEADERS = [f for f in os.listdir(CSRC) if f.endswith((".hpp", ".cuh", ".h"))]
 
@@ -89,7 +90,7 @@ def build(clean: bool = False, verbose: bool = False, checked: bool = False) -> 
         objs = [f.result() for f in futures]
     if (not os.path.exists(lib) or
             max(os.path.getmtime(o) for o in objs) > os.path.getmtime(lib)):
-        subprocess.run([NVCC, *ARCH, "-shared", "-o", lib, *objs], check=True)
+        subprocess.run([NVCC, *ARCH, "-shared", "-o", lib, *objs, "-ldl"], check=True)
     if verbose:
         print(lib)
     return lib

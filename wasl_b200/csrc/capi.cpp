@@ -1,4 +1,5 @@
 // extern "C" entry points of libwasl_b200.so (declared in include/wasl_b200.h).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -10,8 +11,10 @@
 #include "solver.hpp"
 
 namespace wasl_b200 {
-std::unique_ptr<Solver> make_euler_tri_solver(const wasl_gpu_config &cfg, TriTopology &&topo);
-std::unique_ptr<Solver> make_scalar_tri_solver(const wasl_gpu_config &cfg, TriTopology &&topo);
+std::unique_ptr<Solver> make_euler_tri_solver(const wasl_gpu_config &cfg, TriTopology &&topo,
+                                              const PartBoundary *part);
+std::unique_ptr<Solver> make_scalar_tri_solver(const wasl_gpu_config &cfg, TriTopology &&topo,
+                                               const PartBoundary *part);
 std::unique_ptr<Solver> make_line_solver(const wasl_gpu_config &cfg, LineTopology &&topo);
 
 bool form_supported(int precision, int dimensions, int equation, int p) {
@@ -29,7 +32,8 @@ bool form_supported(int precision, int dimensions, int equation, int p) {
 
 std::unique_ptr<Solver> make_solver(const wasl_gpu_config &cfg, std::int64_t node_count,
                                     const std::int64_t *node_tags, const double *coordinates,
-                                    std::int64_t element_count, const std::int64_t *element_nodes) {
+                                    std::int64_t element_count, const std::int64_t *element_nodes,
+                                    const PartBoundary *part) {
   if (!form_supported(cfg.precision, cfg.dimensions, cfg.equation, cfg.polynomial_order))
     throw SolverError(WASL_ERR_ARGUMENT,
                       "unsupported combination of dimension, equation, order and precision");
@@ -40,9 +44,11 @@ std::unique_ptr<Solver> make_solver(const wasl_gpu_config &cfg, std::int64_t nod
     TriTopology topo =
         build_triangle_topology(node_count, node_tags, coordinates, element_count, element_nodes);
     topology.lap(WASL_SETUP_TOPOLOGY);
-    solver = cfg.equation == WASL_EULER ? make_euler_tri_solver(cfg, std::move(topo))
-                                        : make_scalar_tri_solver(cfg, std::move(topo));
+    solver = cfg.equation == WASL_EULER ? make_euler_tri_solver(cfg, std::move(topo), part)
+                                        : make_scalar_tri_solver(cfg, std::move(topo), part);
   } else {
+    if (part)
+      throw SolverError(WASL_ERR_ARGUMENT, "partition boundary: triangle meshes only");
     LineTopology topo =
         build_line_topology(node_count, node_tags, coordinates, element_count, element_nodes);
     topology.lap(WASL_SETUP_TOPOLOGY);
@@ -57,6 +63,15 @@ struct wasl_gpu {
   std::unique_ptr<wasl_b200::Solver> solver;
   std::string error;
 };
+
+namespace wasl_b200 {
+// For the other C entry points built on a handle (halo.cu).
+Solver *solver_of(wasl_gpu *handle) { return handle ? handle->solver.get() : nullptr; }
+void set_handle_error(wasl_gpu *handle, const std::string &message) {
+  if (handle)
+    handle->error = message;
+}
+} // namespace wasl_b200
 
 namespace {
 
@@ -82,6 +97,13 @@ template <typename F> int guarded(wasl_gpu *h, F &&body) {
 void need(bool ok, const char *message) {
   if (!ok)
     throw wasl_b200::SolverError(WASL_ERR_ARGUMENT, message);
+}
+
+void copy_message(const std::string &message, char *error, size_t error_length) {
+  if (error && error_length) {
+    std::strncpy(error, message.c_str(), error_length - 1);
+    error[error_length - 1] = '\0';
+  }
 }
 
 // Checkpoint container: magic, format version 2, then the reference fields in
@@ -120,10 +142,12 @@ int wasl_gpu_form_supported(int precision, int dimensions, int equation, int p) 
   return wasl_b200::form_supported(precision, dimensions, equation, p) ? 1 : 0;
 }
 
-int wasl_gpu_create(const wasl_gpu_config *config, int64_t node_count, const int64_t *node_tags,
-                    const double *node_coordinates, int64_t element_count,
-                    const int64_t *element_nodes, wasl_gpu **handle, char *error,
-                    size_t error_length) {
+namespace {
+
+int create_handle(const wasl_gpu_config *config, int64_t node_count, const int64_t *node_tags,
+                  const double *node_coordinates, int64_t element_count,
+                  const int64_t *element_nodes, const wasl_b200::PartBoundary *part,
+                  wasl_gpu **handle, char *error, size_t error_length) {
   if (!handle || !config)
     return WASL_ERR_ARGUMENT;
   *handle = nullptr;
@@ -134,17 +158,83 @@ int wasl_gpu_create(const wasl_gpu_config *config, int64_t node_count, const int
     need(config->density_floor >= 0.0 && config->pressure_floor >= 0.0,
          "Euler positivity limiter: invalid modes or floors");
     h->solver = wasl_b200::make_solver(*config, node_count, node_tags, node_coordinates,
-                                       element_count, element_nodes);
+                                       element_count, element_nodes, part);
   });
   if (rc != WASL_OK) {
-    if (error && error_length) {
-      std::strncpy(error, h->error.c_str(), error_length - 1);
-      error[error_length - 1] = '\0';
-    }
+    copy_message(h->error, error, error_length);
     return rc;
   }
   *handle = h.release();
   return WASL_OK;
+}
+
+} // namespace
+
+int wasl_gpu_create(const wasl_gpu_config *config, int64_t node_count, const int64_t *node_tags,
+                    const double *node_coordinates, int64_t element_count,
+                    const int64_t *element_nodes, wasl_gpu **handle, char *error,
+                    size_t error_length) {
+  return create_handle(config, node_count, node_tags, node_coordinates, element_count,
+                       element_nodes, nullptr, handle, error, error_length);
+}
+
+int wasl_gpu_create_part(const wasl_gpu_config *config, int64_t node_count,
+                         const int64_t *node_tags, const double *node_coordinates,
+                         int64_t element_count, const int64_t *element_nodes,
+                         int64_t boundary_faces, const int32_t *boundary_donors,
+                         const double *boundary_basis, wasl_gpu **handle, char *error,
+                         size_t error_length) {
+  wasl_b200::PartBoundary part;
+  part.faces = boundary_faces;
+  part.donors = boundary_donors;
+  part.basis = boundary_basis;
+  return create_handle(config, node_count, node_tags, node_coordinates, element_count,
+                       element_nodes, &part, handle, error, error_length);
+}
+
+int wasl_mesh_periodic_trace(int64_t node_count, const int64_t *node_tags,
+                             const double *node_coordinates, int64_t element_count,
+                             const int64_t *element_nodes, int polynomial_order,
+                             int64_t *boundary_faces, int32_t *element, int32_t *edge,
+                             int32_t *donors, double *basis, char *error, size_t error_length) {
+  std::string message;
+  int status = WASL_OK;
+  try {
+    need(boundary_faces != nullptr, "null pointer");
+    need(node_count > 0 && element_count > 0, "mesh: empty node or element list");
+    need(node_tags && node_coordinates && element_nodes, "mesh: null array");
+    need(polynomial_order >= 0 && polynomial_order <= 3,
+         "periodic trace: polynomial order must be 0..3");
+    const wasl_b200::TriTopology mesh = wasl_b200::build_triangle_topology(
+        node_count, node_tags, node_coordinates, element_count, element_nodes);
+    std::int64_t faces = 0;
+    for (std::int64_t f = 0; f < mesh.face_count(); ++f)
+      faces += mesh.face_right[f] < 0;
+    if (!element) { // size query
+      *boundary_faces = faces;
+    } else {
+      need(*boundary_faces == faces, "periodic trace: boundary face count mismatch");
+      need(edge && donors && basis, "null pointer");
+      const wasl_b200::PeriodicTrace trace = wasl_b200::periodic_trace(mesh, polynomial_order);
+      for (std::int64_t f = 0, b = 0; f < mesh.face_count(); ++f)
+        if (mesh.face_right[f] < 0) {
+          element[b] = mesh.face_left[f];
+          edge[b] = mesh.face_left_edge[f];
+          ++b;
+        }
+      std::copy(trace.donors.begin(), trace.donors.end(), donors);
+      std::copy(trace.basis.begin(), trace.basis.end(), basis);
+    }
+  } catch (const wasl_b200::SolverError &e) {
+    message = e.what(), status = e.status;
+  } catch (const std::invalid_argument &e) {
+    message = e.what(), status = WASL_ERR_ARGUMENT;
+  } catch (const std::exception &e) {
+    message = e.what(), status = WASL_ERR_RUNTIME;
+  }
+  if (status != WASL_OK)
+    copy_message(message, error, error_length);
+  return status;
 }
 
 void wasl_gpu_destroy(wasl_gpu *h) { delete h; }

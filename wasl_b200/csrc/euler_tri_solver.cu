@@ -83,7 +83,7 @@ __global__ void scatter_columns(const double *__restrict__ src, double *__restri
 
 class EulerTriSolver final : public Solver {
 public:
-  EulerTriSolver(const wasl_gpu_config &cfg, TriTopology &&topo)
+  EulerTriSolver(const wasl_gpu_config &cfg, TriTopology &&topo, const PartBoundary *part)
       : cfg_(cfg), mesh_(std::move(topo)), p_(cfg.polynomial_order),
         M_(tri_modes(cfg.polynomial_order)) {
     if (!euler_tri_order_supported(p_))
@@ -123,12 +123,19 @@ public:
     // The element maps on the device, for the donor search and the limiter
     // stencil's transforms (freed when setup ends).
     DeviceArray<double> d_maps;
-    const bool periodic_search = has_boundary && boundary_ == WASL_PERIODIC;
+    if (part && boundary_ != WASL_PERIODIC)
+      throw SolverError(WASL_ERR_ARGUMENT, "partition boundary: the handle must be periodic");
+    const bool periodic_search = has_boundary && boundary_ == WASL_PERIODIC && !part;
     if (periodic_search || (cfg.limiting && p_ > 0))
       upload_maps(mesh_, d_maps, stream_);
     PeriodicTrace trace;
-    if (periodic_search)
+    std::vector<std::int32_t> stencil_donors;
+    if (periodic_search) {
       trace = periodic_trace_device(mesh_, p_, d_maps.get(), stream_);
+      stencil_donors = trace.donors;
+    } else if (part) {
+      trace = part_trace(mesh_, p_, *part, stencil_donors);
+    }
     setup_.lap(WASL_SETUP_PERIODIC);
 
     TriSlots t = build_tri_slots(mesh_, boundary_ == WASL_PERIODIC && has_boundary ? &trace : nullptr,
@@ -209,7 +216,7 @@ public:
 
     limiting_ = cfg.limiting && p_ > 0;
     if (limiting_) {
-      stencil_ = triangle_stencil(mesh_, p_, trace.donors, /*transforms=*/false);
+      stencil_ = triangle_stencil(mesh_, p_, stencil_donors, /*transforms=*/false);
       d_neighbors_.upload(blocks(ids(stencil_.neighbors), 3), stream_);
       d_transforms_.resize(static_cast<std::size_t>(ne_) * 3 * M_ * M_);
       stencil_transforms_device(mesh_, p_, stencil_.neighbors, order_, d_maps.get(),
@@ -363,6 +370,10 @@ public:
   double stable_dt(double cfl) override {
     double speed = 0.0, length = 0.0;
     cfl_parts(speed, length);
+    return dt_from_parts(cfl, speed, length);
+  }
+
+  double dt_from_parts(double cfl, double speed, double length) const override {
     return speed > 0.0 ? cfl * length / (speed * (2 * p_ + 1)) : 0.0;
   }
 
@@ -455,6 +466,7 @@ public:
     if (!(lo <= hi))
       throw SolverError(WASL_ERR_ARGUMENT, "learned indicator: need lo <= hi");
     d_mlp_.upload(std::vector<float>(weights, weights + count), stream_);
+    d_mlp_records_.resize(kMlpRecordBytes * ne_);
     d_mlp_stats_.resize(6);
     cuda_check(cudaMemsetAsync(d_mlp_stats_.get(), 0, 6 * sizeof(unsigned long long), stream_),
                "stats");
@@ -512,6 +524,7 @@ public:
     m.troubled = list.get();
     m.troubled_count = list.get() + ne_;
     m.logits = z.get();
+    m.records = d_mlp_records_.get();
     launch_mlp_indicator(m, stream_);
     std::vector<float> zs(relabel_ ? ne_ : 0);
     cuda_check(cudaMemcpyAsync(relabel_ ? zs.data() : logits, z.get(), sizeof(float) * ne_,
@@ -656,8 +669,9 @@ private:
         m.troubled = d_troubled_.get();
         m.troubled_count = d_count_.get();
         m.stats = d_mlp_stats_.get();
+        m.records = d_mlp_records_.get();
         launch_mlp_indicator(m, stream_);
-        count_launches(1);
+        count_launches(2);
       }
       if (limiting_) {
         launch_limit_f64(M_, 3, limit_args(outs[k], d_flags_.get() + k * ne_), stream_);
@@ -815,6 +829,7 @@ private:
   DeviceArray<float> d_mlp_; // learned indicator weights (empty: the reference sensor)
   DeviceArray<double> d_check_bound_;
   DeviceArray<unsigned long long> d_mlp_stats_;
+  DeviceArray<unsigned char> d_mlp_records_; // per-element inference records
   double mlp_lo_ = 0.1, mlp_hi_ = 0.9;
   DeviceArray<std::uint8_t> d_tile_code_;
   DeviceArray<float> d_basis32_;
@@ -835,8 +850,9 @@ private:
   DeviceArray<unsigned long long> d_error_, d_cfl_;
 };
 
-std::unique_ptr<Solver> make_euler_tri_solver(const wasl_gpu_config &cfg, TriTopology &&topo) {
-  return std::make_unique<EulerTriSolver>(cfg, std::move(topo));
+std::unique_ptr<Solver> make_euler_tri_solver(const wasl_gpu_config &cfg, TriTopology &&topo,
+                                              const PartBoundary *part) {
+  return std::make_unique<EulerTriSolver>(cfg, std::move(topo), part);
 }
 
 } // namespace wasl_b200

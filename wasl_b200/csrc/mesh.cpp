@@ -426,6 +426,46 @@ PeriodicTrace periodic_trace_from_donors(const TriTopology &mesh, int p,
   return trace;
 }
 
+PeriodicTrace part_trace(const TriTopology &mesh, int p, const PartBoundary &part,
+                         std::vector<std::int32_t> &stencil_donors) {
+  const int Q = p + 1, M = tri_modes(p);
+  const Rule2D edges = triangle_edges(p);
+  std::int64_t faces = 0;
+  for (std::int64_t f = 0; f < mesh.face_count(); ++f)
+    faces += mesh.face_right[f] < 0;
+  if (part.faces != faces)
+    throw std::invalid_argument("partition boundary: " + std::to_string(part.faces) +
+                                " faces given, the part's mesh has " + std::to_string(faces));
+  if (faces > 0 && (!part.donors || !part.basis))
+    throw std::invalid_argument("partition boundary: null donors or basis");
+  PeriodicTrace trace;
+  trace.donors.resize(static_cast<std::size_t>(faces) * Q);
+  trace.basis.resize(static_cast<std::size_t>(faces) * Q * M);
+  stencil_donors.assign(part.donors, part.donors + faces * Q);
+  for (std::int64_t f = 0, b = 0; f < mesh.face_count(); ++f) {
+    if (mesh.face_right[f] >= 0)
+      continue;
+    const bool own = part.donors[b * Q] == -1;
+    for (int q = 0; q < Q; ++q) {
+      const std::int32_t d = part.donors[b * Q + q];
+      if (own ? d != -1 : (d < 0 || d >= mesh.element_count))
+        throw std::invalid_argument("partition boundary: face " + std::to_string(b) +
+                                    " has a donor outside the part or mixes owner points");
+      std::vector<double> basis;
+      if (own) {
+        const int le = mesh.face_left_edge[f];
+        basis = dubiner(edges.xi[le * Q + q], edges.eta[le * Q + q], p);
+      } else {
+        basis.assign(part.basis + (b * Q + q) * M, part.basis + (b * Q + q + 1) * M);
+      }
+      trace.donors[b * Q + q] = own ? mesh.face_left[f] : d;
+      std::copy(basis.begin(), basis.end(), trace.basis.begin() + (b * Q + q) * M);
+    }
+    ++b;
+  }
+  return trace;
+}
+
 PeriodicTrace periodic_trace(const TriTopology &mesh, int p) {
   const PeriodicImages images = periodic_images(mesh, p);
   const std::int64_t n = static_cast<std::int64_t>(images.x.size());

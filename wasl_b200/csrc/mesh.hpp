@@ -80,6 +80,26 @@ struct PeriodicTrace {
 };
 PeriodicTrace periodic_trace(const TriTopology &mesh, int p);
 
+// The boundary of one part of a partitioned periodic mesh, given by the
+// caller instead of found by the donor search: per boundary face b of the
+// part's mesh (ascending face index) and edge point q, the donor element
+// (an index into the part's elements) and the donor's basis at the point's
+// periodic image, donors [b][q], basis [b][q][mode]; donor -1 on every point
+// of a face marks a face where the part's ghost region ends, whose exterior
+// is its own element's trace.
+struct PartBoundary {
+  std::int64_t faces = 0;
+  const std::int32_t *donors = nullptr;
+  const double *basis = nullptr;
+};
+
+// The periodic trace of a part (owner faces filled with the owner and its
+// own basis at its edge points); stencil_donors: the donors with -1 kept on
+// owner faces, for triangle_stencil.  Throws std::invalid_argument when the
+// boundary does not fit the mesh.
+PeriodicTrace part_trace(const TriTopology &mesh, int p, const PartBoundary &part,
+                         std::vector<std::int32_t> &stencil_donors);
+
 // The mesh's bounding box.
 struct Box {
   double min_x, max_x, min_y, max_y;

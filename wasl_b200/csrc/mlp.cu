@@ -16,6 +16,7 @@
 // the tensor cores (mma.sync m16n8k16 BF16, FP32 accumulate).
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <stdexcept>
 #include <string>
 
@@ -53,7 +54,7 @@ __device__ __forceinline__ void mlp_features_of(const double *state, std::int64_
     const double ninv = n0 != 0.0 ? 1.0 / n0 : 0.0;
     for (int m = 1; m < M; ++m)
       x[(j + 1) * (M - 1) + m - 1] = clamp8(static_cast<float>(state[m * ne + nb] * ninv));
-    x[4 * (M - 1) + j] = clamp8(static_cast<float>(n0 * inv - 1.0));
+    x[4 * (M - 1) + j] = clamp8(static_cast<float>(__dadd_rn(__dmul_rn(n0, inv), -1.0)));
   }
 }
 
@@ -254,16 +255,47 @@ __device__ __forceinline__ void mma_bf16(float *d, const unsigned *a, const unsi
 
 } // namespace
 
-// One CTA of 128 threads: 128 elements.  Each thread builds its element's
-// features (BF16 rows in shared memory) and its reference decision; each
-// warp then runs its 32 rows through the network as two 16-row tiles of
-// m16n8k16 MMAs (the first layer's accumulators become the second layer's A
-// fragments in registers), and the last layer as a quad reduction.  A cell is
-// troubled when sigmoid(logit) >= hi, smooth when <= lo, and otherwise takes
-// the reference decision.  Flags and the compacted troubled list as the
-// sensor writes them; counters: [0] network troubled, [1] network smooth,
-// [2] fallback, [3] reference troubled, [4] missed (reference troubled,
-// decided smooth), [5] false (reference smooth, decided troubled).
+// Per element, the part of the features and of the reference decision that
+// depends on it alone, packed into 32 bytes: its density mean (FP64), its
+// density modes m >= 1 over the mean (clamped to [-8, 8], BF16: the values
+// the network's input rows hold), and the reference modal-decay decision.
+// The inference kernel builds each element's input row from its own record
+// and its three neighbours' (one 32-byte read each) instead of gathering
+// 4 M scattered FP64 modes.
+struct __align__(16) IndicatorRecord {
+  double mean;
+  __nv_bfloat16 high[kMlpMaxModes - 1];
+  unsigned char reference;
+  unsigned char pad[32 - 8 - 2 * (kMlpMaxModes - 1) - 1];
+};
+static_assert(sizeof(IndicatorRecord) == 32, "indicator record is 32 bytes");
+
+__global__ void __launch_bounds__(128) mlp_records_kernel(const MlpIndicatorArgs a) {
+  const std::int64_t e = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= a.ne)
+    return;
+  IndicatorRecord r{};
+  const double c0 = a.state[e];
+  const double inv = c0 != 0.0 ? 1.0 / c0 : 0.0;
+  r.mean = c0;
+  for (int m = 1; m < a.M; ++m)
+    r.high[m - 1] = __float2bfloat16_rn(clamp8(static_cast<float>(a.state[m * a.ne + e] * inv)));
+  r.reference = reference_troubled(a.state, a.ne, a.M, e, a.threshold, a.highest_degree_begin);
+  reinterpret_cast<IndicatorRecord *>(a.records)[e] = r;
+}
+
+// A persistent kernel: each CTA of 128 threads loads the network once (BF16
+// in shared memory) and then takes 128-element tiles in turn.  Per tile, each
+// thread builds its element's input row (BF16, shared memory) from the
+// element's and its neighbours' records; each warp runs its 32 rows through
+// the network as two 16-row tiles of m16n8k16 MMAs (the first layer's
+// accumulators become the second layer's A fragments in registers), and the
+// last layer as a quad reduction.  A cell is troubled when sigmoid(logit) >=
+// hi, smooth when <= lo, and otherwise takes the reference decision.  Flags
+// and the compacted troubled list as the sensor writes them; counters: [0]
+// network troubled, [1] network smooth, [2] fallback, [3] reference
+// troubled, [4] missed (reference troubled, decided smooth), [5] false
+// (reference smooth, decided troubled).
 template <int KF>
 __global__ void __launch_bounds__(128) mlp_indicator_kernel(const MlpIndicatorArgs a) {
   constexpr int Hd = kMlpHidden, F = KF * 16, ROW = F + 8; // +8: fewer bank conflicts
@@ -285,121 +317,140 @@ __global__ void __launch_bounds__(128) mlp_indicator_kernel(const MlpIndicatorAr
   }
   if (t < 6)
     counts[t] = 0;
-  const std::int64_t e = static_cast<std::int64_t>(blockIdx.x) * 128 + t;
-  const bool active = e < a.ne;
-  bool reference = false;
-  {
-    float x[F];
-    if (active) {
-      mlp_features_of(a.state, a.ne, a.M, a.neighbors, e, F, x);
-      reference = reference_troubled(a.state, a.ne, a.M, e, a.threshold, a.highest_degree_begin);
-    } else {
-      for (int i = 0; i < F; ++i)
-        x[i] = 0.0f;
-    }
-    for (int i = 0; i < F; ++i)
-      X[t * ROW + i] = __float2bfloat16_rn(x[i]);
-  }
-  __syncthreads();
-
+  const float b3 = P[a.shape.b3];
+  const IndicatorRecord *records = reinterpret_cast<const IndicatorRecord *>(a.records);
+  const int H = a.M - 1;
   const int warp = t >> 5, lane = t & 31, g = lane >> 2, q = lane & 3;
-  for (int mt = 0; mt < 2; ++mt) {
-    const int row0 = warp * 32 + mt * 16;
-    // Layer 1: 16 rows x 64 outputs, K = F.
-    float h[8][4];
-    for (int nt = 0; nt < 8; ++nt) {
-      const int c = nt * 8 + 2 * q;
-      h[nt][0] = h[nt][2] = b1[c];
-      h[nt][1] = h[nt][3] = b1[c + 1];
-    }
-    for (int kk = 0; kk < KF; ++kk) {
-      unsigned af[4];
-      const __nv_bfloat16 *r0 = X + (row0 + g) * ROW + kk * 16 + 2 * q;
-      const __nv_bfloat16 *r8 = X + (row0 + g + 8) * ROW + kk * 16 + 2 * q;
-      af[0] = *reinterpret_cast<const unsigned *>(r0);
-      af[1] = *reinterpret_cast<const unsigned *>(r8);
-      af[2] = *reinterpret_cast<const unsigned *>(r0 + 8);
-      af[3] = *reinterpret_cast<const unsigned *>(r8 + 8);
-      for (int nt = 0; nt < 8; ++nt) {
-        const __nv_bfloat16 *wb = W1 + (nt * 8 + g) * ROW + kk * 16 + 2 * q;
-        const unsigned bf[2] = {*reinterpret_cast<const unsigned *>(wb),
-                                *reinterpret_cast<const unsigned *>(wb + 8)};
-        mma_bf16(h[nt], af, bf);
+  const std::int64_t tiles = (a.ne + 127) / 128;
+  for (std::int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const std::int64_t e = tile * 128 + t;
+    const bool active = e < a.ne;
+    bool reference = false;
+    {
+      __nv_bfloat16 *x = X + t * ROW;
+      const __nv_bfloat16 zero = __float2bfloat16_rn(0.0f);
+      for (int i = 0; i < F; ++i)
+        x[i] = zero;
+      if (active) {
+        const IndicatorRecord own = records[e];
+        reference = own.reference;
+        const double inv = own.mean != 0.0 ? 1.0 / own.mean : 0.0;
+        for (int m = 0; m < H; ++m)
+          x[m] = own.high[m];
+        for (int j = 0; j < 3; ++j) {
+          const std::int32_t nb = a.neighbors[e * 3 + j];
+          if (nb < 0)
+            continue;
+          const IndicatorRecord n = records[nb];
+          for (int m = 0; m < H; ++m)
+            x[(j + 1) * H + m] = n.high[m];
+          x[4 * H + j] = __float2bfloat16_rn(
+              clamp8(static_cast<float>(__dadd_rn(__dmul_rn(n.mean, inv), -1.0))));
+        }
       }
     }
-    // Layer 2: A fragments straight from layer 1's accumulators (ReLU, BF16).
-    float o[8][4];
-    for (int nt = 0; nt < 8; ++nt) {
-      const int c = nt * 8 + 2 * q;
-      o[nt][0] = o[nt][2] = b2[c];
-      o[nt][1] = o[nt][3] = b2[c + 1];
-    }
-    for (int kk = 0; kk < 4; ++kk) {
-      const float *lo = h[2 * kk], *hi = h[2 * kk + 1];
-      const unsigned af[4] = {pack_bf16(fmaxf(lo[0], 0.0f), fmaxf(lo[1], 0.0f)),
-                              pack_bf16(fmaxf(lo[2], 0.0f), fmaxf(lo[3], 0.0f)),
-                              pack_bf16(fmaxf(hi[0], 0.0f), fmaxf(hi[1], 0.0f)),
-                              pack_bf16(fmaxf(hi[2], 0.0f), fmaxf(hi[3], 0.0f))};
-      for (int nt = 0; nt < 8; ++nt) {
-        const __nv_bfloat16 *wb = W2 + (nt * 8 + g) * (Hd + 8) + kk * 16 + 2 * q;
-        const unsigned bf[2] = {*reinterpret_cast<const unsigned *>(wb),
-                                *reinterpret_cast<const unsigned *>(wb + 8)};
-        mma_bf16(o[nt], af, bf);
-      }
-    }
-    // Layer 3: rows g and g + 8, columns 2q, 2q+1 of each n-tile, then the quad.
-    float z0 = 0.0f, z8 = 0.0f;
-    for (int nt = 0; nt < 8; ++nt) {
-      const int c = nt * 8 + 2 * q;
-      z0 = fmaf(w3[c], fmaxf(o[nt][0], 0.0f), fmaf(w3[c + 1], fmaxf(o[nt][1], 0.0f), z0));
-      z8 = fmaf(w3[c], fmaxf(o[nt][2], 0.0f), fmaf(w3[c + 1], fmaxf(o[nt][3], 0.0f), z8));
-    }
-    z0 += __shfl_xor_sync(0xffffffffu, z0, 1);
-    z0 += __shfl_xor_sync(0xffffffffu, z0, 2);
-    z8 += __shfl_xor_sync(0xffffffffu, z8, 1);
-    z8 += __shfl_xor_sync(0xffffffffu, z8, 2);
-    if (q == 0) {
-      logit[row0 + g] = z0 + P[a.shape.b3];
-      logit[row0 + g + 8] = z8 + P[a.shape.b3];
-    }
-  }
-  __syncthreads();
+    __syncthreads(); // rows built (and, the first time, the network loaded)
 
-  if (active) {
-    const float p = 1.0f / (1.0f + expf(-logit[t]));
-    bool troubled;
-    int kind;
-    if (p >= a.hi) {
-      troubled = true;
-      kind = 0;
-    } else if (p <= a.lo) {
-      troubled = false;
-      kind = 1;
-    } else {
-      troubled = reference;
-      kind = 2;
+    for (int mt = 0; mt < 2; ++mt) {
+      const int row0 = warp * 32 + mt * 16;
+      // Layer 1: 16 rows x 64 outputs, K = F.
+      float h[8][4];
+      for (int nt = 0; nt < 8; ++nt) {
+        const int c = nt * 8 + 2 * q;
+        h[nt][0] = h[nt][2] = b1[c];
+        h[nt][1] = h[nt][3] = b1[c + 1];
+      }
+      for (int kk = 0; kk < KF; ++kk) {
+        unsigned af[4];
+        const __nv_bfloat16 *r0 = X + (row0 + g) * ROW + kk * 16 + 2 * q;
+        const __nv_bfloat16 *r8 = X + (row0 + g + 8) * ROW + kk * 16 + 2 * q;
+        af[0] = *reinterpret_cast<const unsigned *>(r0);
+        af[1] = *reinterpret_cast<const unsigned *>(r8);
+        af[2] = *reinterpret_cast<const unsigned *>(r0 + 8);
+        af[3] = *reinterpret_cast<const unsigned *>(r8 + 8);
+        for (int nt = 0; nt < 8; ++nt) {
+          const __nv_bfloat16 *wb = W1 + (nt * 8 + g) * ROW + kk * 16 + 2 * q;
+          const unsigned bf[2] = {*reinterpret_cast<const unsigned *>(wb),
+                                  *reinterpret_cast<const unsigned *>(wb + 8)};
+          mma_bf16(h[nt], af, bf);
+        }
+      }
+      // Layer 2: A fragments straight from layer 1's accumulators (ReLU, BF16).
+      float o[8][4];
+      for (int nt = 0; nt < 8; ++nt) {
+        const int c = nt * 8 + 2 * q;
+        o[nt][0] = o[nt][2] = b2[c];
+        o[nt][1] = o[nt][3] = b2[c + 1];
+      }
+      for (int kk = 0; kk < 4; ++kk) {
+        const float *lo = h[2 * kk], *hi = h[2 * kk + 1];
+        const unsigned af[4] = {pack_bf16(fmaxf(lo[0], 0.0f), fmaxf(lo[1], 0.0f)),
+                                pack_bf16(fmaxf(lo[2], 0.0f), fmaxf(lo[3], 0.0f)),
+                                pack_bf16(fmaxf(hi[0], 0.0f), fmaxf(hi[1], 0.0f)),
+                                pack_bf16(fmaxf(hi[2], 0.0f), fmaxf(hi[3], 0.0f))};
+        for (int nt = 0; nt < 8; ++nt) {
+          const __nv_bfloat16 *wb = W2 + (nt * 8 + g) * (Hd + 8) + kk * 16 + 2 * q;
+          const unsigned bf[2] = {*reinterpret_cast<const unsigned *>(wb),
+                                  *reinterpret_cast<const unsigned *>(wb + 8)};
+          mma_bf16(o[nt], af, bf);
+        }
+      }
+      // Layer 3: rows g and g + 8, columns 2q, 2q+1 of each n-tile, then the quad.
+      float z0 = 0.0f, z8 = 0.0f;
+      for (int nt = 0; nt < 8; ++nt) {
+        const int c = nt * 8 + 2 * q;
+        z0 = fmaf(w3[c], fmaxf(o[nt][0], 0.0f), fmaf(w3[c + 1], fmaxf(o[nt][1], 0.0f), z0));
+        z8 = fmaf(w3[c], fmaxf(o[nt][2], 0.0f), fmaf(w3[c + 1], fmaxf(o[nt][3], 0.0f), z8));
+      }
+      z0 += __shfl_xor_sync(0xffffffffu, z0, 1);
+      z0 += __shfl_xor_sync(0xffffffffu, z0, 2);
+      z8 += __shfl_xor_sync(0xffffffffu, z8, 1);
+      z8 += __shfl_xor_sync(0xffffffffu, z8, 2);
+      if (q == 0) {
+        logit[row0 + g] = z0 + b3;
+        logit[row0 + g + 8] = z8 + b3;
+      }
     }
-    if (a.logits)
-      a.logits[e] = logit[t];
-    a.flags[e] = troubled ? 1 : 0;
-    atomicAdd(&counts[kind], 1ULL);
-    if (reference)
-      atomicAdd(&counts[3], 1ULL);
-    if (reference && !troubled)
-      atomicAdd(&counts[4], 1ULL);
-    if (!reference && troubled)
-      atomicAdd(&counts[5], 1ULL);
-    const unsigned mask = __activemask();
-    const unsigned ballot = __ballot_sync(mask, troubled);
-    if (ballot) {
-      const int leader = __ffs(ballot) - 1;
-      int base = 0;
-      if (lane == leader)
-        base = atomicAdd(a.troubled_count, __popc(ballot));
-      base = __shfl_sync(mask, base, leader);
-      if (troubled)
-        a.troubled[base + __popc(ballot & ((1u << lane) - 1u))] = static_cast<std::int32_t>(e);
+    __syncthreads(); // logits written; the next tile's rows may overwrite X
+
+    if (active) {
+      const float p = 1.0f / (1.0f + expf(-logit[t]));
+      bool troubled;
+      int kind;
+      if (p >= a.hi) {
+        troubled = true;
+        kind = 0;
+      } else if (p <= a.lo) {
+        troubled = false;
+        kind = 1;
+      } else {
+        troubled = reference;
+        kind = 2;
+      }
+      if (a.logits)
+        a.logits[e] = logit[t];
+      a.flags[e] = troubled ? 1 : 0;
+      atomicAdd(&counts[kind], 1ULL);
+      if (reference)
+        atomicAdd(&counts[3], 1ULL);
+      if (reference && !troubled)
+        atomicAdd(&counts[4], 1ULL);
+      if (!reference && troubled)
+        atomicAdd(&counts[5], 1ULL);
+      const unsigned mask = __activemask();
+      const unsigned ballot = __ballot_sync(mask, troubled);
+      if (ballot) {
+        const int leader = __ffs(ballot) - 1;
+        int base = 0;
+        if (lane == leader)
+          base = atomicAdd(a.troubled_count, __popc(ballot));
+        base = __shfl_sync(mask, base, leader);
+        if (troubled)
+          a.troubled[base + __popc(ballot & ((1u << lane) - 1u))] = static_cast<std::int32_t>(e);
+      }
     }
+    // The logits of this tile are read above before the next tile's MMAs
+    // write them: those come after the next tile's first barrier.
   }
   __syncthreads();
   if (t < 6 && a.stats && counts[t])
@@ -475,7 +526,15 @@ void launch_mlp_predict(const MlpShape &sh, const float *params, const float *fe
 void launch_mlp_indicator(const MlpIndicatorArgs &a, cudaStream_t s) {
   if (a.ne <= 0)
     return;
-  const unsigned blocks = static_cast<unsigned>((a.ne + 127) / 128);
+  if (!a.records)
+    throw std::invalid_argument("indicator network: no record scratch");
+  mlp_records_kernel<<<static_cast<unsigned>((a.ne + 127) / 128), 128, 0, s>>>(a);
+  // Persistent CTAs, a few per SM, each loading the network once.
+  int device = 0, sms = 148;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  const std::int64_t tiles = (a.ne + 127) / 128;
+  const unsigned blocks = static_cast<unsigned>(std::min<std::int64_t>(tiles, 4LL * sms));
   switch (a.shape.features / 16) {
   case 1: mlp_indicator_kernel<1><<<blocks, 128, 0, s>>>(a); break;
   case 2: mlp_indicator_kernel<2><<<blocks, 128, 0, s>>>(a); break;

@@ -2,6 +2,7 @@
 // the trainer behind wasl_mlp_*.
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 #include <vector>
 
@@ -13,6 +14,7 @@ namespace wasl_b200 {
 
 constexpr int kMlpHidden = 64;
 constexpr int kMlpMaxFeatures = 48;
+constexpr int kMlpMaxModes = 10; // P3 triangles
 constexpr int kMlpBatch = 64; // samples per training block
 
 // Offsets of each parameter block in the flat FP32 vector:
@@ -41,7 +43,11 @@ struct MlpIndicatorArgs {
   std::int32_t *troubled_count = nullptr;
   unsigned long long *stats = nullptr; // [6], see mlp_indicator_kernel
   float *logits = nullptr;             // optional [ne]
+  void *records = nullptr;             // scratch, kMlpRecordBytes x ne
 };
+
+// Bytes per element of the inference's per-element records.
+constexpr std::size_t kMlpRecordBytes = 32;
 
 void launch_mlp_features(const double *state, std::int64_t ne, int M,
                          const std::int32_t *neighbors, int F, double threshold,

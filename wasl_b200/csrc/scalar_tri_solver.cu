@@ -17,7 +17,7 @@ namespace wasl_b200 {
 
 class ScalarTriSolver final : public Solver {
 public:
-  ScalarTriSolver(const wasl_gpu_config &cfg, TriTopology &&topo)
+  ScalarTriSolver(const wasl_gpu_config &cfg, TriTopology &&topo, const PartBoundary *part)
       : cfg_(cfg), mesh_(std::move(topo)), p_(cfg.polynomial_order), M_(tri_modes(p_)) {
     if (!euler_tri_order_supported(p_))
       throw SolverError(WASL_ERR_ARGUMENT, "2D scalar advection: polynomial order must be 0..3");
@@ -35,7 +35,10 @@ public:
     for (std::int64_t f = 0; f < mesh_.face_count(); ++f)
       has_boundary |= mesh_.face_right[f] < 0;
     PeriodicTrace trace;
-    if (has_boundary) {
+    if (part) {
+      std::vector<std::int32_t> stencil_donors;
+      trace = part_trace(mesh_, p_, *part, stencil_donors);
+    } else if (has_boundary) {
       DeviceArray<double> d_maps;
       upload_maps(mesh_, d_maps, stream_);
       trace = periodic_trace_device(mesh_, p_, d_maps.get(), stream_);
@@ -240,8 +243,9 @@ private:
   DeviceArray<unsigned char> d_face_table_;
 };
 
-std::unique_ptr<Solver> make_scalar_tri_solver(const wasl_gpu_config &cfg, TriTopology &&topo) {
-  return std::make_unique<ScalarTriSolver>(cfg, std::move(topo));
+std::unique_ptr<Solver> make_scalar_tri_solver(const wasl_gpu_config &cfg, TriTopology &&topo,
+                                               const PartBoundary *part) {
+  return std::make_unique<ScalarTriSolver>(cfg, std::move(topo), part);
 }
 
 } // namespace wasl_b200

@@ -124,6 +124,11 @@ public:
     (void)length;
     throw SolverError(WASL_ERR_ARGUMENT, "cfl parts: only for 2D Euler");
   }
+  // stable_dt's formula from the two factors (2D Euler).
+  virtual double dt_from_parts(double cfl, double speed, double length) const {
+    (void)cfl, (void)speed, (void)length;
+    throw SolverError(WASL_ERR_ARGUMENT, "cfl parts: only for 2D Euler");
+  }
   virtual void step(double dt) = 0;
   virtual void limit() = 0; // the stage limiter applied to the current state
   // Enqueues `steps` device-resident steps; returns without waiting for
@@ -224,8 +229,12 @@ private:
   double stage_split_[3] = {0.0, 0.0, 0.0};
 };
 
+struct PartBoundary;
+// part: the explicit boundary of one part of a partitioned periodic mesh
+// (mesh.hpp), or null.
 std::unique_ptr<Solver> make_solver(const wasl_gpu_config &config, std::int64_t node_count,
                                     const std::int64_t *node_tags, const double *coordinates,
-                                    std::int64_t element_count, const std::int64_t *element_nodes);
+                                    std::int64_t element_count, const std::int64_t *element_nodes,
+                                    const PartBoundary *part = nullptr);
 
 } // namespace wasl_b200

@@ -22,17 +22,24 @@ bool pair_periodic_faces(const TriTopology &mesh, int QF, TriSlots &t, std::vect
   const std::size_t nb = bface.size();
   if (t.donors.size() != nb * QF)
     return false;
+  // A face whose donor is its own element (the cut face of a partition
+  // part, which takes its own trace) has no partner and stays unpaired.
   std::vector<std::int32_t> bdonor(nb);
+  std::vector<char> own(nb, 0);
   std::map<std::pair<std::int32_t, std::int32_t>, std::vector<std::size_t>> by_pair;
   for (std::size_t b = 0; b < nb; ++b) {
     bdonor[b] = t.donors[b * QF];
     for (int q = 1; q < QF; ++q)
       if (t.donors[b * QF + q] != bdonor[b])
         return false;
-    by_pair[{mesh.face_left[bface[b]], bdonor[b]}].push_back(b);
+    own[b] = bdonor[b] == mesh.face_left[bface[b]];
+    if (!own[b])
+      by_pair[{mesh.face_left[bface[b]], bdonor[b]}].push_back(b);
   }
   std::vector<std::size_t> partner(nb);
   for (std::size_t b = 0; b < nb; ++b) {
+    if (own[b])
+      continue;
     const auto it = by_pair.find({bdonor[b], mesh.face_left[bface[b]]});
     if (it == by_pair.end() || it->second.size() != 1)
       return false;
@@ -41,9 +48,11 @@ bool pair_periodic_faces(const TriTopology &mesh, int QF, TriSlots &t, std::vect
       return false;
   }
   for (std::size_t b = 0; b < nb; ++b)
-    if (partner[partner[b]] != b)
+    if (!own[b] && partner[partner[b]] != b)
       return false;
   for (std::size_t b = 0; b < nb; ++b) {
+    if (own[b])
+      continue;
     const std::int64_t f = bface[b], c = bface[partner[b]];
     if (f < c)
       continue; // f is the kept face of its pair
@@ -79,6 +88,11 @@ TileSlotArrays build_tile_slots(const TriTopology &mesh, const TriSlots &t, int 
         s.nbr[slot] = left ? R : L;
         s.code[slot] = static_cast<std::uint8_t>(bits | (left ? 1u : 0u));
       } else if (boundary == WASL_TRANSMISSIVE) {
+        s.nbr[slot] = -1;
+        s.code[slot] = static_cast<std::uint8_t>(bits | 1u);
+      } else if (left && t.donors[static_cast<std::size_t>(-R - 1) * QF] == L) {
+        // A face that takes its own element's trace (a partition part's cut
+        // face): the kernels' transmissive face.
         s.nbr[slot] = -1;
         s.code[slot] = static_cast<std::uint8_t>(bits | 1u);
       } else {
@@ -151,7 +165,8 @@ bool build_patch_edges(const TriTopology &mesh, const TriSlots &t, int boundary,
     if (t.donors.size() != bface.size() * QF)
       return false;
     for (std::size_t b = 0; b < bface.size(); ++b)
-      by_pair[{mesh.face_left[bface[b]], t.donors[b * QF]}].push_back(b);
+      if (t.donors[b * QF] != mesh.face_left[bface[b]])
+        by_pair[{mesh.face_left[bface[b]], t.donors[b * QF]}].push_back(b);
   }
   if (QF > kMaxEdgePoints)
     return false;
@@ -188,6 +203,10 @@ bool build_patch_edges(const TriTopology &mesh, const TriSlots &t, int boundary,
     for (int q = 1; q < QF; ++q)
       if (t.donors[bi * QF + q] != D)
         return false;
+    if (D == L) { // takes its own trace (a partition part's cut face)
+      set(L, jl, -1, 1u, f);
+      continue;
+    }
     const auto it = by_pair.find({D, L});
     if (it == by_pair.end() || it->second.size() != 1 || it->second[0] == bi)
       return false;

@@ -17,6 +17,9 @@ namespace wasl_b200 {
 // (slot_code bit 6: its basis on the face is the donor basis row), with the
 // kept face's normal and scale.  Needs every boundary face to have one donor
 // whose boundary face points back; returns false (slots untouched) otherwise.
+// A face whose donor is its own element (a partition part's cut face, which
+// takes its own trace) stays unpaired, and the tile and patch arrays below
+// give it the transmissive exterior.
 // basis32: the donor basis [boundary face][QF][M] in FP32.
 bool pair_periodic_faces(const TriTopology &mesh, int QF, TriSlots &t, std::vector<float> &basis32);
 

@@ -30,9 +30,14 @@ step bit-identical to a run over the whole mesh.  The time step is reduced
 over ranks from each rank's largest wave speed and smallest element length
 (`global_dt`), which gives the whole-mesh dt bit for bit.
 
-Domains whose boundary is periodic are not partitioned here: the periodic
-pairing of a rank's boundary faces would also pair the faces where its ghost
-region ends.
+Periodic domains are partitioned through the whole mesh's periodic trace
+(`periodic_pairs`): the ghost layers grow across the periodic seams as well,
+and each rank's handle is built with its boundary given explicitly
+(`LocalMesh.part_boundary`, wasl_gpu_create_part): a periodic face whose
+donors are on the rank keeps its donors and basis from the whole mesh's
+trace, and every other face of the part's boundary (where the ghost region
+ends) takes its own element's trace.  A rank's own periodic donor search
+would instead pair those cut faces across the period.
 """
 from __future__ import annotations
 
@@ -76,6 +81,56 @@ def face_neighbors(element_nodes) -> np.ndarray:
     return nbr
 
 
+@dataclass
+class PeriodicPairs:
+    """The whole mesh's periodic trace: boundary face b (ascending face
+    order) lies on edge `edge[b]` of element `element[b]` (local edges of the
+    counter-clockwise normalized element), and its edge points' periodic
+    images lie in donors[b][q], whose basis there is basis[b][q][mode]."""
+    element: np.ndarray
+    edge: np.ndarray
+    donors: np.ndarray
+    basis: np.ndarray
+
+
+def periodic_pairs(node_tags, node_coordinates, element_nodes,
+                   polynomial_order: int) -> PeriodicPairs:
+    """The periodic trace of the whole mesh, from the library's host setup."""
+    from . import mesh_periodic_trace
+    pairs = PeriodicPairs(*mesh_periodic_trace(node_tags, node_coordinates, element_nodes,
+                                               polynomial_order))
+    if np.any(pairs.donors != pairs.donors[:, :1]):
+        raise ValueError("partition: a periodic face's points have different donors"
+                         " (non-conforming periodic faces)")
+    return pairs
+
+
+def normalized_edge(node_tags, node_coordinates, element_nodes) -> np.ndarray:
+    """[elements][3]: the caller's local edge (nodes k, k+1) that is the
+    normalized element's edge j.  The library turns clockwise triangles
+    counter-clockwise by swapping their second and third nodes, which maps
+    edge j to the caller's edge 2 - j."""
+    tags = np.asarray(node_tags, dtype=np.int64)
+    xy = np.asarray(node_coordinates, dtype=np.float64).reshape(-1, 2)
+    tris = np.asarray(element_nodes, dtype=np.int64)
+    order = np.argsort(tags, kind="stable")
+    pos = order[np.searchsorted(tags[order], tris)]
+    x, y = xy[pos, 0], xy[pos, 1]
+    area2 = (x[:, 0] * (y[:, 1] - y[:, 2]) + x[:, 1] * (y[:, 2] - y[:, 0])
+             + x[:, 2] * (y[:, 0] - y[:, 1]))
+    edges = np.tile(np.arange(3), (len(tris), 1))
+    edges[area2 < 0] = 2 - edges[area2 < 0]
+    return edges
+
+
+def periodic_neighbors(neighbors: np.ndarray, caller_edge: np.ndarray,
+                       pairs: PeriodicPairs) -> np.ndarray:
+    """face_neighbors with every boundary edge's periodic partner filled in."""
+    nbr = neighbors.copy()
+    nbr[pairs.element, caller_edge[pairs.element, pairs.edge]] = pairs.donors[:, 0]
+    return nbr
+
+
 def ghost_layers(neighbors: np.ndarray, owned: np.ndarray, depth: int) -> list[np.ndarray]:
     """The ghost layers around a set of owned elements (boolean mask): layer k
     holds the elements k face steps away, ascending."""
@@ -101,6 +156,9 @@ class LocalMesh:
     node_tags: np.ndarray         # the nodes the local elements use, ascending
     node_coordinates: np.ndarray
     element_nodes: np.ndarray     # local elements' node tags
+    # For a periodic mesh: (donors [b][Q] int32, basis [b][Q][modes]) of the
+    # part's boundary faces, the handle's wasl_gpu_create_part input.
+    part_boundary: tuple | None = None
 
     @property
     def arrays(self):
@@ -115,11 +173,18 @@ class LocalMesh:
 
 
 def local_mesh(node_tags, node_coordinates, element_nodes, rank: int, ranks: int,
-               depth: int, neighbors: np.ndarray | None = None) -> LocalMesh:
-    """The rank's owned elements plus `depth` ghost layers as a mesh."""
+               depth: int, neighbors: np.ndarray | None = None,
+               pairs: PeriodicPairs | None = None) -> LocalMesh:
+    """The rank's owned elements plus `depth` ghost layers as a mesh; with
+    the whole mesh's periodic pairs, the layers also grow across the periodic
+    seams and the part's boundary is given (LocalMesh.part_boundary)."""
     tris = np.asarray(element_nodes, dtype=np.int64)
     owners = element_owners(tris.shape[0], ranks)
     nbr = face_neighbors(tris) if neighbors is None else neighbors
+    caller_edge = None
+    if pairs is not None:
+        caller_edge = normalized_edge(node_tags, node_coordinates, tris)
+        geometric, nbr = nbr, periodic_neighbors(nbr, caller_edge, pairs)
     owned_mask = owners == rank
     layers = ghost_layers(nbr, owned_mask, depth)
     elements = np.sort(np.concatenate([np.nonzero(owned_mask)[0]] + layers))
@@ -131,7 +196,42 @@ def local_mesh(node_tags, node_coordinates, element_nodes, rank: int, ranks: int
     if np.any(tags[pos] != used):
         raise ValueError("halo: an element uses an unknown node tag")
     coords = np.asarray(node_coordinates, dtype=np.float64)[pos]
-    return LocalMesh(rank, elements, owners[elements] == rank, used, coords, local_tris)
+    boundary = None
+    if pairs is not None:
+        boundary = part_boundary(elements, geometric, caller_edge, pairs)
+    return LocalMesh(rank, elements, owners[elements] == rank, used, coords, local_tris,
+                     boundary)
+
+
+def part_boundary(elements: np.ndarray, geometric: np.ndarray, caller_edge: np.ndarray,
+                  pairs: PeriodicPairs):
+    """The boundary faces of the part made of `elements` (ascending global
+    indices), in the part's face order (by element, then normalized edge):
+    a face of the whole mesh's boundary whose donors are all in the part keeps
+    them (as part indices) and their basis; any other face (a cut face, or a
+    periodic face whose donor lies beyond the ghost region) gets donor -1,
+    its own element's trace."""
+    Q, M = pairs.basis.shape[1], pairs.basis.shape[2]
+    inside = np.full(geometric.shape[0], -1, dtype=np.int64)
+    inside[elements] = np.arange(elements.size)
+    face_of = {(int(e), int(j)): b for b, (e, j) in enumerate(zip(pairs.element, pairs.edge))}
+    donors, basis = [], []
+    for g in elements:
+        for j in range(3):
+            h = geometric[g, caller_edge[g, j]]
+            if h >= 0 and inside[h] >= 0:
+                continue  # an interior face of the part
+            d = np.full(Q, -1, dtype=np.int32)
+            v = np.zeros((Q, M))
+            if h < 0:
+                b = face_of[(int(g), j)]
+                local = inside[pairs.donors[b]]
+                if np.all(local >= 0):
+                    d, v = local.astype(np.int32), pairs.basis[b]
+            donors.append(d)
+            basis.append(v)
+    return (np.array(donors, dtype=np.int32).reshape(-1, Q),
+            np.array(basis, dtype=np.float64).reshape(-1, Q, M))
 
 
 @dataclass
@@ -223,6 +323,111 @@ class HaloExchange:
             state.index_copy_(1, idx, buf)
 
 
+class NativeHalo:
+    """One rank's halo exchange in the library (wasl_halo_*), on its
+    handle's device state: pack and unpack kernels on the handle's stream,
+    per-peer device buffers [rows][columns], and the NCCL transport.  The
+    same schedule as HaloExchange, without torch on the data path."""
+
+    def __init__(self, solver, mesh: LocalMesh, schedule: HaloSchedule):
+        import ctypes as C
+
+        from . import WaslError, _i64, _ptr, library
+        self._lib, self._C, self.solver = library(), C, solver
+        sends, recvs = dict(schedule.sends), dict(schedule.recvs)
+        self.peers = sorted(set(sends) | set(recvs))
+        empty = np.zeros(0, dtype=np.int64)
+        send_lists = [mesh.local_index(sends[p]) if p in sends else empty for p in self.peers]
+        recv_lists = [mesh.local_index(recvs[p]) if p in recvs else empty for p in self.peers]
+        ranks = np.array(self.peers, dtype=np.int32)
+        send_counts = np.array([len(x) for x in send_lists], dtype=np.int64)
+        recv_counts = np.array([len(x) for x in recv_lists], dtype=np.int64)
+        send_elems = np.ascontiguousarray(np.concatenate([empty] + send_lists), dtype=np.int64)
+        recv_elems = np.ascontiguousarray(np.concatenate([empty] + recv_lists), dtype=np.int64)
+        err = C.create_string_buffer(1024)
+        h = C.c_void_p()
+        rc = self._lib.wasl_halo_create(
+            solver._h, len(self.peers), ranks.ctypes.data_as(C.POINTER(C.c_int32)),
+            _ptr(send_counts, _i64), _ptr(send_elems, _i64), _ptr(recv_counts, _i64),
+            _ptr(recv_elems, _i64), C.byref(h), err, len(err))
+        if rc != 0:
+            raise WaslError(rc, err.value.decode())
+        self._h = h
+
+    def _check(self, rc):
+        from . import WaslError
+        if rc != 0:
+            raise WaslError(rc, self._lib.wasl_halo_last_error(self._h).decode())
+
+    def pack(self):
+        self._check(self._lib.wasl_halo_pack(self._h))
+
+    def unpack(self):
+        self._check(self._lib.wasl_halo_unpack(self._h))
+
+    def buffers(self, k: int):
+        """(send pointer, receive pointer, send columns, receive columns, rows)
+        of the k-th peer (self.peers[k])."""
+        C = self._C
+        send, recv = C.c_void_p(), C.c_void_p()
+        ns, nr, rows = C.c_int64(), C.c_int64(), C.c_int64()
+        self._check(self._lib.wasl_halo_buffers(self._h, k, C.byref(send), C.byref(recv),
+                                                C.byref(ns), C.byref(nr), C.byref(rows)))
+        return send.value, recv.value, ns.value, nr.value, rows.value
+
+    def exchange_nccl(self, comm: int):
+        self._check(self._lib.wasl_halo_exchange_nccl(self._h, self._C.c_void_p(comm)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.wasl_halo_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+def nccl_unique_id() -> bytes:
+    """A new NCCL communicator id (128 bytes), made on one rank and shared."""
+    import ctypes as C
+
+    from . import WaslError, library
+    buf = (C.c_uint8 * 128)()
+    rc = library().wasl_nccl_unique_id(buf)
+    if rc != 0:
+        raise WaslError(rc, "NCCL: no unique id")
+    return bytes(buf)
+
+
+def nccl_communicator(ranks: int, uid: bytes, rank: int, device: int) -> int:
+    """An NCCL communicator (ncclComm_t as an int) of this rank."""
+    import ctypes as C
+
+    from . import WaslError, library
+    buf = (C.c_uint8 * 128).from_buffer_copy(uid)
+    comm, err = C.c_void_p(), C.create_string_buffer(1024)
+    rc = library().wasl_nccl_comm_create(ranks, buf, rank, device, C.byref(comm), err, len(err))
+    if rc != 0:
+        raise WaslError(rc, err.value.decode())
+    return comm.value
+
+
+def nccl_destroy(comm: int) -> None:
+    import ctypes as C
+
+    from . import library
+    library().wasl_nccl_comm_destroy(C.c_void_p(comm))
+
+
+def stable_dt_nccl(solver, comm: int, cfl: float) -> float:
+    """The whole mesh's CFL step, the CFL parts all-reduced over comm."""
+    import ctypes as C
+    dt = C.c_double()
+    solver._check(solver._lib.wasl_gpu_stable_dt_nccl(solver._h, C.c_void_p(comm), cfl,
+                                                      C.byref(dt)))
+    return dt.value
+
+
 class _DeviceRows:
     """A [rows][columns] float64 array in device memory, by its pointer."""
 
@@ -245,15 +450,18 @@ def device_state(solver):
 
 
 def check_partitioned_solver(solver) -> None:
-    """A rank's handle must treat its boundary faces as transmissive: with
-    periodic boundaries it would pair the faces where its ghost region is cut
-    across the period and silently compute wrong values there.  Raises
-    ValueError for such a handle."""
+    """A rank's periodic handle must have been built on its part's given
+    boundary (Solver(..., part_boundary=mesh.part_boundary)): its own donor
+    search would pair the faces where its ghost region is cut across the
+    period and silently compute wrong values there.  Raises ValueError for
+    such a handle."""
     from . import BOUNDARY_KINDS
-    if solver.config.boundary_left == BOUNDARY_KINDS["periodic"]:
-        raise ValueError("partitioned runs: periodic boundaries are not supported (a rank's"
-                         " cut faces would be paired across the period); build each rank's"
-                         " handle with boundary='transmissive'")
+    if (solver.config.boundary_left == BOUNDARY_KINDS["periodic"]
+            and not getattr(solver, "part", False)):
+        raise ValueError("partitioned runs: a periodic handle needs its part's boundary (build"
+                         " it with part_boundary=LocalMesh.part_boundary from a local_mesh"
+                         " given the periodic pairs); otherwise its cut faces would be paired"
+                         " across the period")
 
 
 def step_partitioned(solver, exchange: HaloExchange, cfl: float, polynomial_order: int,
