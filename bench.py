@@ -451,12 +451,13 @@ def kernel_description(tuning):
              "shared-face tile 128 el/CTA, 3 CTAs/SM", "patch 128 el/CTA, <=128 regs",
              "patch 128 el/CTA, 5 CTAs/SM", "patch 64 el/CTA, 8 CTAs/SM",
              "patch 64 el/CTA, 10 CTAs/SM", "patch + tensor-core volume 128 el/CTA, <=128 regs",
-             "patch + tensor-core volume 128 el/CTA, 5 CTAs/SM"]
+             "patch + tensor-core volume 128 el/CTA, 5 CTAs/SM",
+             "persistent tile 128 el/CTA, <=128 regs", "persistent tile 256 el/CTA, <=128 regs"]
     if choice < 0:
         return {"name": "single stage kernel"}
     out = {"name": names[choice] if choice < len(names) else str(choice)}
     if ms:
-        out["autotuned_stage_ms"] = {names[i]: round(t, 5) for i, t in enumerate(ms)}
+        out["autotuned_stage_ms"] = {names[i]: round(t, 5) for i, t in enumerate(ms) if t > 0}
     return out
 
 

@@ -11,8 +11,10 @@ from wasl_b200 import cases, meshgen
 
 pytestmark = pytest.mark.gpu
 
-# Launch shapes of the tile kernels (see wasl_gpu_tuning).
-TILE_SHAPES = 8
+# Launch shapes of the tile kernels (see wasl_gpu_tuning): the batch tunes
+# over the tile kernels' shapes 0-7 and the persistent tile kernel's 14-15.
+TILE_SHAPES = 16
+BATCH_SHAPES = list(range(8)) + [14, 15]
 
 
 def small_cases(seed, count=5):
@@ -40,7 +42,7 @@ def milder(problem):
 
 @pytest.mark.parametrize("limiting", [False, True])
 @pytest.mark.parametrize("use_graph", [True, False])
-@pytest.mark.parametrize("shape", [0, 3, 4, 6])
+@pytest.mark.parametrize("shape", [0, 3, 4, 6, 14, 15])
 def test_batch_matches_single_case_solver(limiting, use_graph, shape):
     """Bit-identical states per case, or, if a case fails alone (a positivity
     floor), the same failure from the batch."""
@@ -100,7 +102,9 @@ def test_batch_autotunes_each_order_and_conserves():
         b.advance(0.15, 10)
         for p in set(s[3] for s in specs):
             choice, ms = b.tuning(p)
-            assert len(ms) == TILE_SHAPES and ms[choice] == min(ms)
+            assert len(ms) == TILE_SHAPES and choice in BATCH_SHAPES
+            assert all(ms[k] > 0 for k in BATCH_SHAPES)
+            assert ms[choice] == min(ms[k] for k in BATCH_SHAPES)
         for c, s in enumerate(specs):
             ne, nm = b.case_size(c)
             state = b.get_state(c).reshape(4, nm, ne)

@@ -16,8 +16,9 @@ pytestmark = pytest.mark.gpu
 # (s = 0..3 the tile kernel, 4..7 the shared-face tile kernel, 8..11 the patch
 # kernel, 12..13 the patch kernel with its volume term on the tensor cores).
 KERNELS = [1, 2, 3, 4, 5]
-TILE_SHAPES = 14
+TILE_SHAPES = 16
 SHARED_KERNELS = [6, 7, 8, 9]
+PERSISTENT_KERNELS = [16, 17]
 PATCH_KERNELS = [10, 11, 12, 13]
 MMA_KERNELS = [14, 15]
 
@@ -144,13 +145,14 @@ def test_tile_kernel_matches_face_centric(p, kernel, boundary):
 @pytest.mark.parametrize("boundary", ["periodic", "transmissive"])
 def test_shared_face_kernel_is_bit_identical(p, limiting, boundary):
     """The shared-face tile kernel evaluates a face inside a tile once instead
-    of once per element, with the same arithmetic: every launch shape gives
+    of once per element, with the same arithmetic, and the persistent tile
+    kernel loops its resident CTAs over the tiles: every launch shape gives
     the tile kernel's states bit for bit, with and without the limiter (whose
     rough pass takes the elements next to jumps of the means)."""
     arrays = meshgen.jittered_box(20, jitter=0.15, seed=50 + p)
     c = seeded_state(2 * 20 * 20, p, 70 + p, amplitude=0.02)
     out = {}
-    for k in [2] + SHARED_KERNELS:
+    for k in [2] + SHARED_KERNELS + PERSISTENT_KERNELS:
         with wasl_b200.Solver(*arrays, polynomial_order=p, precision="mixed", mixed_kernel=k,
                               boundary=boundary, limiting=limiting,
                               positivity_all=limiting) as g:
@@ -160,7 +162,7 @@ def test_shared_face_kernel_is_bit_identical(p, limiting, boundary):
             out[k] = (g.get_state(), g.flags())
             assert g.tuning()[0] == k - 1
     assert np.max(np.abs(out[2][0] - c)) > 0
-    for k in SHARED_KERNELS:
+    for k in SHARED_KERNELS + PERSISTENT_KERNELS:
         assert np.array_equal(out[k][0], out[2][0]), f"kernel {k}"
         assert np.array_equal(out[k][1], out[2][1]), f"kernel {k}"
 

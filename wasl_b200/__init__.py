@@ -471,7 +471,7 @@ class Solver:
     def tuning(self):
         """(kernel choice, per-variant stage ms) of the mixed form; see wasl_gpu_tuning."""
         choice, count = C.c_int(), C.c_int()
-        ms = np.zeros(16)
+        ms = np.zeros(64)
         self._check(self._lib.wasl_gpu_tuning(self._h, C.byref(choice), _ptr(ms), len(ms),
                                               C.byref(count)))
         return choice.value, ms[:count.value].tolist()
@@ -653,7 +653,7 @@ class Batch:
 
     def tuning(self, polynomial_order):
         choice, count = C.c_int(), C.c_int()
-        ms = np.zeros(16)
+        ms = np.zeros(64)
         self._check(self._lib.wasl_batch_tuning(self._h, polynomial_order, C.byref(choice),
                                                 _ptr(ms), len(ms), C.byref(count)))
         return choice.value, ms[:count.value].tolist()

@@ -397,16 +397,21 @@ void BatchSolver::tune() {
     const std::string key = "batch_tile/p" + std::to_string(g.p) + "/rule" +
                             std::to_string(g.rule) + "/bnd" + std::to_string(cfg_.boundary) +
                             "/size" + std::to_string(size_class(g.ne));
-    int shapes = 0; // the tile kernels' shapes (the patch kernel's come after them)
-    while (shapes < euler_tri_tile_shapes() && !euler_tri_tile_is_patch(shapes))
-      ++shapes;
-    g.tuning = autotune(key, shapes, [&](int shape) {
-      g.shape = shape;
+    std::vector<int> shapes; // the tile kernels' shapes (not the patch kernel's)
+    for (int shape = 0; shape < euler_tri_tile_shapes(); ++shape)
+      if (!euler_tri_tile_is_patch(shape))
+        shapes.push_back(shape);
+    const TuneResult timed = autotune(key, static_cast<int>(shapes.size()), [&](int i) {
+      g.shape = shapes[i];
       StageArgs a = stage_args(g, 0);
       a.sense = 0;
-      launch_euler_tri_stage_tile(g.p, g.rule, shape, a, stream_);
+      launch_euler_tri_stage_tile(g.p, g.rule, shapes[i], a, stream_);
     }, stream_);
-    g.shape = g.tuning.choice;
+    // By shape (0 for the shapes not timed).
+    g.tuning.ms.assign(euler_tri_tile_shapes(), 0.0);
+    for (std::size_t i = 0; i < shapes.size(); ++i)
+      g.tuning.ms[shapes[i]] = timed.ms[i];
+    g.shape = g.tuning.choice = shapes[timed.choice];
   }
 }
 

@@ -778,67 +778,20 @@ __device__ __forceinline__ void tile_finish(const StageArgs &a, std::int64_t e, 
 // read from global memory); faces with a jump are evaluated in FP64
 // (face_fp64), the others with the same FP32 code as the FP32 pass, so both
 // elements of every face still compute the same values.
-template <int P, int R, int TILE, int MINB, bool ROUGH>
-__global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_mixed(const StageArgs a) {
+// One element's share of the tile kernel's stage, once its tile is staged:
+// volume term, the three faces, and the finish.  An element of the FP32 pass
+// with a face across a jump of the means returns early (handed to the rough
+// pass).  Shared by the one-tile-per-CTA and the persistent kernels.
+template <int P, int R, int TILE, bool ROUGH>
+__device__ __forceinline__ void tile_element(const StageArgs &a, const FaceTable<P, float> &table,
+                                             const double (*sstate)[TILE], int t,
+                                             std::int64_t e, std::int64_t first,
+                                             std::int64_t count, int case_id) {
   using S = TriShape<P>;
   constexpr int M = S::M, QV = MixedVolume<P, R>::QV, QF = S::QF, H = M - 1;
   constexpr double phi0 = 0.70710678118654752440;
-  __shared__ FaceTable<P, float> table;
-  // The tile's FP64 state, row v M + m (dynamic shared memory, 4 M TILE doubles).
-  extern __shared__ __align__(16) double tile_state[];
-  double(*sstate)[TILE] = reinterpret_cast<double(*)[TILE]>(tile_state);
-
-  const int t = threadIdx.x;
   const std::int64_t ne = a.mesh.ne;
-  std::int64_t first = 0, count = 0, e = 0;
-  int case_id = 0;
-  bool active;
-  if (ROUGH) {
-    const std::int64_t list = *a.rough_count;
-    if (static_cast<std::int64_t>(blockIdx.x) * TILE >= list)
-      return; // the whole CTA is past the list (uniform: no barrier reached)
-    const std::int64_t i = static_cast<std::int64_t>(blockIdx.x) * TILE + t;
-    active = i < list;
-    if (active) {
-      e = a.rough[i];
-      case_id = a.element_case ? a.element_case[e] : 0;
-    }
-  } else {
-    if (a.work) {
-      const TileWork w = a.work[blockIdx.x];
-      first = w.first;
-      count = w.count;
-      case_id = w.case_id;
-    } else {
-      first = static_cast<std::int64_t>(blockIdx.x) * TILE;
-      count = a.mesh.ne - first < TILE ? a.mesh.ne - first : TILE;
-    }
-    active = t < count;
-    e = first + t;
-  }
   const double *__restrict__ in = a.in;
-
-  // Stage this tile's state (asynchronous 8-byte copies, coalesced per row)
-  // and the face tables.
-  if (active) {
-    const unsigned base = static_cast<unsigned>(__cvta_generic_to_shared(&sstate[0][t]));
-#pragma unroll
-    for (int r = 0; r < 4 * M; ++r)
-      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(base + r * TILE * 8),
-                   "l"(in + r * ne + e)
-                   : "memory");
-  }
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-  {
-    const float *src = static_cast<const float *>(a.face_table);
-    float *dst = reinterpret_cast<float *>(&table);
-    for (int i = t; i < static_cast<int>(sizeof(table) / sizeof(float)); i += TILE)
-      dst[i] = src[i];
-  }
-  asm volatile("cp.async.wait_all;\n" ::: "memory");
-  __syncthreads();
-  if (!active)
-    return;
   double mean[4];
   float ch[4][H];
 #pragma unroll
@@ -1057,6 +1010,122 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_mixed(const StageAr
   }
 
   tile_finish<P, TILE>(a, e, t, case_id, sstate, r0, racc);
+}
+
+template <int P, int R, int TILE, int MINB, bool ROUGH>
+__global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_mixed(const StageArgs a) {
+  using S = TriShape<P>;
+  constexpr int M = S::M;
+  __shared__ FaceTable<P, float> table;
+  // The tile's FP64 state, row v M + m (dynamic shared memory, 4 M TILE doubles).
+  extern __shared__ __align__(16) double tile_state[];
+  double(*sstate)[TILE] = reinterpret_cast<double(*)[TILE]>(tile_state);
+
+  const int t = threadIdx.x;
+  const std::int64_t ne = a.mesh.ne;
+  std::int64_t first = 0, count = 0, e = 0;
+  int case_id = 0;
+  bool active;
+  if (ROUGH) {
+    const std::int64_t list = *a.rough_count;
+    if (static_cast<std::int64_t>(blockIdx.x) * TILE >= list)
+      return; // the whole CTA is past the list (uniform: no barrier reached)
+    const std::int64_t i = static_cast<std::int64_t>(blockIdx.x) * TILE + t;
+    active = i < list;
+    if (active) {
+      e = a.rough[i];
+      case_id = a.element_case ? a.element_case[e] : 0;
+    }
+  } else {
+    if (a.work) {
+      const TileWork w = a.work[blockIdx.x];
+      first = w.first;
+      count = w.count;
+      case_id = w.case_id;
+    } else {
+      first = static_cast<std::int64_t>(blockIdx.x) * TILE;
+      count = a.mesh.ne - first < TILE ? a.mesh.ne - first : TILE;
+    }
+    active = t < count;
+    e = first + t;
+  }
+  const double *__restrict__ in = a.in;
+
+  // Stage this tile's state (asynchronous 8-byte copies, coalesced per row)
+  // and the face tables.
+  if (active) {
+    const unsigned base = static_cast<unsigned>(__cvta_generic_to_shared(&sstate[0][t]));
+#pragma unroll
+    for (int r = 0; r < 4 * M; ++r)
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(base + r * TILE * 8),
+                   "l"(in + r * ne + e)
+                   : "memory");
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  {
+    const float *src = static_cast<const float *>(a.face_table);
+    float *dst = reinterpret_cast<float *>(&table);
+    for (int i = t; i < static_cast<int>(sizeof(table) / sizeof(float)); i += TILE)
+      dst[i] = src[i];
+  }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncthreads();
+  if (!active)
+    return;
+  tile_element<P, R, TILE, ROUGH>(a, table, sstate, t, e, first, count, case_id);
+}
+
+// The FP32 pass of the tile kernel as a persistent kernel: each CTA loads the
+// face tables once and then takes the work list's tiles (or the mesh's
+// TILE-element tiles) gridDim.x apart, staging each one's state in turn; the
+// per-element arithmetic is the tile kernel's, so the results are the same
+// bit for bit.
+template <int P, int R, int TILE, int MINB>
+__global__ void __launch_bounds__(TILE, MINB) euler_tri_tile_persistent(const StageArgs a) {
+  using S = TriShape<P>;
+  constexpr int M = S::M;
+  __shared__ FaceTable<P, float> table;
+  extern __shared__ __align__(16) double tile_state[];
+  double(*sstate)[TILE] = reinterpret_cast<double(*)[TILE]>(tile_state);
+  const int t = threadIdx.x;
+  const std::int64_t ne = a.mesh.ne;
+  const double *__restrict__ in = a.in;
+  {
+    const float *src = static_cast<const float *>(a.face_table);
+    float *dst = reinterpret_cast<float *>(&table);
+    for (int i = t; i < static_cast<int>(sizeof(table) / sizeof(float)); i += TILE)
+      dst[i] = src[i];
+  }
+  const std::int64_t tiles = a.work ? a.work_count : (ne + TILE - 1) / TILE;
+  for (std::int64_t b = blockIdx.x; b < tiles; b += gridDim.x) {
+    std::int64_t first, count;
+    int case_id = 0;
+    if (a.work) {
+      const TileWork w = a.work[b];
+      first = w.first;
+      count = w.count;
+      case_id = w.case_id;
+    } else {
+      first = b * TILE;
+      count = ne - first < TILE ? ne - first : TILE;
+    }
+    const bool active = t < count;
+    const std::int64_t e = first + t;
+    if (active) {
+      const unsigned base = static_cast<unsigned>(__cvta_generic_to_shared(&sstate[0][t]));
+#pragma unroll
+      for (int r = 0; r < 4 * M; ++r)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(base + r * TILE * 8),
+                     "l"(in + r * ne + e)
+                     : "memory");
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncthreads(); // the tile is staged (and, the first time, the tables)
+    if (active)
+      tile_element<P, R, TILE, false>(a, table, sstate, t, e, first, count, case_id);
+    __syncthreads(); // every element is done with the tile before the next one lands
+  }
 }
 
 // Dynamic shared memory of the shared-face tile kernel, in this order:
@@ -2461,6 +2530,48 @@ void stage_tile(const StageArgs &a, cudaStream_t s) {
            tile_smem<P, kRoughTile>(), s>>>(a);
 }
 
+// The persistent tile kernel's attributes and its grid: every CTA resident
+// at once (CTAs per SM at this shape's registers and shared memory, times the
+// SMs), found once per device.
+template <int P, int R, int TILE, int MINB> int persistent_prepare() {
+  static bool opted_in[64] = {};
+  static int resident[64] = {};
+  smem_opt_in(euler_tri_tile_persistent<P, R, TILE, MINB>, tile_smem<P, TILE>(),
+              sizeof(FaceTable<P, float>), opted_in);
+  int device = 0;
+  check(cudaGetDevice(&device), "cudaGetDevice");
+  if (device < 64 && resident[device])
+    return resident[device];
+  int per_sm = 0, sms = 0;
+  check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, euler_tri_tile_persistent<P, R, TILE, MINB>, TILE, tile_smem<P, TILE>()),
+        "persistent tile occupancy");
+  check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+  const int blocks = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+  if (device < 64)
+    resident[device] = blocks;
+  return blocks;
+}
+
+// The FP32 pass as the persistent tile kernel (one wave of resident CTAs
+// looping over the tiles), then the rough pass as stage_tile runs it.
+template <int P, int R, int TILE, int MINB>
+void stage_tile_persistent(const StageArgs &a, cudaStream_t s) {
+  const int resident = persistent_prepare<P, R, TILE, MINB>();
+  const std::int64_t tiles = a.work ? a.work_count : (a.mesh.ne + TILE - 1) / TILE;
+  if (tiles <= 0)
+    return;
+  if (a.rough)
+    check(cudaMemsetAsync(a.rough_count, 0, sizeof(std::int32_t), s), "rough count");
+  const std::int64_t blocks = tiles < resident ? tiles : resident;
+  euler_tri_tile_persistent<P, R, TILE, MINB>
+      <<<static_cast<unsigned>(blocks), TILE, tile_smem<P, TILE>(), s>>>(a);
+  if (a.rough)
+    euler_tri_tile_mixed<P, R, kRoughTile, 1, true>
+        <<<static_cast<unsigned>((a.mesh.ne + kRoughTile - 1) / kRoughTile), kRoughTile,
+           tile_smem<P, kRoughTile>(), s>>>(a);
+}
+
 template <int P, int R, int TILE, int MINB, bool MMA> void patch_opt_in() {
   static bool opted_in[64] = {};
   smem_opt_in(euler_tri_patch<P, R, TILE, MINB, MMA>, PatchSmem<P, R, TILE, MMA>::bytes,
@@ -2500,10 +2611,14 @@ void stage_patch(const StageArgs &a, cudaStream_t s) {
 // and of the patch kernel with its volume term on the tensor cores:
 //  12: 128 elements, <= 128 registers
 //  13: 128 elements, sized for 5 CTAs per SM
+// and of the persistent tile kernel (one wave of resident CTAs looping over
+// the tiles of the mesh or of the batch's work list):
+//  14: 128 elements, <= 128 registers
+//  15: 256 elements, <= 128 registers
 constexpr int kTileShapes = kTileShapeCount;
 constexpr int kTileElements[kTileShapes] = {128, 128, 256, 64, 64, 96, 128, 128,
-                                            128, 128, 64, 64, 128, 128};
-constexpr int kFirstPatchShape = 8;
+                                            128, 128, 64, 64, 128, 128, 128, 256};
+constexpr int kFirstPatchShape = 8, kPatchShapeEnd = 14;
 
 template <int P, int R> struct StageTile {
   static void run(int shape, const StageArgs &a, cudaStream_t s) {
@@ -2522,6 +2637,8 @@ template <int P, int R> struct StageTile {
     case 11: stage_patch<P, R, 64, 10>(a, s); break;
     case 12: stage_patch<P, R, 128, 4, true>(a, s); break;
     case 13: stage_patch<P, R, 128, 5, true>(a, s); break;
+    case 14: stage_tile_persistent<P, R, 128, 4>(a, s); break;
+    case 15: stage_tile_persistent<P, R, 256, 2>(a, s); break;
     default: throw std::invalid_argument("tile kernel: unknown launch shape");
     }
   }
@@ -2543,6 +2660,8 @@ template <int P, int R> struct PrepareTile {
     patch_opt_in<P, R, 64, 10, false>();
     patch_opt_in<P, R, 128, 4, true>();
     patch_opt_in<P, R, 128, 5, true>();
+    persistent_prepare<P, R, 128, 4>();
+    persistent_prepare<P, R, 256, 2>();
   }
 };
 
@@ -2605,7 +2724,7 @@ int euler_tri_tile_elements(int shape) {
   return shape >= 0 && shape < kTileShapes ? kTileElements[shape] : 0;
 }
 
-bool euler_tri_tile_is_patch(int shape) { return shape >= kFirstPatchShape && shape < kTileShapes; }
+bool euler_tri_tile_is_patch(int shape) { return shape >= kFirstPatchShape && shape < kPatchShapeEnd; }
 
 
 

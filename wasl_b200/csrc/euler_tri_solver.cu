@@ -700,11 +700,13 @@ private:
     // whose second pass evaluates faces at discontinuities in FP64, competes;
     // the patch kernel's shapes only where its edge arrays were built.
     const int base = tile_ok_ && limiting_ ? 1 : 0;
-    int shapes = 0;
-    for (int sh = 0; sh < euler_tri_tile_shapes(); ++sh)
-      if (!euler_tri_tile_is_patch(sh) || patch_ok_)
-        shapes = sh + 1;
-    const int variants = tile_ok_ ? 1 + shapes - base : 1;
+    std::vector<int> kernels; // kernel_ values: 0 face-centric, 1 + shape
+    if (!base)
+      kernels.push_back(0);
+    if (tile_ok_)
+      for (int sh = 0; sh < euler_tri_tile_shapes(); ++sh)
+        if (!euler_tri_tile_is_patch(sh) || patch_ok_)
+          kernels.push_back(1 + sh);
     // Each variant runs the three stages of a step on the current state, into
     // the stage buffers only (the last stage writes the first stage buffer
     // instead of u^n), so the stages that also read u^n weigh in.
@@ -718,8 +720,9 @@ private:
                             std::to_string(cfg_.volume_rule_order ? cfg_.volume_rule_order : p_ + 2) +
                             "/bnd" + std::to_string(boundary_count_ > 0 ? boundary_ : -1) +
                             "/size" + std::to_string(size_class(ne_));
-    tuning_ = autotune(key + (base ? "/tile-only" : ""), variants, [&](int i) {
-      kernel_ = i + base;
+    const TuneResult timed = autotune(key + (base ? "/tile-only" : ""),
+                                      static_cast<int>(kernels.size()), [&](int i) {
+      kernel_ = kernels[i];
       for (int k = 0; k < 3; ++k) {
         a.stage = k;
         a.in = ins[k];
@@ -727,11 +730,11 @@ private:
         launch_mixed(a);
       }
     }, stream_);
-    for (double &ms : tuning_.ms)
-      ms /= 3.0; // per stage
-    if (base)
-      tuning_.ms.insert(tuning_.ms.begin(), 0.0); // face-centric: not timed
-    kernel_ = tuning_.choice + base;
+    // Per stage, by kernel value (0 for the variants not timed).
+    tuning_.ms.assign(1 + euler_tri_tile_shapes(), 0.0);
+    for (std::size_t i = 0; i < kernels.size(); ++i)
+      tuning_.ms[kernels[i]] = timed.ms[i] / 3.0;
+    kernel_ = kernels[timed.choice];
     tuning_.choice = kernel_;
   }
 

@@ -307,7 +307,7 @@ void launch_batch_speed(const double *state, std::int64_t ne, int M, double gamm
                         unsigned long long *error, int *status, cudaStream_t stream);
 // Number of launch shapes of the tile kernels (euler_tri_tile_shapes()
 // returns it; per-shape host arrays are sized by it).
-constexpr int kTileShapeCount = 14;
+constexpr int kTileShapeCount = 16;
 int euler_tri_tile_shapes();
 int euler_tri_tile_elements(int shape);
 // Shapes of the patch kernel (StageArgs::patch; no rough pass, so runs

@@ -319,7 +319,8 @@ __global__ void __launch_bounds__(128) mlp_indicator_kernel(const MlpIndicatorAr
     counts[t] = 0;
   const float b3 = P[a.shape.b3];
   const IndicatorRecord *records = reinterpret_cast<const IndicatorRecord *>(a.records);
-  const int H = a.M - 1;
+  constexpr int H = KF == 1 ? 2 : KF == 2 ? 5 : 9; // high modes per element (P1, P2, P3)
+  static_assert(4 * H + 3 <= F, "features do not fit the row");
   const int warp = t >> 5, lane = t & 31, g = lane >> 2, q = lane & 3;
   const std::int64_t tiles = (a.ne + 127) / 128;
   for (std::int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
@@ -327,27 +328,40 @@ __global__ void __launch_bounds__(128) mlp_indicator_kernel(const MlpIndicatorAr
     const bool active = e < a.ne;
     bool reference = false;
     {
-      __nv_bfloat16 *x = X + t * ROW;
-      const __nv_bfloat16 zero = __float2bfloat16_rn(0.0f);
-      for (int i = 0; i < F; ++i)
-        x[i] = zero;
+      // The row in registers (zero padded), then 16-byte stores: a row is
+      // (F + 8) x 2 bytes, a multiple of 16, and eight consecutive rows fill
+      // distinct 16-byte bank groups.
+      union {
+        uint4 v[F / 8];
+        __nv_bfloat16 h[F];
+      } row;
+#pragma unroll
+      for (int k = 0; k < F / 8; ++k)
+        row.v[k] = make_uint4(0u, 0u, 0u, 0u);
       if (active) {
         const IndicatorRecord own = records[e];
         reference = own.reference;
         const double inv = own.mean != 0.0 ? 1.0 / own.mean : 0.0;
+#pragma unroll
         for (int m = 0; m < H; ++m)
-          x[m] = own.high[m];
+          row.h[m] = own.high[m];
+#pragma unroll
         for (int j = 0; j < 3; ++j) {
           const std::int32_t nb = a.neighbors[e * 3 + j];
           if (nb < 0)
             continue;
           const IndicatorRecord n = records[nb];
+#pragma unroll
           for (int m = 0; m < H; ++m)
-            x[(j + 1) * H + m] = n.high[m];
-          x[4 * H + j] = __float2bfloat16_rn(
+            row.h[(j + 1) * H + m] = n.high[m];
+          row.h[4 * H + j] = __float2bfloat16_rn(
               clamp8(static_cast<float>(__dadd_rn(__dmul_rn(n.mean, inv), -1.0))));
         }
       }
+      uint4 *dst = reinterpret_cast<uint4 *>(X + t * ROW);
+#pragma unroll
+      for (int k = 0; k < F / 8; ++k)
+        dst[k] = row.v[k];
     }
     __syncthreads(); // rows built (and, the first time, the network loaded)
 
@@ -529,17 +543,29 @@ void launch_mlp_indicator(const MlpIndicatorArgs &a, cudaStream_t s) {
   if (!a.records)
     throw std::invalid_argument("indicator network: no record scratch");
   mlp_records_kernel<<<static_cast<unsigned>((a.ne + 127) / 128), 128, 0, s>>>(a);
-  // Persistent CTAs, a few per SM, each loading the network once.
-  int device = 0, sms = 148;
+  const int KF = a.shape.features / 16;
+  if (KF < 1 || KF > 3 || a.M != (KF == 1 ? 3 : KF == 2 ? 6 : 10))
+    throw std::invalid_argument("indicator network: unsupported feature count");
+  // Persistent CTAs, every one resident at once, each loading the network once.
+  const void *kernel = KF == 1   ? reinterpret_cast<const void *>(mlp_indicator_kernel<1>)
+                       : KF == 2 ? reinterpret_cast<const void *>(mlp_indicator_kernel<2>)
+                                 : reinterpret_cast<const void *>(mlp_indicator_kernel<3>);
+  static int resident[64][4] = {};
+  int device = 0;
   cudaGetDevice(&device);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  int &slots = resident[device & 63][KF];
+  if (!slots) {
+    int per_sm = 0, sms = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, 0);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    slots = std::max(1, per_sm) * std::max(1, sms);
+  }
   const std::int64_t tiles = (a.ne + 127) / 128;
-  const unsigned blocks = static_cast<unsigned>(std::min<std::int64_t>(tiles, 4LL * sms));
-  switch (a.shape.features / 16) {
+  const unsigned blocks = static_cast<unsigned>(std::min<std::int64_t>(tiles, slots));
+  switch (KF) {
   case 1: mlp_indicator_kernel<1><<<blocks, 128, 0, s>>>(a); break;
   case 2: mlp_indicator_kernel<2><<<blocks, 128, 0, s>>>(a); break;
-  case 3: mlp_indicator_kernel<3><<<blocks, 128, 0, s>>>(a); break;
-  default: throw std::invalid_argument("indicator network: unsupported feature count");
+  default: mlp_indicator_kernel<3><<<blocks, 128, 0, s>>>(a); break;
   }
 }
 
