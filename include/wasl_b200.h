@@ -361,6 +361,12 @@ int wasl_gpu_indicator_features(const wasl_gpu *handle, int *features);
  * sensor's flags [element] (training data). */
 int wasl_gpu_indicator_data(wasl_gpu *handle, float *features, uint8_t *labels, int64_t count);
 
+/* The learned indicator's inference kernel: 0 (the default) the tcgen05
+ * tensor cores (single-CTA MMAs of 128 rows, accumulators in TMEM), 1 the
+ * warp-level mma.sync kernel; both give the same decisions up to the FP32
+ * rounding of the accumulation order.  No counterpart in the reference. */
+int wasl_gpu_indicator_kernel(wasl_gpu *handle, int kernel);
+
 /* Use the network with FP32 weights (wasl_mlp_get_weights layout) and the
  * confidence band (lo, hi) handed to the reference sensor (lo < 0 and hi > 1:
  * every cell falls back, which reproduces the reference sensor exactly). */

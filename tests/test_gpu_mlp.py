@@ -60,11 +60,13 @@ def test_training_learns_a_separable_rule():
     assert accuracy > 0.95
 
 
+@pytest.mark.parametrize("kernel", ["tcgen05", "mma.sync"])
 @pytest.mark.parametrize("p", [1, 2, 3])
-def test_features_labels_and_inference_match_oracle(p, oracle):
-    """Features and reference labels of a state, and the tensor-core
-    inference kernel's logits (BF16 MMAs, FP32 accumulation) against the
-    oracle's network on the oracle's features."""
+def test_features_labels_and_inference_match_oracle(p, kernel, oracle):
+    """Features and reference labels of a state, and each tensor-core
+    inference kernel's logits (BF16 MMAs, FP32 accumulation: tcgen05 with
+    TMEM accumulators, and warp-level mma.sync) against the oracle's network
+    on the oracle's features."""
     arrays = meshgen.jittered_box(10, jitter=0.15, seed=p)
     with wasl_b200.Solver(*arrays, polynomial_order=p, limiting=True) as g:
         state = seeded_state(g.elements, p, 50 + p, amplitude=0.05)
@@ -74,6 +76,7 @@ def test_features_labels_and_inference_match_oracle(p, oracle):
         with wasl_b200.Mlp(F, seed=p) as net:
             w = net.weights()
         g.set_indicator(w, lo=0.1, hi=0.9)
+        g.set_indicator_kernel(kernel)
         z = g.indicator_logits()
     mesh = oracle.tri_mesh(*arrays)
     donors, _ = mesh.periodic_trace(p)
@@ -116,3 +119,22 @@ def test_fallback_band_reproduces_the_reference_sensor(precision):
     assert stats["fallback"] == 5 * 3 * len(arrays[2])
     assert stats["missed"] == 0 and stats["false"] == 0
     assert stats["reference_troubled"] > 0
+
+
+def test_inference_kernels_agree_on_a_large_mesh():
+    """The tcgen05 and mma.sync inference kernels on 65k elements (many
+    persistent tiles per CTA): logits within FP32 accumulation-order rounding
+    of each other, and the same decisions away from the band's edges."""
+    arrays = meshgen.jittered_box(160, jitter=0.15, seed=9)
+    with wasl_b200.Solver(*arrays, polynomial_order=3, limiting=True) as g:
+        g.set_state(seeded_state(g.elements, 3, 77, amplitude=0.05))
+        with wasl_b200.Mlp(g.indicator_features(), seed=3) as net:
+            g.set_indicator(net.weights(), lo=0.1, hi=0.9)
+        z = {}
+        for kernel in ("tcgen05", "mma.sync"):
+            g.set_indicator_kernel(kernel)
+            z[kernel] = g.indicator_logits()
+    a, b = z["tcgen05"], z["mma.sync"]
+    assert np.all(np.isfinite(a)) and np.std(a) > 0
+    assert np.max(np.abs(a - b)) <= 1e-2 * (1.0 + np.max(np.abs(b)))
+    assert np.mean(np.abs(a - b) <= 1e-3 * (1.0 + np.abs(b))) >= 0.99

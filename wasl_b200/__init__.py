@@ -152,6 +152,7 @@ SIGNATURES = {
     "wasl_gpu_indicator_features": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "wasl_gpu_indicator_data": (C.c_int, [C.c_void_p, _f, _u8, C.c_int64]),
     "wasl_gpu_set_indicator": (C.c_int, [C.c_void_p, _f, C.c_int64, C.c_double, C.c_double]),
+    "wasl_gpu_indicator_kernel": (C.c_int, [C.c_void_p, C.c_int]),
     "wasl_gpu_indicator_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.c_int]),
     "wasl_gpu_indicator_logits": (C.c_int, [C.c_void_p, _f, C.c_int64]),
     "wasl_mlp_create": (C.c_int, [C.c_int, C.c_uint64, C.c_int, C.POINTER(C.c_void_p),
@@ -496,6 +497,11 @@ class Solver:
     def set_indicator(self, weights, lo=0.1, hi=0.9):
         w = np.ascontiguousarray(weights, dtype=np.float32)
         self._check(self._lib.wasl_gpu_set_indicator(self._h, _ptr(w, _f), w.size, lo, hi))
+
+    def set_indicator_kernel(self, kernel="tcgen05"):
+        """The inference kernel: "tcgen05" (default) or "mma.sync"."""
+        self._check(self._lib.wasl_gpu_indicator_kernel(
+            self._h, {"tcgen05": 0, "mma.sync": 1}[kernel]))
 
     def indicator_logits(self):
         z = np.empty(self.elements, dtype=np.float32)

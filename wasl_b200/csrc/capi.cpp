@@ -484,6 +484,10 @@ int wasl_gpu_indicator_data(wasl_gpu *h, float *features, uint8_t *labels, int64
   });
 }
 
+int wasl_gpu_indicator_kernel(wasl_gpu *h, int kernel) {
+  return guarded(h, [&] { h->solver->set_indicator_kernel(kernel); });
+}
+
 int wasl_gpu_set_indicator(wasl_gpu *h, const float *weights, int64_t count, double lo,
                            double hi) {
   return guarded(h, [&] {

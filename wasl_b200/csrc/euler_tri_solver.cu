@@ -44,6 +44,8 @@ void throw_device_error(unsigned long long word) {
   if (code == 4)
     throw SolverError(WASL_ERR_RUNTIME, "device index check: element index " +
                                             std::to_string(element) + " out of range");
+  if (code == 5)
+    throw SolverError(WASL_ERR_CUDA, "learned indicator: a tensor-core wait ran out");
   throw SolverError(WASL_ERR_FLOOR, "Euler positivity limiter: cell average is below a floor"
                                     " (element " + std::to_string(element) + ")");
 }
@@ -525,6 +527,8 @@ public:
     m.troubled_count = list.get() + ne_;
     m.logits = z.get();
     m.records = d_mlp_records_.get();
+    m.error = d_error_.get();
+    m.kernel = mlp_kernel_;
     launch_mlp_indicator(m, stream_);
     std::vector<float> zs(relabel_ ? ne_ : 0);
     cuda_check(cudaMemcpyAsync(relabel_ ? zs.data() : logits, z.get(), sizeof(float) * ne_,
@@ -534,6 +538,13 @@ public:
     if (relabel_)
       for (std::int64_t i = 0; i < ne_; ++i)
         logits[order_[i]] = zs[i];
+  }
+
+  void set_indicator_kernel(int kernel) override {
+    if (kernel != 0 && kernel != 1)
+      throw SolverError(WASL_ERR_ARGUMENT, "learned indicator: kernel must be 0 (tcgen05) or 1"
+                                           " (mma.sync)");
+    mlp_kernel_ = kernel;
   }
 
   void indicator_stats(unsigned long long *stats, bool reset) override {
@@ -670,6 +681,8 @@ private:
         m.troubled_count = d_count_.get();
         m.stats = d_mlp_stats_.get();
         m.records = d_mlp_records_.get();
+        m.error = d_error_.get();
+        m.kernel = mlp_kernel_;
         launch_mlp_indicator(m, stream_);
         count_launches(2);
       }
@@ -834,6 +847,7 @@ private:
   DeviceArray<unsigned long long> d_mlp_stats_;
   DeviceArray<unsigned char> d_mlp_records_; // per-element inference records
   double mlp_lo_ = 0.1, mlp_hi_ = 0.9;
+  int mlp_kernel_ = 0; // inference: 0 tcgen05 MMAs, 1 mma.sync
   DeviceArray<std::uint8_t> d_tile_code_;
   DeviceArray<float> d_basis32_;
   double length_ = 0.0;

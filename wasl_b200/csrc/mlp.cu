@@ -284,6 +284,191 @@ __global__ void __launch_bounds__(128) mlp_records_kernel(const MlpIndicatorArgs
   reinterpret_cast<IndicatorRecord *>(a.records)[e] = r;
 }
 
+// ---- the fifth-generation tensor cores (tcgen05), for the inference kernel ----
+//
+// Operands in shared memory in the canonical K-major layout without swizzle:
+// 8 x 8 BF16 core matrices of 128 contiguous bytes (8 rows of 16 bytes), the
+// core matrices of one 8-row group consecutive along K.  Element (r, k) of a
+// rows x K operand sits at byte umma_offset(r, k, K).  The matrix descriptor
+// gives the start address, the byte step between core matrices along K
+// (leading byte offset, 128) and between 8-row groups (stride byte offset,
+// K / 8 x 128), all in 16-byte units, with the descriptor version of this
+// architecture (bit 46) and no swizzle.
+__device__ __forceinline__ unsigned umma_offset(int r, int k, int K) {
+  return static_cast<unsigned>(((r >> 3) * (K >> 3) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ unsigned long long umma_desc(unsigned smem_address, int K) {
+  const unsigned long long lbo = 128 >> 4, sbo = static_cast<unsigned long long>((K >> 3) * 128) >> 4;
+  return static_cast<unsigned long long>((smem_address >> 4) & 0x3FFFu) | (lbo << 16) |
+         (sbo << 32) | (1ULL << 46);
+}
+
+// Instruction descriptor of kind::f16: BF16 A and B (both K-major), FP32
+// accumulator, M = 128 rows, N = 64 columns.
+constexpr unsigned kUmmaIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) |
+                                ((128u >> 4) << 24);
+
+// D (TMEM) (+)= A B^T for one K = 16 step; issued by one thread.
+__device__ __forceinline__ void umma_bf16(unsigned d_tmem, unsigned long long a_desc,
+                                          unsigned long long b_desc, bool accumulate) {
+  asm volatile("{\n\t.reg .pred p;\n\t"
+               "setp.ne.b32 p, %4, 0;\n\t"
+               "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+               :
+               : "r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(kUmmaIdesc),
+                 "r"(accumulate ? 1u : 0u)
+               : "memory");
+}
+
+// The MMAs issued so far by this thread arrive on the mbarrier when done.
+__device__ __forceinline__ void umma_commit(unsigned mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+               ::"r"(mbar)
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_fence_before_sync() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_fence_after_sync() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// Plain shared-memory stores made visible to the tensor cores' reads.
+__device__ __forceinline__ void fence_async_shared() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Waits until the mbarrier's phase of the given parity has completed, for at
+// most about `cycles` SM clocks; false when it gave up.
+__device__ __forceinline__ bool mbar_wait(unsigned mbar, unsigned parity, long long cycles) {
+  const long long start = clock64();
+  for (;;) {
+    unsigned done = 0;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.b32 %0, 1, 0, p;\n\t}"
+                 : "=r"(done)
+                 : "r"(mbar), "r"(parity)
+                 : "memory");
+    if (done)
+      return true;
+    if (clock64() - start > cycles)
+      return false;
+  }
+}
+
+// This thread's TMEM lane, 64 consecutive 32-bit columns from taddr (the
+// load and its wait in one statement: the registers are defined after both).
+__device__ __forceinline__ void tmem_load64(unsigned taddr, float (&v)[64]) {
+  unsigned r[64];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x64.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, "
+      "%32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, "
+      "%48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
+        "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]),
+        "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]),
+        "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]),
+        "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]),
+        "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]),
+        "=r"(r[62]), "=r"(r[63])
+      : "r"(taddr)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 64; ++i)
+    v[i] = __uint_as_float(r[i]);
+}
+
+// One element's network input row (BF16, zero padded to F values) from its
+// own record and its three neighbours': its high modes, each neighbour's,
+// then each neighbour's mean over its own minus 1; returns the element's
+// reference decision.  H: high modes per element (P1, P2, P3 by F / 16).
+template <int F> union IndicatorRow {
+  uint4 v[F / 8];
+  __nv_bfloat16 h[F];
+};
+
+template <int KF>
+__device__ __forceinline__ bool indicator_row(const MlpIndicatorArgs &a, std::int64_t e,
+                                              bool active, IndicatorRow<KF * 16> &row) {
+  constexpr int F = KF * 16, H = KF == 1 ? 2 : KF == 2 ? 5 : 9;
+  static_assert(4 * H + 3 <= F, "features do not fit the row");
+  const IndicatorRecord *records = reinterpret_cast<const IndicatorRecord *>(a.records);
+#pragma unroll
+  for (int k = 0; k < F / 8; ++k)
+    row.v[k] = make_uint4(0u, 0u, 0u, 0u);
+  if (!active)
+    return false;
+  const IndicatorRecord own = records[e];
+  const double inv = own.mean != 0.0 ? 1.0 / own.mean : 0.0;
+#pragma unroll
+  for (int m = 0; m < H; ++m)
+    row.h[m] = own.high[m];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const std::int32_t nb = a.neighbors[e * 3 + j];
+    if (nb < 0)
+      continue;
+    const IndicatorRecord n = records[nb];
+#pragma unroll
+    for (int m = 0; m < H; ++m)
+      row.h[(j + 1) * H + m] = n.high[m];
+    row.h[4 * H + j] = __float2bfloat16_rn(
+        clamp8(static_cast<float>(__dadd_rn(__dmul_rn(n.mean, inv), -1.0))));
+  }
+  return own.reference;
+}
+
+// The decision for element e from its logit: troubled when sigmoid(logit) >=
+// hi, smooth when <= lo, else the reference decision; the flag, the
+// compacted troubled list (one atomic per warp) and the CTA's counters.
+__device__ __forceinline__ void indicator_decide(const MlpIndicatorArgs &a, std::int64_t e,
+                                                 float logit, bool reference,
+                                                 unsigned long long *counts, int lane) {
+  const float p = 1.0f / (1.0f + expf(-logit));
+  bool troubled;
+  int kind;
+  if (p >= a.hi) {
+    troubled = true;
+    kind = 0;
+  } else if (p <= a.lo) {
+    troubled = false;
+    kind = 1;
+  } else {
+    troubled = reference;
+    kind = 2;
+  }
+  if (a.logits)
+    a.logits[e] = logit;
+  a.flags[e] = troubled ? 1 : 0;
+  atomicAdd(&counts[kind], 1ULL);
+  if (reference)
+    atomicAdd(&counts[3], 1ULL);
+  if (reference && !troubled)
+    atomicAdd(&counts[4], 1ULL);
+  if (!reference && troubled)
+    atomicAdd(&counts[5], 1ULL);
+  const unsigned mask = __activemask();
+  const unsigned ballot = __ballot_sync(mask, troubled);
+  if (ballot) {
+    const int leader = __ffs(ballot) - 1;
+    int base = 0;
+    if (lane == leader)
+      base = atomicAdd(a.troubled_count, __popc(ballot));
+    base = __shfl_sync(mask, base, leader);
+    if (troubled)
+      a.troubled[base + __popc(ballot & ((1u << lane) - 1u))] = static_cast<std::int32_t>(e);
+  }
+}
+
 // A persistent kernel: each CTA of 128 threads loads the network once (BF16
 // in shared memory) and then takes 128-element tiles in turn.  Per tile, each
 // thread builds its element's input row (BF16, shared memory) from the
@@ -318,9 +503,6 @@ __global__ void __launch_bounds__(128) mlp_indicator_kernel(const MlpIndicatorAr
   if (t < 6)
     counts[t] = 0;
   const float b3 = P[a.shape.b3];
-  const IndicatorRecord *records = reinterpret_cast<const IndicatorRecord *>(a.records);
-  constexpr int H = KF == 1 ? 2 : KF == 2 ? 5 : 9; // high modes per element (P1, P2, P3)
-  static_assert(4 * H + 3 <= F, "features do not fit the row");
   const int warp = t >> 5, lane = t & 31, g = lane >> 2, q = lane & 3;
   const std::int64_t tiles = (a.ne + 127) / 128;
   for (std::int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
@@ -331,33 +513,8 @@ __global__ void __launch_bounds__(128) mlp_indicator_kernel(const MlpIndicatorAr
       // The row in registers (zero padded), then 16-byte stores: a row is
       // (F + 8) x 2 bytes, a multiple of 16, and eight consecutive rows fill
       // distinct 16-byte bank groups.
-      union {
-        uint4 v[F / 8];
-        __nv_bfloat16 h[F];
-      } row;
-#pragma unroll
-      for (int k = 0; k < F / 8; ++k)
-        row.v[k] = make_uint4(0u, 0u, 0u, 0u);
-      if (active) {
-        const IndicatorRecord own = records[e];
-        reference = own.reference;
-        const double inv = own.mean != 0.0 ? 1.0 / own.mean : 0.0;
-#pragma unroll
-        for (int m = 0; m < H; ++m)
-          row.h[m] = own.high[m];
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-          const std::int32_t nb = a.neighbors[e * 3 + j];
-          if (nb < 0)
-            continue;
-          const IndicatorRecord n = records[nb];
-#pragma unroll
-          for (int m = 0; m < H; ++m)
-            row.h[(j + 1) * H + m] = n.high[m];
-          row.h[4 * H + j] = __float2bfloat16_rn(
-              clamp8(static_cast<float>(__dadd_rn(__dmul_rn(n.mean, inv), -1.0))));
-        }
-      }
+      IndicatorRow<F> row;
+      reference = indicator_row<KF>(a, e, active, row);
       uint4 *dst = reinterpret_cast<uint4 *>(X + t * ROW);
 #pragma unroll
       for (int k = 0; k < F / 8; ++k)
@@ -427,46 +584,155 @@ __global__ void __launch_bounds__(128) mlp_indicator_kernel(const MlpIndicatorAr
     }
     __syncthreads(); // logits written; the next tile's rows may overwrite X
 
-    if (active) {
-      const float p = 1.0f / (1.0f + expf(-logit[t]));
-      bool troubled;
-      int kind;
-      if (p >= a.hi) {
-        troubled = true;
-        kind = 0;
-      } else if (p <= a.lo) {
-        troubled = false;
-        kind = 1;
-      } else {
-        troubled = reference;
-        kind = 2;
-      }
-      if (a.logits)
-        a.logits[e] = logit[t];
-      a.flags[e] = troubled ? 1 : 0;
-      atomicAdd(&counts[kind], 1ULL);
-      if (reference)
-        atomicAdd(&counts[3], 1ULL);
-      if (reference && !troubled)
-        atomicAdd(&counts[4], 1ULL);
-      if (!reference && troubled)
-        atomicAdd(&counts[5], 1ULL);
-      const unsigned mask = __activemask();
-      const unsigned ballot = __ballot_sync(mask, troubled);
-      if (ballot) {
-        const int leader = __ffs(ballot) - 1;
-        int base = 0;
-        if (lane == leader)
-          base = atomicAdd(a.troubled_count, __popc(ballot));
-        base = __shfl_sync(mask, base, leader);
-        if (troubled)
-          a.troubled[base + __popc(ballot & ((1u << lane) - 1u))] = static_cast<std::int32_t>(e);
-      }
-    }
+    if (active)
+      indicator_decide(a, e, logit[t], reference, counts, lane);
     // The logits of this tile are read above before the next tile's MMAs
     // write them: those come after the next tile's first barrier.
   }
   __syncthreads();
+  if (t < 6 && a.stats && counts[t])
+    atomicAdd(a.stats + t, counts[t]);
+}
+
+// The inference on the fifth-generation tensor cores: the persistent kernel's
+// work per 128-element tile, with the two hidden layers as single-CTA
+// tcgen05 MMAs (M = 128 rows, N = 64, K = F then 64; BF16 operands in shared
+// memory, FP32 accumulators in 64 TMEM columns).  One thread issues the MMAs
+// and commits them to an mbarrier; every thread then reads its own row (its
+// TMEM lane) with tcgen05.ld, adds the bias and applies ReLU; layer 1's BF16
+// activations become layer 2's A operand in shared memory, and the last
+// layer is each thread's dot product over its row.  Waits on the mbarrier
+// are bounded (about a second of SM clock): a wait that runs out records
+// kIndicatorWait in the error word, the CTA leaves its loop, waits once more
+// (bounded) for the MMAs it issued and frees its TMEM.
+template <int KF>
+__global__ void __launch_bounds__(128) mlp_indicator_tc_kernel(const MlpIndicatorArgs a) {
+  constexpr int Hd = kMlpHidden, F = KF * 16;
+  __shared__ __align__(1024) __nv_bfloat16 A[128 * Hd]; // the rows (K = F), then layer 1's output
+  __shared__ __align__(1024) __nv_bfloat16 W1[Hd * F];
+  __shared__ __align__(1024) __nv_bfloat16 W2[Hd * Hd];
+  __shared__ float b1[Hd], b2[Hd], w3[Hd];
+  __shared__ unsigned long long counts[6];
+  __shared__ __align__(8) unsigned long long mbar;
+  __shared__ unsigned tmem_base;
+  __shared__ int failed; // 0, or 1 + the parity of the wait that ran out
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const float *P = a.params;
+  unsigned char *a_bytes = reinterpret_cast<unsigned char *>(A);
+  unsigned char *w1_bytes = reinterpret_cast<unsigned char *>(W1);
+  unsigned char *w2_bytes = reinterpret_cast<unsigned char *>(W2);
+  for (int i = t; i < Hd * F; i += 128)
+    *reinterpret_cast<__nv_bfloat16 *>(w1_bytes + umma_offset(i / F, i % F, F)) =
+        __float2bfloat16_rn(P[a.shape.w1 + i]);
+  for (int i = t; i < Hd * Hd; i += 128)
+    *reinterpret_cast<__nv_bfloat16 *>(w2_bytes + umma_offset(i / Hd, i % Hd, Hd)) =
+        __float2bfloat16_rn(P[a.shape.w2 + i]);
+  for (int i = t; i < Hd; i += 128) {
+    b1[i] = P[a.shape.b1 + i];
+    b2[i] = P[a.shape.b2 + i];
+    w3[i] = bf16_round(P[a.shape.w3 + i]);
+  }
+  if (t < 6)
+    counts[t] = 0;
+  const unsigned bar = static_cast<unsigned>(__cvta_generic_to_shared(&mbar));
+  if (t == 0) {
+    failed = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    const unsigned slot = static_cast<unsigned>(__cvta_generic_to_shared(&tmem_base));
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;" ::"r"(slot)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_async_shared(); // the weights, for the tensor cores
+  tmem_fence_before_sync();
+  __syncthreads();
+  tmem_fence_after_sync();
+  const unsigned tmem = tmem_base;
+  const unsigned my_lanes = tmem + (static_cast<unsigned>(warp * 32) << 16);
+  const unsigned a_addr = static_cast<unsigned>(__cvta_generic_to_shared(A));
+  const unsigned w1_addr = static_cast<unsigned>(__cvta_generic_to_shared(W1));
+  const unsigned w2_addr = static_cast<unsigned>(__cvta_generic_to_shared(W2));
+  const float b3 = P[a.shape.b3];
+  constexpr long long kWaitCycles = 1LL << 31;
+  const std::int64_t tiles = (a.ne + 127) / 128;
+  for (std::int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const std::int64_t e = tile * 128 + t;
+    const bool active = e < a.ne;
+    bool reference;
+    {
+      IndicatorRow<F> row;
+      reference = indicator_row<KF>(a, e, active, row);
+#pragma unroll
+      for (int c = 0; c < F / 8; ++c)
+        *reinterpret_cast<uint4 *>(a_bytes + umma_offset(t, 8 * c, F)) = row.v[c];
+    }
+    fence_async_shared();
+    tmem_fence_before_sync();
+    __syncthreads(); // rows in place; last tile's TMEM reads done
+    if (t == 0) {
+      tmem_fence_after_sync();
+#pragma unroll
+      for (int k = 0; k < KF; ++k)
+        umma_bf16(tmem, umma_desc(a_addr + 256 * k, F), umma_desc(w1_addr + 256 * k, F), k > 0);
+      umma_commit(bar);
+    }
+    if (!mbar_wait(bar, 0, kWaitCycles))
+      atomicCAS(&failed, 0, 1);
+    __syncthreads();
+    if (failed)
+      break;
+    tmem_fence_after_sync();
+    float v[64];
+    tmem_load64(my_lanes, v);
+#pragma unroll
+    for (int c = 0; c < Hd / 8; ++c) {
+      uint4 packed;
+      unsigned *u = reinterpret_cast<unsigned *>(&packed);
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        u[j] = pack_bf16(fmaxf(v[8 * c + 2 * j] + b1[8 * c + 2 * j], 0.0f),
+                         fmaxf(v[8 * c + 2 * j + 1] + b1[8 * c + 2 * j + 1], 0.0f));
+      *reinterpret_cast<uint4 *>(a_bytes + umma_offset(t, 8 * c, Hd)) = packed;
+    }
+    fence_async_shared();
+    tmem_fence_before_sync();
+    __syncthreads(); // layer 1's activations in place; its TMEM reads done
+    if (t == 0) {
+      tmem_fence_after_sync();
+#pragma unroll
+      for (int k = 0; k < Hd / 16; ++k)
+        umma_bf16(tmem, umma_desc(a_addr + 256 * k, Hd), umma_desc(w2_addr + 256 * k, Hd), k > 0);
+      umma_commit(bar);
+    }
+    if (!mbar_wait(bar, 1, kWaitCycles))
+      atomicCAS(&failed, 0, 2);
+    __syncthreads();
+    if (failed)
+      break;
+    tmem_fence_after_sync();
+    tmem_load64(my_lanes, v);
+    float z = 0.0f;
+#pragma unroll
+    for (int c = 0; c < Hd; ++c)
+      z = fmaf(w3[c], fmaxf(v[c] + b2[c], 0.0f), z);
+    if (active)
+      indicator_decide(a, e, z + b3, reference, counts, lane);
+  }
+  __syncthreads();
+  if (failed && t == 0) {
+    mbar_wait(bar, static_cast<unsigned>(failed - 1), kWaitCycles); // the MMAs still in flight
+    if (a.error)
+      atomicCAS(a.error, 0ULL, static_cast<unsigned long long>(kMlpWaitCode) << 56);
+  }
+  tmem_fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tmem_fence_after_sync();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" ::"r"(tmem) : "memory");
+  }
   if (t < 6 && a.stats && counts[t])
     atomicAdd(a.stats + t, counts[t]);
 }
@@ -546,26 +812,56 @@ void launch_mlp_indicator(const MlpIndicatorArgs &a, cudaStream_t s) {
   const int KF = a.shape.features / 16;
   if (KF < 1 || KF > 3 || a.M != (KF == 1 ? 3 : KF == 2 ? 6 : 10))
     throw std::invalid_argument("indicator network: unsupported feature count");
-  // Persistent CTAs, every one resident at once, each loading the network once.
-  const void *kernel = KF == 1   ? reinterpret_cast<const void *>(mlp_indicator_kernel<1>)
-                       : KF == 2 ? reinterpret_cast<const void *>(mlp_indicator_kernel<2>)
-                                 : reinterpret_cast<const void *>(mlp_indicator_kernel<3>);
-  static int resident[64][4] = {};
+  // Persistent CTAs, every one resident at once, each loading the network once
+  // (the tcgen05 kernel holds 64 TMEM columns, so at most 8 fit an SM).
+  const bool tc = a.kernel == 0;
+  const void *kernel =
+      tc ? (KF == 1   ? reinterpret_cast<const void *>(mlp_indicator_tc_kernel<1>)
+            : KF == 2 ? reinterpret_cast<const void *>(mlp_indicator_tc_kernel<2>)
+                      : reinterpret_cast<const void *>(mlp_indicator_tc_kernel<3>))
+         : (KF == 1   ? reinterpret_cast<const void *>(mlp_indicator_kernel<1>)
+            : KF == 2 ? reinterpret_cast<const void *>(mlp_indicator_kernel<2>)
+                      : reinterpret_cast<const void *>(mlp_indicator_kernel<3>));
+  static int resident[64][2][4] = {};
   int device = 0;
   cudaGetDevice(&device);
-  int &slots = resident[device & 63][KF];
+  int &slots = resident[device & 63][tc ? 0 : 1][KF];
   if (!slots) {
     int per_sm = 0, sms = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, 0);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (tc) {
+      // The occupancy calculator cannot see how much tensor memory a kernel
+      // allocates, and answers one CTA per SM; count the registers, the shared
+      // memory and the 64 TMEM columns (512 per SM) instead.
+      cudaFuncAttributes attr{};
+      int smem_sm = 0, reserved = 0;
+      cudaFuncGetAttributes(&attr, kernel);
+      cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device);
+      cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, device);
+      const int warp_regs = (attr.numRegs * 32 + 255) / 256 * 256;
+      const int by_regs = attr.numRegs > 0 ? 65536 / (4 * warp_regs) : 1;
+      const int by_smem =
+          static_cast<int>(smem_sm / (attr.sharedSizeBytes + static_cast<std::size_t>(reserved)));
+      per_sm = std::min({by_regs, by_smem, 512 / 64, 16});
+    } else {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, 0);
+    }
     slots = std::max(1, per_sm) * std::max(1, sms);
   }
   const std::int64_t tiles = (a.ne + 127) / 128;
   const unsigned blocks = static_cast<unsigned>(std::min<std::int64_t>(tiles, slots));
-  switch (KF) {
-  case 1: mlp_indicator_kernel<1><<<blocks, 128, 0, s>>>(a); break;
-  case 2: mlp_indicator_kernel<2><<<blocks, 128, 0, s>>>(a); break;
-  default: mlp_indicator_kernel<3><<<blocks, 128, 0, s>>>(a); break;
+  if (tc) {
+    switch (KF) {
+    case 1: mlp_indicator_tc_kernel<1><<<blocks, 128, 0, s>>>(a); break;
+    case 2: mlp_indicator_tc_kernel<2><<<blocks, 128, 0, s>>>(a); break;
+    default: mlp_indicator_tc_kernel<3><<<blocks, 128, 0, s>>>(a); break;
+    }
+  } else {
+    switch (KF) {
+    case 1: mlp_indicator_kernel<1><<<blocks, 128, 0, s>>>(a); break;
+    case 2: mlp_indicator_kernel<2><<<blocks, 128, 0, s>>>(a); break;
+    default: mlp_indicator_kernel<3><<<blocks, 128, 0, s>>>(a); break;
+    }
   }
 }
 

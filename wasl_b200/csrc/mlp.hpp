@@ -44,7 +44,12 @@ struct MlpIndicatorArgs {
   unsigned long long *stats = nullptr; // [6], see mlp_indicator_kernel
   float *logits = nullptr;             // optional [ne]
   void *records = nullptr;             // scratch, kMlpRecordBytes x ne
+  unsigned long long *error = nullptr; // the handle's error word (kMlpWaitCode)
+  int kernel = 0;                      // 0 tcgen05 MMAs, 1 mma.sync
 };
+
+// Error-word code of an inference kernel whose tensor-core wait ran out.
+constexpr int kMlpWaitCode = 5;
 
 // Bytes per element of the inference's per-element records.
 constexpr std::size_t kMlpRecordBytes = 32;

@@ -168,6 +168,11 @@ public:
     (void)weights, (void)count, (void)lo, (void)hi;
     throw SolverError(WASL_ERR_ARGUMENT, "learned indicator: 2D Euler with limiting only");
   }
+  // The inference kernel of the learned indicator: 0 tcgen05, 1 mma.sync.
+  virtual void set_indicator_kernel(int kernel) {
+    (void)kernel;
+    throw SolverError(WASL_ERR_ARGUMENT, "learned indicator: 2D Euler with limiting only");
+  }
   virtual int indicator_features() const { return 0; }
   virtual void indicator_data(float *features, std::uint8_t *labels) {
     (void)features, (void)labels;
