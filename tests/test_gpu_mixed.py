@@ -314,11 +314,65 @@ def test_patch_kernel_matches_face_centric(p, boundary):
         assert np.array_equal(out[k], out[10]), f"kernel {k}"
 
 
-def test_patch_kernel_needs_the_limiter_off():
+def test_tensor_core_patch_kernel_needs_the_limiter_off():
     arrays = meshgen.jittered_box(6, jitter=0.1, seed=2)
-    with pytest.raises(wasl_b200.WaslError, match="patch kernel"):
+    with pytest.raises(wasl_b200.WaslError, match="tensor-core volume"):
         wasl_b200.Solver(*arrays, polynomial_order=2, precision="mixed", limiting=True,
-                         mixed_kernel=PATCH_KERNELS[0])
+                         mixed_kernel=MMA_KERNELS[0])
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+@pytest.mark.parametrize("boundary", ["periodic", "transmissive"])
+def test_patch_kernel_with_the_limiter(p, boundary):
+    """With the limiter the patch kernel evaluates a face across a jump of
+    the cell means in FP64 from both sides (the tile kernels' islands) and
+    raises the sensor's flags.  On four-quadrant data it stays as close to
+    the plain FP64 path as the tile kernel does (the limiter's nonlinear
+    weights amplify FP32 rounding differences, so the two mixed kernels are
+    compared through the FP64 run), every patch shape agrees bit for bit,
+    and mass, momentum and energy stay conserved to FP64 round-off
+    (periodic)."""
+    arrays = meshgen.jittered_box(24, jitter=0.15, seed=110 + p)
+    problem = cases.QuadrantRiemann(seed=3)
+    out = {}
+    for k in [0, 2, 10, 11, 12, 13]:
+        precision = "plain" if k == 0 else "mixed"
+        kw = {} if k == 0 else {"mixed_kernel": k}
+        with wasl_b200.Solver(*arrays, polynomial_order=p, precision=precision, boundary=boundary,
+                              limiting=True, positivity_all=True, **kw) as g:
+            cases.project_initial(g, problem.conserved)
+            g.limit()
+            m0, e0 = g.mass_energy()
+            flagged = 0
+            for _ in range(4):
+                g.step(g.stable_dt(0.1))
+                flagged += int(g.flags().sum())
+            out[k] = g.get_state()
+            m1, e1 = g.mass_energy()
+            assert flagged > 0
+            if k:
+                assert g.tuning()[0] == k - 1
+            if boundary == "periodic":
+                assert abs(m1 - m0) <= 1e-13 * abs(m0) and abs(e1 - e0) <= 1e-13 * abs(e0)
+    tile = np.abs(out[2] - out[0])
+    patch = np.abs(out[10] - out[0])
+    assert np.mean(patch) <= 1.5 * np.mean(tile) + 1e-12
+    assert np.max(patch) <= 3.0 * np.max(tile) + 1e-12
+    for k in (11, 12, 13):
+        assert np.array_equal(out[k], out[10]), f"kernel {k}"
+
+
+def test_autotuner_includes_the_patch_kernel_with_the_limiter():
+    arrays = cases.vortex_mesh(24, seed=3)
+    vortex = cases.IsentropicVortex()
+    with wasl_b200.Solver(*arrays, polynomial_order=2, precision="mixed", limiting=True) as g:
+        cases.project_initial(g, vortex.conserved)
+        g.step(g.stable_dt(0.15))
+        choice, ms = g.tuning()
+    assert ms[0] == 0.0  # the face-centric kernels have no FP64 islands
+    assert all(ms[1 + sh] > 0 for sh in range(12))
+    assert ms[1 + 12] == 0.0 and ms[1 + 13] == 0.0  # tensor-core volume: no limiter
+    assert all(ms[1 + sh] > 0 for sh in (14, 15))
 
 
 @pytest.mark.parametrize("kernel,limiting", [(1, False), (2, False), (8, False), (10, False),

@@ -668,6 +668,7 @@ __device__ __noinline__ void face_fp64(double gamma, const double *own, std::int
   }
 }
 
+
 // The end of a tile kernel's stage for element e (thread t of the tile):
 // residual scaling by 1/det J, the Shu-Osher combination in FP64
 // (cpp/include/wasl/time/ssp_rk3.hpp:44-60), and, when asked for, the next
@@ -1986,7 +1987,7 @@ __device__ __forceinline__ void patch_finish(const StageArgs &a, std::int64_t e,
   }
 }
 
-template <int P, int R, int TILE, int MINB, bool MMA>
+template <int P, int R, int TILE, int MINB, bool MMA, bool ISLANDS>
 __global__ void __launch_bounds__(TILE, MINB) euler_tri_patch(const StageArgs a) {
   using S = TriShape<P>;
   using L = PatchSmem<P, R, TILE, MMA>;
@@ -2023,6 +2024,8 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_patch(const StageArgs a)
   const double *__restrict__ in = a.in;
   const double gamma = a.gamma;
   const PatchEdges pe = a.patch;
+  // ISLANDS (with the limiter): faces across jumps of the cell means in FP64.
+  constexpr bool islands = ISLANDS;
 
   {
     const float *src = reinterpret_cast<const float *>(&c_patch<P>);
@@ -2163,6 +2166,10 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_patch(const StageArgs a)
         for (int v = 0; v < 4; ++v)
           nmean[v] = __ldg(in + static_cast<std::int64_t>(v) * M * ne + nb) * phi0;
       }
+      // A face across a jump of the means is evaluated in FP64 by each of its
+      // elements in phase C (with the limiter): no record here.
+      if (islands && !boundary && mean_jump(nmean[0], mean[0], nmean[3], mean[3]))
+        return;
       // The face's left mean state: the reference of the perturbation form.
       MeanState ml;
       if (self_left || boundary)
@@ -2305,6 +2312,7 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_patch(const StageArgs a)
     const int jl = self_left ? j : jn; // the face's left local edge (its weights)
     // The face's flux perturbations in the face's point order: from this
     // element's record, or from its left neighbour's inside the patch.
+    // (An FP64 face overwrites these with its own values below.)
     float fq[QF][4];
     if (near && !self_left) {
 #pragma unroll
@@ -2321,20 +2329,62 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_patch(const StageArgs a)
           fq[q][v] = sedge[(j * QF + qs) * 4 + v][t];
       }
     }
+    // The face's left mean state; with islands, the neighbour's mean for the
+    // jump test as well.
     MeanState ml;
+    double nmean[4] = {0.0, 0.0, 0.0, 0.0};
+    if constexpr (ISLANDS) {
+      if (near) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+          nmean[v] = smean[v][local];
+      } else if (!boundary) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+          nmean[v] = __ldg(in + static_cast<std::int64_t>(v) * M * ne + nb) * phi0;
+      }
+    }
     if (self_left || boundary) {
       ml = own;
     } else if (near) {
       ml = patch_mean<P, TILE>(smean, sprim, static_cast<int>(local));
     } else {
-      double nmean[4];
+      if constexpr (!ISLANDS) {
 #pragma unroll
-      for (int v = 0; v < 4; ++v)
-        nmean[v] = __ldg(in + static_cast<std::int64_t>(v) * M * ne + nb) * phi0;
+        for (int v = 0; v < 4; ++v)
+          nmean[v] = __ldg(in + static_cast<std::int64_t>(v) * M * ne + nb) * phi0;
+      }
       ml = mean_state(gamma, nmean);
     }
     double fln[4];
     mean_normal_flux(ml, nx, ny, fln);
+    const bool fp64 = ISLANDS && !boundary &&
+                      mean_jump(nmean[0], smean[0][t], nmean[3], smean[3][t]);
+    double m0[4] = {0.0, 0.0, 0.0, 0.0};
+    if constexpr (ISLANDS) {
+      if (fp64) {
+        // The face in FP64 from both elements' coefficients, as the tile
+        // kernels' rough pass evaluates it (the same call with the same roles
+        // on both sides, so both elements apply the same bits).
+        const FaceTable<P, double> *T64 =
+            static_cast<const FaceTable<P, double> *>(a.face_table64);
+        const int le = self_left ? j : jn, re = self_left ? jn : j;
+        // The tables' flip is the edges' relative direction along the
+        // counter-clockwise parametrization; rev compares the edges' own
+        // point orders, and edge 2's points run against it.
+        const int flip = (rev ? 1 : 0) ^ (le == 2 ? 1 : 0) ^ (re == 2 ? 1 : 0);
+        const double *lb64 = &T64->lb[le][0][0];
+        const double *rb64 = &T64->rb[(le * 3 + re) * 2 + flip][0][0];
+        float dq[QF][4];
+        face_fp64<P>(gamma, in + e, ne, in + nb, ne, false, self_left, self_left ? lb64 : rb64,
+                     self_left ? rb64 : lb64, &T64->ew[le][0], nx, ny, fln, dq, m0);
+#pragma unroll
+        for (int q = 0; q < QF; ++q)
+#pragma unroll
+          for (int v = 0; v < 4; ++v)
+            fq[q][v] = dq[q][v];
+      }
+    }
     float shift[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     if (!boundary && !self_left) {
       double frn[4];
@@ -2344,19 +2394,25 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_patch(const StageArgs a)
         shift[v] = static_cast<float>(fln[v] - frn[v]);
     }
     const float fscale = static_cast<float>(scale);
-    float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-#pragma unroll
-    for (int q = 0; q < QF; ++q) {
-      const float w = table.w[jl][q];
+    const double sgn = self_left ? -1.0 : 1.0;
+    if (fp64) {
 #pragma unroll
       for (int v = 0; v < 4; ++v)
-        acc[v] = fmaf(w, fq[q][v], acc[v]);
-    }
-    const double sgn = self_left ? -1.0 : 1.0;
+        r0[v] += sgn * scale * phi0 * m0[v];
+    } else {
+      float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
-    for (int v = 0; v < 4; ++v) {
-      const double mode0 = fln[v] * c_edge_wsum<P>[jl] + static_cast<double>(acc[v]);
-      r0[v] += sgn * scale * phi0 * mode0;
+      for (int q = 0; q < QF; ++q) {
+        const float w = table.w[jl][q];
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+          acc[v] = fmaf(w, fq[q][v], acc[v]);
+      }
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const double mode0 = fln[v] * c_edge_wsum<P>[jl] + static_cast<double>(acc[v]);
+        r0[v] += sgn * scale * phi0 * mode0;
+      }
     }
     // High modes at this element's own points qo (the face's point q).
 #pragma unroll
@@ -2573,24 +2629,34 @@ void stage_tile_persistent(const StageArgs &a, cudaStream_t s) {
 }
 
 template <int P, int R, int TILE, int MINB, bool MMA> void patch_opt_in() {
-  static bool opted_in[64] = {};
-  smem_opt_in(euler_tri_patch<P, R, TILE, MINB, MMA>, PatchSmem<P, R, TILE, MMA>::bytes,
+  static bool opted_in[64] = {}, opted_in_islands[64] = {};
+  smem_opt_in(euler_tri_patch<P, R, TILE, MINB, MMA, false>, PatchSmem<P, R, TILE, MMA>::bytes,
               sizeof(PatchEdge<P>) + sizeof(int), opted_in);
+  if constexpr (!MMA)
+    smem_opt_in(euler_tri_patch<P, R, TILE, MINB, false, true>, PatchSmem<P, R, TILE, false>::bytes,
+                sizeof(PatchEdge<P>) + sizeof(int), opted_in_islands);
 }
 
 // The patch kernel over all patches (no rough pass: runs without the limiter).
 template <int P, int R, int TILE, int MINB, bool MMA = false>
 void stage_patch(const StageArgs &a, cudaStream_t s) {
-  if (a.rough)
-    throw std::invalid_argument("patch kernel: no rough pass (runs without the limiter)");
   if (!a.patch.nbr)
     throw std::invalid_argument("patch kernel: the mesh has no patch edge arrays");
   patch_opt_in<P, R, TILE, MINB, MMA>();
   const std::int64_t blocks = a.work ? a.work_count : (a.mesh.ne + TILE - 1) / TILE;
   if (blocks <= 0)
     return;
-  euler_tri_patch<P, R, TILE, MINB, MMA>
-      <<<static_cast<unsigned>(blocks), TILE, PatchSmem<P, R, TILE, MMA>::bytes, s>>>(a);
+  if (!a.rough) {
+    euler_tri_patch<P, R, TILE, MINB, MMA, false>
+        <<<static_cast<unsigned>(blocks), TILE, PatchSmem<P, R, TILE, MMA>::bytes, s>>>(a);
+  } else if constexpr (!MMA) {
+    // With the limiter: faces across jumps of the means in FP64, inline.
+    euler_tri_patch<P, R, TILE, MINB, false, true>
+        <<<static_cast<unsigned>(blocks), TILE, PatchSmem<P, R, TILE, false>::bytes, s>>>(a);
+  } else {
+    throw std::invalid_argument("patch kernel with the tensor-core volume: runs without the"
+                                " limiter");
+  }
 }
 
 // Launch shapes of the tile kernels (elements per CTA, register budget):
@@ -2725,6 +2791,8 @@ int euler_tri_tile_elements(int shape) {
 }
 
 bool euler_tri_tile_is_patch(int shape) { return shape >= kFirstPatchShape && shape < kPatchShapeEnd; }
+
+bool euler_tri_tile_limits(int shape) { return shape != 12 && shape != 13; }
 
 
 

@@ -176,7 +176,7 @@ public:
         d_tile_code_.upload(columns(ts.code, 3), stream_);
         d_tile_aux_.upload(columns(ts.aux, 3), stream_);
         PatchEdgeArrays pe;
-        patch_ok_ = !cfg.limiting && build_patch_edges(mesh_, t, boundary_, QF, pe);
+        patch_ok_ = build_patch_edges(mesh_, t, boundary_, QF, pe);
         if (patch_ok_) {
           d_patch_nbr_.upload(columns(ids(pe.nbr), 3), stream_);
           d_patch_info_.upload(columns(pe.info, 3), stream_);
@@ -184,8 +184,11 @@ public:
         }
       }
       if (cfg.mixed_kernel >= 2 && euler_tri_tile_is_patch(cfg.mixed_kernel - 2) && !patch_ok_)
-        throw SolverError(WASL_ERR_ARGUMENT, "2D Euler mixed form: the patch kernel runs without"
-                                             " the limiter on conforming meshes only");
+        throw SolverError(WASL_ERR_ARGUMENT, "2D Euler mixed form: the patch kernel runs on"
+                                             " conforming meshes only");
+      if (cfg.mixed_kernel >= 2 && cfg.limiting && !euler_tri_tile_limits(cfg.mixed_kernel - 2))
+        throw SolverError(WASL_ERR_ARGUMENT, "2D Euler mixed form: the patch kernel with the"
+                                             " tensor-core volume runs without the limiter");
       d_face_left_.upload(ids(mesh_.face_left), stream_);
       d_face_right_.upload(ids(face_right), stream_);
       d_face_code_.upload(face_code, stream_);
@@ -718,7 +721,8 @@ private:
       kernels.push_back(0);
     if (tile_ok_)
       for (int sh = 0; sh < euler_tri_tile_shapes(); ++sh)
-        if (!euler_tri_tile_is_patch(sh) || patch_ok_)
+        if ((!euler_tri_tile_is_patch(sh) || patch_ok_) &&
+            (!limiting_ || euler_tri_tile_limits(sh)))
           kernels.push_back(1 + sh);
     // Each variant runs the three stages of a step on the current state, into
     // the stage buffers only (the last stage writes the first stage buffer
@@ -832,7 +836,7 @@ private:
   bool relabel_ = false;  // elements stored along a space-filling curve
   std::vector<std::int32_t> order_, rank_; // storage -> caller, caller -> storage
   DeviceArray<std::int32_t> d_order_;
-  bool patch_ok_ = false; // the patch kernel's edge arrays exist (no limiter)
+  bool patch_ok_ = false; // the patch kernel's edge arrays exist
   DeviceArray<std::int32_t> d_patch_nbr_;
   DeviceArray<std::uint8_t> d_patch_info_;
   DeviceArray<double> d_patch_geo_;

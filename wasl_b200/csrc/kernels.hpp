@@ -313,6 +313,9 @@ int euler_tri_tile_elements(int shape);
 // Shapes of the patch kernel (StageArgs::patch; no rough pass, so runs
 // without the limiter only).
 bool euler_tri_tile_is_patch(int shape);
+// Shapes that run with the limiter (all but the patch kernel with its volume
+// term on the tensor cores).
+bool euler_tri_tile_limits(int shape);
 
 void launch_euler_tri_stage_tile(int p, int rule, int shape, const StageArgs &a,
                                  cudaStream_t stream);
