@@ -102,7 +102,13 @@ __global__ void __launch_bounds__(128) euler_tri_stage_f64(const StageArgs a) {
     }
   }
 
-  // Face terms in ascending global face index.
+  // Face terms in ascending global face index.  A neighbour's trace at the
+  // face's points is gathered once per face: each of its coefficients is
+  // loaded once and added into every point's sum (each sum still runs over
+  // the modes 0..M-1 from 0.0), and the sums wait in this thread's column of
+  // shared memory for the point loop.
+  __shared__ double outside[QF * 4][128];
+  const int t = threadIdx.x;
 #pragma unroll 1
   for (int k = 0; k < 3; ++k) {
     const std::int32_t raw = a.mesh.slot_nbr[k * ne + e];
@@ -116,13 +122,35 @@ __global__ void __launch_bounds__(128) euler_tri_stage_f64(const StageArgs a) {
     const int le = (code >> 1) & 3u, re = (code >> 3) & 3u, flip = (code >> 5) & 1u;
     const double(*lb)[M] = F->lb[le];
     const double(*rb)[M] = F->rb[(le * 3 + re) * 2 + flip];
+    if (nb >= 0) {
+      const double(*ob)[M] = self_left ? rb : lb;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        double acc[QF];
+#pragma unroll
+        for (int q = 0; q < QF; ++q)
+          acc[q] = 0.0;
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+          const double x = __ldg(in + (static_cast<std::int64_t>(v) * M + m) * ne + nb);
+#pragma unroll
+          for (int q = 0; q < QF; ++q)
+            acc[q] += x * ob[q][m];
+        }
+#pragma unroll
+        for (int q = 0; q < QF; ++q)
+          outside[q * 4 + v][t] = acc[q];
+      }
+    }
 #pragma unroll 1
     for (int q = 0; q < QF; ++q) {
       double ls[4], rs[4], f[4];
       if (self_left) {
         eval_local<M>(c, lb[q], ls);
         if (nb >= 0) {
-          eval_global<M>(in, ne, nb, rb[q], rs);
+#pragma unroll
+          for (int v = 0; v < 4; ++v)
+            rs[v] = outside[q * 4 + v][t];
         } else if (a.mesh.boundary == 3) {
 #pragma unroll
           for (int v = 0; v < 4; ++v)
@@ -133,7 +161,9 @@ __global__ void __launch_bounds__(128) euler_tri_stage_f64(const StageArgs a) {
                          a.mesh.donor_basis + point * M, rs);
         }
       } else {
-        eval_global<M>(in, ne, nb, lb[q], ls);
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+          ls[v] = outside[q * 4 + v][t];
         eval_local<M>(c, rb[q], rs);
       }
       hllc(gamma, ls, rs, nx, ny, f);
