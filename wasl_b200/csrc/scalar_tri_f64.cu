@@ -105,19 +105,36 @@ __global__ void __launch_bounds__(128) scalar_tri_stage_f64(const StageArgs a) {
     const double(*lb)[M] = F->lb[le];
     const double(*rb)[M] = F->rb[(le * 3 + re) * 2 + flip];
     const double normal_speed = vx * nx + vy * ny;
-#pragma unroll 1
+    // The neighbour's trace at every point of the face from one load of each
+    // of its coefficients (each sum over the modes 0..M-1 from 0.0, as
+    // modal_sum_global).
+    double outside[QF];
+    if (nb >= 0) {
+      const double(*ob)[M] = self_left ? rb : lb;
+#pragma unroll
+      for (int q = 0; q < QF; ++q)
+        outside[q] = 0.0;
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        const double x = in[static_cast<std::int64_t>(m) * ne + nb];
+#pragma unroll
+        for (int q = 0; q < QF; ++q)
+          outside[q] += x * ob[q][m];
+      }
+    }
+#pragma unroll
     for (int q = 0; q < QF; ++q) {
       double ls, rs;
       if (self_left) {
         ls = modal_sum<M>(c, lb[q]);
         if (nb >= 0) {
-          rs = modal_sum_global<M>(in, ne, nb, rb[q]);
+          rs = outside[q];
         } else {
           const std::int64_t point = static_cast<std::int64_t>(-nb - 1) * QF + q;
           rs = modal_sum_global<M>(in, ne, a.mesh.donor[point], a.mesh.donor_basis + point * M);
         }
       } else {
-        ls = modal_sum_global<M>(in, ne, nb, lb[q]);
+        ls = outside[q];
         rs = modal_sum<M>(c, rb[q]);
       }
       const double flux = normal_speed * (normal_speed >= 0.0 ? ls : rs);
