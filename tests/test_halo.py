@@ -112,6 +112,62 @@ def test_split_reproduces_the_serial_step(oracle, p, limiting, ranks):
     assert flagged > 0 or not limiting
 
 
+@pytest.mark.parametrize("p, pressure, width", [(1, 1.0, 0.0), (2, 10.0, 0.02)])
+def test_split_strong_shock_across_the_cut(oracle, p, pressure, width):
+    """A planar shock on the two-rank cut (density ratio 8; pressure ratio 10
+    with a sharp jump at P1, 100 with the jump smoothed over a third of a cell
+    at P2: the reference's algorithm goes non-finite on the projection of
+    stronger or sharper jumps, serial or split), limiter on: the ghost layers
+    that the cut spoils stay physical (no rank's step raises) and every owned
+    element equals the serial run bit for bit while the shock crosses from one
+    rank into the other."""
+    tags, xy, tris = meshgen.jittered_box(16, jitter=0.15, seed=40 + p)
+    ne, ranks = len(tris), 2
+    serial = oracle.tri_mesh(tags, xy, tris)
+    rule = max(p, 5)
+    xs, ys = serial.rule_points(rule)
+    cut_y = float(ys[: ne // 2].mean(axis=1).max())  # rank 0 holds the first half
+
+    def state(rho, p_):
+        return np.array([rho, 0.0, 0.0, p_ / (GAMMA - 1.0)])
+
+    below, above = state(1.0, pressure), state(0.125, 0.1)
+    if width > 0.0:
+        vals = below + (above - below) * (0.5 * (1.0 + np.tanh((ys - cut_y) / width)))[..., None]
+    else:
+        vals = np.where((ys < cut_y)[..., None], below, above)
+    c = serial.project(p, rule, vals)
+    M = (p + 1) * (p + 2) // 2
+    depth = halo.halo_depth(True)
+    meshes = [halo.local_mesh(tags, xy, tris, r, ranks, depth) for r in range(ranks)]
+    schedules = [halo.build_halo_schedule(meshes, ranks, ne, r) for r in range(ranks)]
+    locals_ = [oracle.tri_mesh(*m.arrays) for m in meshes]
+    stencils = [lm.stencil(p) for lm in locals_]
+    st_serial = serial.stencil(p)
+    states = [np.ascontiguousarray(c.reshape(4 * M, ne)[:, m.elements]) for m in meshes]
+    start = c.reshape(4 * M, ne)[0].copy()
+    flagged = 0
+    for _ in range(8):
+        dt = serial.cfl(GAMMA, c, p, 0.1)
+        flags = serial.euler_step(GAMMA, p, dt, c, boundary="transmissive", stencil=st_serial,
+                                  return_flags=True)
+        flagged += int(flags.sum())
+        for r, m in enumerate(meshes):
+            u = states[r].ravel()
+            locals_[r].euler_step(GAMMA, p, dt, u, boundary="transmissive", stencil=stencils[r])
+            states[r] = u.reshape(4 * M, -1)
+        halo.exchange_in_process(states, meshes, schedules)
+        full = c.reshape(4 * M, ne)
+        assert np.all(np.isfinite(full))
+        for r, m in enumerate(meshes):
+            assert np.array_equal(states[r], full[:, m.elements]), f"rank {r}"
+    assert flagged > 0
+    # the shock moved into rank 1's elements
+    rank1 = meshes[1].elements[meshes[1].owned]
+    assert np.count_nonzero(np.abs(c.reshape(4 * M, ne)[0, rank1] - start[rank1])
+                            > 0.02 * start[rank1]) >= 8
+
+
 def dense_part_trace(oracle, om, part, p):
     """A part's boundary (LocalMesh.part_boundary) as the oracle's per-face
     periodic trace: owner faces (donor -1) take the face's own element and its
