@@ -109,6 +109,13 @@ __global__ void __launch_bounds__(128) euler_tri_stage_f64(const StageArgs a) {
   // shared memory for the point loop.
   __shared__ double outside[QF * 4][128];
   const int t = threadIdx.x;
+  // u^n (read by the combination at the end of stages 2 and 3) into L1 while
+  // the faces run; no registers wait on it.
+  if (a.stage > 0) {
+#pragma unroll
+    for (int row = 0; row < 4 * M; ++row)
+      asm volatile("prefetch.global.L1 [%0];\n" ::"l"(a.u0 + static_cast<std::int64_t>(row) * ne + e));
+  }
 #pragma unroll 1
   for (int k = 0; k < 3; ++k) {
     const std::int32_t raw = a.mesh.slot_nbr[k * ne + e];

@@ -93,6 +93,14 @@ __global__ void __launch_bounds__(128) scalar_tri_stage_f64(const StageArgs a) {
     }
   }
 
+  // u^n (read by the combination at the end of stages 2 and 3) into L1 while
+  // the faces run.
+  if (a.stage > 0) {
+#pragma unroll
+    for (int m = 0; m < M; ++m)
+      asm volatile("prefetch.global.L1 [%0];\n" ::"l"(a.u0 + static_cast<std::int64_t>(m) * ne + e));
+  }
+
 #pragma unroll 1
   for (int k = 0; k < 3; ++k) {
     const std::int32_t nb = a.mesh.slot_nbr[k * ne + e];
