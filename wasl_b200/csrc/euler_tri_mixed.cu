@@ -2005,6 +2005,10 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_patch(const StageArgs a)
   float4 *sfrag = reinterpret_cast<float4 *>(smem + L::frag);
   float(*sbb)[TILE] = reinterpret_cast<float(*)[TILE]>(smem + L::bb);
   float(*sgeo)[TILE] = reinterpret_cast<float(*)[TILE]>(smem + L::geo);
+  // The next launch on the stream may start its CTAs (into SM slots this
+  // grid's tail leaves free) and run up to its own wait, which holds until
+  // this grid has completed.
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
 
   const int t = threadIdx.x;
   const std::int64_t ne = a.mesh.ne;
@@ -2059,6 +2063,14 @@ __global__ void __launch_bounds__(TILE, MINB) euler_tri_patch(const StageArgs a)
       prefetch_row_l2(row, bytes);
     }
   }
+
+  // Launched as a programmatic dependent of the launch before it on the
+  // stream (the previous RK stage, or the dt kernel): everything above reads
+  // only the mesh, the tables and (as a prefetch hint) u^n.  Wait here for
+  // that launch to complete and its writes to be visible before the state,
+  // dt or any output is touched.  Without the launch attribute the wait
+  // returns at once.
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
 
   // A. State, traces, and the faces this element evaluates.
   bool evaluates[3] = {false, false, false};
@@ -2543,6 +2555,25 @@ void smem_opt_in(Kernel kernel, std::size_t dynamic, std::size_t fixed, bool (&o
     opted_in[device] = true;
 }
 
+// A stage kernel launched as a programmatic dependent of the launch before
+// it on the stream: its CTAs may start while that launch drains, and wait
+// (griddepcontrol.wait) before reading what it wrote.
+template <typename Kernel>
+void launch_dependent(Kernel kernel, unsigned blocks, unsigned threads, std::size_t smem,
+                      cudaStream_t s, const StageArgs &a) {
+  cudaLaunchConfig_t config = {};
+  config.gridDim = dim3(blocks);
+  config.blockDim = dim3(threads);
+  config.dynamicSmemBytes = smem;
+  config.stream = s;
+  cudaLaunchAttribute attribute[1];
+  attribute[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attribute[0].val.programmaticStreamSerializationAllowed = 1;
+  config.attrs = attribute;
+  config.numAttrs = 1;
+  check(cudaLaunchKernelEx(&config, kernel, a), "patch kernel launch");
+}
+
 template <int P, int R, int TILE, int MINB> void tile_opt_in() {
   static bool opted_in[64] = {};
   smem_opt_in(euler_tri_tile_mixed<P, R, TILE, MINB, false>, tile_smem<P, TILE>(),
@@ -2647,12 +2678,12 @@ void stage_patch(const StageArgs &a, cudaStream_t s) {
   if (blocks <= 0)
     return;
   if (!a.rough) {
-    euler_tri_patch<P, R, TILE, MINB, MMA, false>
-        <<<static_cast<unsigned>(blocks), TILE, PatchSmem<P, R, TILE, MMA>::bytes, s>>>(a);
+    launch_dependent(euler_tri_patch<P, R, TILE, MINB, MMA, false>,
+                     static_cast<unsigned>(blocks), TILE, PatchSmem<P, R, TILE, MMA>::bytes, s, a);
   } else if constexpr (!MMA) {
     // With the limiter: faces across jumps of the means in FP64, inline.
-    euler_tri_patch<P, R, TILE, MINB, false, true>
-        <<<static_cast<unsigned>(blocks), TILE, PatchSmem<P, R, TILE, false>::bytes, s>>>(a);
+    launch_dependent(euler_tri_patch<P, R, TILE, MINB, false, true>,
+                     static_cast<unsigned>(blocks), TILE, PatchSmem<P, R, TILE, false>::bytes, s, a);
   } else {
     throw std::invalid_argument("patch kernel with the tensor-core volume: runs without the"
                                 " limiter");
