@@ -214,22 +214,33 @@ def build_solver(args, form, device):
 
 
 def time_device_steps(g, args, torch, flush, stream):
-    """W untimed steps, then K steps each bracketed by events; L2 flushed between."""
+    """W untimed steps, then K timed steps, each bracketed by an event pair on
+    the handle's stream with L2 flushed between: the headline pass, with no
+    event inside a step (timing events between kernels serialise their
+    launches: about 15 us per step of three stage kernels).  Then the same K
+    steps once more with an event pair around every stage kernel, for the
+    stage-kernel times of the roofline and the launch count."""
     g.advance(CFL, args.warmup)
     torch.cuda.synchronize()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    g.profile_begin()
-    with torch.cuda.stream(stream):
-        for k in range(args.steps):
-            flush.zero_()
-            starts[k].record(stream)
-            g.advance(CFL, 1, sync=False)  # enqueue only: no host round trip inside the events
-            ends[k].record(stream)
-    torch.cuda.synchronize()
-    g.sync()  # device errors of the timed steps
+
+    def timed(per_stage_events):
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        if per_stage_events:
+            g.profile_begin()
+        with torch.cuda.stream(stream):
+            for k in range(args.steps):
+                flush.zero_()
+                starts[k].record(stream)
+                g.advance(CFL, 1, sync=False)  # enqueue only: no host round trip inside the events
+                ends[k].record(stream)
+        torch.cuda.synchronize()
+        g.sync()  # device errors of the timed steps
+        return sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+
+    total_ms = timed(False)
+    timed(True)
     stage_ms, stage_kernels, launches = g.profile_end()
-    total_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
     # Mean stage-kernel ms of RK stages 0, 1, 2 (stage 0 reads u^n after the
     # L2 flush; stages 1 and 2 also read u^n for the Shu-Osher combination).
     by_stage = [round(ms / args.steps, 5) for ms in g.profile_stages()]
@@ -408,7 +419,10 @@ def ours(args, rank, world, local_rank):
                    "volume_rule": rule_description(rule_order(args, form), args.p),
                    "kernel": kernel_description(g.tuning()),
                    "elements": g.elements, "dof": dofs, "parallelism": f"replicas x{world}",
-                   "l2": "flushed between timed steps (256 MiB write)"},
+                   "l2": "flushed between timed steps (256 MiB write)",
+                   "timing": "K steps with an event pair per step (value); the stage-kernel"
+                             " times of the roofline from a second pass of the same K steps"
+                             " with an event pair around each stage kernel"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "steps": e2e_steps,
                 "path": "C-ABI set_state/stable_dt/step/get_state with pinned host buffers"},
