@@ -438,3 +438,25 @@ def test_tensor_core_volume_vortex_accuracy(p):
             steps, t = g.run(0.15, 0.0, 0.5)
             errors[form] = cases.l1_density_error(g, lambda x, y: vortex.conserved(x, y, t))
     assert errors["mixed"] <= 1.5 * errors["plain"]
+
+
+@pytest.mark.parametrize("kernel", [11, 13])
+def test_dependent_stage_launches_are_deterministic(kernel):
+    """Each RK stage's patch kernel is launched as a programmatic dependent of
+    the launch before it: its CTAs start while that launch drains and wait in
+    hardware before reading the state.  Device-resident steps over a mesh of
+    many CTA waves (131,072 triangles: 1,024 CTAs of 128) give the same bits
+    on every run."""
+    arrays = cases.vortex_mesh(256)
+    vortex = cases.IsentropicVortex()
+    runs = []
+    with wasl_b200.Solver(*arrays, polynomial_order=2, precision="mixed",
+                          mixed_kernel=kernel) as g:
+        cases.project_initial(g, vortex.conserved)
+        c = g.get_state()
+        for _ in range(3):
+            g.set_state(c)
+            g.advance(0.15, 12)
+            runs.append(g.get_state())
+    assert not np.array_equal(runs[0], c)
+    assert np.array_equal(runs[1], runs[0]) and np.array_equal(runs[2], runs[0])
