@@ -223,15 +223,19 @@ def test_resident_run_is_the_host_loop_bit_for_bit():
     assert same(out[0][2], out[1][2])
 
 
-@pytest.mark.parametrize("p,ends", [(1, "periodic"), (2, "periodic"), (2, "outflow")])
-def test_resident_euler_run_is_the_host_loop_bit_for_bit(p, ends):
+@pytest.mark.parametrize("p,ends,n", [(1, "periodic", 96), (2, "periodic", 96),
+                                      (2, "outflow", 96), (2, "periodic", 40),
+                                      (2, "outflow", 192), (2, "periodic", 397),
+                                      (3, "periodic", 397)])
+def test_resident_euler_run_is_the_host_loop_bit_for_bit(p, ends, n):
     """1D Euler with the CFL step taken from the state every step, on the
-    device in one launch: the host loop's steps, time and state."""
-    arrays = meshgen.jittered_line(96, jitter=0.2, seed=3)
+    device in one launch, on line meshes of 40 to 397 elements: the host
+    loop's steps, time and state."""
+    arrays = meshgen.jittered_line(n, jitter=0.2, seed=3)
     rng = np.random.Generator(np.random.PCG64(8))
     M = p + 1
-    c = 0.02 * rng.standard_normal((4, M, 96))
-    c[0, 0] = np.sqrt(2) * (1.0 + 0.2 * rng.uniform(-1, 1, 96))
+    c = 0.02 * rng.standard_normal((4, M, n))
+    c[0, 0] = np.sqrt(2) * (1.0 + 0.2 * rng.uniform(-1, 1, n))
     c[1, 0] = np.sqrt(2) * 0.3
     c[3, 0] = np.sqrt(2) * 2.5
     out = []
