@@ -793,6 +793,12 @@ __global__ void __launch_bounds__(256) cfl_reduce(const CflArgs a) {
 __global__ void dt_from_speed(std::int64_t cases, unsigned long long *speed, double cfl,
                               const double *length, const int *p, double length_all, int p_all,
                               double *dt, double *elapsed, const int *status) {
+  // As a programmatic dependent launch: the next launch (the step's first
+  // stage) may start its CTAs now, and this kernel waits for the launch
+  // before it (the last stage, which max-reduced the speed) to complete.
+  // Launched plainly, both are no-ops.
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
   const std::int64_t c = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (c >= cases)
     return;
@@ -902,9 +908,25 @@ std::vector<double> positivity_check_bound(const std::vector<double> &check_basi
 
 void launch_dt_from_speed(std::int64_t cases, unsigned long long *speed, double cfl,
                           const double *length, const int *p, double length_all, int p_all,
-                          double *dt, double *elapsed, const int *status, cudaStream_t s) {
-  dt_from_speed<<<static_cast<unsigned>((cases + 255) / 256), 256, 0, s>>>(
-      cases, speed, cfl, length, p, length_all, p_all, dt, elapsed, status);
+                          double *dt, double *elapsed, const int *status, cudaStream_t s,
+                          bool dependent) {
+  if (!dependent) {
+    dt_from_speed<<<static_cast<unsigned>((cases + 255) / 256), 256, 0, s>>>(
+        cases, speed, cfl, length, p, length_all, p_all, dt, elapsed, status);
+    return;
+  }
+  cudaLaunchConfig_t config = {};
+  config.gridDim = dim3(static_cast<unsigned>((cases + 255) / 256));
+  config.blockDim = dim3(256);
+  config.stream = s;
+  cudaLaunchAttribute attribute[1];
+  attribute[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attribute[0].val.programmaticStreamSerializationAllowed = 1;
+  config.attrs = attribute;
+  config.numAttrs = 1;
+  check(cudaLaunchKernelEx(&config, dt_from_speed, cases, speed, cfl, length, p, length_all, p_all,
+                           dt, elapsed, status),
+        "dt launch");
 }
 
 void launch_cfl_speed(const CflArgs &a, cudaStream_t s) {

@@ -445,7 +445,7 @@ public:
         count_launches(1);
       }
       launch_dt_from_speed(1, d_speed_.get(), cfl, nullptr, nullptr, length_, p_, d_dt_.get(),
-                           nullptr, nullptr, stream_);
+                           nullptr, nullptr, stream_, true);
       count_launches(1);
       fused_speed_ = mixed_ && !limiting_;
       enqueue_step(d_dt_.get(), 0.0);

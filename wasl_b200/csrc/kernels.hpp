@@ -336,6 +336,7 @@ void launch_cfl_speed(const CflArgs &a, cudaStream_t stream);
 // arrays, or null for the shared length_all/p_all; status may be null.
 void launch_dt_from_speed(std::int64_t cases, unsigned long long *speed, double cfl,
                           const double *length, const int *p, double length_all, int p_all,
-                          double *dt, double *elapsed, const int *status, cudaStream_t stream);
+                          double *dt, double *elapsed, const int *status, cudaStream_t stream,
+                          bool dependent = false); // as a programmatic dependent launch
 
 } // namespace wasl_b200
